@@ -1,0 +1,151 @@
+/*
+ * rblas_b200.h -- C ABI of the B200 (sm_100a) GEMM engine that stands behind
+ * rblas's Level-3 API (blasrodri/rblas).
+ *
+ * Every entry point is extern "C" with plain pointers and sizes. Enum values
+ * mirror rblas's Rust enums (src/types.rs). Errors mirror rblas's BlasError
+ * (src/error.rs:15-39) and are returned, never raised: a binding that wants
+ * rblas's panicking `gemm` unwraps the status itself.
+ *
+ * Two pointer conventions:
+ *   - host entry points (rb_sgemm, ...) take host buffers plus their slice
+ *     lengths, exactly the arguments of rblas's slice-based functions; they
+ *     copy to the GPU, compute, copy back, and return when C is written.
+ *   - device entry points (*_dev) take device pointers and a CUDA stream
+ *     (as void*), enqueue, and return without synchronising.
+ *
+ * Sizes are size_t (Rust usize). Leading dimensions are in elements.
+ */
+#ifndef RBLAS_B200_H
+#define RBLAS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/types.rs:9-14 */
+typedef enum { RB_ROW_MAJOR = 0, RB_COL_MAJOR = 1 } rb_layout;
+/* src/types.rs:30-37 (ConjTrans == Trans for real types, src/types.rs:42-44) */
+typedef enum { RB_NO_TRANS = 0, RB_TRANS = 1, RB_CONJ_TRANS = 2 } rb_transpose;
+/* src/types.rs:49-54 */
+typedef enum { RB_UPPER = 0, RB_LOWER = 1 } rb_uplo;
+/* src/types.rs:58-63 */
+typedef enum { RB_LEFT = 0, RB_RIGHT = 1 } rb_side;
+/* src/types.rs:67-72 */
+typedef enum { RB_NON_UNIT = 0, RB_UNIT = 1 } rb_diag;
+
+/* Arithmetic form of a call. PLAIN is the drop-in (true FP32 / FP64
+ * products). BF16X3 (f32 only): split each operand into bf16 hi+lo and sum
+ * hi*hi + hi*lo + lo*hi on the tensor cores with FP32 accumulation. OZAKI
+ * (f64 only): INT8 slice emulation with per-row/column power-of-two scaling
+ * and exact INT32 slice products; the slice count is rb_set_ozaki_slices(). */
+typedef enum { RB_PREC_PLAIN = 0, RB_PREC_BF16X3 = 1, RB_PREC_OZAKI = 2 } rb_precision;
+
+typedef enum {
+    RB_OK = 0,
+    RB_ERR_INVALID_LEADING_DIM = 1, /* BlasError::InvalidLeadingDim, src/error.rs:17-24 */
+    RB_ERR_BUFFER_TOO_SMALL = 2,    /* BlasError::BufferTooSmall,   src/error.rs:26-33 */
+    RB_ERR_ZERO_STRIDE = 3,         /* BlasError::ZeroStride,       src/error.rs:35-38 */
+    RB_ERR_INVALID_ARG = 4,         /* enum value out of range, null pointer with nonzero size */
+    RB_ERR_UNSUPPORTED = 5,         /* precision form not available for this dtype/op */
+    RB_ERR_CUDA = 6,                /* a CUDA runtime/driver call failed (see cuda_error) */
+    RB_ERR_ALLOC = 7,               /* device or pinned allocation failed */
+    RB_ERR_TIMEOUT = 8,             /* a bounded device-side wait gave up */
+    RB_ERR_DEVICE = 9,              /* a kernel reported an error word */
+    RB_ERR_BUSY = 10,               /* admission refused (serving budget) */
+    RB_ERR_CANCELLED = 11           /* request cancelled before it ran */
+} rb_status;
+
+/* Mirrors BlasError's fields: which operand ('a', 'b', 'c', 'x', 'y'),
+ * the value supplied and the minimum (InvalidLeadingDim) or required length
+ * (BufferTooSmall). cuda_error carries the cudaError_t / CUresult for
+ * RB_ERR_CUDA. */
+typedef struct {
+    int32_t code;
+    char which;
+    uint64_t got;
+    uint64_t min_or_need;
+    int32_t cuda_error;
+} rb_error;
+
+/* src/complex.rs:17-24: #[repr(C)] Complex<T> { re, im } -- interleaved. */
+typedef struct { float re, im; } rb_complex32;
+typedef struct { double re, im; } rb_complex64;
+
+/* Human-readable text of a status, in the wording of BlasError's Display
+ * (src/error.rs:41-57) for the validation errors. */
+const char* rb_status_string(int32_t status);
+
+/* ---------------------------------------------------------------------------
+ * Real GEMM: C := alpha * op(A) * op(B) + beta * C
+ * ------------------------------------------------------------------------- */
+
+/* Drop-in for level3::try_gemm (src/level3.rs:68-103) over host slices:
+ * validates a, b, c in that order with check_matrix's rules
+ * (src/level3.rs:107-140), then computes with the plain form
+ * (level3::gemm, src/level3.rs:32-62, true FP32 products). */
+rb_status rb_sgemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                   size_t k, float alpha, const float* a, size_t lda, size_t a_len, const float* b,
+                   size_t ldb, size_t b_len, float beta, float* c, size_t ldc, size_t c_len,
+                   rb_error* err);
+/* Same for f64 (plain form: FP64 products). */
+rb_status rb_dgemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                   size_t k, double alpha, const double* a, size_t lda, size_t a_len,
+                   const double* b, size_t ldb, size_t b_len, double beta, double* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+
+/* Host-slice GEMM with a chosen arithmetic form (level3::try_gemm semantics). */
+rb_status rb_sgemm_prec(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                        size_t n, size_t k, float alpha, const float* a, size_t lda, size_t a_len,
+                        const float* b, size_t ldb, size_t b_len, float beta, float* c,
+                        size_t ldc, size_t c_len, rb_precision prec, rb_error* err);
+rb_status rb_dgemm_prec(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                        size_t n, size_t k, double alpha, const double* a, size_t lda,
+                        size_t a_len, const double* b, size_t ldb, size_t b_len, double beta,
+                        double* c, size_t ldc, size_t c_len, rb_precision prec, rb_error* err);
+
+/* Device-pointer GEMM (same math as level3::gemm, src/level3.rs:32-62),
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Leading dimensions are validated (InvalidLeadingDim); buffer lengths are
+ * the caller's responsibility. Returns when the work is enqueued. */
+rb_status rb_sgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                       size_t n, size_t k, float alpha, const float* a, size_t lda,
+                       const float* b, size_t ldb, float beta, float* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err);
+rb_status rb_dgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                       size_t n, size_t k, double alpha, const double* a, size_t lda,
+                       const double* b, size_t ldb, double beta, double* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err);
+
+/* ---------------------------------------------------------------------------
+ * Library state
+ * ------------------------------------------------------------------------- */
+
+/* Number of slices used by RB_PREC_OZAKI (3..12; default 8). */
+rb_status rb_set_ozaki_slices(int slices);
+int rb_get_ozaki_slices(void);
+
+/* Kernels this library has launched since load (all devices). */
+uint64_t rb_launch_count(void);
+
+/* Reads (and with clear != 0 resets) the current device's error word, set
+ * by a kernel whose bounded wait gave up or whose own bounds check failed.
+ * Synchronises the device. Returns RB_OK when no error was recorded. */
+rb_status rb_device_error(int clear, uint32_t* detail);
+
+/* Releases the cached device/pinned staging buffers of the current device. */
+void rb_release_cached_memory(void);
+
+/* Measures the current GPU's FMA throughput in TFLOP/s (is_f64: FP64 DFMA,
+ * else FP32 FFMA; iters <= 0 picks a default). The roofline denominator of
+ * the plain forms, which the tensor-core peaks do not cover. -1 on error. */
+double rb_probe_fma_peak_tflops(int is_f64, int iters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBLAS_B200_H */

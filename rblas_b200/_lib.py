@@ -1,0 +1,102 @@
+"""ctypes binding of librblas_b200.so (include/rblas_b200.h).
+
+The library is built in-tree (rblas_b200/_build.py). There is no CPU
+fallback: if the shared library is missing or cannot be loaded, every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from .error import BlasError, BufferTooSmall, DeviceError, InvalidLeadingDim, ZeroStride
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librblas_b200.so")
+
+_lib = None
+_lock = threading.Lock()
+
+
+class RbError(C.Structure):
+    _fields_ = [("code", C.c_int32), ("which", C.c_char), ("got", C.c_uint64),
+                ("min_or_need", C.c_uint64), ("cuda_error", C.c_int32)]
+
+
+class RbComplex32(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+class RbComplex64(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+_sz, _i, _f, _d, _vp = C.c_size_t, C.c_int, C.c_float, C.c_double, C.c_void_p
+_perr = C.POINTER(RbError)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rb_status_string": (C.c_char_p, [C.c_int32]),
+    "rb_sgemm": (_i, [_i, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _f, _vp, _sz, _sz, _perr]),
+    "rb_dgemm": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _perr]),
+    "rb_sgemm_prec": (_i, [_i, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _f, _vp, _sz, _sz, _i, _perr]),
+    "rb_dgemm_prec": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _i, _perr]),
+    "rb_sgemm_dev": (_i, [_i, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz, _i, _vp, _perr]),
+    "rb_dgemm_dev": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _i, _vp, _perr]),
+    "rb_set_ozaki_slices": (_i, [_i]),
+    "rb_get_ozaki_slices": (_i, []),
+    "rb_launch_count": (C.c_uint64, []),
+    "rb_device_error": (_i, [_i, C.POINTER(C.c_uint32)]),
+    "rb_release_cached_memory": (None, []),
+    "rb_probe_fma_peak_tflops": (C.c_double, [_i, _i]),
+}
+
+
+def load():
+    """Load (once) and return the CDLL. Raises if the library is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `python -m rblas_b200._build` "
+                    "(there is no CPU fallback)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name, None)
+                if fn is None:
+                    continue
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    lib = load()
+    return [n for n in SIGNATURES if hasattr(lib, n)]
+
+
+def raise_for(status: int, err: RbError):
+    """Map an rb_status + rb_error to the matching BlasError."""
+    if status == 0:
+        return None
+    which = err.which.decode() if err.which else ""
+    if status == 1:
+        return InvalidLeadingDim(which, int(err.got), int(err.min_or_need))
+    if status == 2:
+        return BufferTooSmall(which, int(err.got), int(err.min_or_need))
+    if status == 3:
+        return ZeroStride(which)
+    msg = load().rb_status_string(status).decode()
+    detail = int(err.cuda_error) if status == 6 else int(err.got)
+    return DeviceError(status, msg, detail)
+
+
+def check(status: int, err: RbError):
+    e = raise_for(status, err)
+    if e is not None:
+        raise e

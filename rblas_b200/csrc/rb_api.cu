@@ -1,0 +1,451 @@
+// rb_api.cu -- the extern "C" boundary (include/rblas_b200.h).
+//
+// Host entry points mirror rblas's slice-based Level-3 functions: argument
+// order, validation order and error fields follow level3::try_gemm and
+// check_matrix (src/level3.rs:68-140); the math follows level3::gemm
+// (src/level3.rs:32-62) and gemm_contig's early-outs (src/kernel/gemm.rs:
+// 185-205): m == 0 || n == 0 returns before touching C; otherwise C is scaled
+// by beta (beta == 0 writes zeros without reading C, so NaNs in C vanish) and
+// k == 0 || alpha == 0 stops there.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "../../include/rblas_b200.h"
+#include "rb_internal.h"
+
+namespace rb {
+
+std::atomic<uint64_t> g_launches{0};
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+// Per-device state for host-slice calls: an internal stream, grow-only
+// staging buffers for A, B, C, and the device error word.
+struct DeviceCtx {
+    std::mutex mu;
+    bool init = false;
+    cudaStream_t stream = nullptr;
+    uint32_t* err_word = nullptr;
+    void* buf[3] = {nullptr, nullptr, nullptr};
+    size_t cap[3] = {0, 0, 0};
+};
+DeviceCtx g_ctx[kMaxDevices];
+std::mutex g_init_mu;
+
+int current_device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return -1;
+    return d;
+}
+
+DeviceCtx* ctx_for_current(cudaError_t* e) {
+    const int d = current_device();
+    if (d < 0 || d >= kMaxDevices) {
+        *e = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    DeviceCtx& c = g_ctx[d];
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (!c.init) {
+        *e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
+        if (*e != cudaSuccess) return nullptr;
+        *e = cudaMalloc(&c.err_word, 64);
+        if (*e != cudaSuccess) return nullptr;
+        *e = cudaMemset(c.err_word, 0, 64);
+        if (*e != cudaSuccess) return nullptr;
+        c.init = true;
+    }
+    *e = cudaSuccess;
+    return &c;
+}
+
+cudaError_t ensure_buf(DeviceCtx* c, int slot, size_t bytes) {
+    if (bytes <= c->cap[slot]) return cudaSuccess;
+    if (c->buf[slot]) cudaFree(c->buf[slot]);
+    c->buf[slot] = nullptr;
+    c->cap[slot] = 0;
+    size_t want = std::max(bytes, c->cap[slot] * 2);
+    cudaError_t e = cudaMalloc(&c->buf[slot], want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&c->buf[slot], bytes);
+        if (e != cudaSuccess) return e;
+        want = bytes;
+    }
+    c->cap[slot] = want;
+    return cudaSuccess;
+}
+
+void set_err(rb_error* err, int32_t code, char which = 0, uint64_t got = 0, uint64_t need = 0,
+             int32_t cuda_error = 0) {
+    if (err) {
+        err->code = code;
+        err->which = which;
+        err->got = got;
+        err->min_or_need = need;
+        err->cuda_error = cuda_error;
+    }
+}
+
+rb_status cuda_fail(rb_error* err, cudaError_t e) {
+    set_err(err, RB_ERR_CUDA, 0, 0, 0, static_cast<int32_t>(e));
+    return RB_ERR_CUDA;
+}
+
+// src/level3.rs:107-140. Zero dims are valid; InvalidLeadingDim before
+// BufferTooSmall. check_len == false skips the length check (device calls).
+rb_status check_matrix(rb_layout layout, char which, size_t rows, size_t cols, size_t lead,
+                       size_t len, bool check_len, rb_error* err) {
+    if (rows == 0 || cols == 0) return RB_OK;
+    const size_t min_lead = (layout == RB_ROW_MAJOR) ? cols : rows;
+    if (lead < min_lead) {
+        set_err(err, RB_ERR_INVALID_LEADING_DIM, which, lead, min_lead);
+        return RB_ERR_INVALID_LEADING_DIM;
+    }
+    const size_t need = (layout == RB_ROW_MAJOR) ? (rows - 1) * lead + cols : (cols - 1) * lead + rows;
+    if (check_len && len < need) {
+        set_err(err, RB_ERR_BUFFER_TOO_SMALL, which, len, need);
+        return RB_ERR_BUFFER_TOO_SMALL;
+    }
+    return RB_OK;
+}
+
+bool valid_layout(int v) { return v == RB_ROW_MAJOR || v == RB_COL_MAJOR; }
+bool valid_trans(int v) { return v >= RB_NO_TRANS && v <= RB_CONJ_TRANS; }
+
+// A GEMM problem after row-major normalisation (src/level3.rs:52-60):
+// column-major, C is m x n; op(A) m x k; op(B) k x n.
+template <typename T>
+struct ColProblem {
+    bool ta, tb;
+    size_t m, n, k;
+    T alpha, beta;
+    const T* a; size_t lda;
+    const T* b; size_t ldb;
+    T* c; size_t ldc;
+};
+
+template <typename T>
+ColProblem<T> normalise(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                        size_t n, size_t k, T alpha, const T* a, size_t lda, const T* b, size_t ldb,
+                        T beta, T* c, size_t ldc) {
+    ColProblem<T> p;
+    if (layout == RB_COL_MAJOR) {
+        p = {transa != RB_NO_TRANS, transb != RB_NO_TRANS, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
+    } else {
+        // C^T = alpha * op(B)^T op(A)^T + beta * C^T: swap A<->B, m<->n, trans flags.
+        p = {transb != RB_NO_TRANS, transa != RB_NO_TRANS, n, m, k, alpha, beta, b, ldb, a, lda, c, ldc};
+    }
+    return p;
+}
+
+constexpr size_t kMaxDim = 0x7fffffff;
+
+template <typename T>
+bool tma_ok(const T* p, size_t ld) {
+    return (reinterpret_cast<uintptr_t>(p) % 16 == 0) && ((ld * sizeof(T)) % 16 == 0);
+}
+
+// Enqueue the column-major problem on `st` with device operands. Operands
+// that TMA cannot address directly (unaligned base or leading dimension) are
+// repacked into stream-ordered scratch first.
+template <typename T>
+rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb_error* err) {
+    if (p.m == 0 || p.n == 0) return RB_OK;
+    if (p.m > kMaxDim || p.n > kMaxDim || p.k > kMaxDim) {
+        set_err(err, RB_ERR_INVALID_ARG);
+        return RB_ERR_INVALID_ARG;
+    }
+    cudaError_t e;
+    if (p.k == 0 || p.alpha == T(0)) {
+        e = launch_scale_c<T>((int)p.m, (int)p.n, p.beta, p.c, p.ldc, st);
+        return e == cudaSuccess ? RB_OK : cuda_fail(err, e);
+    }
+    if (prec != RB_PREC_PLAIN) {
+        set_err(err, RB_ERR_UNSUPPORTED);
+        return RB_ERR_UNSUPPORTED;
+    }
+    const T* A = p.a;
+    const T* B = p.b;
+    size_t lda = p.lda, ldb = p.ldb;
+    void* scratch[2] = {nullptr, nullptr};
+    const size_t vec = 16 / sizeof(T);
+    // stored extents (column-major)
+    const size_t a_rows = p.ta ? p.k : p.m, a_cols = p.ta ? p.m : p.k;
+    const size_t b_rows = p.tb ? p.n : p.k, b_cols = p.tb ? p.k : p.n;
+    if (!tma_ok(A, lda)) {
+        const size_t ld2 = (a_rows + vec - 1) / vec * vec;
+        e = cudaMallocAsync(&scratch[0], ld2 * a_cols * sizeof(T), st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+        e = cudaMemcpy2DAsync(scratch[0], ld2 * sizeof(T), A, lda * sizeof(T), a_rows * sizeof(T),
+                              a_cols, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+        A = static_cast<const T*>(scratch[0]);
+        lda = ld2;
+    }
+    if (!tma_ok(B, ldb)) {
+        const size_t ld2 = (b_rows + vec - 1) / vec * vec;
+        e = cudaMallocAsync(&scratch[1], ld2 * b_cols * sizeof(T), st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+        e = cudaMemcpy2DAsync(scratch[1], ld2 * sizeof(T), B, ldb * sizeof(T), b_rows * sizeof(T),
+                              b_cols, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+        B = static_cast<const T*>(scratch[1]);
+        ldb = ld2;
+    }
+    CUresult cu = CUDA_SUCCESS;
+    // op(A): Trans -> stored k x m, k-contiguous; op(B): NoTrans -> stored k x n, k-contiguous.
+    e = launch_simt_gemm<T>(p.ta, !p.tb, (int)p.m, (int)p.n, (int)p.k, p.alpha, A, lda, B, ldb,
+                            p.beta, p.c, p.ldc, st, &cu);
+    for (void* s : scratch)
+        if (s) cudaFreeAsync(s, st);
+    if (cu != CUDA_SUCCESS) {
+        set_err(err, RB_ERR_CUDA, 0, 0, 0, static_cast<int32_t>(cu));
+        return RB_ERR_CUDA;
+    }
+    return e == cudaSuccess ? RB_OK : cuda_fail(err, e);
+}
+
+rb_status check_device_word(DeviceCtx* c, rb_error* err) {
+    uint32_t w = 0;
+    cudaError_t e = cudaMemcpyAsync(&w, c->err_word, sizeof(w), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(err, e);
+    if (w != 0) {
+        cudaMemsetAsync(c->err_word, 0, sizeof(uint32_t), c->stream);
+        cudaStreamSynchronize(c->stream);
+        const rb_status s = ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
+        set_err(err, s, 0, w, 0);
+        return s;
+    }
+    return RB_OK;
+}
+
+// Host-slice GEMM: validate (try_gemm), stage into device buffers with padded
+// leading dimensions, run, copy C back, report any device error.
+template <typename T>
+rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                    size_t k, T alpha, const T* a, size_t lda, size_t a_len, const T* b, size_t ldb,
+                    size_t b_len, T beta, T* c, size_t ldc, size_t c_len, rb_precision prec,
+                    rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_layout(layout) || !valid_trans(transa) || !valid_trans(transb) ||
+        (prec != RB_PREC_PLAIN && prec != RB_PREC_BF16X3 && prec != RB_PREC_OZAKI)) {
+        set_err(err, RB_ERR_INVALID_ARG);
+        return RB_ERR_INVALID_ARG;
+    }
+    // src/level3.rs:86-98: stored shapes, then a, b, c in that order.
+    const bool ta = transa != RB_NO_TRANS, tb = transb != RB_NO_TRANS;
+    const size_t ar = ta ? k : m, ac = ta ? m : k;
+    const size_t br = tb ? n : k, bc = tb ? k : n;
+    rb_status s;
+    if ((s = check_matrix(layout, 'a', ar, ac, lda, a_len, true, err)) != RB_OK) return s;
+    if ((s = check_matrix(layout, 'b', br, bc, ldb, b_len, true, err)) != RB_OK) return s;
+    if ((s = check_matrix(layout, 'c', m, n, ldc, c_len, true, err)) != RB_OK) return s;
+    if (m == 0 || n == 0) return RB_OK;  // src/kernel/gemm.rs:198-200
+    if ((k > 0 && (!a || !b)) || !c) {
+        set_err(err, RB_ERR_INVALID_ARG);
+        return RB_ERR_INVALID_ARG;
+    }
+
+    cudaError_t e;
+    DeviceCtx* ctx = ctx_for_current(&e);
+    if (!ctx) return cuda_fail(err, e);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+
+    ColProblem<T> p = normalise<T>(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    const size_t vec = 16 / sizeof(T);
+    const bool need_ab = p.k > 0 && p.alpha != T(0);
+    const bool read_c = p.beta != T(0);
+    // column-major stored extents after normalisation
+    const size_t a_rows = p.ta ? p.k : p.m, a_cols = p.ta ? p.m : p.k;
+    const size_t b_rows = p.tb ? p.n : p.k, b_cols = p.tb ? p.k : p.n;
+    const size_t lda_d = (a_rows + vec - 1) / vec * vec;
+    const size_t ldb_d = (b_rows + vec - 1) / vec * vec;
+    const size_t ldc_d = (p.m + vec - 1) / vec * vec;
+
+    if (need_ab) {
+        if ((e = ensure_buf(ctx, 0, lda_d * a_cols * sizeof(T))) != cudaSuccess) return cuda_fail(err, e);
+        if ((e = ensure_buf(ctx, 1, ldb_d * b_cols * sizeof(T))) != cudaSuccess) return cuda_fail(err, e);
+    }
+    if ((e = ensure_buf(ctx, 2, ldc_d * p.n * sizeof(T))) != cudaSuccess) return cuda_fail(err, e);
+    T* dA = static_cast<T*>(ctx->buf[0]);
+    T* dB = static_cast<T*>(ctx->buf[1]);
+    T* dC = static_cast<T*>(ctx->buf[2]);
+    cudaStream_t st = ctx->stream;
+
+    if (need_ab) {
+        e = cudaMemcpy2DAsync(dA, lda_d * sizeof(T), p.a, p.lda * sizeof(T), a_rows * sizeof(T), a_cols,
+                              cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(dB, ldb_d * sizeof(T), p.b, p.ldb * sizeof(T), b_rows * sizeof(T),
+                                  b_cols, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+    }
+    if (read_c) {
+        e = cudaMemcpy2DAsync(dC, ldc_d * sizeof(T), p.c, p.ldc * sizeof(T), p.m * sizeof(T), p.n,
+                              cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(err, e);
+    }
+    ColProblem<T> q = p;
+    q.a = dA; q.lda = lda_d;
+    q.b = dB; q.ldb = ldb_d;
+    q.c = dC; q.ldc = ldc_d;
+    // beta == 0: C is never uploaded nor read (apply_beta writes zeros).
+    s = run_dev<T>(q, prec, st, err);
+    if (s != RB_OK) return s;
+    e = cudaMemcpy2DAsync(p.c, p.ldc * sizeof(T), dC, ldc_d * sizeof(T), p.m * sizeof(T), p.n,
+                          cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_fail(err, e);
+    return check_device_word(ctx, err);
+}
+
+template <typename T>
+rb_status dev_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                   size_t k, T alpha, const T* a, size_t lda, const T* b, size_t ldb, T beta, T* c,
+                   size_t ldc, rb_precision prec, void* stream, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_layout(layout) || !valid_trans(transa) || !valid_trans(transb) ||
+        (prec != RB_PREC_PLAIN && prec != RB_PREC_BF16X3 && prec != RB_PREC_OZAKI)) {
+        set_err(err, RB_ERR_INVALID_ARG);
+        return RB_ERR_INVALID_ARG;
+    }
+    const bool ta = transa != RB_NO_TRANS, tb = transb != RB_NO_TRANS;
+    rb_status s;
+    if ((s = check_matrix(layout, 'a', ta ? k : m, ta ? m : k, lda, 0, false, err)) != RB_OK) return s;
+    if ((s = check_matrix(layout, 'b', tb ? n : k, tb ? k : n, ldb, 0, false, err)) != RB_OK) return s;
+    if ((s = check_matrix(layout, 'c', m, n, ldc, 0, false, err)) != RB_OK) return s;
+    if (m == 0 || n == 0) return RB_OK;
+    cudaError_t e;
+    if (!ctx_for_current(&e)) return cuda_fail(err, e);
+    ColProblem<T> p = normalise<T>(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return run_dev<T>(p, prec, static_cast<cudaStream_t>(stream), err);
+}
+
+}  // namespace
+
+uint32_t* device_error_word() {
+    cudaError_t e;
+    DeviceCtx* c = ctx_for_current(&e);
+    return c ? c->err_word : nullptr;
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+const char* rb_status_string(int32_t status) {
+    switch (status) {
+        case RB_OK: return "ok";
+        case RB_ERR_INVALID_LEADING_DIM: return "invalid leading dimension";
+        case RB_ERR_BUFFER_TOO_SMALL: return "buffer too small";
+        case RB_ERR_ZERO_STRIDE: return "stride must be positive (got 0)";
+        case RB_ERR_INVALID_ARG: return "invalid argument";
+        case RB_ERR_UNSUPPORTED: return "unsupported precision form for this operation";
+        case RB_ERR_CUDA: return "CUDA error";
+        case RB_ERR_ALLOC: return "allocation failed";
+        case RB_ERR_TIMEOUT: return "device wait timed out";
+        case RB_ERR_DEVICE: return "device-side error";
+        case RB_ERR_BUSY: return "admission refused";
+        case RB_ERR_CANCELLED: return "cancelled";
+        default: return "unknown status";
+    }
+}
+
+rb_status rb_sgemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                   size_t k, float alpha, const float* a, size_t lda, size_t a_len, const float* b,
+                   size_t ldb, size_t b_len, float beta, float* c, size_t ldc, size_t c_len,
+                   rb_error* err) {
+    return host_gemm<float>(layout, transa, transb, m, n, k, alpha, a, lda, a_len, b, ldb, b_len,
+                            beta, c, ldc, c_len, RB_PREC_PLAIN, err);
+}
+
+rb_status rb_dgemm(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m, size_t n,
+                   size_t k, double alpha, const double* a, size_t lda, size_t a_len,
+                   const double* b, size_t ldb, size_t b_len, double beta, double* c, size_t ldc,
+                   size_t c_len, rb_error* err) {
+    return host_gemm<double>(layout, transa, transb, m, n, k, alpha, a, lda, a_len, b, ldb, b_len,
+                             beta, c, ldc, c_len, RB_PREC_PLAIN, err);
+}
+
+rb_status rb_sgemm_prec(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                        size_t n, size_t k, float alpha, const float* a, size_t lda, size_t a_len,
+                        const float* b, size_t ldb, size_t b_len, float beta, float* c,
+                        size_t ldc, size_t c_len, rb_precision prec, rb_error* err) {
+    return host_gemm<float>(layout, transa, transb, m, n, k, alpha, a, lda, a_len, b, ldb, b_len,
+                            beta, c, ldc, c_len, prec, err);
+}
+
+rb_status rb_dgemm_prec(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                        size_t n, size_t k, double alpha, const double* a, size_t lda,
+                        size_t a_len, const double* b, size_t ldb, size_t b_len, double beta,
+                        double* c, size_t ldc, size_t c_len, rb_precision prec, rb_error* err) {
+    return host_gemm<double>(layout, transa, transb, m, n, k, alpha, a, lda, a_len, b, ldb, b_len,
+                             beta, c, ldc, c_len, prec, err);
+}
+
+rb_status rb_sgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                       size_t n, size_t k, float alpha, const float* a, size_t lda,
+                       const float* b, size_t ldb, float beta, float* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err) {
+    return dev_gemm<float>(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                           prec, stream, err);
+}
+
+rb_status rb_dgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
+                       size_t n, size_t k, double alpha, const double* a, size_t lda,
+                       const double* b, size_t ldb, double beta, double* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err) {
+    return dev_gemm<double>(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                            prec, stream, err);
+}
+
+static std::atomic<int> g_ozaki_slices{8};
+
+rb_status rb_set_ozaki_slices(int slices) {
+    if (slices < 3 || slices > 12) return RB_ERR_INVALID_ARG;
+    g_ozaki_slices.store(slices);
+    return RB_OK;
+}
+
+int rb_get_ozaki_slices(void) { return g_ozaki_slices.load(); }
+
+uint64_t rb_launch_count(void) { return g_launches.load(); }
+
+rb_status rb_device_error(int clear, uint32_t* detail) {
+    cudaError_t e;
+    DeviceCtx* c = ctx_for_current(&e);
+    if (!c) return RB_ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess) return RB_ERR_CUDA;
+    uint32_t w = 0;
+    if (cudaMemcpy(&w, c->err_word, sizeof(w), cudaMemcpyDeviceToHost) != cudaSuccess) return RB_ERR_CUDA;
+    if (detail) *detail = w;
+    if (clear && w) cudaMemset(c->err_word, 0, sizeof(uint32_t));
+    if (w == 0) return RB_OK;
+    return ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
+}
+
+void rb_release_cached_memory(void) {
+    cudaError_t e;
+    DeviceCtx* c = ctx_for_current(&e);
+    if (!c) return;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < 3; ++i) {
+        if (c->buf[i]) cudaFree(c->buf[i]);
+        c->buf[i] = nullptr;
+        c->cap[i] = 0;
+    }
+}
+
+}  // extern "C"

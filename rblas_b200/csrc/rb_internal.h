@@ -1,0 +1,54 @@
+// rb_internal.h -- host-side declarations shared by the library's translation
+// units: tensor-map encoding, kernel launchers and the per-device context.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <mutex>
+
+// Device error word layout: [31:24] kind, [23:0] site.
+#define RB_DEVERR_TIMEOUT 0x01000000u
+#define RB_DEVERR_BOUNDS 0x02000000u
+#define RB_DEVERR_ARG 0x03000000u
+
+namespace rb {
+
+// ---- tensor maps --------------------------------------------------------------
+
+// 2-D tiled tensor map over a column-major matrix whose contiguous extent is
+// `rows` elements and which has `cols` lines `ld` elements apart; the box is
+// box_rows x box_cols. swizzle128: 128-byte swizzle (box_rows*elem == 128).
+// Returns CUDA_SUCCESS or the driver error.
+CUresult make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
+                      uint64_t rows, uint64_t cols, uint64_t ld, uint32_t box_rows,
+                      uint32_t box_cols, bool swizzle128);
+
+// ---- launch bookkeeping ----------------------------------------------------------
+
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Per-device error word (device memory, zero when healthy).
+uint32_t* device_error_word();
+
+// ---- launchers (all operands column-major after row-major normalisation) ------
+
+// Plain SIMT GEMM, C = alpha*op(A)op(B) + beta*C. a_kmajor: op(A) is stored
+// k-contiguous (Trans); otherwise m-contiguous (NoTrans). b_kmajor: op(B) is
+// stored k-contiguous (NoTrans); otherwise n-contiguous (Trans).
+// Requirements: A/B 16-byte aligned with lda/ldb*sizeof(T) % 16 == 0.
+template <typename T>
+cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
+                             const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
+                             size_t ldc, cudaStream_t st, CUresult* cu_err);
+
+// C := beta*C over an m x n column-major block (beta == 0 writes zeros
+// without reading; beta == 1 is a no-op and launches nothing).
+template <typename T>
+cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st);
+
+}  // namespace rb

@@ -1,0 +1,109 @@
+"""CPU tests of the C-ABI boundary: the library loads, exports every symbol
+include/rblas_b200.h declares, and the host-side validation reproduces
+rblas's try_gemm error contract (src/level3.rs:68-140) -- none of these
+calls reach the GPU."""
+from __future__ import annotations
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rblas_b200 as rb
+from rblas_b200 import _lib, level3
+from rblas_b200.types import Layout, Transpose
+from tests.golden_runner import load_cases
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "rblas_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(rb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_builds_and_loads():
+    lib = _lib.load()
+    assert lib is not None
+
+
+def test_every_declared_symbol_is_exported():
+    lib = _lib.load()
+    missing = [f for f in header_functions() if not hasattr(lib, f)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_every_declared_symbol_has_a_binding():
+    missing = [f for f in header_functions() if f not in _lib.SIGNATURES]
+    assert not missing, f"no ctypes signature for: {missing}"
+
+
+def test_status_strings():
+    lib = _lib.load()
+    assert lib.rb_status_string(0) == b"ok"
+    assert lib.rb_status_string(2) == b"buffer too small"
+
+
+def test_try_gemm_error_contract_matches_reference():
+    """src/level3.rs:567-640 with the exact error fields."""
+    meta, _ = load_cases()["try_gemm_errors"]
+    m, n, k = meta["m"], meta["n"], meta["k"]
+    for call in meta["calls"][1:]:
+        a = np.ones(call["a_len"])
+        b = np.ones(call["b_len"])
+        c = np.zeros(call["c_len"])
+        e = level3.try_gemm(Layout.ColMajor, Transpose.NoTrans, Transpose.NoTrans, m, n, k, 1.0,
+                            a, call["lda"], b, call["ldb"], 0.0, c, call["ldc"])
+        w = call["want"]
+        if w["code"] == 1:
+            assert e == rb.InvalidLeadingDim(w["which"], w["got"], w["min_or_need"])
+            assert str(e) == "invalid leading dimension for `a`: got 3, need ≥ 4"
+        else:
+            assert e == rb.BufferTooSmall(w["which"], w["got"], w["min_or_need"])
+
+
+@pytest.mark.parametrize("layout", [Layout.RowMajor, Layout.ColMajor])
+def test_validation_order_and_fields(layout):
+    """a, b, c in order; InvalidLeadingDim before BufferTooSmall; stored
+    shapes follow the transpose (src/level3.rs:86-98, 121-138)."""
+    m, n, k = 5, 7, 3
+    ta, tb = Transpose.Trans, Transpose.NoTrans
+    # stored A is k x m; row-major min lead = cols = m, col-major = rows = k
+    min_a = m if layout == Layout.RowMajor else k
+    a = np.zeros(100)
+    b = np.zeros(100)
+    c = np.zeros(100)
+    e = level3.try_gemm(layout, ta, tb, m, n, k, 1.0, a, min_a - 1, b, 100, 0.0, c, 100)
+    assert e == rb.InvalidLeadingDim("a", min_a - 1, min_a)
+    # bad b and bad c: a is reported first only when a is bad
+    min_b = n if layout == Layout.RowMajor else k
+    e = level3.try_gemm(layout, ta, tb, m, n, k, 1.0, a, min_a, b, min_b - 1, 0.0, c, 0)
+    assert e == rb.InvalidLeadingDim("b", min_b - 1, min_b)
+    # buffer too small on c: need = (n-1)*ldc + m (col) / (m-1)*ldc + n (row)
+    ldc = 9
+    need = (n - 1) * ldc + m if layout == Layout.ColMajor else (m - 1) * ldc + n
+    cs = np.zeros(need - 1)
+    e = level3.try_gemm(layout, ta, tb, m, n, k, 1.0, a, min_a, b, min_b, 0.0, cs, ldc)
+    assert e == rb.BufferTooSmall("c", need - 1, need)
+
+
+def test_zero_dims_are_valid_and_touch_nothing():
+    """check_matrix returns Ok for zero dims; gemm_contig returns before beta."""
+    c = np.full(4, np.nan)
+    e = level3.try_gemm(Layout.ColMajor, Transpose.NoTrans, Transpose.NoTrans, 0, 4, 3, 1.0,
+                        np.zeros(0), 0, np.zeros(12), 3, 0.0, c, 1)
+    assert e is None and np.all(np.isnan(c))
+
+
+def test_invalid_enum_rejected_by_the_c_layer():
+    import ctypes as C
+    lib = _lib.load()
+    err = _lib.RbError()
+    buf = np.zeros(4)
+    p = C.c_void_p(buf.ctypes.data)
+    st = lib.rb_dgemm(7, 0, 0, 2, 2, 2, 1.0, p, 2, 4, p, 2, 4, 0.0, p, 2, 4, C.byref(err))
+    assert st == 4 and err.code == 4
+    with pytest.raises(ValueError):
+        level3.try_gemm(7, 0, 0, 2, 2, 2, 1.0, buf, 2, buf, 2, 0.0, buf, 2)
