@@ -384,6 +384,39 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_kernel_only(args):
+    """One GEMM shape, launched warmup + steps times on the device (for ncu
+    captures of a single kernel on a bounded case)."""
+    import torch
+
+    from rblas_b200 import level3
+    from rblas_b200.types import Layout, Precision
+
+    m, n, k = args.shape
+    dt = torch.float64 if args.dtype == "f64" else torch.float32
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    A = torch.randn(m * k, dtype=dt, device="cuda", generator=g)
+    B = torch.randn(k * n, dtype=dt, device="cuda", generator=g)
+    C = torch.randn(m * n, dtype=dt, device="cuda", generator=g)
+    prec = {"plain": Precision.Plain, "ozaki": Precision.Ozaki, "bf16x3": Precision.Bf16x3}[
+        args.form if args.form != "auto" else "plain"]
+    sh = torch.cuda.current_stream().cuda_stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            e0.record()
+        level3.gemm_dev(Layout.ColMajor, args.ta, args.tb, m, n, k, 1.0, A.data_ptr(),
+                        k if args.ta else m, B.data_ptr(), n if args.tb else k, 0.5, C.data_ptr(), m,
+                        np.float64 if args.dtype == "f64" else np.float32, prec=prec, stream=sh)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"kernel_only": [m, n, k], "dtype": args.dtype, "form": args.form,
+                      "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -393,8 +426,15 @@ def main():
     ap.add_argument("--form", choices=["auto", "plain", "ozaki"], default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,
+                    metavar=("M", "N", "K"), help="time one column-major GEMM shape only")
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--ta", type=int, default=0)
+    ap.add_argument("--tb", type=int, default=0)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.shape:
+        run_kernel_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

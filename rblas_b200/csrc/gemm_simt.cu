@@ -78,8 +78,9 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "swizzled tiles need 1 KiB alignment");
 
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
-                                               ~static_cast<uintptr_t>(1023));
+    // Align by offsetting the __shared__ array itself (not through an integer
+    // cast) so every access below stays a shared-window load.
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE_BYTES);
     uint64_t* empty = full + ST;
 

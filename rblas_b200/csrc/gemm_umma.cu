@@ -1,0 +1,570 @@
+// gemm_umma.cu -- the split-precision GEMM forms on the 5th-generation tensor
+// cores (tcgen05.mma, accumulators in TMEM):
+//
+//   BF16X3 (SGEMM): x = hi + lo with hi = bf16(x), lo = bf16(x - hi);
+//     C = alpha * (Ah*Bh + Ah*Bl + Al*Bh) + beta * C, FP32 accumulation.
+//   OZAKI (DGEMM): Ozaki-scheme INT8 slice emulation (Ozaki, Ogita, Oishi &
+//     Rump, "Error-free transformations of matrix multiplication by using
+//     fast routines of matrix multiplication and its applications", Numer.
+//     Algorithms 59, 2012; Ootomo, Ozaki & Yokota, "DGEMM on integer matrix
+//     multiplication unit", IJHPCA 2024). Each row of op(A) / column of op(B)
+//     is scaled by a power of two 2^-e so |x| < 1, then cut into `s` signed
+//     7-bit slices: x * 2^-e = sum_t sigma_t 2^-7(t+1). Slice products are
+//     exact in INT32; the products of equal weight (t+u = d) share one TMEM
+//     accumulator, and C = alpha * 2^(e_i+f_j) sum_d 2^-7(d+2) S_d + beta * C
+//     is summed in FP64 from the smallest weight up. Pairs with t+u >= s are
+//     dropped (the scheme's truncation).
+//
+// Both replace rblas's CPU blocking/packing/microkernel path
+// (src/kernel/gemm.rs:185-429) for the precision forms that rblas does not
+// have; the plain forms live in gemm_simt.cu.
+//
+// Kernel structure (persistent, one CTA per SM, 6 warps):
+//   warp 0 lane 0  TMA producer: K-major operand tiles (128-byte rows, 128-byte
+//                  swizzle) into a STAGES-deep shared-memory ring.
+//   warp 1         allocates 512 TMEM columns; lane 0 issues tcgen05.mma
+//                  (M=128, N=256) into one of two 256-column accumulators and
+//                  commits each stage back to the producer.
+//   warps 2..5     epilogue: tcgen05.ld the accumulator (warp w reads TMEM
+//                  lanes 32*(w%4)..+31 = tile rows), apply the form's
+//                  scaling and alpha/beta, store C coalesced; release the
+//                  accumulator so the next unit's MMAs overlap this drain.
+// Operands are first rewritten by a pre-pass into K-major bf16 hi/lo planes
+// or int8 slice planes (this also absorbs every transpose and layout).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "rb_device.cuh"
+#include "rb_internal.h"
+
+namespace rb {
+
+namespace {
+
+constexpr int kUM = 128, kUN = 256;
+constexpr int kRowBytes = 128;                  // K bytes per tile row (one swizzle row)
+constexpr int kATile = kUM * kRowBytes;         // 16 KiB
+constexpr int kBTile = kUN * kRowBytes;         // 32 KiB
+constexpr int kUmmaThreads = 192;
+constexpr int kAccCols = 256;
+constexpr int kExpSentinel = -(1 << 30);        // row exponent of an all-zero row
+
+enum { kModeBf16x3 = 0, kModeOzaki = 1 };
+
+template <int MODE> struct UCfg;
+template <> struct UCfg<kModeBf16x3> { static constexpr int NA = 2, NB = 2, STAGES = 2; };
+template <> struct UCfg<kModeOzaki> { static constexpr int NA = 1, NB = 1, STAGES = 4; };
+
+template <int MODE>
+constexpr int umma_smem_bytes() {
+    return UCfg<MODE>::STAGES * (UCfg<MODE>::NA * kATile + UCfg<MODE>::NB * kBTile) + 256 + 1024;
+}
+
+struct UParams {
+    int m, n, k;
+    int tiles_m, tiles_n, num_tiles;
+    int num_kt;        // 128-byte K tiles over the whole K
+    int slices;        // Ozaki
+    int kt_per_chunk;  // Ozaki: K tiles per exact-INT32 chunk
+    int kchunks;
+    int beta_mode;     // 0 beta == 0, 1 beta == 1, 2 general
+    float alpha_f, beta_f;
+    double alpha_d, beta_d;
+    void* c;
+    size_t ldc;
+    const int* row_exp;
+    const int* col_exp;
+    uint32_t* err;
+};
+
+struct Bar {
+    uint64_t full[4], empty[4], acc_full[2], acc_empty[2], drain;
+    uint32_t tmem_base;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kUmmaThreads, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const UParams p) {
+    constexpr int NA = UCfg<MODE>::NA, NB = UCfg<MODE>::NB, ST = UCfg<MODE>::STAGES;
+    constexpr int STAGE_BYTES = NA * kATile + NB * kBTile;
+    constexpr int KSTEPS = 4;  // UMMA K steps of 32 bytes per 128-byte tile row
+    constexpr uint32_t IDESC = (MODE == kModeBf16x3) ? umma_idesc(1, 1, kUM, kUN)   // f32 <- bf16
+                                                     : umma_idesc(2, 1, kUM, kUN);  // s32 <- s8
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    Bar* bar = reinterpret_cast<Bar*>(smem + ST * STAGE_BYTES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(&bar->full[s], 1);
+            mbar_init(&bar->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&bar->acc_full[b], 1);
+            mbar_init(&bar->acc_empty[b], 4);
+        }
+        mbar_init(&bar->drain, 1);
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&bar->tmem_base, 2 * kAccCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bar->tmem_base;
+
+    // units per tile: BF16X3 one; OZAKI kchunks x slices diagonals
+    const int units = (MODE == kModeBf16x3) ? 1 : p.kchunks * p.slices;
+    bool ok = true;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------ TMA producer ------------------------------
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+        uint32_t it = 0;
+        constexpr int kElems = (MODE == kModeBf16x3) ? 64 : 128;  // elements per 128-byte row
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            int tm, tn;
+            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * kUN;
+            for (int u = 0; ok && u < units; ++u) {
+                int pairs = 1, d = 0, kt0 = 0, kt1 = p.num_kt;
+                if (MODE == kModeOzaki) {
+                    const int chunk = u / p.slices;
+                    d = p.slices - 1 - (u % p.slices);
+                    pairs = d + 1;
+                    kt0 = chunk * p.kt_per_chunk;
+                    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+                }
+                for (int pi = 0; ok && pi < pairs; ++pi) {
+                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                        const int s = it % ST;
+                        if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x201)) {
+                            ok = false;
+                            break;
+                        }
+                        uint8_t* sa = smem + s * STAGE_BYTES;
+                        uint8_t* sb = sa + NA * kATile;
+                        mbar_arrive_expect_tx(&bar->full[s], STAGE_BYTES);
+                        const int k0 = kt * kElems;
+                        if (MODE == kModeBf16x3) {
+                            tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, 0);
+                            tma_load_3d(sa + kATile, &tmA, &bar->full[s], k0, m0, 1);
+                            tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, 0);
+                            tma_load_3d(sb + kBTile, &tmB, &bar->full[s], k0, n0, 1);
+                        } else {
+                            tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, pi);
+                            tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, d - pi);
+                        }
+                    }
+                }
+            }
+        }
+        if (!ok) {
+            const uint32_t first = it > (uint32_t)ST ? it - ST : 0;
+            for (uint32_t j = first; j < it; ++j) mbar_wait_drain(&bar->full[j % ST], (j / ST) & 1);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------ MMA issuer ------------------------------
+        uint32_t it = 0, uc = 0;
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            for (int u = 0; ok && u < units; ++u, ++uc) {
+                int pairs = 1, kt0 = 0, kt1 = p.num_kt;
+                if (MODE == kModeOzaki) {
+                    const int chunk = u / p.slices;
+                    pairs = p.slices - (u % p.slices);
+                    kt0 = chunk * p.kt_per_chunk;
+                    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+                }
+                const uint32_t b = uc & 1;
+                if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, p.err, 0x202)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + b * kAccCols;
+                uint32_t accumulate = 0;
+                for (int pi = 0; ok && pi < pairs; ++pi) {
+                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                        const int s = it % ST;
+                        if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x203)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+                        const uint32_t sb = sa + NA * kATile;
+#pragma unroll
+                        for (int kk = 0; kk < KSTEPS; ++kk) {
+                            if (MODE == kModeBf16x3) {
+                                const uint64_t ah = sw128_kmajor_desc(sa) + 2 * kk;
+                                const uint64_t al = sw128_kmajor_desc(sa + kATile) + 2 * kk;
+                                const uint64_t bh = sw128_kmajor_desc(sb) + 2 * kk;
+                                const uint64_t bl = sw128_kmajor_desc(sb + kBTile) + 2 * kk;
+                                // small terms first into the fresh accumulator
+                                umma_f16(d_tmem, al, bh, IDESC, accumulate);
+                                umma_f16(d_tmem, ah, bl, IDESC, 1);
+                                umma_f16(d_tmem, ah, bh, IDESC, 1);
+                            } else {
+                                const uint64_t a = sw128_kmajor_desc(sa) + 2 * kk;
+                                const uint64_t bb = sw128_kmajor_desc(sb) + 2 * kk;
+                                umma_i8(d_tmem, a, bb, IDESC, accumulate);
+                            }
+                            accumulate = 1;
+                        }
+                        tc_commit(&bar->empty[s]);  // stage free once these MMAs complete
+                    }
+                }
+                if (ok) tc_commit(&bar->acc_full[b]);
+            }
+        }
+        // make sure nothing of ours is still in flight before TMEM is released
+        tc_commit(&bar->drain);
+        mbar_wait_drain(&bar->drain, 0);
+    } else if (warp >= 2) {
+        // ------------------------------ epilogue ------------------------------
+        const int quarter = warp & 3;
+        const int row_in_tile = quarter * 32 + lane;
+        uint32_t uc = 0;
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            int tm, tn;
+            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * kUN;
+            const int r = m0 + row_in_tile;
+            const bool row_ok = r < p.m;
+            int er = 0;
+            if (MODE == kModeOzaki && row_ok) er = p.row_exp[r];
+            for (int u = 0; ok && u < units; ++u, ++uc) {
+                const uint32_t b = uc & 1;
+                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * kAccCols;
+                const int d = (MODE == kModeOzaki) ? p.slices - 1 - (u % p.slices) : 0;
+                const bool first_unit = (u == 0);
+#pragma unroll 1
+                for (int ch = 0; ch < kAccCols / 32; ++ch) {
+                    uint32_t v[32];
+                    tmem_ld32(taddr + ch * 32, v);
+                    tmem_ld_wait();
+                    if (!row_ok) continue;
+                    const int cbase = n0 + ch * 32;
+                    if (MODE == kModeBf16x3) {
+                        float* C = static_cast<float*>(p.c);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = cbase + j;
+                            if (col >= p.n) break;
+                            float* cp = C + r + static_cast<size_t>(col) * p.ldc;
+                            float tb = 0.f;
+                            if (p.beta_mode == 1) tb = *cp;
+                            else if (p.beta_mode == 2) tb = p.beta_f * *cp;
+                            *cp = fmaf(p.alpha_f, __uint_as_float(v[j]), tb);
+                        }
+                    } else {
+                        double* C = static_cast<double*>(p.c);
+                        if (er == kExpSentinel && !first_unit) continue;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = cbase + j;
+                            if (col >= p.n) break;
+                            double* cp = C + r + static_cast<size_t>(col) * p.ldc;
+                            const int fc = __ldg(p.col_exp + col);
+                            double term = 0.0;
+                            if (er != kExpSentinel && fc != kExpSentinel)
+                                term = scalbn(static_cast<double>(static_cast<int32_t>(v[j])),
+                                              er + fc - 7 * (d + 2));
+                            double acc;
+                            if (first_unit) {
+                                acc = 0.0;
+                                if (p.beta_mode == 1) acc = *cp;
+                                else if (p.beta_mode == 2) acc = p.beta_d * *cp;
+                            } else {
+                                acc = *cp;
+                            }
+                            *cp = fma(p.alpha_d, term, acc);
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 2 * kAccCols);
+    }
+}
+
+// ------------------------------------------------------------------------------
+// Pre-pass kernels. An operand is viewed as R x K with element (r, p) at
+// x[r*rs + p*ps]; outputs are K-major planes [plane][R][kp] (kp = padded K).
+// ------------------------------------------------------------------------------
+
+__device__ __forceinline__ int frexp_exp(double x) {
+    // exponent e with |x| in [2^(e-1), 2^e); x != 0
+    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
+    const int f = static_cast<int>((bits >> 52) & 0x7FF);
+    if (f != 0) return f - 1022;
+    int e;
+    frexp(x, &e);
+    return e;
+}
+
+__global__ void fill_int_kernel(int* p, int n, int v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// e[r] = max over p of frexp_exp(x(r,p)) (kExpSentinel if the row is zero).
+// 2-D grid over (rows, K-blocks of 1024); atomicMax merges K-blocks.
+__global__ void row_exp_kernel(const double* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                               int* __restrict__ e) {
+    const int p0 = blockIdx.y * 1024;
+    const int p1 = min(K, p0 + 1024);
+    if (ps == 1) {
+        // K-contiguous: one warp per row
+        const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+        if (r >= R) return;
+        int best = kExpSentinel;
+        for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) {
+            const double v = x[static_cast<size_t>(r) * rs + q];
+            if (v != 0.0) best = max(best, frexp_exp(v));
+        }
+        for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if ((threadIdx.x & 31) == 0 && best != kExpSentinel) atomicMax(e + r, best);
+    } else {
+        // R-contiguous: one thread per row, consecutive threads read consecutive rows
+        const int r = blockIdx.x * blockDim.x + threadIdx.x;
+        if (r >= R) return;
+        int best = kExpSentinel;
+        for (int q = p0; q < p1; ++q) {
+            const double v = x[r + static_cast<size_t>(q) * ps];
+            if (v != 0.0) best = max(best, frexp_exp(v));
+        }
+        if (best != kExpSentinel) atomicMax(e + r, best);
+    }
+}
+
+constexpr int kTile = 64;
+
+// Load a 64 x 64 tile of the R x K view into shared memory (coalesced along
+// the view's contiguous dimension); out-of-range elements read as 0.
+template <typename T>
+__device__ __forceinline__ void load_tile(const T* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                                          int r0, int p0, T (*tile)[kTile + 1]) {
+    const bool kcontig = (ps == 1);
+    for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+        const int a = idx % kTile, b = idx / kTile;
+        const int r = kcontig ? b : a;
+        const int q = kcontig ? a : b;
+        T v = T(0);
+        if (r0 + r < R && p0 + q < K) v = x[static_cast<size_t>(r0 + r) * rs + static_cast<size_t>(p0 + q) * ps];
+        tile[r][q] = v;
+    }
+}
+
+// Ozaki slicing: out[t][r][q] = sigma_t of x(r,q) * 2^-e[r], t < slices.
+__global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
+                                                          int R, int K, const int* __restrict__ e,
+                                                          int slices, int8_t* __restrict__ out, size_t kp,
+                                                          size_t plane) {
+    __shared__ double tile[kTile][kTile + 1];
+    const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
+    load_tile<double>(x, rs, ps, R, K, r0, p0, tile);
+    __syncthreads();
+    const int r = threadIdx.x >> 2, c = threadIdx.x & 3;  // 64 rows x 4 chunks of 16
+    if (r0 + r >= R) return;
+    const int er = e[r0 + r];
+    double xs[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) xs[i] = (er == kExpSentinel) ? 0.0 : scalbn(tile[r][c * 16 + i], -er);
+    for (int t = 0; t < slices; ++t) {
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double v = xs[i] * 128.0;
+            const double s = trunc(v);
+            xs[i] = v - s;
+            w[i >> 2] |= (static_cast<uint32_t>(static_cast<int>(s)) & 0xFFu) << (8 * (i & 3));
+        }
+        const size_t off = t * plane + static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
+        if (p0 + c * 16 < static_cast<int>(kp))
+            *reinterpret_cast<uint4*>(out + off) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// BF16 split: out[0][r][q] = bf16(x), out[1][r][q] = bf16(x - bf16(x)).
+__global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict__ x, size_t rs, size_t ps,
+                                                         int R, int K, __nv_bfloat16* __restrict__ out,
+                                                         size_t kp, size_t plane) {
+    __shared__ float tile[kTile][kTile + 1];
+    const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
+    load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
+    __syncthreads();
+    for (int job = threadIdx.x; job < kTile * 8; job += blockDim.x) {
+        const int r = job >> 3, c = job & 7;  // 64 rows x 8 chunks of 8
+        if (r0 + r >= R || p0 + c * 8 >= static_cast<int>(kp)) continue;
+        __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float v = tile[r][c * 8 + i];
+            hi[i] = __float2bfloat16_rn(v);
+            lo[i] = __float2bfloat16_rn(v - __bfloat162float(hi[i]));
+        }
+        const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 8;
+        *reinterpret_cast<uint4*>(out + off) = *reinterpret_cast<const uint4*>(hi);
+        *reinterpret_cast<uint4*>(out + plane + off) = *reinterpret_cast<const uint4*>(lo);
+    }
+}
+
+CUresult make_tmap_planes(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
+                          uint64_t k, uint64_t rows, uint64_t planes, uint64_t kp, uint32_t box_rows) {
+    return make_tmap_3d(map, base, dtype, elem, k, rows, planes, kp, kp * rows, kRowBytes / elem,
+                        box_rows, 1, true);
+}
+
+template <int MODE>
+cudaError_t launch_umma(const CUtensorMap& ta, const CUtensorMap& tb, const UParams& p, cudaStream_t st) {
+    auto kern = umma_gemm_kernel<MODE>;
+    constexpr int smem = umma_smem_bytes<MODE>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = p.num_tiles < sms ? p.num_tiles : sms;
+    kern<<<grid, kUmmaThreads, smem, st>>>(ta, tb, p);
+    count_launch();
+    return cudaGetLastError();
+}
+
+inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+// op(A) viewed as m x k: (i,p) at A[i + p*lda] (NoTrans) or A[p + i*lda] (Trans).
+// op(B)^T viewed as n x k: (j,p) at B[p + j*ldb] (NoTrans) or B[j + p*ldb] (Trans).
+static void operand_views(bool ta, bool tb, size_t lda, size_t ldb, size_t& ars, size_t& aps,
+                          size_t& brs, size_t& bps) {
+    if (!ta) { ars = 1; aps = lda; } else { ars = lda; aps = 1; }
+    if (!tb) { brs = ldb; bps = 1; } else { brs = 1; bps = ldb; }
+}
+
+cudaError_t launch_bf16x3_gemm(bool ta, bool tb, int m, int n, int k, float alpha, const float* A,
+                               size_t lda, const float* B, size_t ldb, float beta, float* C,
+                               size_t ldc, cudaStream_t st, CUresult* cu_err) {
+    const size_t kp = round_up(static_cast<size_t>(k), 8);  // 16-byte rows of bf16
+    const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
+    void* sa = nullptr;
+    void* sb = nullptr;
+    cudaError_t e = cudaMallocAsync(&sa, 2 * pa * sizeof(__nv_bfloat16), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocAsync(&sb, 2 * pb * sizeof(__nv_bfloat16), st);
+    if (e != cudaSuccess) { cudaFreeAsync(sa, st); return e; }
+    size_t ars, aps, brs, bps;
+    operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
+    const dim3 ga((k + kTile - 1) / kTile, (m + kTile - 1) / kTile);
+    const dim3 gb((k + kTile - 1) / kTile, (n + kTile - 1) / kTile);
+    bf16_split_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, static_cast<__nv_bfloat16*>(sa), kp, pa);
+    bf16_split_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, static_cast<__nv_bfloat16*>(sb), kp, pb);
+    count_launch(2);
+    CUtensorMap tma, tmb;
+    CUresult r = make_tmap_planes(&tma, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, m, 2, kp, kUM);
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, sb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, n, 2, kp, kUN);
+    if (r != CUDA_SUCCESS) {
+        if (cu_err) *cu_err = r;
+        cudaFreeAsync(sa, st);
+        cudaFreeAsync(sb, st);
+        return cudaErrorInvalidValue;
+    }
+    UParams p{};
+    p.m = m; p.n = n; p.k = k;
+    p.tiles_m = (m + kUM - 1) / kUM;
+    p.tiles_n = (n + kUN - 1) / kUN;
+    p.num_tiles = p.tiles_m * p.tiles_n;
+    p.num_kt = static_cast<int>((k + 63) / 64);
+    p.slices = 1; p.kt_per_chunk = p.num_kt; p.kchunks = 1;
+    p.beta_mode = (beta == 0.f) ? 0 : (beta == 1.f ? 1 : 2);
+    p.alpha_f = alpha; p.beta_f = beta;
+    p.c = C; p.ldc = ldc;
+    p.err = device_error_word();
+    e = launch_umma<kModeBf16x3>(tma, tmb, p, st);
+    cudaFreeAsync(sa, st);
+    cudaFreeAsync(sb, st);
+    return e;
+}
+
+cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A,
+                              size_t lda, const double* B, size_t ldb, double beta, double* C,
+                              size_t ldc, int slices, cudaStream_t st, CUresult* cu_err) {
+    const size_t kp = round_up(static_cast<size_t>(k), 16);
+    const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
+    void* buf = nullptr;
+    const size_t exps = round_up((static_cast<size_t>(m) + n) * sizeof(int), 256);
+    cudaError_t e = cudaMallocAsync(&buf, exps + slices * (pa + pb), st);
+    if (e != cudaSuccess) return e;
+    int* ea = static_cast<int*>(buf);
+    int* eb = ea + m;
+    int8_t* sla = static_cast<int8_t*>(buf) + exps;
+    int8_t* slb = sla + slices * pa;
+    size_t ars, aps, brs, bps;
+    operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
+    fill_int_kernel<<<64, 256, 0, st>>>(ea, m + n, kExpSentinel);
+    const int kb = (k + 1023) / 1024;
+    if (aps == 1) row_exp_kernel<<<dim3((m + 7) / 8, kb), 256, 0, st>>>(A, ars, aps, m, k, ea);
+    else          row_exp_kernel<<<dim3((m + 255) / 256, kb), 256, 0, st>>>(A, ars, aps, m, k, ea);
+    if (bps == 1) row_exp_kernel<<<dim3((n + 7) / 8, kb), 256, 0, st>>>(B, brs, bps, n, k, eb);
+    else          row_exp_kernel<<<dim3((n + 255) / 256, kb), 256, 0, st>>>(B, brs, bps, n, k, eb);
+    const dim3 ga((kp + kTile - 1) / kTile, (m + kTile - 1) / kTile);
+    const dim3 gb((kp + kTile - 1) / kTile, (n + kTile - 1) / kTile);
+    ozaki_slice_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, ea, slices, sla, kp, pa);
+    ozaki_slice_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, eb, slices, slb, kp, pb);
+    count_launch(5);
+    CUtensorMap tma, tmb;
+    CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, m, slices, kp, kUM);
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, kUN);
+    if (r != CUDA_SUCCESS) {
+        if (cu_err) *cu_err = r;
+        cudaFreeAsync(buf, st);
+        return cudaErrorInvalidValue;
+    }
+    UParams p{};
+    p.m = m; p.n = n; p.k = k;
+    p.tiles_m = (m + kUM - 1) / kUM;
+    p.tiles_n = (n + kUN - 1) / kUN;
+    p.num_tiles = p.tiles_m * p.tiles_n;
+    p.num_kt = static_cast<int>((k + 127) / 128);
+    p.slices = slices;
+    // exact INT32: (pairs per diagonal <= slices) * k_chunk * 127^2 < 2^31
+    const long long max_k = (2147483647LL / (static_cast<long long>(slices) * 127 * 127)) / 128 * 128;
+    p.kt_per_chunk = static_cast<int>(max_k / 128);
+    if (p.kt_per_chunk < 1) p.kt_per_chunk = 1;
+    p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
+    p.beta_mode = (beta == 0.0) ? 0 : (beta == 1.0 ? 1 : 2);
+    p.alpha_d = alpha; p.beta_d = beta;
+    p.c = C; p.ldc = ldc;
+    p.row_exp = ea; p.col_exp = eb;
+    p.err = device_error_word();
+    e = launch_umma<kModeOzaki>(tma, tmb, p, st);
+    cudaFreeAsync(buf, st);
+    return e;
+}
+
+}  // namespace rb

@@ -22,6 +22,8 @@
 namespace rb {
 
 std::atomic<uint64_t> g_launches{0};
+static std::atomic<int> g_ozaki_slices{8};
+static int ozaki_slices() { return g_ozaki_slices.load(); }
 
 namespace {
 
@@ -154,6 +156,34 @@ bool tma_ok(const T* p, size_t ld) {
     return (reinterpret_cast<uintptr_t>(p) % 16 == 0) && ((ld * sizeof(T)) % 16 == 0);
 }
 
+// The split-precision forms: BF16X3 for f32, OZAKI for f64. Their pre-pass
+// reads the operands with plain loads, so no TMA alignment repack is needed.
+template <typename T>
+rb_status run_precision_form(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb_error* err) {
+    cudaError_t e;
+    CUresult cu = CUDA_SUCCESS;
+    if constexpr (sizeof(T) == 4) {
+        if (prec != RB_PREC_BF16X3) {
+            set_err(err, RB_ERR_UNSUPPORTED);
+            return RB_ERR_UNSUPPORTED;
+        }
+        e = launch_bf16x3_gemm(p.ta, p.tb, (int)p.m, (int)p.n, (int)p.k, p.alpha, p.a, p.lda, p.b, p.ldb,
+                               p.beta, p.c, p.ldc, st, &cu);
+    } else {
+        if (prec != RB_PREC_OZAKI) {
+            set_err(err, RB_ERR_UNSUPPORTED);
+            return RB_ERR_UNSUPPORTED;
+        }
+        e = launch_ozaki_gemm(p.ta, p.tb, (int)p.m, (int)p.n, (int)p.k, p.alpha, p.a, p.lda, p.b, p.ldb,
+                              p.beta, p.c, p.ldc, ozaki_slices(), st, &cu);
+    }
+    if (cu != CUDA_SUCCESS) {
+        set_err(err, RB_ERR_CUDA, 0, 0, 0, static_cast<int32_t>(cu));
+        return RB_ERR_CUDA;
+    }
+    return e == cudaSuccess ? RB_OK : cuda_fail(err, e);
+}
+
 // Enqueue the column-major problem on `st` with device operands. Operands
 // that TMA cannot address directly (unaligned base or leading dimension) are
 // repacked into stream-ordered scratch first.
@@ -169,10 +199,7 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
         e = launch_scale_c<T>((int)p.m, (int)p.n, p.beta, p.c, p.ldc, st);
         return e == cudaSuccess ? RB_OK : cuda_fail(err, e);
     }
-    if (prec != RB_PREC_PLAIN) {
-        set_err(err, RB_ERR_UNSUPPORTED);
-        return RB_ERR_UNSUPPORTED;
-    }
+    if (prec != RB_PREC_PLAIN) return run_precision_form(p, prec, st, err);
     const T* A = p.a;
     const T* B = p.b;
     size_t lda = p.lda, ldb = p.ldb;
@@ -410,7 +437,6 @@ rb_status rb_dgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose trans
                             prec, stream, err);
 }
 
-static std::atomic<int> g_ozaki_slices{8};
 
 rb_status rb_set_ozaki_slices(int slices) {
     if (slices < 3 || slices > 12) return RB_ERR_INVALID_ARG;

@@ -27,6 +27,12 @@ CUresult make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dt
                       uint64_t rows, uint64_t cols, uint64_t ld, uint32_t box_rows,
                       uint32_t box_cols, bool swizzle128);
 
+// 3-D tiled tensor map: dims d0 (contiguous), d1, d2; strides s1, s2 in
+// elements between consecutive d1 / d2 indices; box b0 x b1 x b2.
+CUresult make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
+                      uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
+                      uint32_t b0, uint32_t b1, uint32_t b2, bool swizzle128);
+
 // ---- launch bookkeeping ----------------------------------------------------------
 
 extern std::atomic<uint64_t> g_launches;
@@ -50,5 +56,18 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
 // without reading; beta == 1 is a no-op and launches nothing).
 template <typename T>
 cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st);
+
+// 3xBF16 split SGEMM on tcgen05 (kind::f16, FP32 accumulation in TMEM).
+// Operands may have any alignment (a pre-pass rewrites them into bf16 hi/lo
+// planes in stream-ordered scratch).
+cudaError_t launch_bf16x3_gemm(bool ta, bool tb, int m, int n, int k, float alpha, const float* A,
+                               size_t lda, const float* B, size_t ldb, float beta, float* C,
+                               size_t ldc, cudaStream_t st, CUresult* cu_err);
+
+// Ozaki INT8-slice DGEMM on tcgen05 (kind::i8, exact INT32 in TMEM, FP64
+// summation and alpha/beta epilogue).
+cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A,
+                              size_t lda, const double* B, size_t ldb, double beta, double* C,
+                              size_t ldc, int slices, cudaStream_t st, CUresult* cu_err);
 
 }  // namespace rb

@@ -37,4 +37,19 @@ CUresult make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dt
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
+CUresult make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
+                      uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
+                      uint32_t b0, uint32_t b1, uint32_t b2, bool swizzle128) {
+    std::call_once(g_encode_once, load_encode);
+    if (!g_encode) return CUDA_ERROR_NOT_FOUND;
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {s1 * elem, s2 * elem};
+    cuuint32_t box[3] = {b0, b1, b2};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return g_encode(map, dtype, 3, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
 }  // namespace rb

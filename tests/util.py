@@ -28,6 +28,8 @@ def make_buffer(rng, layout, rows, cols, ld, dtype, dist="uniform"):
 
 
 def sample(rng, shape, dtype, dist="uniform"):
+    if dist == "uniform" and np.dtype(dtype) == np.float32:
+        return (rng.random(shape, dtype=np.float32) * np.float32(2.0) - np.float32(1.0))
     if dist == "uniform":
         x = rng.uniform(-1.0, 1.0, shape)
     elif dist == "normal":
@@ -110,8 +112,7 @@ class Problem:
         diff = (r.astype(np.float64) - hi) - lo
         den = self.denom()
         if rows is not None:  # scale the denominator to the sampled rows
-            A = self.opA().astype(np.float64)
-            an = np.linalg.norm(A[rows])
+            an = np.linalg.norm(self.opA()[rows].astype(np.float64))
             bn = np.linalg.norm(self.B.astype(np.float64))
             cn = np.linalg.norm(self.C0.astype(np.float64)[rows]) if self.beta != 0 else 0.0
             den = abs(self.alpha) * an * bn + abs(self.beta) * cn
