@@ -209,6 +209,20 @@ def config_block(args):
 # our arm
 # --------------------------------------------------------------------------
 
+def kernel_report():
+    """Per-kernel {name: (launches, total_ms, total_work)} since the last call."""
+    import ctypes as C
+
+    from rblas_b200 import _lib
+    buf = C.create_string_buffer(1 << 16)
+    _lib.load().rb_kernel_timing_report(buf, len(buf))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms, work = line.split()
+        out[name] = (int(cnt), float(ms), float(work))
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -224,7 +238,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    rb.load_library()
+    lib = rb.load_library()
     dev = torch.device("cuda", local)
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
@@ -248,34 +262,45 @@ def run_ours(args):
                             b.data_ptr(), k if tb else n, BETA, c.data_ptr(), n, np.float64,
                             prec=prec, stream=sh)
 
-    def timed(prec, steps, warmup):
+    def timed(fn, steps, warmup):
         for _ in range(warmup):
-            dev_step(prec)
+            fn()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         l0 = rb.launch_count()
+        kernel_report()
+        lib.rb_kernel_timing_enable(1)
         e0.record(stream)
         for _ in range(steps):
-            dev_step(prec)
+            fn()
         e1.record(stream)
         torch.cuda.synchronize()
+        lib.rb_kernel_timing_enable(0)
+        kr = kernel_report()
         launches = rb.launch_count() - l0
         ms = e0.elapsed_time(e1)
         if dist:
             t = torch.tensor([ms], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        return ms / steps, launches
+        return ms / steps, launches, kr
+
+    # ---- pipe peaks measured in this run (roofline denominators) ----------
+    peaks = {"fp64_fma_tflops": float(lib.rb_probe_fma_peak_tflops(1, 0)),
+             "fp32_fma_tflops": float(lib.rb_probe_fma_peak_tflops(0, 0)),
+             "int8_tensor_tops": float(lib.rb_probe_tensor_peak_tflops(1, 0)),
+             "bf16_tensor_tflops": float(lib.rb_probe_tensor_peak_tflops(0, 0))}
 
     forms = {}
-    headline = Precision.Plain
+    kreports = {}
+    headline_name = "plain"
+    clocks = None
     candidates = [("plain", Precision.Plain)]
     if args.form in ("auto", "ozaki"):
         candidates.append(("ozaki", Precision.Ozaki))
-    clocks = None
     for name, prec in candidates:
         try:
             dev_step(prec)
@@ -284,39 +309,54 @@ def run_ours(args):
             forms[name] = {"unavailable": str(e)}
             continue
         with ClockSampler(local) as cs:
-            ms, launches = timed(prec, args.steps, args.warmup)
+            ms, launches, kr = timed(lambda: dev_step(prec), args.steps, args.warmup)
         forms[name] = {"tflops": step_flops() * ws / (ms * 1e-3) / 1e12, "ms_per_step": ms,
-                       "gpu_launches": launches}
-        csum = cs.summary()
-        forms[name]["clocks"] = csum
-        if name == "ozaki" or headline == Precision.Plain:
+                       "gpu_launches": launches, "clocks": cs.summary()}
+        kreports[name] = kr
+        if name == "plain" or args.form != "plain":
             headline_name = name
-            headline = prec
-            clocks = csum
-    if args.form == "plain":
-        headline_name = "plain"
+            clocks = forms[name]["clocks"]
     hl = forms[headline_name]
     err_status = rb.device_error()
 
-    # ---- roofline of the dominant kernel: time one 4096^3 N/N launch alone
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    reps = 3
-    e0.record(stream)
-    for _ in range(reps):
-        level3.gemm_dev(Layout.RowMajor, 0, 0, BIG, BIG, BIG, ALPHA, A.data_ptr(), BIG, B.data_ptr(),
-                        BIG, BETA, Cs[0].data_ptr(), BIG, np.float64, prec=headline, stream=sh)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    kernel_ms = e0.elapsed_time(e1) / reps
-    f64_peak = float(_lib.load().rb_probe_fma_peak_tflops(1, 0))
-    achieved = 2.0 * BIG ** 3 / (kernel_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp64" if headline == Precision.Plain else "tensor",
-                "achieved": achieved, "peak": f64_peak, "unit": "TFLOP/s",
-                "frac": achieved / f64_peak if f64_peak > 0 else None, "traffic": None,
-                "kernel": "simt_gemm_kernel<double> (one 4096^3 launch)",
-                "peak_source": "FP64 DFMA throughput measured in-run by rb_probe_fma_peak_tflops "
-                               "(not in MEASURED_PEAKS.json)"}
+    # ---- roofline of the headline form's dominant kernel (live event timing)
+    kr = kreports[headline_name]
+    kname = max(kr, key=lambda n: kr[n][1])
+    cnt, kms, work = kr[kname]
+    achieved = work / (kms * 1e-3) / 1e12
+    if kname.startswith("umma_ozaki"):
+        peak, unit, bound = peaks["int8_tensor_tops"], "TOP/s", "tensor"
+        psrc = "INT8 tcgen05 throughput measured in-run by rb_probe_tensor_peak_tflops (back-to-back M128 N256 K32 UMMAs, smem operands); not in MEASURED_PEAKS.json"
+    else:
+        peak, unit, bound = peaks["fp64_fma_tflops"], "TFLOP/s", "fp64"
+        psrc = "FP64 DFMA throughput measured in-run by rb_probe_fma_peak_tflops; not in MEASURED_PEAKS.json"
+    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                "kernel": kname, "launches": cnt, "avg_launch_ms": kms / cnt,
+                "work_per_launch": work / cnt, "peak_source": psrc,
+                "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in kr.items()}}
+
+    # ---- SGEMM 8192^3 col-major alpha=1 beta=1: plain vs BF16 split forms
+    sgemm = {}
+    if not args.no_sgemm:
+        n8 = 8192
+        gs = torch.Generator(device=dev)
+        gs.manual_seed(77)
+        SA = torch.rand(n8 * n8, dtype=torch.float32, device=dev, generator=gs) * 2 - 1
+        SB = torch.rand(n8 * n8, dtype=torch.float32, device=dev, generator=gs) * 2 - 1
+        SC = torch.rand(n8 * n8, dtype=torch.float32, device=dev, generator=gs) * 2 - 1
+        for name, prec, reps in (("plain", Precision.Plain, 3), ("bf16x3", Precision.Bf16x3, 5),
+                                 ("bf16x6", Precision.Bf16x6, 5)):
+            def one():
+                level3.gemm_dev(Layout.ColMajor, 0, 0, n8, n8, n8, 1.0, SA.data_ptr(), n8, SB.data_ptr(),
+                                n8, 1.0, SC.data_ptr(), n8, np.float32, prec=prec, stream=sh)
+            ms, launches, kr2 = timed(one, reps, 2)
+            sgemm[name] = {"tflops": 2.0 * n8 ** 3 / (ms * 1e-3) / 1e12, "ms": ms,
+                           "kernels": {k: {"launches": v[0], "ms": v[1],
+                                           "pipe_tflops": v[2] / (v[1] * 1e-3) / 1e12}
+                                       for k, v in kr2.items()}}
+        del SA, SB, SC
+        torch.cuda.empty_cache()
 
     # ---- e2e through the public host API (pinned host buffers) -------------
     e2e = None
@@ -328,15 +368,15 @@ def run_ours(args):
         hA, hB = pinned(BIG * BIG, A), pinned(BIG * BIG, B)
         hC = [pinned(BIG * BIG, c) for c in Cs]
         hA2, hB2, hC2 = pinned(m2 * k2, A2), pinned(k2 * n2, B2), pinned(m2 * n2, C2)
-        na = {id(t): t.numpy() for t in [hA, hB, hA2, hB2, hC2] + hC}
+        prec = Precision.Ozaki if headline_name == "ozaki" else Precision.Plain
 
-        def host_step(prec):
+        def host_step():
             h2d = d2h = 0
             for i, (ta, tb, m, n, k) in enumerate(step_gemms()):
                 if m == BIG:
-                    a, b, c = na[id(hA)], na[id(hB)], na[id(hC[i])]
+                    a, b, c = hA.numpy(), hB.numpy(), hC[i].numpy()
                 else:
-                    a, b, c = na[id(hA2)], na[id(hB2)], na[id(hC2)]
+                    a, b, c = hA2.numpy(), hB2.numpy(), hC2.numpy()
                 level3.gemm(Layout.RowMajor, ta, tb, m, n, k, ALPHA, a, m if ta else k, b,
                             k if tb else n, BETA, c, n, prec=prec)
                 h2d += (a.nbytes + b.nbytes + c.nbytes)
@@ -344,14 +384,14 @@ def run_ours(args):
             return h2d, d2h
 
         for _ in range(max(1, args.warmup)):
-            host_step(headline)
+            host_step()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         k_e2e = max(2, args.steps // 2)
         t0 = time.perf_counter()
         for _ in range(k_e2e):
-            h2d, d2h = host_step(headline)
+            h2d, d2h = host_step()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / k_e2e
         if dist:
@@ -360,7 +400,7 @@ def run_ours(args):
             dt = float(t.item())
         e2e = {"value": step_flops() * ws / dt / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": k_e2e,
-               "timing": "host wall clock around synchronous API calls"}
+               "timing": "host wall clock around synchronous host-API calls (pinned buffers)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -375,8 +415,8 @@ def run_ours(args):
             "data": "synthetic (seeded standard normal, generated on device)",
             "form": headline_name, "config": config_block(args), "forms": forms,
             "clocks": clocks, "e2e": e2e, "gpu_launches": hl["gpu_launches"],
-            "roofline": roofline, "cpu_baseline": cpu,
-            "device_error": err_status[0],
+            "roofline": roofline, "cpu_baseline": cpu, "peaks_measured": peaks,
+            "sgemm_8192": sgemm, "device_error": err_status[0],
         }
         print(json.dumps(line))
     if dist:
@@ -399,8 +439,8 @@ def run_kernel_only(args):
     A = torch.randn(m * k, dtype=dt, device="cuda", generator=g)
     B = torch.randn(k * n, dtype=dt, device="cuda", generator=g)
     C = torch.randn(m * n, dtype=dt, device="cuda", generator=g)
-    prec = {"plain": Precision.Plain, "ozaki": Precision.Ozaki, "bf16x3": Precision.Bf16x3}[
-        args.form if args.form != "auto" else "plain"]
+    prec = {"plain": Precision.Plain, "ozaki": Precision.Ozaki, "bf16x3": Precision.Bf16x3,
+            "bf16x6": Precision.Bf16x6}[args.form if args.form != "auto" else "plain"]
     sh = torch.cuda.current_stream().cuda_stream
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -423,7 +463,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["auto", "plain", "ozaki"], default="auto")
+    ap.add_argument("--form", choices=["auto", "plain", "ozaki", "bf16x3", "bf16x6"], default="auto")
+    ap.add_argument("--no-sgemm", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,

@@ -39,10 +39,17 @@ typedef enum { RB_NON_UNIT = 0, RB_UNIT = 1 } rb_diag;
 
 /* Arithmetic form of a call. PLAIN is the drop-in (true FP32 / FP64
  * products). BF16X3 (f32 only): split each operand into bf16 hi+lo and sum
- * hi*hi + hi*lo + lo*hi on the tensor cores with FP32 accumulation. OZAKI
- * (f64 only): INT8 slice emulation with per-row/column power-of-two scaling
- * and exact INT32 slice products; the slice count is rb_set_ozaki_slices(). */
-typedef enum { RB_PREC_PLAIN = 0, RB_PREC_BF16X3 = 1, RB_PREC_OZAKI = 2 } rb_precision;
+ * hi*hi + hi*lo + lo*hi on the tensor cores with FP32 accumulation. BF16X6
+ * (f32 only): three bf16 planes hi/mid/lo and the six products of weight
+ * <= 2. OZAKI (f64 only): INT8 slice emulation with per-row/column
+ * power-of-two scaling and exact INT32 slice products; the slice count is
+ * rb_set_ozaki_slices(). */
+typedef enum {
+    RB_PREC_PLAIN = 0,
+    RB_PREC_BF16X3 = 1,
+    RB_PREC_OZAKI = 2,
+    RB_PREC_BF16X6 = 3
+} rb_precision;
 
 typedef enum {
     RB_OK = 0,
@@ -136,6 +143,15 @@ uint64_t rb_launch_count(void);
  * Synchronises the device. Returns RB_OK when no error was recorded. */
 rb_status rb_device_error(int clear, uint32_t* detail);
 
+/* Per-kernel timing of the main GEMM kernels: while enabled, CUDA events are
+ * recorded on the launching stream around each main kernel launch.
+ * rb_kernel_timing_report synchronises those events, writes one line per
+ * kernel ("<name> <launches> <total_ms> <total_work>\n", work in flop or
+ * integer ops of the kernel's own pipe) into buf, clears the record and
+ * returns the text length (-1 on error). */
+void rb_kernel_timing_enable(int on);
+int rb_kernel_timing_report(char* buf, size_t buf_len);
+
 /* Releases the cached device/pinned staging buffers of the current device. */
 void rb_release_cached_memory(void);
 
@@ -143,6 +159,13 @@ void rb_release_cached_memory(void);
  * else FP32 FFMA; iters <= 0 picks a default). The roofline denominator of
  * the plain forms, which the tensor-core peaks do not cover. -1 on error. */
 double rb_probe_fma_peak_tflops(int is_f64, int iters);
+
+/* Measures the tcgen05 tensor-pipe throughput of back-to-back M=128 N=256
+ * MMAs with shared-memory operands (no loads in the loop): is_i8 selects
+ * kind::i8 (TOP/s) else kind::f16 with bf16 inputs (TFLOP/s). The roofline
+ * denominator of the INT8 Ozaki form, for which no vendor-measured figure is
+ * at hand. -1 on error. */
+double rb_probe_tensor_peak_tflops(int is_i8, int iters);
 
 #ifdef __cplusplus
 }

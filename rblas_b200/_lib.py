@@ -50,6 +50,9 @@ SIGNATURES = {
     "rb_device_error": (_i, [_i, C.POINTER(C.c_uint32)]),
     "rb_release_cached_memory": (None, []),
     "rb_probe_fma_peak_tflops": (C.c_double, [_i, _i]),
+    "rb_probe_tensor_peak_tflops": (C.c_double, [_i, _i]),
+    "rb_kernel_timing_enable": (None, [_i]),
+    "rb_kernel_timing_report": (_i, [C.c_char_p, _sz]),
 }
 
 

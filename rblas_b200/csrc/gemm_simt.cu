@@ -272,7 +272,10 @@ static cudaError_t launch_variant(const CUtensorMap& ta, const CUtensorMap& tb, 
         attr_set = true;
     }
     const int grid = p.tiles_m * p.tiles_n;
+    KernelTimer tm;
+    kernel_timing_begin(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", 2.0 * p.m * p.n * p.k, st, &tm);
     kern<<<grid, kSimtThreads, smem, st>>>(ta, tb, p);
+    kernel_timing_end(&tm, st);
     count_launch();
     return cudaGetLastError();
 }

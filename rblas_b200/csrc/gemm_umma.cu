@@ -42,23 +42,38 @@ namespace rb {
 
 namespace {
 
-constexpr int kUM = 128, kUN = 256;
+constexpr int kUM = 128;
 constexpr int kRowBytes = 128;                  // K bytes per tile row (one swizzle row)
 constexpr int kATile = kUM * kRowBytes;         // 16 KiB
-constexpr int kBTile = kUN * kRowBytes;         // 32 KiB
-constexpr int kUmmaThreads = 192;
-constexpr int kAccCols = 256;
 constexpr int kExpSentinel = -(1 << 30);        // row exponent of an all-zero row
 
-enum { kModeBf16x3 = 0, kModeOzaki = 1 };
+enum { kModeBf16x3 = 0, kModeBf16x6 = 1, kModeOzaki = 2 };
 
+// Per form: tile N, operand planes per stage, ring depth, and the plane
+// products issued per UMMA K step (smallest weights first).
 template <int MODE> struct UCfg;
-template <> struct UCfg<kModeBf16x3> { static constexpr int NA = 2, NB = 2, STAGES = 2; };
-template <> struct UCfg<kModeOzaki> { static constexpr int NA = 1, NB = 1, STAGES = 4; };
+template <> struct UCfg<kModeBf16x3> {
+    static constexpr int UN = 128, NA = 2, NB = 2, STAGES = 3, NPROD = 3, THREADS = 192;
+    // lo*hi, hi*lo, hi*hi
+    __host__ __device__ static constexpr int pa(int q) { return q == 0 ? 1 : 0; }
+    __host__ __device__ static constexpr int pb(int q) { return q == 1 ? 1 : 0; }
+};
+template <> struct UCfg<kModeBf16x6> {
+    static constexpr int UN = 128, NA = 3, NB = 3, STAGES = 2, NPROD = 6, THREADS = 192;
+    // weight 2 (lo*hi, mid*mid, hi*lo), weight 1 (mid*hi, hi*mid), weight 0 (hi*hi)
+    __host__ __device__ static constexpr int pa(int q) { return q == 0 ? 2 : (q == 1 || q == 3) ? 1 : 0; }
+    __host__ __device__ static constexpr int pb(int q) { return q == 2 ? 2 : (q == 1 || q == 4) ? 1 : 0; }
+};
+template <> struct UCfg<kModeOzaki> {
+    static constexpr int UN = 256, NA = 1, NB = 1, STAGES = 4, NPROD = 1, THREADS = 192;
+    __host__ __device__ static constexpr int pa(int) { return 0; }
+    __host__ __device__ static constexpr int pb(int) { return 0; }
+};
 
 template <int MODE>
 constexpr int umma_smem_bytes() {
-    return UCfg<MODE>::STAGES * (UCfg<MODE>::NA * kATile + UCfg<MODE>::NB * kBTile) + 256 + 1024;
+    using C = UCfg<MODE>;
+    return C::STAGES * (C::NA * kATile + C::NB * C::UN * kRowBytes) + 256 + 1024;
 }
 
 struct UParams {
@@ -66,7 +81,7 @@ struct UParams {
     int tiles_m, tiles_n, num_tiles;
     int num_kt;        // 128-byte K tiles over the whole K
     int slices;        // Ozaki
-    int kt_per_chunk;  // Ozaki: K tiles per exact-INT32 chunk
+    int kt_per_chunk;  // K tiles per accumulation unit (Ozaki: exact INT32; bf16: promotion)
     int kchunks;
     int beta_mode;     // 0 beta == 0, 1 beta == 1, 2 general
     float alpha_f, beta_f;
@@ -83,15 +98,40 @@ struct Bar {
     uint32_t tmem_base;
 };
 
+// Work of one tile is a sequence of accumulation units, each a run of
+// (A plane, B plane, K tile) loads feeding one TMEM accumulator:
+//   bf16 forms: unit c = K tiles [c*G, (c+1)*G) with all plane products;
+//     the epilogue promotes each unit's FP32 partial into FP32 registers
+//     (tcgen05's accumulation truncates; short units keep that error small).
+//   Ozaki: unit (chunk, d) = pairs (i, d-i), i = 0..d, over the chunk's K tiles.
 template <int MODE>
-__global__ void __launch_bounds__(kUmmaThreads, 1)
+__device__ __forceinline__ void unit_shape(const UParams& p, int u, int& pairs, int& d, int& kt0,
+                                           int& kt1) {
+    if (MODE == kModeOzaki) {
+        const int chunk = u / p.slices;
+        d = p.slices - 1 - (u % p.slices);
+        pairs = d + 1;
+        kt0 = chunk * p.kt_per_chunk;
+    } else {
+        d = 0;
+        pairs = 1;
+        kt0 = u * p.kt_per_chunk;
+    }
+    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const UParams p) {
-    constexpr int NA = UCfg<MODE>::NA, NB = UCfg<MODE>::NB, ST = UCfg<MODE>::STAGES;
-    constexpr int STAGE_BYTES = NA * kATile + NB * kBTile;
+    using Cfg = UCfg<MODE>;
+    constexpr int UN = Cfg::UN, NA = Cfg::NA, NB = Cfg::NB, ST = Cfg::STAGES;
+    constexpr int BTILE = UN * kRowBytes;
+    constexpr int STAGE_BYTES = NA * kATile + NB * BTILE;
     constexpr int KSTEPS = 4;  // UMMA K steps of 32 bytes per 128-byte tile row
-    constexpr uint32_t IDESC = (MODE == kModeBf16x3) ? umma_idesc(1, 1, kUM, kUN)   // f32 <- bf16
-                                                     : umma_idesc(2, 1, kUM, kUN);  // s32 <- s8
+    constexpr uint32_t IDESC = (MODE == kModeOzaki) ? umma_idesc(2, 1, kUM, UN)   // s32 <- s8
+                                                    : umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
+    constexpr uint32_t TMEM_COLS = 2 * UN;
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -111,7 +151,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
         fence_barrier_init();
     }
     if (warp == 1) {
-        tmem_alloc(&bar->tmem_base, 2 * kAccCols);
+        tmem_alloc(&bar->tmem_base, TMEM_COLS);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -119,8 +159,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
     tc_fence_after();
     const uint32_t tmem_base = bar->tmem_base;
 
-    // units per tile: BF16X3 one; OZAKI kchunks x slices diagonals
-    const int units = (MODE == kModeBf16x3) ? 1 : p.kchunks * p.slices;
+    const int units = p.kchunks * ((MODE == kModeOzaki) ? p.slices : 1);
     bool ok = true;
 
     if (warp == 0 && lane == 0) {
@@ -128,20 +167,14 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
         prefetch_tmap(&tmA);
         prefetch_tmap(&tmB);
         uint32_t it = 0;
-        constexpr int kElems = (MODE == kModeBf16x3) ? 64 : 128;  // elements per 128-byte row
+        constexpr int kElems = (MODE == kModeOzaki) ? 128 : 64;  // elements per 128-byte row
         for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
             int tm, tn;
             raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
-            const int m0 = tm * kUM, n0 = tn * kUN;
+            const int m0 = tm * kUM, n0 = tn * UN;
             for (int u = 0; ok && u < units; ++u) {
-                int pairs = 1, d = 0, kt0 = 0, kt1 = p.num_kt;
-                if (MODE == kModeOzaki) {
-                    const int chunk = u / p.slices;
-                    d = p.slices - 1 - (u % p.slices);
-                    pairs = d + 1;
-                    kt0 = chunk * p.kt_per_chunk;
-                    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                }
+                int pairs, d, kt0, kt1;
+                unit_shape<MODE>(p, u, pairs, d, kt0, kt1);
                 for (int pi = 0; ok && pi < pairs; ++pi) {
                     for (int kt = kt0; kt < kt1; ++kt, ++it) {
                         const int s = it % ST;
@@ -153,14 +186,14 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
                         uint8_t* sb = sa + NA * kATile;
                         mbar_arrive_expect_tx(&bar->full[s], STAGE_BYTES);
                         const int k0 = kt * kElems;
-                        if (MODE == kModeBf16x3) {
-                            tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, 0);
-                            tma_load_3d(sa + kATile, &tmA, &bar->full[s], k0, m0, 1);
-                            tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, 0);
-                            tma_load_3d(sb + kBTile, &tmB, &bar->full[s], k0, n0, 1);
-                        } else {
+                        if (MODE == kModeOzaki) {
                             tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, pi);
                             tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, d - pi);
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < NA; ++q) tma_load_3d(sa + q * kATile, &tmA, &bar->full[s], k0, m0, q);
+#pragma unroll
+                            for (int q = 0; q < NB; ++q) tma_load_3d(sb + q * BTILE, &tmB, &bar->full[s], k0, n0, q);
                         }
                     }
                 }
@@ -175,20 +208,15 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
         uint32_t it = 0, uc = 0;
         for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
             for (int u = 0; ok && u < units; ++u, ++uc) {
-                int pairs = 1, kt0 = 0, kt1 = p.num_kt;
-                if (MODE == kModeOzaki) {
-                    const int chunk = u / p.slices;
-                    pairs = p.slices - (u % p.slices);
-                    kt0 = chunk * p.kt_per_chunk;
-                    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                }
+                int pairs, d, kt0, kt1;
+                unit_shape<MODE>(p, u, pairs, d, kt0, kt1);
                 const uint32_t b = uc & 1;
                 if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, p.err, 0x202)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d_tmem = tmem_base + b * kAccCols;
+                const uint32_t d_tmem = tmem_base + b * UN;
                 uint32_t accumulate = 0;
                 for (int pi = 0; ok && pi < pairs; ++pi) {
                     for (int kt = kt0; kt < kt1; ++kt, ++it) {
@@ -202,19 +230,16 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
                         const uint32_t sb = sa + NA * kATile;
 #pragma unroll
                         for (int kk = 0; kk < KSTEPS; ++kk) {
-                            if (MODE == kModeBf16x3) {
-                                const uint64_t ah = sw128_kmajor_desc(sa) + 2 * kk;
-                                const uint64_t al = sw128_kmajor_desc(sa + kATile) + 2 * kk;
-                                const uint64_t bh = sw128_kmajor_desc(sb) + 2 * kk;
-                                const uint64_t bl = sw128_kmajor_desc(sb + kBTile) + 2 * kk;
-                                // small terms first into the fresh accumulator
-                                umma_f16(d_tmem, al, bh, IDESC, accumulate);
-                                umma_f16(d_tmem, ah, bl, IDESC, 1);
-                                umma_f16(d_tmem, ah, bh, IDESC, 1);
+                            if (MODE == kModeOzaki) {
+                                umma_i8(d_tmem, sw128_kmajor_desc(sa) + 2 * kk, sw128_kmajor_desc(sb) + 2 * kk,
+                                        IDESC, accumulate);
                             } else {
-                                const uint64_t a = sw128_kmajor_desc(sa) + 2 * kk;
-                                const uint64_t bb = sw128_kmajor_desc(sb) + 2 * kk;
-                                umma_i8(d_tmem, a, bb, IDESC, accumulate);
+#pragma unroll
+                                for (int q = 0; q < Cfg::NPROD; ++q) {
+                                    umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
+                                             sw128_kmajor_desc(sb + Cfg::pb(q) * BTILE) + 2 * kk, IDESC,
+                                             (q == 0) ? accumulate : 1u);
+                                }
                             }
                             accumulate = 1;
                         }
@@ -235,43 +260,29 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
         for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
             int tm, tn;
             raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
-            const int m0 = tm * kUM, n0 = tn * kUN;
+            const int m0 = tm * kUM, n0 = tn * UN;
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
-            int er = 0;
-            if (MODE == kModeOzaki && row_ok) er = p.row_exp[r];
-            for (int u = 0; ok && u < units; ++u, ++uc) {
-                const uint32_t b = uc & 1;
-                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * kAccCols;
-                const int d = (MODE == kModeOzaki) ? p.slices - 1 - (u % p.slices) : 0;
-                const bool first_unit = (u == 0);
+            if constexpr (MODE == kModeOzaki) {
+                const int er = row_ok ? p.row_exp[r] : kExpSentinel;
+                for (int u = 0; ok && u < units; ++u, ++uc) {
+                    const uint32_t b = uc & 1;
+                    if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+                    const int d = p.slices - 1 - (u % p.slices);
+                    const bool first_unit = (u == 0);
 #pragma unroll 1
-                for (int ch = 0; ch < kAccCols / 32; ++ch) {
-                    uint32_t v[32];
-                    tmem_ld32(taddr + ch * 32, v);
-                    tmem_ld_wait();
-                    if (!row_ok) continue;
-                    const int cbase = n0 + ch * 32;
-                    if (MODE == kModeBf16x3) {
-                        float* C = static_cast<float*>(p.c);
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = cbase + j;
-                            if (col >= p.n) break;
-                            float* cp = C + r + static_cast<size_t>(col) * p.ldc;
-                            float tb = 0.f;
-                            if (p.beta_mode == 1) tb = *cp;
-                            else if (p.beta_mode == 2) tb = p.beta_f * *cp;
-                            *cp = fmaf(p.alpha_f, __uint_as_float(v[j]), tb);
-                        }
-                    } else {
+                    for (int ch = 0; ch < UN / 32; ++ch) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + ch * 32, v);
+                        tmem_ld_wait();
+                        if (!row_ok || (er == kExpSentinel && !first_unit)) continue;
                         double* C = static_cast<double*>(p.c);
-                        if (er == kExpSentinel && !first_unit) continue;
+                        const int cbase = n0 + ch * 32;
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
                             const int col = cbase + j;
@@ -280,8 +291,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
                             const int fc = __ldg(p.col_exp + col);
                             double term = 0.0;
                             if (er != kExpSentinel && fc != kExpSentinel)
-                                term = scalbn(static_cast<double>(static_cast<int32_t>(v[j])),
-                                              er + fc - 7 * (d + 2));
+                                term = scalbn(static_cast<double>(static_cast<int32_t>(v[j])), er + fc - 7 * (d + 2));
                             double acc;
                             if (first_unit) {
                                 acc = 0.0;
@@ -293,10 +303,47 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
                             *cp = fma(p.alpha_d, term, acc);
                         }
                     }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+            } else {
+                float sum[UN];
+#pragma unroll
+                for (int j = 0; j < UN; ++j) sum[j] = 0.f;
+                for (int u = 0; ok && u < units; ++u, ++uc) {
+                    const uint32_t b = uc & 1;
+                    if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+#pragma unroll
+                    for (int ch = 0; ch < UN / 32; ++ch) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + ch * 32, v);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+                }
+                if (ok && row_ok) {
+                    float* C = static_cast<float*>(p.c);
+#pragma unroll
+                    for (int j = 0; j < UN; ++j) {
+                        const int col = n0 + j;
+                        if (col >= p.n) break;
+                        float* cp = C + r + static_cast<size_t>(col) * p.ldc;
+                        float tb = 0.f;
+                        if (p.beta_mode == 1) tb = *cp;
+                        else if (p.beta_mode == 2) tb = p.beta_f * *cp;
+                        *cp = fmaf(p.alpha_f, sum[j], tb);
+                    }
+                }
             }
         }
     }
@@ -305,7 +352,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, 2 * kAccCols);
+        tmem_dealloc(tmem_base, TMEM_COLS);
     }
 }
 
@@ -328,34 +375,35 @@ __global__ void fill_int_kernel(int* p, int n, int v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
 
-// e[r] = max over p of frexp_exp(x(r,p)) (kExpSentinel if the row is zero).
-// 2-D grid over (rows, K-blocks of 1024); atomicMax merges K-blocks.
-__global__ void row_exp_kernel(const double* __restrict__ x, size_t rs, size_t ps, int R, int K,
-                               int* __restrict__ e) {
-    const int p0 = blockIdx.y * 1024;
-    const int p1 = min(K, p0 + 1024);
-    if (ps == 1) {
-        // K-contiguous: one warp per row
-        const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-        if (r >= R) return;
-        int best = kExpSentinel;
-        for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) {
-            const double v = x[static_cast<size_t>(r) * rs + q];
-            if (v != 0.0) best = max(best, frexp_exp(v));
-        }
-        for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if ((threadIdx.x & 31) == 0 && best != kExpSentinel) atomicMax(e + r, best);
-    } else {
-        // R-contiguous: one thread per row, consecutive threads read consecutive rows
-        const int r = blockIdx.x * blockDim.x + threadIdx.x;
-        if (r >= R) return;
-        int best = kExpSentinel;
-        for (int q = p0; q < p1; ++q) {
-            const double v = x[r + static_cast<size_t>(q) * ps];
-            if (v != 0.0) best = max(best, frexp_exp(v));
-        }
-        if (best != kExpSentinel) atomicMax(e + r, best);
+// e[r] = max over p of frexp_exp(x(r,p)) (kExpSentinel if the row is zero);
+// atomicMax merges the K slabs.
+// K-contiguous view: one warp per row, a 1024-wide K slab per blockIdx.y.
+__global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, int R, int K,
+                                       int* __restrict__ e) {
+    const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (r >= R) return;
+    const int p0 = blockIdx.y * 1024, p1 = min(K, p0 + 1024);
+    int best = kExpSentinel;
+    for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) {
+        const double v = x[static_cast<size_t>(r) * rs + q];
+        if (v != 0.0) best = max(best, frexp_exp(v));
     }
+    for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0 && best != kExpSentinel) atomicMax(e + r, best);
+}
+// R-contiguous view: one thread per row (coalesced across the warp), a
+// 32-wide K slab per blockIdx.y so the grid covers the whole matrix.
+__global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, int R, int K,
+                                       int* __restrict__ e) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    const int p0 = blockIdx.y * 32, p1 = min(K, p0 + 32);
+    int best = kExpSentinel;
+    for (int q = p0; q < p1; ++q) {
+        const double v = x[r + static_cast<size_t>(q) * ps];
+        if (v != 0.0) best = max(best, frexp_exp(v));
+    }
+    if (best != kExpSentinel) atomicMax(e + r, best);
 }
 
 constexpr int kTile = 64;
@@ -406,10 +454,13 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     }
 }
 
-// BF16 split: out[0][r][q] = bf16(x), out[1][r][q] = bf16(x - bf16(x)).
+// BF16 split into `planes` (2 or 3) planes: out[0] = bf16(x),
+// out[1] = bf16(x - out[0]), out[2] = bf16(x - out[0] - out[1]); every
+// difference is exact in FP32.
 __global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict__ x, size_t rs, size_t ps,
-                                                         int R, int K, __nv_bfloat16* __restrict__ out,
-                                                         size_t kp, size_t plane) {
+                                                         int R, int K, int planes,
+                                                         __nv_bfloat16* __restrict__ out, size_t kp,
+                                                         size_t plane) {
     __shared__ float tile[kTile][kTile + 1];
     const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
     load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
@@ -417,16 +468,19 @@ __global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict
     for (int job = threadIdx.x; job < kTile * 8; job += blockDim.x) {
         const int r = job >> 3, c = job & 7;  // 64 rows x 8 chunks of 8
         if (r0 + r >= R || p0 + c * 8 >= static_cast<int>(kp)) continue;
-        __align__(16) __nv_bfloat16 hi[8], lo[8];
+        __align__(16) __nv_bfloat16 h[3][8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const float v = tile[r][c * 8 + i];
-            hi[i] = __float2bfloat16_rn(v);
-            lo[i] = __float2bfloat16_rn(v - __bfloat162float(hi[i]));
+            float v = tile[r][c * 8 + i];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                h[q][i] = __float2bfloat16_rn(v);
+                v = v - __bfloat162float(h[q][i]);
+            }
         }
         const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 8;
-        *reinterpret_cast<uint4*>(out + off) = *reinterpret_cast<const uint4*>(hi);
-        *reinterpret_cast<uint4*>(out + plane + off) = *reinterpret_cast<const uint4*>(lo);
+        for (int q = 0; q < planes; ++q)
+            *reinterpret_cast<uint4*>(out + q * plane + off) = *reinterpret_cast<const uint4*>(h[q]);
     }
 }
 
@@ -450,14 +504,92 @@ cudaError_t launch_umma(const CUtensorMap& ta, const CUtensorMap& tb, const UPar
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = p.num_tiles < sms ? p.num_tiles : sms;
-    kern<<<grid, kUmmaThreads, smem, st>>>(ta, tb, p);
+    const double mnk2 = 2.0 * p.m * p.n * p.k;
+    const double work = (MODE == kModeOzaki) ? mnk2 * p.slices * (p.slices + 1) / 2
+                                             : mnk2 * UCfg<MODE>::NPROD;
+    const char* name = (MODE == kModeOzaki) ? "umma_ozaki_i8" : (MODE == kModeBf16x3 ? "umma_bf16x3" : "umma_bf16x6");
+    KernelTimer tm;
+    kernel_timing_begin(name, work, st, &tm);
+    kern<<<grid, UCfg<MODE>::THREADS, smem, st>>>(ta, tb, p);
+    kernel_timing_end(&tm, st);
     count_launch();
     return cudaGetLastError();
 }
 
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
+// Tensor-pipe throughput probe: one CTA per SM, smem operands filled once
+// with a fixed bit pattern, thread 0 issues `iters` back-to-back MMAs
+// (M=128, N=256, one 32-byte K step) into a TMEM accumulator.
+template <bool I8>
+__global__ void __launch_bounds__(128, 1) umma_peak_kernel(int iters, uint32_t* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t* done = reinterpret_cast<uint64_t*>(smem + kATile + 256 * kRowBytes);
+    uint32_t* tbase = reinterpret_cast<uint32_t*>(done + 1);
+    for (int i = threadIdx.x; i < (kATile + 256 * kRowBytes) / 4; i += blockDim.x)
+        reinterpret_cast<uint32_t*>(smem)[i] = 0x3c003c00u ^ (i * 2654435761u & 0x00ff00ffu);
+    fence_proxy_async_smem();
+    if (threadIdx.x == 0) {
+        mbar_init(done, 1);
+        fence_barrier_init();
+    }
+    if ((threadIdx.x >> 5) == 0) {
+        tmem_alloc(tbase, 256);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tbase;
+    if (threadIdx.x == 0) {
+        const uint32_t sa = smem_u32(smem), sb = sa + kATile;
+        constexpr uint32_t idesc = I8 ? umma_idesc(2, 1, kUM, 256) : umma_idesc(1, 1, kUM, 256);
+        for (int i = 0; i < iters; ++i) {
+            const uint64_t a = sw128_kmajor_desc(sa) + 2 * (i & 3), b = sw128_kmajor_desc(sb) + 2 * (i & 3);
+            if (I8) umma_i8(tmem, a, b, idesc, i > 0);
+            else    umma_f16(tmem, a, b, idesc, i > 0);
+        }
+        tc_commit(done);
+        mbar_wait(done, 0, err, 0x2f0);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 256);
+    }
+}
+
 }  // namespace
+
+double probe_umma_peak(int i8, int iters) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int smem = kATile + 256 * kRowBytes + 64 + 1024;
+    auto k0 = umma_peak_kernel<false>;
+    auto k1 = umma_peak_kernel<true>;
+    auto kern = i8 ? k1 : k0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1.0;
+    uint32_t* err = device_error_word();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    kern<<<sms, 128, smem>>>(iters / 8 + 1, err);  // warm-up
+    cudaEventRecord(e0);
+    kern<<<sms, 128, smem>>>(iters, err);
+    cudaEventRecord(e1);
+    count_launch(2);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
+    const double per_mma = 2.0 * kUM * 256 * (i8 ? 32 : 16);
+    return per_mma * iters * sms / (ms * 1e-3) / 1e12;
+}
 
 // op(A) viewed as m x k: (i,p) at A[i + p*lda] (NoTrans) or A[p + i*lda] (Trans).
 // op(B)^T viewed as n x k: (j,p) at B[p + j*ldb] (NoTrans) or B[j + p*ldb] (Trans).
@@ -467,47 +599,48 @@ static void operand_views(bool ta, bool tb, size_t lda, size_t ldb, size_t& ars,
     if (!tb) { brs = ldb; bps = 1; } else { brs = 1; bps = ldb; }
 }
 
-cudaError_t launch_bf16x3_gemm(bool ta, bool tb, int m, int n, int k, float alpha, const float* A,
-                               size_t lda, const float* B, size_t ldb, float beta, float* C,
-                               size_t ldc, cudaStream_t st, CUresult* cu_err) {
+cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, int k, float alpha,
+                                   const float* A, size_t lda, const float* B, size_t ldb, float beta,
+                                   float* C, size_t ldc, cudaStream_t st, CUresult* cu_err) {
+    constexpr int UN = 128;
     const size_t kp = round_up(static_cast<size_t>(k), 8);  // 16-byte rows of bf16
     const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
-    void* sa = nullptr;
-    void* sb = nullptr;
-    cudaError_t e = cudaMallocAsync(&sa, 2 * pa * sizeof(__nv_bfloat16), st);
+    void* buf = nullptr;
+    const size_t a_bytes = round_up(planes * pa * sizeof(__nv_bfloat16), 256);
+    cudaError_t e = cudaMallocAsync(&buf, a_bytes + planes * pb * sizeof(__nv_bfloat16), st);
     if (e != cudaSuccess) return e;
-    e = cudaMallocAsync(&sb, 2 * pb * sizeof(__nv_bfloat16), st);
-    if (e != cudaSuccess) { cudaFreeAsync(sa, st); return e; }
+    __nv_bfloat16* sa = static_cast<__nv_bfloat16*>(buf);
+    __nv_bfloat16* sb = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(buf) + a_bytes);
     size_t ars, aps, brs, bps;
     operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
     const dim3 ga((k + kTile - 1) / kTile, (m + kTile - 1) / kTile);
     const dim3 gb((k + kTile - 1) / kTile, (n + kTile - 1) / kTile);
-    bf16_split_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, static_cast<__nv_bfloat16*>(sa), kp, pa);
-    bf16_split_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, static_cast<__nv_bfloat16*>(sb), kp, pb);
+    bf16_split_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, planes, sa, kp, pa);
+    bf16_split_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, planes, sb, kp, pb);
     count_launch(2);
     CUtensorMap tma, tmb;
-    CUresult r = make_tmap_planes(&tma, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, m, 2, kp, kUM);
-    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, sb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, n, 2, kp, kUN);
+    CUresult r = make_tmap_planes(&tma, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, m, planes, kp, kUM);
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, sb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, n, planes, kp, UN);
     if (r != CUDA_SUCCESS) {
         if (cu_err) *cu_err = r;
-        cudaFreeAsync(sa, st);
-        cudaFreeAsync(sb, st);
+        cudaFreeAsync(buf, st);
         return cudaErrorInvalidValue;
     }
     UParams p{};
     p.m = m; p.n = n; p.k = k;
     p.tiles_m = (m + kUM - 1) / kUM;
-    p.tiles_n = (n + kUN - 1) / kUN;
+    p.tiles_n = (n + UN - 1) / UN;
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 63) / 64);
-    p.slices = 1; p.kt_per_chunk = p.num_kt; p.kchunks = 1;
+    p.slices = 1;
+    p.kt_per_chunk = 2;  // FP32 promotion every 128 elements of K
+    p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
     p.beta_mode = (beta == 0.f) ? 0 : (beta == 1.f ? 1 : 2);
     p.alpha_f = alpha; p.beta_f = beta;
     p.c = C; p.ldc = ldc;
     p.err = device_error_word();
-    e = launch_umma<kModeBf16x3>(tma, tmb, p, st);
-    cudaFreeAsync(sa, st);
-    cudaFreeAsync(sb, st);
+    e = (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
+    cudaFreeAsync(buf, st);
     return e;
 }
 
@@ -527,11 +660,11 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     size_t ars, aps, brs, bps;
     operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
     fill_int_kernel<<<64, 256, 0, st>>>(ea, m + n, kExpSentinel);
-    const int kb = (k + 1023) / 1024;
-    if (aps == 1) row_exp_kernel<<<dim3((m + 7) / 8, kb), 256, 0, st>>>(A, ars, aps, m, k, ea);
-    else          row_exp_kernel<<<dim3((m + 255) / 256, kb), 256, 0, st>>>(A, ars, aps, m, k, ea);
-    if (bps == 1) row_exp_kernel<<<dim3((n + 7) / 8, kb), 256, 0, st>>>(B, brs, bps, n, k, eb);
-    else          row_exp_kernel<<<dim3((n + 255) / 256, kb), 256, 0, st>>>(B, brs, bps, n, k, eb);
+    const int kb = (k + 1023) / 1024, k32 = (k + 31) / 32;
+    if (aps == 1) row_exp_kcontig_kernel<<<dim3((m + 7) / 8, kb), 256, 0, st>>>(A, ars, m, k, ea);
+    else          row_exp_rcontig_kernel<<<dim3((m + 255) / 256, k32), 256, 0, st>>>(A, aps, m, k, ea);
+    if (bps == 1) row_exp_kcontig_kernel<<<dim3((n + 7) / 8, kb), 256, 0, st>>>(B, brs, n, k, eb);
+    else          row_exp_rcontig_kernel<<<dim3((n + 255) / 256, k32), 256, 0, st>>>(B, bps, n, k, eb);
     const dim3 ga((kp + kTile - 1) / kTile, (m + kTile - 1) / kTile);
     const dim3 gb((kp + kTile - 1) / kTile, (n + kTile - 1) / kTile);
     ozaki_slice_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, ea, slices, sla, kp, pa);
@@ -539,7 +672,8 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     count_launch(5);
     CUtensorMap tma, tmb;
     CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, m, slices, kp, kUM);
-    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, kUN);
+    constexpr int UN = UCfg<kModeOzaki>::UN;
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, UN);
     if (r != CUDA_SUCCESS) {
         if (cu_err) *cu_err = r;
         cudaFreeAsync(buf, st);
@@ -548,7 +682,7 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     UParams p{};
     p.m = m; p.n = n; p.k = k;
     p.tiles_m = (m + kUM - 1) / kUM;
-    p.tiles_n = (n + kUN - 1) / kUN;
+    p.tiles_n = (n + UN - 1) / UN;
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 127) / 128);
     p.slices = slices;

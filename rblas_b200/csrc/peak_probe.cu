@@ -55,6 +55,11 @@ static double probe(int iters) {
 
 }  // namespace rb
 
+extern "C" double rb_probe_tensor_peak_tflops(int is_i8, int iters) {
+    if (iters <= 0) iters = 65536;
+    return rb::probe_umma_peak(is_i8, iters);
+}
+
 extern "C" double rb_probe_fma_peak_tflops(int is_f64, int iters) {
     if (iters <= 0) iters = 4096;
     return is_f64 ? rb::probe<double>(iters) : rb::probe<float>(iters);

@@ -13,7 +13,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/rblas_b200.h"
@@ -22,6 +24,38 @@
 namespace rb {
 
 std::atomic<uint64_t> g_launches{0};
+
+// ---- kernel timing registry ---------------------------------------------------
+namespace {
+struct TimedLaunch {
+    std::string name;
+    double work;
+    cudaEvent_t e0, e1;
+};
+std::mutex g_timing_mu;
+std::atomic<bool> g_timing_on{false};
+std::vector<TimedLaunch*> g_timed;
+}  // namespace
+
+bool kernel_timing_on() { return g_timing_on.load(std::memory_order_relaxed); }
+
+void kernel_timing_begin(const char* name, double work, cudaStream_t st, KernelTimer* t) {
+    t->slot = nullptr;
+    if (!kernel_timing_on()) return;
+    TimedLaunch* L = new TimedLaunch{name, work, nullptr, nullptr};
+    cudaEventCreate(&L->e0);
+    cudaEventCreate(&L->e1);
+    cudaEventRecord(L->e0, st);
+    t->slot = L;
+}
+
+void kernel_timing_end(KernelTimer* t, cudaStream_t st) {
+    if (!t->slot) return;
+    TimedLaunch* L = static_cast<TimedLaunch*>(t->slot);
+    cudaEventRecord(L->e1, st);
+    std::lock_guard<std::mutex> lk(g_timing_mu);
+    g_timed.push_back(L);
+}
 static std::atomic<int> g_ozaki_slices{8};
 static int ozaki_slices() { return g_ozaki_slices.load(); }
 
@@ -122,6 +156,7 @@ rb_status check_matrix(rb_layout layout, char which, size_t rows, size_t cols, s
 
 bool valid_layout(int v) { return v == RB_ROW_MAJOR || v == RB_COL_MAJOR; }
 bool valid_trans(int v) { return v >= RB_NO_TRANS && v <= RB_CONJ_TRANS; }
+bool valid_prec(int v) { return v >= RB_PREC_PLAIN && v <= RB_PREC_BF16X6; }
 
 // A GEMM problem after row-major normalisation (src/level3.rs:52-60):
 // column-major, C is m x n; op(A) m x k; op(B) k x n.
@@ -163,12 +198,12 @@ rb_status run_precision_form(const ColProblem<T>& p, rb_precision prec, cudaStre
     cudaError_t e;
     CUresult cu = CUDA_SUCCESS;
     if constexpr (sizeof(T) == 4) {
-        if (prec != RB_PREC_BF16X3) {
+        if (prec != RB_PREC_BF16X3 && prec != RB_PREC_BF16X6) {
             set_err(err, RB_ERR_UNSUPPORTED);
             return RB_ERR_UNSUPPORTED;
         }
-        e = launch_bf16x3_gemm(p.ta, p.tb, (int)p.m, (int)p.n, (int)p.k, p.alpha, p.a, p.lda, p.b, p.ldb,
-                               p.beta, p.c, p.ldc, st, &cu);
+        e = launch_bf16_split_gemm(prec == RB_PREC_BF16X3 ? 2 : 3, p.ta, p.tb, (int)p.m, (int)p.n, (int)p.k,
+                                   p.alpha, p.a, p.lda, p.b, p.ldb, p.beta, p.c, p.ldc, st, &cu);
     } else {
         if (prec != RB_PREC_OZAKI) {
             set_err(err, RB_ERR_UNSUPPORTED);
@@ -265,7 +300,7 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
                     rb_error* err) {
     set_err(err, RB_OK);
     if (!valid_layout(layout) || !valid_trans(transa) || !valid_trans(transb) ||
-        (prec != RB_PREC_PLAIN && prec != RB_PREC_BF16X3 && prec != RB_PREC_OZAKI)) {
+        !valid_prec(prec)) {
         set_err(err, RB_ERR_INVALID_ARG);
         return RB_ERR_INVALID_ARG;
     }
@@ -341,7 +376,7 @@ rb_status dev_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, s
                    size_t ldc, rb_precision prec, void* stream, rb_error* err) {
     set_err(err, RB_OK);
     if (!valid_layout(layout) || !valid_trans(transa) || !valid_trans(transb) ||
-        (prec != RB_PREC_PLAIN && prec != RB_PREC_BF16X3 && prec != RB_PREC_OZAKI)) {
+        !valid_prec(prec)) {
         set_err(err, RB_ERR_INVALID_ARG);
         return RB_ERR_INVALID_ARG;
     }
@@ -459,6 +494,44 @@ rb_status rb_device_error(int clear, uint32_t* detail) {
     if (clear && w) cudaMemset(c->err_word, 0, sizeof(uint32_t));
     if (w == 0) return RB_OK;
     return ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
+}
+
+void rb_kernel_timing_enable(int on) { g_timing_on.store(on != 0); }
+
+int rb_kernel_timing_report(char* buf, size_t buf_len) {
+    std::vector<TimedLaunch*> items;
+    {
+        std::lock_guard<std::mutex> lk(g_timing_mu);
+        items.swap(g_timed);
+    }
+    std::map<std::string, std::pair<uint64_t, std::pair<double, double>>> agg;
+    int status = 0;
+    for (TimedLaunch* L : items) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(L->e1) != cudaSuccess || cudaEventElapsedTime(&ms, L->e0, L->e1) != cudaSuccess)
+            status = -1;
+        auto& a = agg[L->name];
+        a.first += 1;
+        a.second.first += ms;
+        a.second.second += L->work;
+        cudaEventDestroy(L->e0);
+        cudaEventDestroy(L->e1);
+        delete L;
+    }
+    std::string out;
+    for (auto& kv : agg) {
+        char line[256];
+        snprintf(line, sizeof line, "%s %llu %.6f %.6e\n", kv.first.c_str(),
+                 static_cast<unsigned long long>(kv.second.first), kv.second.second.first,
+                 kv.second.second.second);
+        out += line;
+    }
+    if (buf && buf_len) {
+        const size_t n = std::min(buf_len - 1, out.size());
+        memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    return status == 0 ? static_cast<int>(out.size()) : -1;
 }
 
 void rb_release_cached_memory(void) {

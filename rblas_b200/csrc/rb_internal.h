@@ -38,6 +38,15 @@ CUresult make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dt
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Optional per-kernel timing of the main GEMM kernels (CUDA events recorded
+// on the launching stream around each launch; off unless enabled).
+struct KernelTimer {
+    void* slot = nullptr;  // opaque
+};
+bool kernel_timing_on();
+void kernel_timing_begin(const char* name, double work, cudaStream_t st, KernelTimer* t);
+void kernel_timing_end(KernelTimer* t, cudaStream_t st);
+
 // Per-device error word (device memory, zero when healthy).
 uint32_t* device_error_word();
 
@@ -57,17 +66,22 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
 template <typename T>
 cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st);
 
-// 3xBF16 split SGEMM on tcgen05 (kind::f16, FP32 accumulation in TMEM).
-// Operands may have any alignment (a pre-pass rewrites them into bf16 hi/lo
-// planes in stream-ordered scratch).
-cudaError_t launch_bf16x3_gemm(bool ta, bool tb, int m, int n, int k, float alpha, const float* A,
-                               size_t lda, const float* B, size_t ldb, float beta, float* C,
-                               size_t ldc, cudaStream_t st, CUresult* cu_err);
+// BF16-split SGEMM on tcgen05 (kind::f16): planes == 2 is 3xBF16
+// (hi*hi + hi*lo + lo*hi), planes == 3 is the 6-product form over hi/mid/lo.
+// Operands may have any alignment (a pre-pass rewrites them into bf16 planes
+// in stream-ordered scratch).
+cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, int k, float alpha,
+                                   const float* A, size_t lda, const float* B, size_t ldb, float beta,
+                                   float* C, size_t ldc, cudaStream_t st, CUresult* cu_err);
 
 // Ozaki INT8-slice DGEMM on tcgen05 (kind::i8, exact INT32 in TMEM, FP64
 // summation and alpha/beta epilogue).
 cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A,
                               size_t lda, const double* B, size_t ldb, double beta, double* C,
                               size_t ldc, int slices, cudaStream_t st, CUresult* cu_err);
+
+// Tensor-pipe throughput (TFLOP/s or TOP/s) of back-to-back M128 N256 UMMAs
+// on every SM: i8 != 0 -> kind::i8, else kind::f16 (bf16).
+double probe_umma_peak(int i8, int iters);
 
 }  // namespace rb

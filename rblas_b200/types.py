@@ -48,3 +48,4 @@ class Precision(IntEnum):
     Plain = 0
     Bf16x3 = 1
     Ozaki = 2
+    Bf16x6 = 3

@@ -8,6 +8,8 @@ Tolerances (stated here, used below):
   * BF16X3 normwise error vs the double-double oracle <= 2^-15 (three bf16
     products keep ~16 significand bits per product; the dropped lo*lo term
     and split residuals are ~2^-17 relative).
+  * BF16X6 (three planes, six products) normwise error <= 4*k*u_f32, the
+    plain SGEMM parity bound.
 """
 from __future__ import annotations
 
@@ -65,6 +67,19 @@ def test_bf16x3_accuracy_all_transposes(layout, ta, tb):
     assert rb.device_error()[0] == 0
 
 
+@pytest.mark.parametrize("layout", [Layout.ColMajor, Layout.RowMajor])
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("tb", [0, 1])
+def test_bf16x6_accuracy_all_transposes(layout, ta, tb):
+    for i, (m, n, k) in enumerate(SHAPES):
+        p = Problem(layout, ta, tb, m, n, k, np.float32, alpha=1.0, beta=1.0, seed=400 + i)
+        c = run(p, Precision.Bf16x6)
+        err = p.normwise_vs_dd(c)
+        assert err <= p.tol(), f"{(m, n, k)} bf16x6 {err:.3e}"
+        assert err <= p.normwise_vs_dd(run(p, Precision.Bf16x3)) + 1e-12
+    assert rb.device_error()[0] == 0
+
+
 def test_ozaki_wide_exponent_stress():
     """Entries sign*2^e, e ~ U{-30..30}: per-row scaling still meets the bound."""
     for ta, tb in [(0, 0), (1, 1)]:
@@ -99,7 +114,8 @@ def test_ozaki_zero_rows_and_columns():
     assert np.array_equal(R[:, 7], 0.5 * p.C0[:, 7])
 
 
-@pytest.mark.parametrize("prec,dtype", [(Precision.Ozaki, np.float64), (Precision.Bf16x3, np.float32)])
+@pytest.mark.parametrize("prec,dtype", [(Precision.Ozaki, np.float64), (Precision.Bf16x3, np.float32),
+                                        (Precision.Bf16x6, np.float32)])
 def test_beta_zero_nan_c_and_alpha_zero(prec, dtype):
     p = Problem(Layout.ColMajor, 0, 1, 40, 33, 50, dtype, alpha=1.0, beta=0.0, seed=24, c0_nan=True)
     c = run(p, prec)
@@ -161,8 +177,10 @@ def test_config_sizes_error_report():
             rows = np.sort(rng.choice(m, 32, replace=False))
             e_pl = p.normwise_vs_dd(run(p, Precision.Plain), rows=rows)
             e_b3 = p.normwise_vs_dd(run(p, Precision.Bf16x3), rows=rows)
-            report[f"sgemm_{m}x{n}x{k}_{dist}"] = {"plain": e_pl, "bf16x3": e_b3,
-                                                  "ratio": e_b3 / e_pl if e_pl else None}
+            e_b6 = p.normwise_vs_dd(run(p, Precision.Bf16x6), rows=rows)
+            report[f"sgemm_{m}x{n}x{k}_{dist}"] = {"plain": e_pl, "bf16x3": e_b3, "bf16x6": e_b6,
+                                                  "ratio_x3": e_b3 / e_pl if e_pl else None,
+                                                  "ratio_x6": e_b6 / e_pl if e_pl else None}
     path = _report_path()
     if path:
         with open(path, "w") as f:
