@@ -128,10 +128,104 @@ rb_status rb_dgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose trans
                        rb_precision prec, void* stream, rb_error* err);
 
 /* ---------------------------------------------------------------------------
+ * Complex GEMM (col-major, interleaved {re, im}): C := alpha*op(A)*op(B) + beta*C
+ * op = NoTrans / Trans / ConjTrans per operand.
+ * ------------------------------------------------------------------------- */
+
+/* Drop-in for complex3::gemm (src/complex3.rs:27-74; C32 = rb_complex32,
+ * C64 = rb_complex64). rblas splits into planes and runs four real GEMMs
+ * (4M); here the four products share one real GEMM over block operands
+ * (same 8mnk flops) and a complex alpha/beta epilogue with rblas's complex
+ * multiply. prec: PLAIN, or BF16X3/BF16X6 (C32), OZAKI (C64). The slice
+ * lengths are validated like check_matrix (col-major). */
+rb_status rb_cgemm(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                   rb_complex32 alpha, const rb_complex32* a, size_t lda, size_t a_len,
+                   const rb_complex32* b, size_t ldb, size_t b_len, rb_complex32 beta,
+                   rb_complex32* c, size_t ldc, size_t c_len, rb_precision prec, rb_error* err);
+rb_status rb_zgemm(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                   rb_complex64 alpha, const rb_complex64* a, size_t lda, size_t a_len,
+                   const rb_complex64* b, size_t ldb, size_t b_len, rb_complex64 beta,
+                   rb_complex64* c, size_t ldc, size_t c_len, rb_precision prec, rb_error* err);
+/* Device-pointer twins (enqueue on `stream`, no synchronisation). */
+rb_status rb_cgemm_dev(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                       rb_complex32 alpha, const rb_complex32* a, size_t lda, const rb_complex32* b,
+                       size_t ldb, rb_complex32 beta, rb_complex32* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err);
+rb_status rb_zgemm_dev(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                       rb_complex64 alpha, const rb_complex64* a, size_t lda, const rb_complex64* b,
+                       size_t ldb, rb_complex64 beta, rb_complex64* c, size_t ldc,
+                       rb_precision prec, void* stream, rb_error* err);
+
+/* ---------------------------------------------------------------------------
+ * syrk / symm / hemm / trsm (col-major), routed through the GEMM kernels
+ * ------------------------------------------------------------------------- */
+
+/* level3::syrk (src/level3.rs:236-294): C := alpha*op(A)*op(A)^T + beta*C on
+ * the uplo triangle of the n x n C only; op(A) is n x k. */
+rb_status rb_ssyrk(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, float alpha,
+                   const float* a, size_t lda, size_t a_len, float beta, float* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+rb_status rb_dsyrk(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, double alpha,
+                   const double* a, size_t lda, size_t a_len, double beta, double* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+
+/* level3::symm (src/level3.rs:301-354): A symmetric, uplo triangle stored;
+ * C := alpha*A*B + beta*C (Left) or alpha*B*A + beta*C (Right). */
+rb_status rb_ssymm(rb_side side, rb_uplo uplo, size_t m, size_t n, float alpha, const float* a,
+                   size_t lda, size_t a_len, const float* b, size_t ldb, size_t b_len, float beta,
+                   float* c, size_t ldc, size_t c_len, rb_error* err);
+rb_status rb_dsymm(rb_side side, rb_uplo uplo, size_t m, size_t n, double alpha, const double* a,
+                   size_t lda, size_t a_len, const double* b, size_t ldb, size_t b_len, double beta,
+                   double* c, size_t ldc, size_t c_len, rb_error* err);
+/* complex3::symm (src/complex3.rs:130-145): complex symmetric A = A^T. */
+rb_status rb_csymm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex32 alpha,
+                   const rb_complex32* a, size_t lda, size_t a_len, const rb_complex32* b,
+                   size_t ldb, size_t b_len, rb_complex32 beta, rb_complex32* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+rb_status rb_zsymm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex64 alpha,
+                   const rb_complex64* a, size_t lda, size_t a_len, const rb_complex64* b,
+                   size_t ldb, size_t b_len, rb_complex64 beta, rb_complex64* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+/* complex3::hemm (src/complex3.rs:151-166): Hermitian A = A^H (mirrored half
+ * conjugated, diagonal imaginary part taken as zero). */
+rb_status rb_chemm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex32 alpha,
+                   const rb_complex32* a, size_t lda, size_t a_len, const rb_complex32* b,
+                   size_t ldb, size_t b_len, rb_complex32 beta, rb_complex32* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+rb_status rb_zhemm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex64 alpha,
+                   const rb_complex64* a, size_t lda, size_t a_len, const rb_complex64* b,
+                   size_t ldb, size_t b_len, rb_complex64 beta, rb_complex64* c, size_t ldc,
+                   size_t c_len, rb_error* err);
+
+/* level3::trsm (src/level3.rs:390-437) and complex3::trsm
+ * (src/complex3.rs:252-340): op(A)*X = alpha*B (Left) or X*op(A) = alpha*B
+ * (Right), B overwritten by X. Blocked: diagonal blocks by substitution,
+ * off-diagonal updates as GEMMs. */
+rb_status rb_strsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                   size_t n, float alpha, const float* a, size_t lda, size_t a_len, float* b,
+                   size_t ldb, size_t b_len, rb_error* err);
+rb_status rb_dtrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                   size_t n, double alpha, const double* a, size_t lda, size_t a_len, double* b,
+                   size_t ldb, size_t b_len, rb_error* err);
+rb_status rb_ctrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                   size_t n, rb_complex32 alpha, const rb_complex32* a, size_t lda, size_t a_len,
+                   rb_complex32* b, size_t ldb, size_t b_len, rb_error* err);
+rb_status rb_ztrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                   size_t n, rb_complex64 alpha, const rb_complex64* a, size_t lda, size_t a_len,
+                   rb_complex64* b, size_t ldb, size_t b_len, rb_error* err);
+/* Device-pointer f64 trsm (enqueue on `stream`). */
+rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                       size_t n, double alpha, const double* a, size_t lda, double* b, size_t ldb,
+                       void* stream, rb_error* err);
+
+/* ---------------------------------------------------------------------------
  * Library state
  * ------------------------------------------------------------------------- */
 
-/* Number of slices used by RB_PREC_OZAKI (3..12; default 8). */
+/* Number of slices used by RB_PREC_OZAKI (2..12; default 7). Slice 0 is a
+ * signed 8-bit digit (7 bits), the rest unsigned 8-bit digits, so s slices
+ * carry 7 + 8(s-1) bits of each scaled row/column entry; s(s+1)/2 INT8
+ * GEMMs are run. */
 rb_status rb_set_ozaki_slices(int slices);
 int rb_get_ozaki_slices(void);
 

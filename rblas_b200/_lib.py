@@ -44,6 +44,23 @@ SIGNATURES = {
     "rb_dgemm_prec": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _i, _perr]),
     "rb_sgemm_dev": (_i, [_i, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz, _i, _vp, _perr]),
     "rb_dgemm_dev": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _i, _vp, _perr]),
+    "rb_cgemm": (_i, [_i, _i, _sz, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex32, _vp, _sz, _sz, _i, _perr]),
+    "rb_zgemm": (_i, [_i, _i, _sz, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex64, _vp, _sz, _sz, _i, _perr]),
+    "rb_cgemm_dev": (_i, [_i, _i, _sz, _sz, _sz, RbComplex32, _vp, _sz, _vp, _sz, RbComplex32, _vp, _sz, _i, _vp, _perr]),
+    "rb_zgemm_dev": (_i, [_i, _i, _sz, _sz, _sz, RbComplex64, _vp, _sz, _vp, _sz, RbComplex64, _vp, _sz, _i, _vp, _perr]),
+    "rb_ssyrk": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _sz, _f, _vp, _sz, _sz, _perr]),
+    "rb_dsyrk": (_i, [_i, _i, _sz, _sz, _d, _vp, _sz, _sz, _d, _vp, _sz, _sz, _perr]),
+    "rb_ssymm": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _f, _vp, _sz, _sz, _perr]),
+    "rb_dsymm": (_i, [_i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _perr]),
+    "rb_csymm": (_i, [_i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex32, _vp, _sz, _sz, _perr]),
+    "rb_zsymm": (_i, [_i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex64, _vp, _sz, _sz, _perr]),
+    "rb_chemm": (_i, [_i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex32, _vp, _sz, _sz, _perr]),
+    "rb_zhemm": (_i, [_i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex64, _vp, _sz, _sz, _perr]),
+    "rb_strsm": (_i, [_i, _i, _i, _i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_dtrsm": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_ctrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_dtrsm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
     "rb_set_ozaki_slices": (_i, [_i]),
     "rb_get_ozaki_slices": (_i, []),
     "rb_launch_count": (C.c_uint64, []),

@@ -39,6 +39,7 @@ struct SimtParams {
     int tiles_m, tiles_n;
     T alpha, beta;
     int beta_mode;  // 0: beta == 0 (C not read), 1: beta == 1, 2: general
+    int tri;        // 0 full C; 1 upper triangle only (row <= col); 2 lower (row >= col)
     T* c;
     size_t ldc;
     uint32_t* err;
@@ -90,6 +91,8 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     raster_tile(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
     const int m0 = tm * BM, n0 = tn * BN;
     const int num_kt = (p.k + BK - 1) / BK;
+    // syrk: tiles wholly outside the referenced triangle do nothing
+    if ((p.tri == 1 && m0 > n0 + BN - 1) || (p.tri == 2 && m0 + BM - 1 < n0)) return;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
@@ -224,6 +227,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
             const int cidx = n0 + (B_K ? (wn0 + lane_n * TN + j)
                                        : (wn0 + (j / VEC) * 4 * VEC + lane_n * VEC + (j % VEC)));
             if (cidx >= p.n) continue;
+            if ((p.tri == 1 && r > cidx) || (p.tri == 2 && r < cidx)) continue;
             T* cp = p.c + r + static_cast<size_t>(cidx) * p.ldc;
             T t = T(0);
             if (p.beta_mode == 1) t = *cp;
@@ -234,23 +238,24 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
 }
 
 template <typename T>
-__global__ void scale_c_kernel(int m, int n, T beta, T* c, size_t ldc) {
+__global__ void scale_c_kernel(int m, int n, T beta, T* c, size_t ldc, int tri) {
     const size_t total = static_cast<size_t>(m) * n;
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const size_t j = idx / m, i = idx - j * m;
+        if ((tri == 1 && i > j) || (tri == 2 && i < j)) continue;
         T* cp = c + i + j * ldc;
         *cp = (beta == T(0)) ? T(0) : beta * *cp;
     }
 }
 
 template <typename T>
-cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st) {
+cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st, int tri) {
     if (beta == T(1) || m == 0 || n == 0) return cudaSuccess;
     const size_t total = static_cast<size_t>(m) * n;
     int blocks = static_cast<int>((total + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    scale_c_kernel<T><<<blocks, 256, 0, st>>>(m, n, beta, C, ldc);
+    scale_c_kernel<T><<<blocks, 256, 0, st>>>(m, n, beta, C, ldc, tri);
     count_launch();
     return cudaGetLastError();
 }
@@ -283,7 +288,7 @@ static cudaError_t launch_variant(const CUtensorMap& ta, const CUtensorMap& tb, 
 template <typename T>
 cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
                              const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
-                             size_t ldc, cudaStream_t st, CUresult* cu_err) {
+                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri) {
     using Cfg = SimtCfg<T>;
     CUtensorMap ta, tb;
     CUresult r;
@@ -306,6 +311,7 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
     p.tiles_n = (n + Cfg::BN - 1) / Cfg::BN;
     p.alpha = alpha; p.beta = beta;
     p.beta_mode = (beta == T(0)) ? 0 : (beta == T(1) ? 1 : 2);
+    p.tri = tri;
     p.c = C; p.ldc = ldc;
     p.err = device_error_word();
     if (!p.err) return cudaErrorMemoryAllocation;
@@ -319,11 +325,11 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
 
 template cudaError_t launch_simt_gemm<float>(bool, bool, int, int, int, float, const float*, size_t,
                                              const float*, size_t, float, float*, size_t, cudaStream_t,
-                                             CUresult*);
+                                             CUresult*, int);
 template cudaError_t launch_simt_gemm<double>(bool, bool, int, int, int, double, const double*, size_t,
                                               const double*, size_t, double, double*, size_t,
-                                              cudaStream_t, CUresult*);
-template cudaError_t launch_scale_c<float>(int, int, float, float*, size_t, cudaStream_t);
-template cudaError_t launch_scale_c<double>(int, int, double, double*, size_t, cudaStream_t);
+                                              cudaStream_t, CUresult*, int);
+template cudaError_t launch_scale_c<float>(int, int, float, float*, size_t, cudaStream_t, int);
+template cudaError_t launch_scale_c<double>(int, int, double, double*, size_t, cudaStream_t, int);
 
 }  // namespace rb

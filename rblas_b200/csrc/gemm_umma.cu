@@ -47,9 +47,9 @@ constexpr int kRowBytes = 128;                  // K bytes per tile row (one swi
 constexpr int kATile = kUM * kRowBytes;         // 16 KiB
 constexpr int kExpSentinel = -(1 << 30);        // row exponent of an all-zero row
 
-enum { kModeBf16x3 = 0, kModeBf16x6 = 1, kModeOzaki = 2 };
+enum { kModeBf16x3 = 0, kModeBf16x6 = 1 };
 
-// Per form: tile N, operand planes per stage, ring depth, and the plane
+// Per BF16 form: tile N, operand planes per stage, ring depth, and the plane
 // products issued per UMMA K step (smallest weights first).
 template <int MODE> struct UCfg;
 template <> struct UCfg<kModeBf16x3> {
@@ -64,11 +64,6 @@ template <> struct UCfg<kModeBf16x6> {
     __host__ __device__ static constexpr int pa(int q) { return q == 0 ? 2 : (q == 1 || q == 3) ? 1 : 0; }
     __host__ __device__ static constexpr int pb(int q) { return q == 2 ? 2 : (q == 1 || q == 4) ? 1 : 0; }
 };
-template <> struct UCfg<kModeOzaki> {
-    static constexpr int UN = 256, NA = 1, NB = 1, STAGES = 4, NPROD = 1, THREADS = 192;
-    __host__ __device__ static constexpr int pa(int) { return 0; }
-    __host__ __device__ static constexpr int pb(int) { return 0; }
-};
 
 template <int MODE>
 constexpr int umma_smem_bytes() {
@@ -80,16 +75,12 @@ struct UParams {
     int m, n, k;
     int tiles_m, tiles_n, num_tiles;
     int num_kt;        // 128-byte K tiles over the whole K
-    int slices;        // Ozaki
-    int kt_per_chunk;  // K tiles per accumulation unit (Ozaki: exact INT32; bf16: promotion)
+    int kt_per_chunk;  // K tiles per accumulation unit (FP32 promotion interval)
     int kchunks;
     int beta_mode;     // 0 beta == 0, 1 beta == 1, 2 general
     float alpha_f, beta_f;
-    double alpha_d, beta_d;
-    void* c;
+    float* c;
     size_t ldc;
-    const int* row_exp;
-    const int* col_exp;
     uint32_t* err;
 };
 
@@ -98,28 +89,10 @@ struct Bar {
     uint32_t tmem_base;
 };
 
-// Work of one tile is a sequence of accumulation units, each a run of
-// (A plane, B plane, K tile) loads feeding one TMEM accumulator:
-//   bf16 forms: unit c = K tiles [c*G, (c+1)*G) with all plane products;
-//     the epilogue promotes each unit's FP32 partial into FP32 registers
-//     (tcgen05's accumulation truncates; short units keep that error small).
-//   Ozaki: unit (chunk, d) = pairs (i, d-i), i = 0..d, over the chunk's K tiles.
-template <int MODE>
-__device__ __forceinline__ void unit_shape(const UParams& p, int u, int& pairs, int& d, int& kt0,
-                                           int& kt1) {
-    if (MODE == kModeOzaki) {
-        const int chunk = u / p.slices;
-        d = p.slices - 1 - (u % p.slices);
-        pairs = d + 1;
-        kt0 = chunk * p.kt_per_chunk;
-    } else {
-        d = 0;
-        pairs = 1;
-        kt0 = u * p.kt_per_chunk;
-    }
-    kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-}
-
+// Work of one tile is a sequence of accumulation units: unit c covers K
+// tiles [c*G, (c+1)*G) with all plane products, and the epilogue promotes
+// each unit's FP32 partial into FP32 registers (tcgen05's accumulation
+// truncates; short units keep that error small).
 template <int MODE>
 __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -129,8 +102,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     constexpr int BTILE = UN * kRowBytes;
     constexpr int STAGE_BYTES = NA * kATile + NB * BTILE;
     constexpr int KSTEPS = 4;  // UMMA K steps of 32 bytes per 128-byte tile row
-    constexpr uint32_t IDESC = (MODE == kModeOzaki) ? umma_idesc(2, 1, kUM, UN)   // s32 <- s8
-                                                    : umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
+    constexpr uint32_t IDESC = umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
     constexpr uint32_t TMEM_COLS = 2 * UN;
 
     extern __shared__ uint8_t smem_raw[];
@@ -158,8 +130,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = bar->tmem_base;
-
-    const int units = p.kchunks * ((MODE == kModeOzaki) ? p.slices : 1);
+    const int units = p.kchunks;
     bool ok = true;
 
     if (warp == 0 && lane == 0) {
@@ -167,36 +138,24 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
         prefetch_tmap(&tmA);
         prefetch_tmap(&tmB);
         uint32_t it = 0;
-        constexpr int kElems = (MODE == kModeOzaki) ? 128 : 64;  // elements per 128-byte row
         for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
             int tm, tn;
             raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
-            for (int u = 0; ok && u < units; ++u) {
-                int pairs, d, kt0, kt1;
-                unit_shape<MODE>(p, u, pairs, d, kt0, kt1);
-                for (int pi = 0; ok && pi < pairs; ++pi) {
-                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
-                        const int s = it % ST;
-                        if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x201)) {
-                            ok = false;
-                            break;
-                        }
-                        uint8_t* sa = smem + s * STAGE_BYTES;
-                        uint8_t* sb = sa + NA * kATile;
-                        mbar_arrive_expect_tx(&bar->full[s], STAGE_BYTES);
-                        const int k0 = kt * kElems;
-                        if (MODE == kModeOzaki) {
-                            tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, pi);
-                            tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, d - pi);
-                        } else {
-#pragma unroll
-                            for (int q = 0; q < NA; ++q) tma_load_3d(sa + q * kATile, &tmA, &bar->full[s], k0, m0, q);
-#pragma unroll
-                            for (int q = 0; q < NB; ++q) tma_load_3d(sb + q * BTILE, &tmB, &bar->full[s], k0, n0, q);
-                        }
-                    }
+            for (int kt = 0; kt < p.num_kt; ++kt, ++it) {
+                const int s = it % ST;
+                if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x201)) {
+                    ok = false;
+                    break;
                 }
+                uint8_t* sa = smem + s * STAGE_BYTES;
+                uint8_t* sb = sa + NA * kATile;
+                mbar_arrive_expect_tx(&bar->full[s], STAGE_BYTES);
+                const int k0 = kt * 64;  // bf16 elements per 128-byte row
+#pragma unroll
+                for (int q = 0; q < NA; ++q) tma_load_3d(sa + q * kATile, &tmA, &bar->full[s], k0, m0, q);
+#pragma unroll
+                for (int q = 0; q < NB; ++q) tma_load_3d(sb + q * BTILE, &tmB, &bar->full[s], k0, n0, q);
             }
         }
         if (!ok) {
@@ -208,8 +167,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
         uint32_t it = 0, uc = 0;
         for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
             for (int u = 0; ok && u < units; ++u, ++uc) {
-                int pairs, d, kt0, kt1;
-                unit_shape<MODE>(p, u, pairs, d, kt0, kt1);
+                const int kt0 = u * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
                 const uint32_t b = uc & 1;
                 if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, p.err, 0x202)) {
                     ok = false;
@@ -218,33 +176,26 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + b * UN;
                 uint32_t accumulate = 0;
-                for (int pi = 0; ok && pi < pairs; ++pi) {
-                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
-                        const int s = it % ST;
-                        if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x203)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-                        const uint32_t sb = sa + NA * kATile;
-#pragma unroll
-                        for (int kk = 0; kk < KSTEPS; ++kk) {
-                            if (MODE == kModeOzaki) {
-                                umma_i8(d_tmem, sw128_kmajor_desc(sa) + 2 * kk, sw128_kmajor_desc(sb) + 2 * kk,
-                                        IDESC, accumulate);
-                            } else {
-#pragma unroll
-                                for (int q = 0; q < Cfg::NPROD; ++q) {
-                                    umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
-                                             sw128_kmajor_desc(sb + Cfg::pb(q) * BTILE) + 2 * kk, IDESC,
-                                             (q == 0) ? accumulate : 1u);
-                                }
-                            }
-                            accumulate = 1;
-                        }
-                        tc_commit(&bar->empty[s]);  // stage free once these MMAs complete
+                for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                    const int s = it % ST;
+                    if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x203)) {
+                        ok = false;
+                        break;
                     }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+                    const uint32_t sb = sa + NA * kATile;
+#pragma unroll
+                    for (int kk = 0; kk < KSTEPS; ++kk) {
+#pragma unroll
+                        for (int q = 0; q < Cfg::NPROD; ++q) {
+                            umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
+                                     sw128_kmajor_desc(sb + Cfg::pb(q) * BTILE) + 2 * kk, IDESC,
+                                     (q == 0) ? accumulate : 1u);
+                        }
+                        accumulate = 1;
+                    }
+                    tc_commit(&bar->empty[s]);  // stage free once these MMAs complete
                 }
                 if (ok) tc_commit(&bar->acc_full[b]);
             }
@@ -263,86 +214,39 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
             const int m0 = tm * kUM, n0 = tn * UN;
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
-            if constexpr (MODE == kModeOzaki) {
-                const int er = row_ok ? p.row_exp[r] : kExpSentinel;
-                for (int u = 0; ok && u < units; ++u, ++uc) {
-                    const uint32_t b = uc & 1;
-                    if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
-                    const int d = p.slices - 1 - (u % p.slices);
-                    const bool first_unit = (u == 0);
-#pragma unroll 1
-                    for (int ch = 0; ch < UN / 32; ++ch) {
-                        uint32_t v[32];
-                        tmem_ld32(taddr + ch * 32, v);
-                        tmem_ld_wait();
-                        if (!row_ok || (er == kExpSentinel && !first_unit)) continue;
-                        double* C = static_cast<double*>(p.c);
-                        const int cbase = n0 + ch * 32;
+            float sum[UN];
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = cbase + j;
-                            if (col >= p.n) break;
-                            double* cp = C + r + static_cast<size_t>(col) * p.ldc;
-                            const int fc = __ldg(p.col_exp + col);
-                            double term = 0.0;
-                            if (er != kExpSentinel && fc != kExpSentinel)
-                                term = scalbn(static_cast<double>(static_cast<int32_t>(v[j])), er + fc - 7 * (d + 2));
-                            double acc;
-                            if (first_unit) {
-                                acc = 0.0;
-                                if (p.beta_mode == 1) acc = *cp;
-                                else if (p.beta_mode == 2) acc = p.beta_d * *cp;
-                            } else {
-                                acc = *cp;
-                            }
-                            *cp = fma(p.alpha_d, term, acc);
-                        }
-                    }
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+            for (int j = 0; j < UN; ++j) sum[j] = 0.f;
+            for (int u = 0; ok && u < units; ++u, ++uc) {
+                const uint32_t b = uc & 1;
+                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
+                    ok = false;
+                    break;
                 }
-            } else {
-                float sum[UN];
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
 #pragma unroll
-                for (int j = 0; j < UN; ++j) sum[j] = 0.f;
-                for (int u = 0; ok && u < units; ++u, ++uc) {
-                    const uint32_t b = uc & 1;
-                    if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+                for (int ch = 0; ch < UN / 32; ++ch) {
+                    uint32_t v[32];
+                    tmem_ld32(taddr + ch * 32, v);
+                    tmem_ld_wait();
 #pragma unroll
-                    for (int ch = 0; ch < UN / 32; ++ch) {
-                        uint32_t v[32];
-                        tmem_ld32(taddr + ch * 32, v);
-                        tmem_ld_wait();
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
-                    }
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+                    for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
                 }
-                if (ok && row_ok) {
-                    float* C = static_cast<float*>(p.c);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+            }
+            if (ok && row_ok) {
 #pragma unroll
-                    for (int j = 0; j < UN; ++j) {
-                        const int col = n0 + j;
-                        if (col >= p.n) break;
-                        float* cp = C + r + static_cast<size_t>(col) * p.ldc;
-                        float tb = 0.f;
-                        if (p.beta_mode == 1) tb = *cp;
-                        else if (p.beta_mode == 2) tb = p.beta_f * *cp;
-                        *cp = fmaf(p.alpha_f, sum[j], tb);
-                    }
+                for (int j = 0; j < UN; ++j) {
+                    const int col = n0 + j;
+                    if (col >= p.n) break;
+                    float* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
+                    float tb = 0.f;
+                    if (p.beta_mode == 1) tb = *cp;
+                    else if (p.beta_mode == 2) tb = p.beta_f * *cp;
+                    *cp = fmaf(p.alpha_f, sum[j], tb);
                 }
             }
         }
@@ -353,6 +257,246 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     if (warp == 1) {
         tc_fence_after();
         tmem_dealloc(tmem_base, TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------------------
+// Ozaki GEMM kernel.
+//
+// Slice products of equal weight (t + u = d: slice t has weight 2^-(7+8t))
+// form diagonal d; S_d = sum_{t+u=d} A_t B_u^T is exact in INT32 over a K
+// chunk. Diagonals are processed two at a time ("units" {d0, d0+1}) with
+// both accumulators in TMEM (2 x 256 columns): for each B slice j the stage
+// holds B_j and the two A slices it pairs with, A_{d0-j} -> S_d0 and
+// A_{d0+1-j} -> S_{d0+1}, so every B tile feeds two MMAs. The epilogue
+// folds the unit exactly, S_d0 * 2^8 + S_{d0+1} (< 2^40), scales by
+// alpha * 2^(e_i + f_j - 14 - 8(d0+1)) and accumulates into C in FP64;
+// units run from the smallest weight up, the first one adding beta*C0.
+// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 epilogue (two
+// warps per TMEM lane quarter, 128 columns each).
+// ------------------------------------------------------------------------------
+
+__host__ __device__ constexpr uint32_t kBTileOz() { return 256u * kRowBytes; }
+constexpr int kOzST = 3;                         // stages of (B_j, A, A)
+constexpr int kOzStage = 2 * kATile + 256 * kRowBytes;  // 64 KiB
+constexpr int kOzThreads = 320;
+
+struct OzParams {
+    int m, n, k;
+    int tiles_m, tiles_n, num_tiles;
+    int num_kt;        // 128-byte K tiles
+    int slices;
+    int kt_per_chunk;  // exact-INT32 K chunk
+    int kchunks;
+    int beta_mode;
+    double alpha, beta;
+    double* c;
+    size_t ldc;
+    const int* row_exp;
+    const int* col_exp;
+    uint32_t* err;
+};
+
+// unit u (0-based) of a chunk covers diagonals d0 and d1 = d0 + 1 (d1 < 0
+// when absent); units go from the highest diagonals down.
+__device__ __forceinline__ void oz_unit(int slices, int u, int& d0, int& d1) {
+    const int units = (slices + 1) / 2;
+    d0 = 2 * (units - 1 - u);
+    d1 = (d0 + 1 < slices) ? d0 + 1 : -1;
+}
+
+__global__ void __launch_bounds__(kOzThreads, 1)
+    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const OzParams p) {
+    constexpr int ST = kOzST;
+    constexpr int UN = 256;
+    constexpr int KSTEPS = 4;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    Bar* bar = reinterpret_cast<Bar*>(smem + ST * kOzStage);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(&bar->full[s], 1);
+            mbar_init(&bar->empty[s], 1);
+        }
+        mbar_init(&bar->acc_full[0], 1);
+        mbar_init(&bar->acc_empty[0], 8);
+        mbar_init(&bar->drain, 1);
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&bar->tmem_base, 2 * UN);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bar->tmem_base;
+    const int upc = (p.slices + 1) / 2;  // units per chunk
+    const int units = p.kchunks * upc;
+    bool ok = true;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------ TMA producer ------------------------------
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+        uint32_t it = 0;
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            int tm, tn;
+            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * UN;
+            for (int u = 0; ok && u < units; ++u) {
+                int d0, d1;
+                oz_unit(p.slices, u % upc, d0, d1);
+                const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+                const int jmax = d1 >= 0 ? d1 : d0;
+                for (int j = 0; ok && j <= jmax; ++j) {
+                    const bool a0 = j <= d0, a1 = d1 >= 0;  // A_{d0-j} valid; A_{d1-j} valid (j <= d1)
+                    const uint32_t bytes = kBTileOz() + (a0 ? kATile : 0) + (a1 ? kATile : 0);
+                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                        const int s = it % ST;
+                        if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x301)) {
+                            ok = false;
+                            break;
+                        }
+                        uint8_t* sb = smem + s * kOzStage;
+                        uint8_t* sa0 = sb + kBTileOz();
+                        uint8_t* sa1 = sa0 + kATile;
+                        mbar_arrive_expect_tx(&bar->full[s], bytes);
+                        const int k0 = kt * 128;
+                        tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, j);
+                        if (a0) tma_load_3d(sa0, &tmA, &bar->full[s], k0, m0, d0 - j);
+                        if (a1) tma_load_3d(sa1, &tmA, &bar->full[s], k0, m0, d1 - j);
+                    }
+                }
+            }
+        }
+        if (!ok) {
+            const uint32_t first = it > (uint32_t)ST ? it - ST : 0;
+            for (uint32_t j = first; j < it; ++j) mbar_wait_drain(&bar->full[j % ST], (j / ST) & 1);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------ MMA issuer ------------------------------
+        uint32_t it = 0, uc = 0;
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            for (int u = 0; ok && u < units; ++u, ++uc) {
+                int d0, d1;
+                oz_unit(p.slices, u % upc, d0, d1);
+                const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+                const int jmax = d1 >= 0 ? d1 : d0;
+                if (uc >= 1 && !mbar_wait(&bar->acc_empty[0], (uc - 1) & 1, p.err, 0x302)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint32_t acc0 = 0, acc1 = 0;
+                for (int j = 0; ok && j <= jmax; ++j) {
+                    const bool a0 = j <= d0, a1 = d1 >= 0;
+                    // slice 0 is signed, the others unsigned
+                    const uint32_t fb = (j == 0) ? 1u : 0u;
+                    const uint32_t id0 = (2u << 4) | ((d0 - j == 0 ? 1u : 0u) << 7) | (fb << 10) |
+                                         (static_cast<uint32_t>(UN >> 3) << 17) | (static_cast<uint32_t>(kUM >> 4) << 24);
+                    const uint32_t id1 = (2u << 4) | ((d1 - j == 0 ? 1u : 0u) << 7) | (fb << 10) |
+                                         (static_cast<uint32_t>(UN >> 3) << 17) | (static_cast<uint32_t>(kUM >> 4) << 24);
+                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                        const int s = it % ST;
+                        if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x303)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sb = smem_u32(smem + s * kOzStage);
+                        const uint32_t sa0 = sb + kBTileOz(), sa1 = sa0 + kATile;
+#pragma unroll
+                        for (int kk = 0; kk < KSTEPS; ++kk) {
+                            const uint64_t bd = sw128_kmajor_desc(sb) + 2 * kk;
+                            if (a0) {
+                                umma_i8(tmem_base, sw128_kmajor_desc(sa0) + 2 * kk, bd, id0, acc0);
+                                acc0 = 1;
+                            }
+                            if (a1) {
+                                umma_i8(tmem_base + UN, sw128_kmajor_desc(sa1) + 2 * kk, bd, id1, acc1);
+                                acc1 = 1;
+                            }
+                        }
+                        tc_commit(&bar->empty[s]);
+                    }
+                }
+                if (ok) tc_commit(&bar->acc_full[0]);
+            }
+        }
+        tc_commit(&bar->drain);
+        mbar_wait_drain(&bar->drain, 0);
+    } else if (warp >= 2) {
+        // ------------------------------ epilogue ------------------------------
+        const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;  // which 128 columns
+        const int row_in_tile = quarter * 32 + lane;
+        uint32_t uc = 0;
+        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+            int tm, tn;
+            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * UN;
+            const int r = m0 + row_in_tile;
+            const bool row_ok = r < p.m;
+            const int er = row_ok ? p.row_exp[r] : kExpSentinel;
+            for (int u = 0; ok && u < units; ++u, ++uc) {
+                int d0, d1;
+                oz_unit(p.slices, u % upc, d0, d1);
+                if (!mbar_wait(&bar->acc_full[0], uc & 1, p.err, 0x304)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
+                const bool first_unit = (u == 0);
+                const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0);
+#pragma unroll 1
+                for (int ch = 0; ch < 4; ++ch) {
+                    const int col0 = half * 128 + ch * 32;
+                    uint32_t v0[32], v1[32];
+                    tmem_ld32(lanebase + col0, v0);
+                    if (d1 >= 0) tmem_ld32(lanebase + UN + col0, v1);
+                    tmem_ld_wait();
+                    if (!row_ok || (er == kExpSentinel && !first_unit)) continue;
+                    const int cbase = n0 + col0;
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const int col = cbase + jj;
+                        if (col >= p.n) break;
+                        double* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
+                        const int fc = __ldg(p.col_exp + col);
+                        double term = 0.0;
+                        if (er != kExpSentinel && fc != kExpSentinel) {
+                            double sv = static_cast<double>(static_cast<int32_t>(v0[jj]));
+                            if (d1 >= 0) sv = fma(sv, 256.0, static_cast<double>(static_cast<int32_t>(v1[jj])));
+                            term = scalbn(sv, er + fc - wexp);
+                        }
+                        double acc;
+                        if (first_unit) {
+                            acc = 0.0;
+                            if (p.beta_mode == 1) acc = *cp;
+                            else if (p.beta_mode == 2) acc = p.beta * *cp;
+                        } else {
+                            acc = *cp;
+                        }
+                        *cp = fma(p.alpha, term, acc);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->acc_empty[0]);
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 2 * UN);
     }
 }
 
@@ -424,10 +568,14 @@ __device__ __forceinline__ void load_tile(const T* __restrict__ x, size_t rs, si
     }
 }
 
-// Ozaki slicing: out[t][r][q] = sigma_t of x(r,q) * 2^-e[r], t < slices.
+// Ozaki slicing: x(r,q) * 2^-e[r] in (-1, 1) is cut into
+//   sigma_0 = floor(x * 2^7)          in [-128, 127]  (signed int8),
+//   sigma_t = floor(rem_{t-1} * 2^8)  in [0, 255]     (unsigned, t >= 1),
+// with rem in [0, 1); every step is exact in FP64, and
+// x * 2^-e = sum_t sigma_t 2^-(7+8t) + (remainder < 2^-(7+8(s-1))).
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
                                                           int R, int K, const int* __restrict__ e,
-                                                          int slices, int8_t* __restrict__ out, size_t kp,
+                                                          int slices, uint8_t* __restrict__ out, size_t kp,
                                                           size_t plane) {
     __shared__ double tile[kTile][kTile + 1];
     const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
@@ -441,12 +589,13 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     for (int i = 0; i < 16; ++i) xs[i] = (er == kExpSentinel) ? 0.0 : scalbn(tile[r][c * 16 + i], -er);
     for (int t = 0; t < slices; ++t) {
         uint32_t w[4] = {0u, 0u, 0u, 0u};
+        const double scale = (t == 0) ? 128.0 : 256.0;
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            const double v = xs[i] * 128.0;
-            const double s = trunc(v);
-            xs[i] = v - s;
-            w[i >> 2] |= (static_cast<uint32_t>(static_cast<int>(s)) & 0xFFu) << (8 * (i & 3));
+            const double v = xs[i] * scale;
+            const double f = floor(v);
+            xs[i] = v - f;
+            w[i >> 2] |= (static_cast<uint32_t>(static_cast<int>(f)) & 0xFFu) << (8 * (i & 3));
         }
         const size_t off = t * plane + static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
         if (p0 + c * 16 < static_cast<int>(kp))
@@ -504,10 +653,8 @@ cudaError_t launch_umma(const CUtensorMap& ta, const CUtensorMap& tb, const UPar
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = p.num_tiles < sms ? p.num_tiles : sms;
-    const double mnk2 = 2.0 * p.m * p.n * p.k;
-    const double work = (MODE == kModeOzaki) ? mnk2 * p.slices * (p.slices + 1) / 2
-                                             : mnk2 * UCfg<MODE>::NPROD;
-    const char* name = (MODE == kModeOzaki) ? "umma_ozaki_i8" : (MODE == kModeBf16x3 ? "umma_bf16x3" : "umma_bf16x6");
+    const double work = 2.0 * p.m * p.n * static_cast<double>(p.k) * UCfg<MODE>::NPROD;
+    const char* name = (MODE == kModeBf16x3) ? "umma_bf16x3" : "umma_bf16x6";
     KernelTimer tm;
     kernel_timing_begin(name, work, st, &tm);
     kern<<<grid, UCfg<MODE>::THREADS, smem, st>>>(ta, tb, p);
@@ -632,7 +779,6 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     p.tiles_n = (n + UN - 1) / UN;
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 63) / 64);
-    p.slices = 1;
     p.kt_per_chunk = 2;  // FP32 promotion every 128 elements of K
     p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
     p.beta_mode = (beta == 0.f) ? 0 : (beta == 1.f ? 1 : 2);
@@ -651,12 +797,13 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
     void* buf = nullptr;
     const size_t exps = round_up((static_cast<size_t>(m) + n) * sizeof(int), 256);
-    cudaError_t e = cudaMallocAsync(&buf, exps + slices * (pa + pb), st);
+    const size_t a_bytes = round_up(slices * pa, 256);
+    cudaError_t e = cudaMallocAsync(&buf, exps + a_bytes + slices * pb, st);
     if (e != cudaSuccess) return e;
     int* ea = static_cast<int*>(buf);
     int* eb = ea + m;
-    int8_t* sla = static_cast<int8_t*>(buf) + exps;
-    int8_t* slb = sla + slices * pa;
+    uint8_t* sla = static_cast<uint8_t*>(buf) + exps;
+    uint8_t* slb = sla + a_bytes;
     size_t ars, aps, brs, bps;
     operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
     fill_int_kernel<<<64, 256, 0, st>>>(ea, m + n, kExpSentinel);
@@ -672,31 +819,47 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     count_launch(5);
     CUtensorMap tma, tmb;
     CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, m, slices, kp, kUM);
-    constexpr int UN = UCfg<kModeOzaki>::UN;
-    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, UN);
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, 256);
     if (r != CUDA_SUCCESS) {
         if (cu_err) *cu_err = r;
         cudaFreeAsync(buf, st);
         return cudaErrorInvalidValue;
     }
-    UParams p{};
+    OzParams p{};
     p.m = m; p.n = n; p.k = k;
     p.tiles_m = (m + kUM - 1) / kUM;
-    p.tiles_n = (n + UN - 1) / UN;
+    p.tiles_n = (n + 255) / 256;
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 127) / 128);
     p.slices = slices;
-    // exact INT32: (pairs per diagonal <= slices) * k_chunk * 127^2 < 2^31
-    const long long max_k = (2147483647LL / (static_cast<long long>(slices) * 127 * 127)) / 128 * 128;
+    // exact INT32: a diagonal has <= slices products of <= 255*255 per K element
+    const long long max_k = 2147483647LL / (static_cast<long long>(slices) * 255 * 255);
     p.kt_per_chunk = static_cast<int>(max_k / 128);
     if (p.kt_per_chunk < 1) p.kt_per_chunk = 1;
     p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
     p.beta_mode = (beta == 0.0) ? 0 : (beta == 1.0 ? 1 : 2);
-    p.alpha_d = alpha; p.beta_d = beta;
+    p.alpha = alpha; p.beta = beta;
     p.c = C; p.ldc = ldc;
     p.row_exp = ea; p.col_exp = eb;
     p.err = device_error_word();
-    e = launch_umma<kModeOzaki>(tma, tmb, p, st);
+
+    constexpr int smem = kOzST * kOzStage + 256 + 1024;
+    static bool attr = false;
+    if (!attr) {
+        e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) { cudaFreeAsync(buf, st); return e; }
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = p.num_tiles < sms ? p.num_tiles : sms;
+    KernelTimer tmr;
+    kernel_timing_begin("umma_ozaki_i8", 2.0 * m * n * static_cast<double>(k) * slices * (slices + 1) / 2, st, &tmr);
+    ozaki_gemm_kernel<<<grid, kOzThreads, smem, st>>>(tma, tmb, p);
+    kernel_timing_end(&tmr, st);
+    count_launch();
+    e = cudaGetLastError();
     cudaFreeAsync(buf, st);
     return e;
 }

@@ -56,7 +56,7 @@ void kernel_timing_end(KernelTimer* t, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(g_timing_mu);
     g_timed.push_back(L);
 }
-static std::atomic<int> g_ozaki_slices{8};
+static std::atomic<int> g_ozaki_slices{7};
 static int ozaki_slices() { return g_ozaki_slices.load(); }
 
 namespace {
@@ -168,6 +168,7 @@ struct ColProblem {
     const T* a; size_t lda;
     const T* b; size_t ldb;
     T* c; size_t ldc;
+    int tri = 0;  // syrk: restrict C to one triangle
 };
 
 template <typename T>
@@ -231,10 +232,16 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
     }
     cudaError_t e;
     if (p.k == 0 || p.alpha == T(0)) {
-        e = launch_scale_c<T>((int)p.m, (int)p.n, p.beta, p.c, p.ldc, st);
+        e = launch_scale_c<T>((int)p.m, (int)p.n, p.beta, p.c, p.ldc, st, p.tri);
         return e == cudaSuccess ? RB_OK : cuda_fail(err, e);
     }
-    if (prec != RB_PREC_PLAIN) return run_precision_form(p, prec, st, err);
+    if (prec != RB_PREC_PLAIN) {
+        if (p.tri) {
+            set_err(err, RB_ERR_UNSUPPORTED);
+            return RB_ERR_UNSUPPORTED;
+        }
+        return run_precision_form(p, prec, st, err);
+    }
     const T* A = p.a;
     const T* B = p.b;
     size_t lda = p.lda, ldb = p.ldb;
@@ -266,7 +273,7 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
     CUresult cu = CUDA_SUCCESS;
     // op(A): Trans -> stored k x m, k-contiguous; op(B): NoTrans -> stored k x n, k-contiguous.
     e = launch_simt_gemm<T>(p.ta, !p.tb, (int)p.m, (int)p.n, (int)p.k, p.alpha, A, lda, B, ldb,
-                            p.beta, p.c, p.ldc, st, &cu);
+                            p.beta, p.c, p.ldc, st, &cu, p.tri);
     for (void* s : scratch)
         if (s) cudaFreeAsync(s, st);
     if (cu != CUDA_SUCCESS) {
@@ -392,7 +399,85 @@ rb_status dev_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, s
     return run_dev<T>(p, prec, static_cast<cudaStream_t>(stream), err);
 }
 
+// A host buffer holding a stored rows x cols column-major matrix (`elem`
+// bytes per element) with leading dimension ld.
+struct HostMat {
+    const void* src;  // host pointer read (may be null when !in)
+    void* dst;        // host pointer written back (null when !out)
+    size_t rows, cols, ld, elem;
+    bool in, out;
+};
+
+// Stage up to three matrices into the device context's buffers (leading
+// dimensions padded to 16 bytes), run `body(dev_ptrs, dev_lds, stream,
+// &cuda_err)` on the internal stream, copy results back, and report any
+// device-side error word.
+template <typename F>
+rb_status host_run(HostMat* mats, int nm, rb_error* err, F&& body) {
+    cudaError_t e;
+    DeviceCtx* ctx = ctx_for_current(&e);
+    if (!ctx) return cuda_fail(err, e);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    void* dptr[3] = {nullptr, nullptr, nullptr};
+    size_t dld[3] = {0, 0, 0};
+    for (int i = 0; i < nm; ++i) {
+        HostMat& h = mats[i];
+        const size_t per16 = (h.elem >= 16) ? 1 : 16 / h.elem;
+        dld[i] = std::max<size_t>((h.rows + per16 - 1) / per16 * per16, per16);
+        const size_t bytes = dld[i] * std::max<size_t>(h.cols, 1) * h.elem;
+        if ((e = ensure_buf(ctx, i, bytes)) != cudaSuccess) return cuda_fail(err, e);
+        dptr[i] = ctx->buf[i];
+        if (h.in && h.rows && h.cols) {
+            e = cudaMemcpy2DAsync(dptr[i], dld[i] * h.elem, h.src, h.ld * h.elem, h.rows * h.elem, h.cols,
+                                  cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(err, e);
+        }
+    }
+    int32_t ce = 0;
+    const int rc = body(dptr, dld, ctx->stream, &ce);
+    if (rc != RB_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        set_err(err, rc, 0, 0, 0, ce);
+        return static_cast<rb_status>(rc);
+    }
+    for (int i = 0; i < nm; ++i) {
+        HostMat& h = mats[i];
+        if (h.out && h.rows && h.cols) {
+            e = cudaMemcpy2DAsync(h.dst, h.ld * h.elem, dptr[i], dld[i] * h.elem, h.rows * h.elem, h.cols,
+                                  cudaMemcpyDeviceToHost, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(err, e);
+        }
+    }
+    return check_device_word(ctx, err);
+}
+
+bool valid_uplo(int v) { return v == RB_UPPER || v == RB_LOWER; }
+bool valid_side(int v) { return v == RB_LEFT || v == RB_RIGHT; }
+bool valid_diag(int v) { return v == RB_NON_UNIT || v == RB_UNIT; }
+
+rb_status invalid(rb_error* err) {
+    set_err(err, RB_ERR_INVALID_ARG);
+    return RB_ERR_INVALID_ARG;
+}
+
 }  // namespace
+
+template <typename T>
+int gemm_colmajor_dev(bool ta, bool tb, size_t m, size_t n, size_t k, T alpha, const T* A,
+                      size_t lda, const T* B, size_t ldb, T beta, T* C, size_t ldc, int prec,
+                      cudaStream_t st, int tri, int32_t* cuda_err) {
+    ColProblem<T> p{ta, tb, m, n, k, alpha, beta, A, lda, B, ldb, C, ldc, tri};
+    rb_error e{};
+    const rb_status s = run_dev<T>(p, static_cast<rb_precision>(prec), st, &e);
+    if (cuda_err) *cuda_err = e.cuda_error;
+    return s;
+}
+template int gemm_colmajor_dev<float>(bool, bool, size_t, size_t, size_t, float, const float*, size_t,
+                                      const float*, size_t, float, float*, size_t, int, cudaStream_t,
+                                      int, int32_t*);
+template int gemm_colmajor_dev<double>(bool, bool, size_t, size_t, size_t, double, const double*,
+                                       size_t, const double*, size_t, double, double*, size_t, int,
+                                       cudaStream_t, int, int32_t*);
 
 uint32_t* device_error_word() {
     cudaError_t e;
@@ -474,7 +559,7 @@ rb_status rb_dgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose trans
 
 
 rb_status rb_set_ozaki_slices(int slices) {
-    if (slices < 3 || slices > 12) return RB_ERR_INVALID_ARG;
+    if (slices < 2 || slices > 12) return RB_ERR_INVALID_ARG;
     g_ozaki_slices.store(slices);
     return RB_OK;
 }
@@ -545,6 +630,238 @@ void rb_release_cached_memory(void) {
         c->buf[i] = nullptr;
         c->cap[i] = 0;
     }
+}
+
+}  // extern "C"
+
+// ============================================================================
+// Complex GEMM, syrk, symm/hemm, trsm (host slices and device pointers)
+// ============================================================================
+namespace rb {
+namespace {
+
+template <typename T>
+rb_status cgemm_host(rb_transpose ta, rb_transpose tb, size_t m, size_t n, size_t k, T ar, T ai,
+                     const T* a, size_t lda, size_t a_len, const T* b, size_t ldb, size_t b_len, T br,
+                     T bi, T* c, size_t ldc, size_t c_len, rb_precision prec, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_trans(ta) || !valid_trans(tb) || !valid_prec(prec)) return invalid(err);
+    const bool tra = ta != RB_NO_TRANS, trb = tb != RB_NO_TRANS;
+    rb_status s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'a', tra ? k : m, tra ? m : k, lda, a_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'b', trb ? n : k, trb ? k : n, ldb, b_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'c', m, n, ldc, c_len, true, err))) return s;
+    if (m == 0 || n == 0) return RB_OK;
+    const bool beta0 = (br == T(0) && bi == T(0));
+    HostMat mats[3] = {{a, nullptr, tra ? k : m, tra ? m : k, lda, 2 * sizeof(T), k > 0, false},
+                       {b, nullptr, trb ? n : k, trb ? k : n, ldb, 2 * sizeof(T), k > 0, false},
+                       {c, c, m, n, ldc, 2 * sizeof(T), !beta0, true}};
+    return host_run(mats, 3, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return complex_gemm_dev<T>(ta, tb, m, n, k, ar, ai, static_cast<const T*>(d[0]), ld[0],
+                                   static_cast<const T*>(d[1]), ld[1], br, bi, static_cast<T*>(d[2]), ld[2],
+                                   prec, st, ce);
+    });
+}
+
+template <typename T>
+rb_status syrk_host(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, T alpha, const T* a, size_t lda,
+                    size_t a_len, T beta, T* c, size_t ldc, size_t c_len, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_uplo(uplo) || !valid_trans(trans)) return invalid(err);
+    const bool t = trans != RB_NO_TRANS;
+    rb_status s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'a', t ? k : n, t ? n : k, lda, a_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'c', n, n, ldc, c_len, true, err))) return s;
+    if (n == 0) return RB_OK;
+    // the other triangle of C is preserved, so C is always staged in
+    HostMat mats[2] = {{a, nullptr, t ? k : n, t ? n : k, lda, sizeof(T), k > 0, false},
+                       {c, c, n, n, ldc, sizeof(T), true, true}};
+    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return syrk_dev<T>(uplo, trans, n, k, alpha, static_cast<const T*>(d[0]), ld[0], beta,
+                           static_cast<T*>(d[1]), ld[1], st, ce);
+    });
+}
+
+template <typename T, bool CX>
+rb_status symm_host(int herm, rb_side side, rb_uplo uplo, size_t m, size_t n, T ar, T ai, const T* a,
+                    size_t lda, size_t a_len, const T* b, size_t ldb, size_t b_len, T br, T bi, T* c,
+                    size_t ldc, size_t c_len, rb_precision prec, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_side(side) || !valid_uplo(uplo) || !valid_prec(prec)) return invalid(err);
+    const size_t q = (side == RB_LEFT) ? m : n;
+    rb_status s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'a', q, q, lda, a_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'b', m, n, ldb, b_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'c', m, n, ldc, c_len, true, err))) return s;
+    if (m == 0 || n == 0) return RB_OK;
+    const size_t el = (CX ? 2 : 1) * sizeof(T);
+    const bool beta0 = (br == T(0) && (!CX || bi == T(0)));
+    HostMat mats[3] = {{a, nullptr, q, q, lda, el, true, false},
+                       {b, nullptr, m, n, ldb, el, true, false},
+                       {c, c, m, n, ldc, el, !beta0, true}};
+    return host_run(mats, 3, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        if constexpr (CX)
+            return hesy_dev<T>(herm, side, uplo, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
+                               static_cast<const T*>(d[1]), ld[1], br, bi, static_cast<T*>(d[2]), ld[2], prec, st,
+                               ce);
+        else
+            return symm_dev<T>(side, uplo, m, n, ar, static_cast<const T*>(d[0]), ld[0],
+                               static_cast<const T*>(d[1]), ld[1], br, static_cast<T*>(d[2]), ld[2], prec, st, ce);
+    });
+}
+
+template <typename T, bool CX>
+rb_status trsm_host(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, T ar,
+                    T ai, const T* a, size_t lda, size_t a_len, T* b, size_t ldb, size_t b_len, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_side(side) || !valid_uplo(uplo) || !valid_trans(trans) || !valid_diag(diag)) return invalid(err);
+    const size_t q = (side == RB_LEFT) ? m : n;
+    rb_status s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'a', q, q, lda, a_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'b', m, n, ldb, b_len, true, err))) return s;
+    if (m == 0 || n == 0) return RB_OK;
+    const size_t el = (CX ? 2 : 1) * sizeof(T);
+    HostMat mats[2] = {{a, nullptr, q, q, lda, el, true, false}, {b, b, m, n, ldb, el, true, true}};
+    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return trsm_dev<T, CX>(side, uplo, trans, diag, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
+                               static_cast<T*>(d[1]), ld[1], st, ce);
+    });
+}
+
+rb_status dev_status(int rc, int32_t ce, rb_error* err) {
+    if (rc != RB_OK) set_err(err, rc, 0, 0, 0, ce);
+    return static_cast<rb_status>(rc);
+}
+
+}  // namespace
+}  // namespace rb
+
+extern "C" {
+
+rb_status rb_cgemm(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k, rb_complex32 alpha,
+                   const rb_complex32* a, size_t lda, size_t a_len, const rb_complex32* b, size_t ldb,
+                   size_t b_len, rb_complex32 beta, rb_complex32* c, size_t ldc, size_t c_len,
+                   rb_precision prec, rb_error* err) {
+    return cgemm_host<float>(transa, transb, m, n, k, alpha.re, alpha.im, reinterpret_cast<const float*>(a), lda,
+                             a_len, reinterpret_cast<const float*>(b), ldb, b_len, beta.re, beta.im,
+                             reinterpret_cast<float*>(c), ldc, c_len, prec, err);
+}
+rb_status rb_zgemm(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k, rb_complex64 alpha,
+                   const rb_complex64* a, size_t lda, size_t a_len, const rb_complex64* b, size_t ldb,
+                   size_t b_len, rb_complex64 beta, rb_complex64* c, size_t ldc, size_t c_len,
+                   rb_precision prec, rb_error* err) {
+    return cgemm_host<double>(transa, transb, m, n, k, alpha.re, alpha.im, reinterpret_cast<const double*>(a),
+                              lda, a_len, reinterpret_cast<const double*>(b), ldb, b_len, beta.re, beta.im,
+                              reinterpret_cast<double*>(c), ldc, c_len, prec, err);
+}
+rb_status rb_cgemm_dev(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                       rb_complex32 alpha, const rb_complex32* a, size_t lda, const rb_complex32* b, size_t ldb,
+                       rb_complex32 beta, rb_complex32* c, size_t ldc, rb_precision prec, void* stream,
+                       rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_trans(transa) || !valid_trans(transb) || !valid_prec(prec)) return invalid(err);
+    int32_t ce = 0;
+    const int rc = complex_gemm_dev<float>(transa, transb, m, n, k, alpha.re, alpha.im,
+                                           reinterpret_cast<const float*>(a), lda, reinterpret_cast<const float*>(b),
+                                           ldb, beta.re, beta.im, reinterpret_cast<float*>(c), ldc, prec,
+                                           static_cast<cudaStream_t>(stream), &ce);
+    return dev_status(rc, ce, err);
+}
+rb_status rb_zgemm_dev(rb_transpose transa, rb_transpose transb, size_t m, size_t n, size_t k,
+                       rb_complex64 alpha, const rb_complex64* a, size_t lda, const rb_complex64* b, size_t ldb,
+                       rb_complex64 beta, rb_complex64* c, size_t ldc, rb_precision prec, void* stream,
+                       rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_trans(transa) || !valid_trans(transb) || !valid_prec(prec)) return invalid(err);
+    int32_t ce = 0;
+    const int rc = complex_gemm_dev<double>(transa, transb, m, n, k, alpha.re, alpha.im,
+                                            reinterpret_cast<const double*>(a), lda,
+                                            reinterpret_cast<const double*>(b), ldb, beta.re, beta.im,
+                                            reinterpret_cast<double*>(c), ldc, prec,
+                                            static_cast<cudaStream_t>(stream), &ce);
+    return dev_status(rc, ce, err);
+}
+
+rb_status rb_ssyrk(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, float alpha, const float* a, size_t lda,
+                   size_t a_len, float beta, float* c, size_t ldc, size_t c_len, rb_error* err) {
+    return syrk_host<float>(uplo, trans, n, k, alpha, a, lda, a_len, beta, c, ldc, c_len, err);
+}
+rb_status rb_dsyrk(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, double alpha, const double* a,
+                   size_t lda, size_t a_len, double beta, double* c, size_t ldc, size_t c_len, rb_error* err) {
+    return syrk_host<double>(uplo, trans, n, k, alpha, a, lda, a_len, beta, c, ldc, c_len, err);
+}
+
+rb_status rb_ssymm(rb_side side, rb_uplo uplo, size_t m, size_t n, float alpha, const float* a, size_t lda,
+                   size_t a_len, const float* b, size_t ldb, size_t b_len, float beta, float* c, size_t ldc,
+                   size_t c_len, rb_error* err) {
+    return symm_host<float, false>(0, side, uplo, m, n, alpha, 0.f, a, lda, a_len, b, ldb, b_len, beta, 0.f, c,
+                                   ldc, c_len, RB_PREC_PLAIN, err);
+}
+rb_status rb_dsymm(rb_side side, rb_uplo uplo, size_t m, size_t n, double alpha, const double* a, size_t lda,
+                   size_t a_len, const double* b, size_t ldb, size_t b_len, double beta, double* c, size_t ldc,
+                   size_t c_len, rb_error* err) {
+    return symm_host<double, false>(0, side, uplo, m, n, alpha, 0.0, a, lda, a_len, b, ldb, b_len, beta, 0.0, c,
+                                    ldc, c_len, RB_PREC_PLAIN, err);
+}
+rb_status rb_csymm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* a,
+                   size_t lda, size_t a_len, const rb_complex32* b, size_t ldb, size_t b_len, rb_complex32 beta,
+                   rb_complex32* c, size_t ldc, size_t c_len, rb_error* err) {
+    return symm_host<float, true>(0, side, uplo, m, n, alpha.re, alpha.im, reinterpret_cast<const float*>(a), lda,
+                                  a_len, reinterpret_cast<const float*>(b), ldb, b_len, beta.re, beta.im,
+                                  reinterpret_cast<float*>(c), ldc, c_len, RB_PREC_PLAIN, err);
+}
+rb_status rb_zsymm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* a,
+                   size_t lda, size_t a_len, const rb_complex64* b, size_t ldb, size_t b_len, rb_complex64 beta,
+                   rb_complex64* c, size_t ldc, size_t c_len, rb_error* err) {
+    return symm_host<double, true>(0, side, uplo, m, n, alpha.re, alpha.im, reinterpret_cast<const double*>(a),
+                                   lda, a_len, reinterpret_cast<const double*>(b), ldb, b_len, beta.re, beta.im,
+                                   reinterpret_cast<double*>(c), ldc, c_len, RB_PREC_PLAIN, err);
+}
+rb_status rb_chemm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* a,
+                   size_t lda, size_t a_len, const rb_complex32* b, size_t ldb, size_t b_len, rb_complex32 beta,
+                   rb_complex32* c, size_t ldc, size_t c_len, rb_error* err) {
+    return symm_host<float, true>(1, side, uplo, m, n, alpha.re, alpha.im, reinterpret_cast<const float*>(a), lda,
+                                  a_len, reinterpret_cast<const float*>(b), ldb, b_len, beta.re, beta.im,
+                                  reinterpret_cast<float*>(c), ldc, c_len, RB_PREC_PLAIN, err);
+}
+rb_status rb_zhemm(rb_side side, rb_uplo uplo, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* a,
+                   size_t lda, size_t a_len, const rb_complex64* b, size_t ldb, size_t b_len, rb_complex64 beta,
+                   rb_complex64* c, size_t ldc, size_t c_len, rb_error* err) {
+    return symm_host<double, true>(1, side, uplo, m, n, alpha.re, alpha.im, reinterpret_cast<const double*>(a),
+                                   lda, a_len, reinterpret_cast<const double*>(b), ldb, b_len, beta.re, beta.im,
+                                   reinterpret_cast<double*>(c), ldc, c_len, RB_PREC_PLAIN, err);
+}
+
+rb_status rb_strsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, float alpha,
+                   const float* a, size_t lda, size_t a_len, float* b, size_t ldb, size_t b_len, rb_error* err) {
+    return trsm_host<float, false>(side, uplo, trans, diag, m, n, alpha, 0.f, a, lda, a_len, b, ldb, b_len, err);
+}
+rb_status rb_dtrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, double alpha,
+                   const double* a, size_t lda, size_t a_len, double* b, size_t ldb, size_t b_len, rb_error* err) {
+    return trsm_host<double, false>(side, uplo, trans, diag, m, n, alpha, 0.0, a, lda, a_len, b, ldb, b_len, err);
+}
+rb_status rb_ctrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex32 alpha, const rb_complex32* a, size_t lda, size_t a_len, rb_complex32* b, size_t ldb,
+                   size_t b_len, rb_error* err) {
+    return trsm_host<float, true>(side, uplo, trans, diag, m, n, alpha.re, alpha.im, reinterpret_cast<const float*>(a),
+                                  lda, a_len, reinterpret_cast<float*>(b), ldb, b_len, err);
+}
+rb_status rb_ztrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex64 alpha, const rb_complex64* a, size_t lda, size_t a_len, rb_complex64* b, size_t ldb,
+                   size_t b_len, rb_error* err) {
+    return trsm_host<double, true>(side, uplo, trans, diag, m, n, alpha.re, alpha.im,
+                                   reinterpret_cast<const double*>(a), lda, a_len, reinterpret_cast<double*>(b), ldb,
+                                   b_len, err);
+}
+
+rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                       double alpha, const double* a, size_t lda, double* b, size_t ldb, void* stream, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_side(side) || !valid_uplo(uplo) || !valid_trans(trans) || !valid_diag(diag)) return invalid(err);
+    int32_t ce = 0;
+    const int rc = trsm_dev<double, false>(side, uplo, trans, diag, m, n, alpha, 0.0, a, lda, b, ldb,
+                                           static_cast<cudaStream_t>(stream), &ce);
+    return dev_status(rc, ce, err);
 }
 
 }  // extern "C"

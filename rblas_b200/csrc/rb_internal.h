@@ -56,15 +56,25 @@ uint32_t* device_error_word();
 // k-contiguous (Trans); otherwise m-contiguous (NoTrans). b_kmajor: op(B) is
 // stored k-contiguous (NoTrans); otherwise n-contiguous (Trans).
 // Requirements: A/B 16-byte aligned with lda/ldb*sizeof(T) % 16 == 0.
+// tri: 0 whole C; 1 only the upper triangle (row <= col); 2 only the lower.
 template <typename T>
 cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
                              const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
-                             size_t ldc, cudaStream_t st, CUresult* cu_err);
+                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri = 0);
 
 // C := beta*C over an m x n column-major block (beta == 0 writes zeros
-// without reading; beta == 1 is a no-op and launches nothing).
+// without reading; beta == 1 is a no-op and launches nothing); tri as above.
 template <typename T>
-cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st);
+cudaError_t launch_scale_c(int m, int n, T beta, T* C, size_t ldc, cudaStream_t st, int tri = 0);
+
+// The library's column-major GEMM on device pointers, used by every Level-3
+// routine built on it: C = alpha*op(A)op(B) + beta*C (op = transpose when
+// ta/tb), `prec` an rb_precision value, `tri` as above (plain form only).
+// Returns an rb_status value; *cuda_err receives the CUDA/driver code.
+template <typename T>
+int gemm_colmajor_dev(bool ta, bool tb, size_t m, size_t n, size_t k, T alpha, const T* A,
+                      size_t lda, const T* B, size_t ldb, T beta, T* C, size_t ldc, int prec,
+                      cudaStream_t st, int tri, int32_t* cuda_err);
 
 // BF16-split SGEMM on tcgen05 (kind::f16): planes == 2 is 3xBF16
 // (hi*hi + hi*lo + lo*hi), planes == 3 is the 6-product form over hi/mid/lo.
@@ -79,6 +89,26 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
 cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A,
                               size_t lda, const double* B, size_t ldb, double beta, double* C,
                               size_t ldc, int slices, cudaStream_t st, CUresult* cu_err);
+
+// ---- Level-3 routines on device pointers (all column-major; complex
+// operands interleaved {re, im}; return rb_status values) -------------------
+template <typename T>
+int complex_gemm_dev(int transa, int transb, size_t m, size_t n, size_t k, T ar, T ai, const T* A,
+                     size_t lda, const T* B, size_t ldb, T br, T bi, T* C, size_t ldc, int prec,
+                     cudaStream_t st, int32_t* ce);
+template <typename T>
+int syrk_dev(int uplo, int trans, size_t n, size_t k, T alpha, const T* A, size_t lda, T beta, T* C,
+             size_t ldc, cudaStream_t st, int32_t* ce);
+template <typename T>
+int symm_dev(int side, int uplo, size_t m, size_t n, T alpha, const T* A, size_t lda, const T* B,
+             size_t ldb, T beta, T* C, size_t ldc, int prec, cudaStream_t st, int32_t* ce);
+template <typename T>
+int hesy_dev(int herm, int side, int uplo, size_t m, size_t n, T ar, T ai, const T* A, size_t lda,
+             const T* B, size_t ldb, T br, T bi, T* C, size_t ldc, int prec, cudaStream_t st,
+             int32_t* ce);
+template <typename T, bool CX>
+int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A,
+             size_t lda, T* B, size_t ldb, cudaStream_t st, int32_t* ce);
 
 // Tensor-pipe throughput (TFLOP/s or TOP/s) of back-to-back M128 N256 UMMAs
 // on every SM: i8 != 0 -> kind::i8, else kind::f16 (bf16).

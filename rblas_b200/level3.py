@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from .types import Layout, Precision, Transpose
 
-__all__ = ["gemm", "try_gemm", "gemm_dev"]
+__all__ = ["gemm", "try_gemm", "gemm_dev", "syrk", "symm", "trsm"]
 
 
 def _as_slice(x, dtype, name, writable=False):
@@ -72,4 +72,59 @@ def gemm_dev(layout, transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, bet
     st = fn(int(Layout(layout)), int(Transpose(transa)), int(Transpose(transb)), m, n, k, alpha,
             C.c_void_p(a_ptr), lda, C.c_void_p(b_ptr), ldb, beta, C.c_void_p(c_ptr), ldc,
             int(Precision(prec)), C.c_void_p(stream) if stream else None, C.byref(err))
+    _lib.check(st, err)
+
+
+def _real_fn(lib, dt, name):
+    return getattr(lib, ("rb_s" if dt == np.float32 else "rb_d") + name)
+
+
+def _dtype_of(c):
+    dt = c.dtype if isinstance(c, np.ndarray) else None
+    if dt not in (np.float32, np.float64):
+        raise TypeError("real routines take float32 or float64 slices")
+    return dt
+
+
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """level3::syrk (src/level3.rs:236-294): C := alpha*op(A)*op(A)^T + beta*C
+    on the `uplo` triangle of the n x n C (op(A) is n x k)."""
+    from .types import Uplo
+    dt = _dtype_of(c)
+    a = _as_slice(a, dt, "a")
+    c = _as_slice(c, dt, "c", writable=True)
+    lib = _lib.load()
+    err = _lib.RbError()
+    st = _real_fn(lib, dt, "syrk")(int(Uplo(uplo)), int(Transpose(trans)), n, k, alpha, _ptr(a), lda,
+                                   a.size, beta, _ptr(c), ldc, c.size, C.byref(err))
+    _lib.check(st, err)
+
+
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    """level3::symm (src/level3.rs:301-354): A symmetric (uplo triangle
+    stored); C := alpha*A*B + beta*C (Left) or alpha*B*A + beta*C (Right)."""
+    from .types import Side, Uplo
+    dt = _dtype_of(c)
+    a = _as_slice(a, dt, "a")
+    b = _as_slice(b, dt, "b")
+    c = _as_slice(c, dt, "c", writable=True)
+    lib = _lib.load()
+    err = _lib.RbError()
+    st = _real_fn(lib, dt, "symm")(int(Side(side)), int(Uplo(uplo)), m, n, alpha, _ptr(a), lda, a.size,
+                                   _ptr(b), ldb, b.size, beta, _ptr(c), ldc, c.size, C.byref(err))
+    _lib.check(st, err)
+
+
+def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    """level3::trsm (src/level3.rs:390-437): solve op(A)*X = alpha*B (Left)
+    or X*op(A) = alpha*B (Right) in place of B."""
+    from .types import Diag, Side, Uplo
+    dt = _dtype_of(b)
+    a = _as_slice(a, dt, "a")
+    b = _as_slice(b, dt, "b", writable=True)
+    lib = _lib.load()
+    err = _lib.RbError()
+    st = _real_fn(lib, dt, "trsm")(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)),
+                                   int(Diag(diag)), m, n, alpha, _ptr(a), lda, a.size, _ptr(b), ldb,
+                                   b.size, C.byref(err))
     _lib.check(st, err)
