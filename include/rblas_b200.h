@@ -222,10 +222,11 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
  * Library state
  * ------------------------------------------------------------------------- */
 
-/* Number of slices used by RB_PREC_OZAKI (2..12; default 7). Slice 0 is a
- * signed 8-bit digit (7 bits), the rest unsigned 8-bit digits, so s slices
- * carry 7 + 8(s-1) bits of each scaled row/column entry; s(s+1)/2 INT8
- * GEMMs are run. */
+/* Number of slices used by RB_PREC_OZAKI (2..12; default 8). Each scaled
+ * row/column entry y in (-1/2, 1/2) is cut into signed 8-bit digits of
+ * weight 2^-(7+8t) (the leading one in [-64, 64], the rest balanced in
+ * [-128, 127]), so s slices carry about 7 + 8(s-1) bits; the s(s+1)/2 digit
+ * products of weight index <= s-1 are computed. */
 rb_status rb_set_ozaki_slices(int slices);
 int rb_get_ozaki_slices(void);
 

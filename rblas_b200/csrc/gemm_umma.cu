@@ -263,14 +263,14 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // ------------------------------------------------------------------------------
 // Ozaki GEMM kernel.
 //
-// Slice products of equal weight (t + u = d: slice t has weight 2^-(7+8t))
+// Slice products of equal weight (t + u = d: digit t has weight 2^-(7+8t))
 // form diagonal d; S_d = sum_{t+u=d} A_t B_u^T is exact in INT32 over a K
 // chunk. Diagonals are processed two at a time ("units" {d0, d0+1}) with
 // both accumulators in TMEM (2 x 256 columns): for each B slice j the stage
 // holds B_j and the two A slices it pairs with, A_{d0-j} -> S_d0 and
 // A_{d0+1-j} -> S_{d0+1}, so every B tile feeds two MMAs. The epilogue
 // folds the unit exactly, S_d0 * 2^8 + S_{d0+1} (< 2^40), scales by
-// alpha * 2^(e_i + f_j - 14 - 8(d0+1)) and accumulates into C in FP64;
+// alpha * 2^(e_i + f_j + 2 - 14 - 8(d0+1)) and accumulates into C in FP64;
 // units run from the smallest weight up, the first one adding beta*C0.
 // Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 epilogue (two
 // warps per TMEM lane quarter, 128 columns each).
@@ -394,12 +394,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 uint32_t acc0 = 0, acc1 = 0;
                 for (int j = 0; ok && j <= jmax; ++j) {
                     const bool a0 = j <= d0, a1 = d1 >= 0;
-                    // slice 0 is signed, the others unsigned
-                    const uint32_t fb = (j == 0) ? 1u : 0u;
-                    const uint32_t id0 = (2u << 4) | ((d0 - j == 0 ? 1u : 0u) << 7) | (fb << 10) |
-                                         (static_cast<uint32_t>(UN >> 3) << 17) | (static_cast<uint32_t>(kUM >> 4) << 24);
-                    const uint32_t id1 = (2u << 4) | ((d1 - j == 0 ? 1u : 0u) << 7) | (fb << 10) |
-                                         (static_cast<uint32_t>(UN >> 3) << 17) | (static_cast<uint32_t>(kUM >> 4) << 24);
+                    constexpr uint32_t id0 = umma_idesc(2, 1, kUM, UN);  // s32 <- s8 x s8
+                    constexpr uint32_t id1 = id0;
                     for (int kt = kt0; kt < kt1; ++kt, ++it) {
                         const int s = it % ST;
                         if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x303)) {
@@ -452,7 +448,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 tc_fence_after();
                 const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
                 const bool first_unit = (u == 0);
-                const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0);
+                // digits of both operands are scaled by 2^-(e+1): weight 2^-(14+8d) per diagonal
+                const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0) - 2;
 #pragma unroll 1
                 for (int ch = 0; ch < 4; ++ch) {
                     const int col0 = half * 128 + ch * 32;
@@ -568,14 +565,18 @@ __device__ __forceinline__ void load_tile(const T* __restrict__ x, size_t rs, si
     }
 }
 
-// Ozaki slicing: x(r,q) * 2^-e[r] in (-1, 1) is cut into
-//   sigma_0 = floor(x * 2^7)          in [-128, 127]  (signed int8),
-//   sigma_t = floor(rem_{t-1} * 2^8)  in [0, 255]     (unsigned, t >= 1),
-// with rem in [0, 1); every step is exact in FP64, and
-// x * 2^-e = sum_t sigma_t 2^-(7+8t) + (remainder < 2^-(7+8(s-1))).
+// Ozaki slicing. With e[r] the row exponent (|x| < 2^e), y = x * 2^-(e+1)
+// lies in (-1/2, 1/2). Digits are extracted exactly in FP64,
+//   d_0 = floor(y * 2^7) in [-64, 63],  d_t = floor(rem * 2^8) in [0, 255],
+// then balanced from the least significant up: d_t >= 128 becomes
+// d_t - 256 with a carry of 1 into d_{t-1} (d_0 <= 64 after the carry).
+// The result: signed 8-bit digits with y = sum_t d_t 2^-(7+8t) + rem,
+// 0 <= rem < 2^-(7+8(s-1)), and tail digits that are symmetric about zero,
+// so the dropped cross products do not accumulate a bias along K.
+constexpr int kMaxSlices = 12;
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
                                                           int R, int K, const int* __restrict__ e,
-                                                          int slices, uint8_t* __restrict__ out, size_t kp,
+                                                          int slices, int8_t* __restrict__ out, size_t kp,
                                                           size_t plane) {
     __shared__ double tile[kTile][kTile + 1];
     const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
@@ -584,23 +585,44 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;  // 64 rows x 4 chunks of 16
     if (r0 + r >= R) return;
     const int er = e[r0 + r];
-    double xs[16];
+    uint32_t w[kMaxSlices][4];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) xs[i] = (er == kExpSentinel) ? 0.0 : scalbn(tile[r][c * 16 + i], -er);
-    for (int t = 0; t < slices; ++t) {
-        uint32_t w[4] = {0u, 0u, 0u, 0u};
-        const double scale = (t == 0) ? 128.0 : 256.0;
+    for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
+#pragma unroll 1
+    for (int i = 0; i < 16; ++i) {
+        const double y = (er == kExpSentinel) ? 0.0 : scalbn(tile[r][c * 16 + i], -(er + 1));
+        int d[kMaxSlices];
+        double v = y * 128.0;
+        double f = floor(v);
+        d[0] = static_cast<int>(f);
+        double rem = v - f;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const double v = xs[i] * scale;
-            const double f = floor(v);
-            xs[i] = v - f;
-            w[i >> 2] |= (static_cast<uint32_t>(static_cast<int>(f)) & 0xFFu) << (8 * (i & 3));
+        for (int t = 1; t < kMaxSlices; ++t) {
+            if (t < slices) {
+                v = rem * 256.0;
+                f = floor(v);
+                d[t] = static_cast<int>(f);
+                rem = v - f;
+            } else {
+                d[t] = 0;
+            }
         }
-        const size_t off = t * plane + static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
-        if (p0 + c * 16 < static_cast<int>(kp))
-            *reinterpret_cast<uint4*>(out + off) = make_uint4(w[0], w[1], w[2], w[3]);
+#pragma unroll
+        for (int t = kMaxSlices - 1; t >= 1; --t) {
+            if (d[t] >= 128) {
+                d[t] -= 256;
+                d[t - 1] += 1;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < kMaxSlices; ++t)
+            w[t][i >> 2] |= (static_cast<uint32_t>(d[t]) & 0xFFu) << (8 * (i & 3));
     }
+    if (p0 + c * 16 >= static_cast<int>(kp)) return;
+    const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
+#pragma unroll
+    for (int t = 0; t < kMaxSlices; ++t)
+        if (t < slices) *reinterpret_cast<uint4*>(out + t * plane + off) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
 }
 
 // BF16 split into `planes` (2 or 3) planes: out[0] = bf16(x),
@@ -802,8 +824,8 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     if (e != cudaSuccess) return e;
     int* ea = static_cast<int*>(buf);
     int* eb = ea + m;
-    uint8_t* sla = static_cast<uint8_t*>(buf) + exps;
-    uint8_t* slb = sla + a_bytes;
+    int8_t* sla = reinterpret_cast<int8_t*>(static_cast<uint8_t*>(buf) + exps);
+    int8_t* slb = sla + a_bytes;
     size_t ars, aps, brs, bps;
     operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
     fill_int_kernel<<<64, 256, 0, st>>>(ea, m + n, kExpSentinel);
@@ -832,8 +854,8 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 127) / 128);
     p.slices = slices;
-    // exact INT32: a diagonal has <= slices products of <= 255*255 per K element
-    const long long max_k = 2147483647LL / (static_cast<long long>(slices) * 255 * 255);
+    // exact INT32: a diagonal has <= slices products of |d_t d_u| <= 128*128 per K element
+    const long long max_k = 2147483647LL / (static_cast<long long>(slices) * 128 * 128);
     p.kt_per_chunk = static_cast<int>(max_k / 128);
     if (p.kt_per_chunk < 1) p.kt_per_chunk = 1;
     p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;

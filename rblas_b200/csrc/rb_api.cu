@@ -56,7 +56,7 @@ void kernel_timing_end(KernelTimer* t, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(g_timing_mu);
     g_timed.push_back(L);
 }
-static std::atomic<int> g_ozaki_slices{7};
+static std::atomic<int> g_ozaki_slices{8};
 static int ozaki_slices() { return g_ozaki_slices.load(); }
 
 namespace {
