@@ -63,7 +63,8 @@ typedef enum {
     RB_ERR_TIMEOUT = 8,             /* a bounded device-side wait gave up */
     RB_ERR_DEVICE = 9,              /* a kernel reported an error word */
     RB_ERR_BUSY = 10,               /* admission refused (serving budget) */
-    RB_ERR_CANCELLED = 11           /* request cancelled before it ran */
+    RB_ERR_CANCELLED = 11,          /* request cancelled before it ran */
+    RB_ERR_SCRATCH_LIMIT = 12       /* problem needs more than the fixed no-allocation scratch */
 } rb_status;
 
 /* Mirrors BlasError's fields: which operand ('a', 'b', 'c', 'x', 'y'),
@@ -217,6 +218,39 @@ rb_status rb_ztrsm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag,
 rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
                        size_t n, double alpha, const double* a, size_t lda, double* b, size_t ldb,
                        void* stream, rb_error* err);
+
+/* ---------------------------------------------------------------------------
+ * Allocation-free DGEMM (no counterpart in the reference: rblas runs on the
+ * CPU and never touches device memory).
+ * ------------------------------------------------------------------------- */
+
+/* Ozaki INT8 DGEMM on device pointers that never allocates: no cudaMalloc,
+ * cudaMallocAsync, cudaFree or allocating library call, in this call or on
+ * its behalf. For callers that cannot have a library allocate device memory:
+ * a process that reserved all of the GPU's memory for its own pool up front,
+ * or a latency-critical path where an allocation could block on the device
+ * or fail in the middle of a run. All scratch (digit planes, exponents, the
+ * kernels' status word) comes from one fixed 64 MiB + 64 KiB device array
+ * that every GPU loading this library holds until the process exits.
+ *   - Same arithmetic and result as rb_dgemm_dev(..., RB_PREC_OZAKI, ...)
+ *     with the current rb_get_ozaki_slices() count; a, b, c, lda/ldb/ldc as
+ *     there, enqueued on `stream` (NULL = legacy default stream).
+ *   - Limit: 256 + (m+n)*4 + slices*(m+n)*round_up(k,16) bytes (each part
+ *     rounded up to 256) must fit the array -- e.g. m = n = k = 2048 at 8
+ *     slices; larger problems get RB_ERR_SCRATCH_LIMIT (err->got = bytes
+ *     needed, err->min_or_need = bytes available) and touch nothing.
+ *   - The first call on a device, with that device current, looks up the
+ *     array's device address (cudaGetSymbolAddress); make that first call
+ *     before any stream capture.
+ *   - Every call shares the array and leaves its contents behind: calls whose
+ *     work overlaps on the GPU (different streams, or different host threads)
+ *     race on it. The call clears the status word it needs, and returns after
+ *     its stream has finished the work, reporting RB_ERR_TIMEOUT /
+ *     RB_ERR_DEVICE from the kernels' status word. */
+rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose transa, rb_transpose transb,
+                                 size_t m, size_t n, size_t k, double alpha, const double* a,
+                                 size_t lda, const double* b, size_t ldb, double beta, double* c,
+                                 size_t ldc, void* stream, rb_error* err);
 
 /* ---------------------------------------------------------------------------
  * Library state

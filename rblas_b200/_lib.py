@@ -61,6 +61,7 @@ SIGNATURES = {
     "rb_ctrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_dtrsm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_dgemm_ozaki_noalloc": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _vp, _perr]),
     "rb_set_ozaki_slices": (_i, [_i]),
     "rb_get_ozaki_slices": (_i, []),
     "rb_launch_count": (C.c_uint64, []),

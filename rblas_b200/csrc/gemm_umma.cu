@@ -35,6 +35,9 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
+#include "../../include/rblas_b200.h"
 #include "rb_device.cuh"
 #include "rb_internal.h"
 
@@ -887,3 +890,161 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
 }
 
 }  // namespace rb
+
+// ==============================================================================
+// Allocation-free Ozaki DGEMM.
+//
+// Some callers cannot let a library call cudaMalloc: a serving process that
+// has handed all of the GPU's memory to its own pool up front, or code on a
+// latency-critical path where an allocation could block on the device or fail
+// halfway through a run. For them, rb_dgemm_ozaki_noalloc runs the same
+// Ozaki kernels as rb_dgemm_dev(..., RB_PREC_OZAKI, ...) with every scratch
+// buffer (digit planes, exponents, the device status word) carved out of the
+// fixed array below. The array is a file-scope __device__ object: every GPU
+// that loads this library holds its 64 MiB + 64 KiB until the process exits.
+// In host code `g_noalloc_scratch` is only a host-side stand-in for the
+// symbol, so its device address is looked up with cudaGetSymbolAddress, once
+// per device, on the first call made with that device current.
+// ==============================================================================
+
+namespace rb {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (64u << 20) + (64u << 10);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+size_t noalloc_bytes_needed(size_t m, size_t n, size_t kp, int slices) {
+    return 256 + round_up((m + n) * sizeof(int), 256) + round_up(slices * m * kp, 256) + slices * n * kp;
+}
+
+}  // namespace
+}  // namespace rb
+
+extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose transa, rb_transpose transb,
+                                            size_t m, size_t n, size_t k, double alpha, const double* a,
+                                            size_t lda, const double* b, size_t ldb, double beta, double* c,
+                                            size_t ldc, void* stream, rb_error* err) {
+    using namespace rb;
+    auto fail = [&](rb_status s, uint64_t got = 0, uint64_t need = 0, int32_t ce = 0, char which = 0) {
+        if (err) {
+            err->code = s;
+            err->which = which;
+            err->got = got;
+            err->min_or_need = need;
+            err->cuda_error = ce;
+        }
+        return s;
+    };
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if ((layout != RB_ROW_MAJOR && layout != RB_COL_MAJOR) || transa < RB_NO_TRANS || transa > RB_CONJ_TRANS ||
+        transb < RB_NO_TRANS || transb > RB_CONJ_TRANS)
+        return fail(RB_ERR_INVALID_ARG);
+    // leading dimensions, as check_matrix (src/level3.rs:107-140)
+    const bool ta = transa != RB_NO_TRANS, tb = transb != RB_NO_TRANS;
+    struct Chk { char w; size_t rows, cols, ld; } chk[3] = {
+        {'a', ta ? k : m, ta ? m : k, lda}, {'b', tb ? n : k, tb ? k : n, ldb}, {'c', m, n, ldc}};
+    for (const Chk& q : chk) {
+        if (q.rows == 0 || q.cols == 0) continue;
+        const size_t min_lead = (layout == RB_ROW_MAJOR) ? q.cols : q.rows;
+        if (q.ld < min_lead) return fail(RB_ERR_INVALID_LEADING_DIM, q.ld, min_lead, 0, q.w);
+    }
+    if (m == 0 || n == 0) return RB_OK;
+    // row-major -> column-major by swapping operands (src/level3.rs:52-60)
+    bool cta = ta, ctb = tb;
+    size_t cm = m, cn = n, clda = lda, cldb = ldb;
+    const double* ca = a;
+    const double* cb = b;
+    if (layout == RB_ROW_MAJOR) {
+        cta = tb; ctb = ta;
+        cm = n; cn = m;
+        ca = b; cb = a;
+        clda = ldb; cldb = lda;
+    }
+    if (cm > 0x7fffffff || cn > 0x7fffffff || k > 0x7fffffff) return fail(RB_ERR_INVALID_ARG);
+    const int slices = rb_get_ozaki_slices();
+    const size_t kp = round_up(k, 16);
+    const size_t need = noalloc_bytes_needed(cm, cn, kp, slices);
+    if (need > kNoAllocScratchBytes) return fail(RB_ERR_SCRATCH_LIMIT, need, kNoAllocScratchBytes);
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) return fail(RB_ERR_CUDA, 0, 0, e);
+    uint8_t* base;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) return fail(RB_ERR_CUDA, 0, 0, e);
+            g_noalloc_ptr[dev] = p;
+        }
+        base = static_cast<uint8_t*>(g_noalloc_ptr[dev]);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t* status = reinterpret_cast<uint32_t*>(base);
+    e = cudaMemsetAsync(status, 0, sizeof(uint32_t), st);  // the previous call's word is stale
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
+
+    if (k == 0 || alpha == 0.0) {
+        e = launch_scale_c<double>(static_cast<int>(cm), static_cast<int>(cn), beta, c, ldc, st);
+    } else {
+        const int M = static_cast<int>(cm), N = static_cast<int>(cn), K = static_cast<int>(k);
+        const size_t exps = round_up((cm + cn) * sizeof(int), 256);
+        const size_t pa = cm * kp, pb = cn * kp;
+        int* ea = reinterpret_cast<int*>(base + 256);
+        int* eb = ea + cm;
+        int8_t* sla = reinterpret_cast<int8_t*>(base + 256 + exps);
+        int8_t* slb = sla + round_up(slices * pa, 256);
+        size_t ars, aps, brs, bps;
+        operand_views(cta, ctb, clda, cldb, ars, aps, brs, bps);
+        fill_int_kernel<<<64, 256, 0, st>>>(ea, M + N, kExpSentinel);
+        const int kb = (K + 1023) / 1024, k32 = (K + 31) / 32;
+        if (aps == 1) row_exp_kcontig_kernel<<<dim3((M + 7) / 8, kb), 256, 0, st>>>(ca, ars, M, K, ea);
+        else          row_exp_rcontig_kernel<<<dim3((M + 255) / 256, k32), 256, 0, st>>>(ca, aps, M, K, ea);
+        if (bps == 1) row_exp_kcontig_kernel<<<dim3((N + 7) / 8, kb), 256, 0, st>>>(cb, brs, N, K, eb);
+        else          row_exp_rcontig_kernel<<<dim3((N + 255) / 256, k32), 256, 0, st>>>(cb, bps, N, K, eb);
+        const dim3 ga((kp + kTile - 1) / kTile, (M + kTile - 1) / kTile);
+        const dim3 gb((kp + kTile - 1) / kTile, (N + kTile - 1) / kTile);
+        ozaki_slice_kernel<<<ga, 256, 0, st>>>(ca, ars, aps, M, K, ea, slices, sla, kp, pa);
+        ozaki_slice_kernel<<<gb, 256, 0, st>>>(cb, brs, bps, N, K, eb, slices, slb, kp, pb);
+        count_launch(5);
+        CUtensorMap tma, tmb;
+        CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, K, M, slices, kp, kUM);
+        if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, K, N, slices, kp, 256);
+        if (r != CUDA_SUCCESS) return fail(RB_ERR_CUDA, 0, 0, static_cast<int32_t>(r));
+        OzParams p{};
+        p.m = M; p.n = N; p.k = K;
+        p.tiles_m = (M + kUM - 1) / kUM;
+        p.tiles_n = (N + 255) / 256;
+        p.num_tiles = p.tiles_m * p.tiles_n;
+        p.num_kt = (K + 127) / 128;
+        p.slices = slices;
+        const long long max_k = 2147483647LL / (static_cast<long long>(slices) * 128 * 128);
+        p.kt_per_chunk = static_cast<int>(max_k / 128) > 0 ? static_cast<int>(max_k / 128) : 1;
+        p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
+        p.beta_mode = (beta == 0.0) ? 0 : (beta == 1.0 ? 1 : 2);
+        p.alpha = alpha; p.beta = beta;
+        p.c = c; p.ldc = ldc;
+        p.row_exp = ea; p.col_exp = eb;
+        p.err = status;
+        constexpr int smem = kOzST * kOzStage + 256 + 1024;
+        e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        ozaki_gemm_kernel<<<p.num_tiles < sms ? p.num_tiles : sms, kOzThreads, smem, st>>>(tma, tmb, p);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
+    // The call returns once its work has finished, with the kernels' status word read back.
+    uint32_t word = 0;
+    e = cudaMemcpyAsync(&word, status, sizeof(word), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
+    if (word != 0) return fail((word >> 24) == (RB_DEVERR_TIMEOUT >> 24) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE, word);
+    return RB_OK;
+}

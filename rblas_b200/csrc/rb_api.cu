@@ -505,6 +505,7 @@ const char* rb_status_string(int32_t status) {
         case RB_ERR_DEVICE: return "device-side error";
         case RB_ERR_BUSY: return "admission refused";
         case RB_ERR_CANCELLED: return "cancelled";
+        case RB_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed scratch of the allocation-free entry point";
         default: return "unknown status";
     }
 }
