@@ -424,6 +424,95 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------
+# serving: the request stream of the serving configuration
+# --------------------------------------------------------------------------
+
+def serving_trace(n_req, seed=5):
+    """Request shapes of the serving configuration: m, n, k log-uniform in
+    [32, 4096], dtype 50/50 f32/f64, layout and transposes uniform, alpha and
+    beta uniform in [-2, 2]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(32), np.log(4096)
+    mnk = np.exp(rng.uniform(lo, hi, (n_req, 3))).astype(np.int64)
+    return dict(mnk=mnk, dtype=rng.integers(0, 2, n_req), layout=rng.integers(0, 2, n_req),
+                ta=rng.integers(0, 3, n_req), tb=rng.integers(0, 3, n_req),
+                alpha=rng.uniform(-2, 2, n_req), beta=rng.uniform(-2, 2, n_req),
+                offs=rng.integers(0, 1 << 20, (n_req, 3)))
+
+
+def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5):
+    """Replay a Poisson stream of n_req requests at each rate through the
+    server in grouped mode and in per-request mode. Operands are standard
+    normal values resident in HBM (pools the requests point into)."""
+    from rblas_b200.serving import Problem, Server
+
+    tr = serving_trace(n_req, seed)
+    big = 4096 * 4096
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    pools = {0: torch.randn(big + (1 << 22), dtype=torch.float32, device="cuda", generator=g),
+             1: torch.randn(big + (1 << 22), dtype=torch.float64, device="cuda", generator=g)}
+    problems, flops = [], 0.0
+    for i in range(n_req):
+        m, n, k = (int(x) for x in tr["mnk"][i])
+        dt = int(tr["dtype"][i])
+        vec = 4 if dt == 0 else 2
+        layout, ta, tb = int(tr["layout"][i]), int(tr["ta"][i]), int(tr["tb"][i])
+        ar, ac = (k, m) if ta else (m, k)
+        br, bc = (n, k) if tb else (k, n)
+        pad = lambda x: (x + vec - 1) // vec * vec
+        lda = pad(ar) if layout == 1 else pad(ac)
+        ldb = pad(br) if layout == 1 else pad(bc)
+        ldc = pad(m) if layout == 1 else pad(n)
+        base = pools[dt].data_ptr()
+        es = 4 if dt == 0 else 8
+        offs = [int(o) // 16 * 16 for o in tr["offs"][i]]  # 16-element aligned
+        problems.append(Problem(np.float32 if dt == 0 else np.float64, layout, ta, tb, m, n, k,
+                                float(tr["alpha"][i]), base + offs[0] * es, lda, base + offs[1] * es, ldb,
+                                float(tr["beta"][i]), base + offs[2] * es, ldc))
+        flops += 2.0 * m * n * k
+    out = {"requests": n_req, "flop": flops, "budget_bytes": budget, "max_batch": max_batch, "rates": []}
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(1.0, n_req)
+    for rate in rates:
+        arrivals = (np.cumsum(gaps) / rate * 1e9).astype(np.uint64)
+        row = {"rate_req_s": rate}
+        for mode, grouped in (("grouped", True), ("per_request", False)):
+            # both modes admit the same sets; per-request mode launches the
+            # single-problem kernel once per request, grouped mode once per set
+            with Server(budget_bytes=budget, max_batch=max_batch, grouped=grouped) as srv:
+                st, times = srv.run_trace(problems, arrivals)
+            lat = (times[:, 2].astype(np.int64) - times[:, 0].astype(np.int64)) / 1e6
+            span = (int(times[:, 2].max()) - int(times[:, 0].min())) / 1e9
+            row[mode] = {"status": int(st), "tflops": flops / span / 1e12, "span_s": span,
+                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+        out["rates"].append(row)
+    # throughput at equal p99: the per-request mode's best rate that kept up
+    # (p99 < 1 s) sets the latency bar; the grouped mode's best throughput
+    # within that bar is compared with it.
+    pr = [r for r in out["rates"] if r["per_request"]["p99_ms"] < 1000.0] or out["rates"]
+    best_pr = max(pr, key=lambda r: r["per_request"]["tflops"])
+    bar = best_pr["per_request"]["p99_ms"]
+    gr = [r for r in out["rates"] if r["grouped"]["p99_ms"] <= bar]
+    best_gr = max(gr, key=lambda r: r["grouped"]["tflops"]) if gr else None
+    out["equal_p99"] = {"p99_bar_ms": bar, "per_request_tflops": best_pr["per_request"]["tflops"],
+                        "grouped_tflops": best_gr["grouped"]["tflops"] if best_gr else None,
+                        "ratio": (best_gr["grouped"]["tflops"] / best_pr["per_request"]["tflops"])
+                        if best_gr else None}
+    del pools
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serve_mode(args):
+    import torch
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.rates.split(",")]
+    res = run_serving(torch, rates, args.requests, int(args.budget_gb * (1 << 30)))
+    print(json.dumps({"serving": res}))
+
+
 def run_kernel_only(args):
     """One GEMM shape, launched warmup + steps times on the device (for ncu
     captures of a single kernel on a bounded case)."""
@@ -470,10 +559,16 @@ def main():
     ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,
                     metavar=("M", "N", "K"), help="time one column-major GEMM shape only")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--serve", action="store_true", help="serving sweep (request stream replay)")
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--rates", default="1000,5000,10000,20000,50000")
+    ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--ta", type=int, default=0)
     ap.add_argument("--tb", type=int, default=0)
     args = ap.parse_args()
-    if args.shape:
+    if args.serve:
+        run_serve_mode(args)
+    elif args.shape:
         run_kernel_only(args)
     elif args.impl == "reference":
         run_reference(args)

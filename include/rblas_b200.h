@@ -220,6 +220,64 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                        void* stream, rb_error* err);
 
 /* ---------------------------------------------------------------------------
+ * Grouped GEMM and the serving loop (no counterpart in the reference: rblas
+ * is a synchronous library; these are the batching and serving forms of its
+ * gemm, level3::gemm src/level3.rs:32-62, on device-resident operands).
+ * ------------------------------------------------------------------------- */
+
+/* One GEMM of a group: C := alpha*op(A)*op(B) + beta*C with device pointers,
+ * any layout / transposes, dtype 0 = f32, 1 = f64 (plain form). */
+typedef struct {
+    int32_t dtype;
+    int32_t layout, transa, transb;
+    size_t m, n, k;
+    double alpha, beta;
+    const void* a;
+    size_t lda;
+    const void* b;
+    size_t ldb;
+    void* c;
+    size_t ldc;
+} rb_gemm_problem;
+
+/* Runs every problem of the table in one persistent launch (a device-side
+ * problem table with per-problem TMA descriptors; tiles of all problems
+ * stream through one pipeline per SM). Problems with m == 0 or n == 0 are
+ * skipped; k == 0 or alpha == 0 only scale C. On a validation error
+ * err->got is the index of the offending problem. Enqueued on `stream`. */
+rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, void* stream,
+                              rb_error* err);
+
+/* Per-request timestamps (CLOCK_MONOTONIC ns): submitted, admitted into a
+ * batch (result memory reserved), finished (batch completion observed). */
+typedef struct {
+    uint64_t enqueue_ns, admit_ns, finish_ns;
+} rb_request_times;
+
+/* A serving loop on the current device. budget_bytes of HBM are reserved
+ * up front for results; a request is admitted when its result fits the
+ * budget and a batch slot is free (max_batch requests per launch).
+ * grouped = 1 packs each admitted set into one grouped launch; grouped = 0
+ * launches every request on its own (the per-request baseline). */
+rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void** server);
+/* Queue D = alpha*op(A)*op(B) + beta*C0 where p->c is the device-resident
+ * C0 (read only when beta != 0) and D is allocated by the server with C's
+ * layout. Returns at once; RB_ERR_BUSY if D could never fit the budget. */
+rb_status rb_server_submit(void* server, const rb_gemm_problem* p, uint64_t* id);
+/* Wait for a request (timeout_us < 0: forever; 0: poll). On RB_OK, *d_out /
+ * *ldd give the result in HBM (valid until rb_server_release). */
+rb_status rb_server_wait(void* server, uint64_t id, int64_t timeout_us, void** d_out, size_t* ldd,
+                         rb_request_times* times);
+/* Return a finished request's result memory to the budget. */
+rb_status rb_server_release(void* server, uint64_t id);
+rb_status rb_server_destroy(void* server);
+/* Replay a trace: submit problems[i] at arrival_ns[i] after the call starts
+ * (a native thread, so the arrival process is not limited by the caller),
+ * release each result as it finishes, and fill times[i]. */
+rb_status rb_server_run_trace(void* server, const rb_gemm_problem* problems,
+                              const uint64_t* arrival_ns, size_t count, rb_request_times* times);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free DGEMM (no counterpart in the reference: rblas runs on the
  * CPU and never touches device memory).
  * ------------------------------------------------------------------------- */

@@ -24,6 +24,17 @@ class RbError(C.Structure):
                 ("min_or_need", C.c_uint64), ("cuda_error", C.c_int32)]
 
 
+class RbGemmProblem(C.Structure):
+    _fields_ = [("dtype", C.c_int32), ("layout", C.c_int32), ("transa", C.c_int32),
+                ("transb", C.c_int32), ("m", C.c_size_t), ("n", C.c_size_t), ("k", C.c_size_t),
+                ("alpha", C.c_double), ("beta", C.c_double), ("a", C.c_void_p), ("lda", C.c_size_t),
+                ("b", C.c_void_p), ("ldb", C.c_size_t), ("c", C.c_void_p), ("ldc", C.c_size_t)]
+
+
+class RbRequestTimes(C.Structure):
+    _fields_ = [("enqueue_ns", C.c_uint64), ("admit_ns", C.c_uint64), ("finish_ns", C.c_uint64)]
+
+
 class RbComplex32(C.Structure):
     _fields_ = [("re", C.c_float), ("im", C.c_float)]
 
@@ -62,6 +73,15 @@ SIGNATURES = {
     "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_dtrsm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
     "rb_dgemm_ozaki_noalloc": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _vp, _perr]),
+    "rb_gemm_grouped_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _vp, _perr]),
+    "rb_server_create": (_i, [_sz, _i, _i, C.POINTER(C.c_void_p)]),
+    "rb_server_submit": (_i, [_vp, C.POINTER(RbGemmProblem), C.POINTER(C.c_uint64)]),
+    "rb_server_wait": (_i, [_vp, C.c_uint64, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                            C.POINTER(RbRequestTimes)]),
+    "rb_server_release": (_i, [_vp, C.c_uint64]),
+    "rb_server_destroy": (_i, [_vp]),
+    "rb_server_run_trace": (_i, [_vp, C.POINTER(RbGemmProblem), C.POINTER(C.c_uint64), _sz,
+                                 C.POINTER(RbRequestTimes)]),
     "rb_set_ozaki_slices": (_i, [_i]),
     "rb_get_ozaki_slices": (_i, []),
     "rb_launch_count": (C.c_uint64, []),

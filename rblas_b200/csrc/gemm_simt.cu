@@ -21,17 +21,9 @@
 
 #include "rb_device.cuh"
 #include "rb_internal.h"
+#include "simt_tile.cuh"
 
 namespace rb {
-
-template <typename T> struct SimtCfg;
-// f32: 128x128 C tile, 8x8 per thread, BK = 32 (one 128-byte swizzle row).
-template <> struct SimtCfg<float> { static constexpr int BM = 128, BN = 128, BK = 32, TN = 8, STAGES = 4; };
-// f64: 128x64 C tile, 8x4 per thread, BK = 16 (one 128-byte swizzle row).
-template <> struct SimtCfg<double> { static constexpr int BM = 128, BN = 64, BK = 16, TN = 4, STAGES = 4; };
-
-constexpr int kSimtComputeWarps = 8;
-constexpr int kSimtThreads = (kSimtComputeWarps + 1) * 32;
 
 template <typename T>
 struct SimtParams {
@@ -42,41 +34,18 @@ struct SimtParams {
     int tri;        // 0 full C; 1 upper triangle only (row <= col); 2 lower (row >= col)
     T* c;
     size_t ldc;
+    const T* cin;  // C0 read for beta != 0 (== c for the in-place update)
+    size_t ldcin;
     uint32_t* err;
 };
-
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; static constexpr int N = 4; };
-template <> struct Vec16<double> { using type = double2; static constexpr int N = 2; };
-
-template <typename T>
-__device__ __forceinline__ void lds16(const uint8_t* p, T (&v)[Vec16<T>::N]) {
-    const typename Vec16<T>::type x = *reinterpret_cast<const typename Vec16<T>::type*>(p);
-    if constexpr (Vec16<T>::N == 4) {
-        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-    } else {
-        v[0] = x.x; v[1] = x.y;
-    }
-}
-
-template <typename T>
-constexpr int simt_smem_bytes() {
-    using Cfg = SimtCfg<T>;
-    return Cfg::STAGES * (Cfg::BM + Cfg::BN) * Cfg::BK * (int)sizeof(T) + 2 * Cfg::STAGES * 8 + 1024;
-}
 
 template <typename T, bool A_K, bool B_K>
 __global__ void __launch_bounds__(kSimtThreads, 1)
     simt_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const SimtParams<T> p) {
     using Cfg = SimtCfg<T>;
-    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, TN = Cfg::TN, ST = Cfg::STAGES;
-    constexpr int VEC = Vec16<T>::N;                 // elements per 16-byte load
-    constexpr int A_BYTES = BM * BK * sizeof(T);
-    constexpr int B_BYTES = BN * BK * sizeof(T);
-    constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-    static_assert(BK * sizeof(T) == 128, "a K-major tile row must be one 128-byte swizzle row");
-    static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "swizzled tiles need 1 KiB alignment");
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, ST = Cfg::STAGES;
+    constexpr int STAGE_BYTES = simt_stage_bytes<T>();
 
     extern __shared__ uint8_t smem_raw[];
     // Align by offsetting the __shared__ array itself (not through an integer
@@ -103,138 +72,17 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
     }
     __syncthreads();
 
+    uint32_t it = 0;
     if (warp == kSimtComputeWarps) {
-        // ---------------- TMA producer ----------------
         if (lane == 0) {
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            int kt = 0;
-            bool ok = true;
-            for (; kt < num_kt; ++kt) {
-                const int s = kt % ST;
-                if (kt >= ST && !mbar_wait(&empty[s], ((kt / ST) - 1) & 1, p.err, 0x101)) {
-                    ok = false;
-                    break;
-                }
-                uint8_t* sa = smem + s * STAGE_BYTES;
-                uint8_t* sb = sa + A_BYTES;
-                mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-                const int k0 = kt * BK;
-                if (A_K) tma_load_2d(sa, &tmA, &full[s], k0, m0);
-                else     tma_load_2d(sa, &tmA, &full[s], m0, k0);
-                if (B_K) tma_load_2d(sb, &tmB, &full[s], k0, n0);
-                else     tma_load_2d(sb, &tmB, &full[s], n0, k0);
-            }
-            if (!ok) {
-                // let this CTA's own copies land before it exits
-                for (int j = (kt > ST ? kt - ST : 0); j < kt; ++j) mbar_wait_drain(&full[j % ST], (j / ST) & 1);
-            }
+            simt_produce<T, A_K, B_K>(&tmA, &tmB, m0, n0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err);
         }
         return;
     }
-
-    // ---------------- compute warps ----------------
-    const int wm = warp & 1, wn = warp >> 1;         // 2 x 4 warps
-    const int lane_m = lane & 7, lane_n = lane >> 3; // 8 x 4 lanes
-    const int wm0 = wm * 64, wn0 = wn * (4 * TN);
-
-    T acc[8][TN];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
-
-    bool ok = true;
-    for (int kt = 0; kt < num_kt; ++kt) {
-        const int s = kt % ST;
-        if (!mbar_wait(&full[s], (kt / ST) & 1, p.err, 0x102)) {
-            ok = false;
-            break;
-        }
-        const uint8_t* sa = smem + s * STAGE_BYTES;
-        const uint8_t* sb = sa + A_BYTES;
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += VEC) {
-            T a[VEC][8];
-            T b[VEC][TN];
-            const int chunk = kk / VEC;  // 16-byte chunk along k within a 128-byte row
-            if constexpr (A_K) {
-                // [m][k] swizzled: a quarter-warp (same lane_n, lane_m 0..7)
-                // touches 8 rows whose swizzled chunks chunk^lane_m differ.
-#pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const int row = wm0 + lane_m + 8 * r;
-                    T v[VEC];
-                    lds16<T>(sa + row * 128 + ((chunk ^ (row & 7)) << 4), v);
-#pragma unroll
-                    for (int q = 0; q < VEC; ++q) a[q][r] = v[q];
-                }
-            } else {
-                // [k][m]: a quarter-warp reads 8 consecutive 16-byte chunks of one row.
-#pragma unroll
-                for (int q = 0; q < VEC; ++q)
-#pragma unroll
-                    for (int g = 0; g < 8 / VEC; ++g) {
-                        const int col = wm0 + g * 8 * VEC + lane_m * VEC;
-                        T v[VEC];
-                        lds16<T>(sa + ((kk + q) * BM + col) * sizeof(T), v);
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) a[q][g * VEC + e] = v[e];
-                    }
-            }
-            if constexpr (B_K) {
-                // [n][k] swizzled: a quarter-warp shares lane_n -> one address (broadcast).
-#pragma unroll
-                for (int j = 0; j < TN; ++j) {
-                    const int row = wn0 + lane_n * TN + j;
-                    T v[VEC];
-                    lds16<T>(sb + row * 128 + ((chunk ^ (row & 7)) << 4), v);
-#pragma unroll
-                    for (int q = 0; q < VEC; ++q) b[q][j] = v[q];
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < VEC; ++q)
-#pragma unroll
-                    for (int g = 0; g < TN / VEC; ++g) {
-                        const int col = wn0 + g * 4 * VEC + lane_n * VEC;
-                        T v[VEC];
-                        lds16<T>(sb + ((kk + q) * BN + col) * sizeof(T), v);
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) b[q][g * VEC + e] = v[e];
-                    }
-            }
-#pragma unroll
-            for (int q = 0; q < VEC; ++q)
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[q][i], b[q][j], acc[i][j]);
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    if (!ok) return;
-
-    // ---------------- epilogue: C = alpha*acc + beta*C ----------------
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int r = m0 + (A_K ? (wm0 + lane_m + 8 * i)
-                                : (wm0 + (i / VEC) * 8 * VEC + lane_m * VEC + (i % VEC)));
-        if (r >= p.m) continue;
-#pragma unroll
-        for (int j = 0; j < TN; ++j) {
-            const int cidx = n0 + (B_K ? (wn0 + lane_n * TN + j)
-                                       : (wn0 + (j / VEC) * 4 * VEC + lane_n * VEC + (j % VEC)));
-            if (cidx >= p.n) continue;
-            if ((p.tri == 1 && r > cidx) || (p.tri == 2 && r < cidx)) continue;
-            T* cp = p.c + r + static_cast<size_t>(cidx) * p.ldc;
-            T t = T(0);
-            if (p.beta_mode == 1) t = *cp;
-            else if (p.beta_mode == 2) t = p.beta * *cp;
-            *cp = fma(p.alpha, acc[i][j], t);
-        }
-    }
+    const SimtOut<T> o{p.c, p.ldc, p.cin, p.ldcin, p.m, p.n, p.alpha, p.beta, p.beta_mode, p.tri};
+    simt_consume<T, A_K, B_K>(o, m0, n0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err, warp, lane);
 }
 
 template <typename T>
@@ -288,7 +136,8 @@ static cudaError_t launch_variant(const CUtensorMap& ta, const CUtensorMap& tb, 
 template <typename T>
 cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
                              const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
-                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri) {
+                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri, const T* Cin,
+                             size_t ldcin) {
     using Cfg = SimtCfg<T>;
     CUtensorMap ta, tb;
     CUresult r;
@@ -313,6 +162,8 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
     p.beta_mode = (beta == T(0)) ? 0 : (beta == T(1) ? 1 : 2);
     p.tri = tri;
     p.c = C; p.ldc = ldc;
+    p.cin = Cin ? Cin : C;
+    p.ldcin = Cin ? ldcin : ldc;
     p.err = device_error_word();
     if (!p.err) return cudaErrorMemoryAllocation;
     if (a_kmajor) {
@@ -325,10 +176,10 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
 
 template cudaError_t launch_simt_gemm<float>(bool, bool, int, int, int, float, const float*, size_t,
                                              const float*, size_t, float, float*, size_t, cudaStream_t,
-                                             CUresult*, int);
+                                             CUresult*, int, const float*, size_t);
 template cudaError_t launch_simt_gemm<double>(bool, bool, int, int, int, double, const double*, size_t,
                                               const double*, size_t, double, double*, size_t,
-                                              cudaStream_t, CUresult*, int);
+                                              cudaStream_t, CUresult*, int, const double*, size_t);
 template cudaError_t launch_scale_c<float>(int, int, float, float*, size_t, cudaStream_t, int);
 template cudaError_t launch_scale_c<double>(int, int, double, double*, size_t, cudaStream_t, int);
 

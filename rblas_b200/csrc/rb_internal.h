@@ -10,6 +10,8 @@
 #include <atomic>
 #include <mutex>
 
+#include "../../include/rblas_b200.h"
+
 // Device error word layout: [31:24] kind, [23:0] site.
 #define RB_DEVERR_TIMEOUT 0x01000000u
 #define RB_DEVERR_BOUNDS 0x02000000u
@@ -57,10 +59,12 @@ uint32_t* device_error_word();
 // stored k-contiguous (NoTrans); otherwise n-contiguous (Trans).
 // Requirements: A/B 16-byte aligned with lda/ldb*sizeof(T) % 16 == 0.
 // tri: 0 whole C; 1 only the upper triangle (row <= col); 2 only the lower.
+// Cin (optional): a separate C0 read for beta != 0, the result going to C.
 template <typename T>
 cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
                              const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
-                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri = 0);
+                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri = 0,
+                             const T* Cin = nullptr, size_t ldcin = 0);
 
 // C := beta*C over an m x n column-major block (beta == 0 writes zeros
 // without reading; beta == 1 is a no-op and launches nothing); tri as above.
@@ -109,6 +113,31 @@ int hesy_dev(int herm, int side, int uplo, size_t m, size_t n, T ar, T ai, const
 template <typename T, bool CX>
 int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A,
              size_t lda, T* B, size_t ldb, cudaStream_t st, int32_t* ce);
+
+// Staging for the grouped kernel's problem table: a pinned host buffer and a
+// device buffer of `bytes` each, owned by the caller, reused once the
+// previous launch that used them has finished (the serving loop keeps one
+// per stream). Without it every launch allocates its table stream-ordered.
+struct GroupStaging {
+    void* host;
+    void* dev;
+    size_t bytes;
+};
+size_t grouped_table_bytes(size_t count);
+
+// rblas's argument checks for one table entry (dtype, layout, transposes,
+// leading dimensions) plus the 32-bit tile-index limit; an rb_status value.
+int validate_problem(const rb_gemm_problem& q);
+
+// Grouped plain GEMM over a problem table (see rb_gemm_grouped_dev). cin /
+// ldcin (optional, per problem) name a separate input C0 read for beta != 0
+// while the result goes to problems[i].c. *bad_index: first invalid problem.
+int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
+                     cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging = nullptr);
+
+// One problem of the serving loop's per-request mode: the single-problem
+// plain kernel (one launch), result to probs->c, C0 read from cin.
+int single_gemm_dev(const rb_gemm_problem* prob, const void* cin, size_t ldcin, cudaStream_t st, int32_t* ce);
 
 // Tensor-pipe throughput (TFLOP/s or TOP/s) of back-to-back M128 N256 UMMAs
 // on every SM: i8 != 0 -> kind::i8, else kind::f16 (bf16).

@@ -1,0 +1,465 @@
+// rb_server.cu -- the serving loop: GEMM requests accepted as they arrive,
+// operands resident in HBM, admission against an HBM budget, continuous
+// batching into the grouped kernel, per-request timestamps.
+//
+// A request names its device-resident inputs A, B (and C0 when beta != 0)
+// and asks for D = alpha*op(A)op(B) + beta*C0. D is allocated from the
+// server's own HBM pool (the budget) when the request is admitted and stays
+// resident until the client releases it. One worker thread:
+//   1. retires finished batches (event polled), marking their requests done;
+//   2. admits queued requests in arrival order while the in-flight batch
+//      count, the per-batch slot count and the pool allow (memory freed by
+//      released results makes room for the next ones);
+//   3. launches the admitted set as one grouped kernel on the next of two
+//      streams, so a batch starts while the previous one drains.
+// In per-request mode (grouped = 0) every request is its own launch on the
+// same two streams -- the baseline the grouped mode is measured against.
+#include <cuda_runtime.h>
+#include <time.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/rblas_b200.h"
+#include "rb_internal.h"
+
+namespace rb {
+
+namespace {
+
+uint64_t now_ns() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return static_cast<uint64_t>(ts.tv_sec) * 1000000000ull + static_cast<uint64_t>(ts.tv_nsec);
+}
+
+size_t rup(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+// First-fit allocator over one device allocation (offsets, 256-byte granules).
+class Pool {
+public:
+    bool init(size_t bytes, cudaError_t* e) {
+        *e = cudaMalloc(&base_, bytes);
+        if (*e != cudaSuccess) return false;
+        size_ = bytes;
+        free_[0] = bytes;
+        return true;
+    }
+    void release_all() {
+        if (base_) cudaFree(base_);
+        base_ = nullptr;
+    }
+    void* alloc(size_t bytes) {
+        bytes = rup(std::max<size_t>(bytes, 1), 256);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                const size_t off = it->first, len = it->second;
+                free_.erase(it);
+                if (len > bytes) free_[off + bytes] = len - bytes;
+                used_ += bytes;
+                sizes_[off] = bytes;
+                return static_cast<uint8_t*>(base_) + off;
+            }
+        }
+        return nullptr;
+    }
+    void free(void* p) {
+        const size_t off = static_cast<uint8_t*>(p) - static_cast<uint8_t*>(base_);
+        auto s = sizes_.find(off);
+        if (s == sizes_.end()) return;
+        size_t len = s->second;
+        sizes_.erase(s);
+        used_ -= len;
+        size_t start = off;
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && next->first == off + len) {
+            len += next->second;
+            free_.erase(next);
+        }
+        auto prev = free_.lower_bound(off);
+        if (prev != free_.begin()) {
+            --prev;
+            if (prev->first + prev->second == off) {
+                start = prev->first;
+                len += prev->second;
+                free_.erase(prev);
+            }
+        }
+        free_[start] = len;
+    }
+    size_t capacity() const { return size_; }
+
+private:
+    void* base_ = nullptr;
+    size_t size_ = 0, used_ = 0;
+    std::map<size_t, size_t> free_;
+    std::unordered_map<size_t, size_t> sizes_;
+};
+
+struct Request {
+    uint64_t id;
+    rb_gemm_problem prob;  // prob.c = C0 (input); the output D is server-owned
+    size_t d_bytes, ldd;
+    void* d = nullptr;
+    int status = -1;  // -1 queued, -2 in flight, else rb_status
+    rb_request_times t{};
+};
+
+struct Batch {
+    std::vector<Request*> reqs;
+    cudaEvent_t done;
+    int stream;
+};
+
+class Server {
+public:
+    size_t budget;
+    int max_batch;
+    int grouped;
+    int device = 0;
+    Pool pool;
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    // per stream: pinned host + device problem table of max_batch entries,
+    // rewritten only after that stream's previous batch has retired
+    GroupStaging staging[2] = {{nullptr, nullptr, 0}, {nullptr, nullptr, 0}};
+    std::vector<cudaEvent_t> free_events;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queue;
+    std::unordered_map<uint64_t, Request*> reqs;
+    std::deque<Batch> inflight;
+    std::vector<uint64_t> completed;  // ids finished since the trace player last looked
+    bool track_completed = false;
+    std::atomic<uint64_t> next_id{1};
+    std::thread worker;
+    bool stop = false;
+    int next_stream = 0;
+
+    rb_status start(cudaError_t* e) {
+        *e = cudaGetDevice(&device);
+        if (*e != cudaSuccess) return RB_ERR_CUDA;
+        if (!pool.init(budget, e)) return RB_ERR_ALLOC;
+        for (auto& s : streams) {
+            *e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (*e != cudaSuccess) return RB_ERR_CUDA;
+        }
+        if (grouped) {
+            const size_t tb = grouped_table_bytes(static_cast<size_t>(max_batch));
+            for (auto& g : staging) {
+                *e = cudaMallocHost(&g.host, tb);
+                if (*e != cudaSuccess) return RB_ERR_ALLOC;
+                *e = cudaMalloc(&g.dev, tb);
+                if (*e != cudaSuccess) return RB_ERR_ALLOC;
+                g.bytes = tb;
+            }
+        }
+        worker = std::thread([this] { loop(); });
+        return RB_OK;
+    }
+
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv_work.notify_all();
+        if (worker.joinable()) worker.join();
+        for (auto& s : streams)
+            if (s) cudaStreamSynchronize(s);
+        for (auto& b : inflight) cudaEventDestroy(b.done);
+        for (auto ev : free_events) cudaEventDestroy(ev);
+        for (auto& s : streams)
+            if (s) cudaStreamDestroy(s);
+        for (auto& g : staging) {
+            if (g.host) cudaFreeHost(g.host);
+            if (g.dev) cudaFree(g.dev);
+            g = GroupStaging{nullptr, nullptr, 0};
+        }
+        for (auto& kv : reqs) delete kv.second;
+        pool.release_all();
+    }
+
+    cudaEvent_t get_event() {
+        if (!free_events.empty()) {
+            cudaEvent_t e = free_events.back();
+            free_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        return e;
+    }
+
+    // retire finished batches (caller holds mu)
+    bool retire() {
+        bool any = false;
+        while (!inflight.empty() && cudaEventQuery(inflight.front().done) == cudaSuccess) {
+            Batch& b = inflight.front();
+            const uint64_t t = now_ns();
+            for (Request* r : b.reqs) {
+                if (r->status < 0) r->status = RB_OK;
+                r->t.finish_ns = t;
+                if (track_completed) completed.push_back(r->id);
+            }
+            free_events.push_back(b.done);
+            inflight.pop_front();
+            any = true;
+        }
+        return any;
+    }
+
+    // Enqueue a batch (worker thread, without the lock); returns the status.
+    int launch(const Batch& b) {
+        cudaStream_t st = streams[b.stream];
+        int32_t ce = 0;
+        std::vector<rb_gemm_problem> probs;
+        std::vector<const void*> cin;
+        std::vector<size_t> ldcin;
+        probs.reserve(b.reqs.size());
+        for (Request* r : b.reqs) {
+            rb_gemm_problem q = r->prob;
+            cin.push_back(q.c);  // C0 is read, D written
+            ldcin.push_back(q.ldc);
+            q.c = r->d;
+            q.ldc = r->ldd;
+            probs.push_back(q);
+        }
+        int rc = RB_OK;
+        if (grouped) {
+            rc = grouped_gemm_dev(probs.data(), probs.size(), cin.data(), ldcin.data(), st, &ce, nullptr,
+                                  &staging[b.stream]);
+        } else {
+            for (size_t i = 0; i < probs.size() && rc == RB_OK; ++i)
+                rc = single_gemm_dev(&probs[i], cin[i], ldcin[i], st, &ce);
+        }
+        cudaEventRecord(b.done, st);
+        return rc;
+    }
+
+    void loop() {
+        cudaSetDevice(device);
+        std::unique_lock<std::mutex> lk(mu);
+        while (!stop) {
+            if (retire()) cv_done.notify_all();
+            std::vector<Request*> batch;
+            // keep two batches in flight: one running, one queued behind it
+            if (!queue.empty() && inflight.size() < 2) {
+                while (!queue.empty() && static_cast<int>(batch.size()) < max_batch) {
+                    Request* r = queue.front();
+                    void* d = pool.alloc(r->d_bytes);
+                    if (!d) break;  // wait for results to be released
+                    r->d = d;
+                    r->status = -2;
+                    r->t.admit_ns = now_ns();
+                    queue.pop_front();
+                    batch.push_back(r);
+                }
+            }
+            if (!batch.empty()) {
+                inflight.push_back(Batch{std::move(batch), get_event(), next_stream});
+                next_stream ^= 1;
+                const Batch& b = inflight.back();
+                lk.unlock();
+                const int rc = launch(b);
+                lk.lock();
+                if (rc != RB_OK)
+                    for (Request* r : b.reqs) r->status = rc;
+                continue;
+            }
+            if (!inflight.empty()) {
+                lk.unlock();
+                std::this_thread::sleep_for(std::chrono::microseconds(10));
+                lk.lock();
+            } else {
+                cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            }
+        }
+    }
+};
+
+}  // namespace
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, void* stream, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if (count && !problems) {
+        if (err) err->code = RB_ERR_INVALID_ARG;
+        return RB_ERR_INVALID_ARG;
+    }
+    int32_t ce = 0;
+    size_t bad = 0;
+    const int rc = grouped_gemm_dev(problems, count, nullptr, nullptr, static_cast<cudaStream_t>(stream), &ce, &bad);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->got = bad;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
+
+rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void** server) {
+    if (!server || max_batch < 1 || budget_bytes < 256) return RB_ERR_INVALID_ARG;
+    Server* s = new Server();
+    s->budget = budget_bytes;
+    s->max_batch = max_batch;
+    s->grouped = grouped;
+    cudaError_t e;
+    const rb_status st = s->start(&e);
+    if (st != RB_OK) {
+        s->shutdown();
+        delete s;
+        return st;
+    }
+    *server = s;
+    return RB_OK;
+}
+
+rb_status rb_server_submit(void* server, const rb_gemm_problem* p, uint64_t* id) {
+    Server* s = static_cast<Server*>(server);
+    if (!s || !p || !id) return RB_ERR_INVALID_ARG;
+    const int v = validate_problem(*p);
+    if (v != RB_OK) return static_cast<rb_status>(v);
+    Request* r = new Request();
+    r->prob = *p;
+    const size_t el = p->dtype ? 8 : 4;
+    // D mirrors C's layout with a compact leading dimension padded to 16 bytes
+    const size_t rows = (p->layout == RB_COL_MAJOR) ? p->m : p->n;
+    const size_t cols = (p->layout == RB_COL_MAJOR) ? p->n : p->m;
+    r->ldd = std::max<size_t>(rup(rows, 16 / el), 16 / el);
+    r->d_bytes = r->ldd * std::max<size_t>(cols, 1) * el;
+    if (r->d_bytes > s->pool.capacity()) {
+        delete r;
+        return RB_ERR_BUSY;  // can never be admitted under this budget
+    }
+    r->t.enqueue_ns = now_ns();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        s->reqs[r->id] = r;
+        s->queue.push_back(r);
+    }
+    s->cv_work.notify_one();
+    *id = r->id;
+    return RB_OK;
+}
+
+rb_status rb_server_wait(void* server, uint64_t id, int64_t timeout_us, void** d_out, size_t* ldd,
+                         rb_request_times* times) {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return RB_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return RB_ERR_INVALID_ARG;
+    Request* r = it->second;
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds(timeout_us < 0 ? 0 : timeout_us);
+    while (r->status < 0) {
+        if (timeout_us >= 0 && std::chrono::steady_clock::now() >= deadline) return RB_ERR_TIMEOUT;
+        s->cv_done.wait_for(lk, std::chrono::microseconds(200));
+    }
+    if (d_out) *d_out = r->d;
+    if (ldd) *ldd = r->ldd;
+    if (times) *times = r->t;
+    return static_cast<rb_status>(r->status);
+}
+
+rb_status rb_server_release(void* server, uint64_t id) {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return RB_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        if (it == s->reqs.end()) return RB_ERR_INVALID_ARG;
+        Request* r = it->second;
+        if (r->status < 0) return RB_ERR_BUSY;  // still queued or running
+        if (r->d) s->pool.free(r->d);
+        s->reqs.erase(it);
+        delete r;
+    }
+    s->cv_work.notify_one();
+    return RB_OK;
+}
+
+rb_status rb_server_destroy(void* server) {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return RB_ERR_INVALID_ARG;
+    s->shutdown();
+    delete s;
+    return RB_OK;
+}
+
+rb_status rb_server_run_trace(void* server, const rb_gemm_problem* problems, const uint64_t* arrival_ns,
+                              size_t count, rb_request_times* times) {
+    Server* s = static_cast<Server*>(server);
+    if (!s || (count && (!problems || !arrival_ns || !times))) return RB_ERR_INVALID_ARG;
+    std::unordered_map<uint64_t, size_t> index;  // request id -> trace position
+    rb_status first_err = RB_OK;
+    for (size_t i = 0; i < count; ++i) times[i] = rb_request_times{0, 0, 0};
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->completed.clear();
+        s->track_completed = true;
+    }
+    const uint64_t t0 = now_ns();
+    size_t next = 0, finished = 0;
+    std::vector<uint64_t> got;
+    while (finished < count) {
+        // submit every request whose arrival time has passed
+        const uint64_t now = now_ns();
+        while (next < count && t0 + arrival_ns[next] <= now) {
+            uint64_t id = 0;
+            const rb_status st = rb_server_submit(server, &problems[next], &id);
+            if (st != RB_OK) {
+                ++finished;
+                if (first_err == RB_OK) first_err = st;
+            } else {
+                index[id] = next;
+            }
+            ++next;
+        }
+        // collect finished requests and release their results
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            got.swap(s->completed);
+        }
+        for (uint64_t id : got) {
+            auto it = index.find(id);
+            if (it == index.end()) continue;
+            rb_request_times t;
+            const rb_status st = rb_server_wait(server, id, 0, nullptr, nullptr, &t);
+            times[it->second] = t;
+            if (st != RB_OK && first_err == RB_OK) first_err = st;
+            rb_server_release(server, id);
+            index.erase(it);
+            ++finished;
+        }
+        got.clear();
+        if (next < count) {
+            const uint64_t due = t0 + arrival_ns[next];
+            const uint64_t n2 = now_ns();
+            if (due > n2 + 20000)
+                std::this_thread::sleep_for(std::chrono::nanoseconds(std::min<uint64_t>(due - n2 - 10000, 100000)));
+        } else {
+            std::this_thread::sleep_for(std::chrono::microseconds(10));
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->track_completed = false;
+        s->completed.clear();
+    }
+    return first_err;
+}
+
+}  // extern "C"

@@ -1,0 +1,215 @@
+// simt_tile.cuh -- the plain (SIMT FFMA / DFMA) GEMM tile pipeline, shared by
+// the single-problem kernel (gemm_simt.cu) and the grouped persistent kernel
+// (gemm_grouped.cu).
+//
+// One C tile = BM x BN. 8 compute warps (2 along M x 4 along N, each lane an
+// 8 x TN register tile) consume a STAGES-deep ring of shared-memory stages
+// that one producer lane fills with TMA. A K-major operand tile lands as
+// [mn][k] 128-byte rows with the hardware 128-byte swizzle; an MN-major tile
+// as [k][mn] rows, unswizzled. Both read patterns are bank-conflict free.
+// The ring's mbarrier phases run on a counter `it` that continues across
+// tiles, so a persistent CTA streams tile after tile through one ring.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "rb_device.cuh"
+
+namespace rb {
+
+template <typename T> struct SimtCfg;
+// f32: 128x128 C tile, 8x8 per thread, BK = 32 (one 128-byte swizzle row).
+template <> struct SimtCfg<float> { static constexpr int BM = 128, BN = 128, BK = 32, TN = 8, STAGES = 4; };
+// f64: 128x64 C tile, 8x4 per thread, BK = 16 (one 128-byte swizzle row).
+template <> struct SimtCfg<double> { static constexpr int BM = 128, BN = 64, BK = 16, TN = 4, STAGES = 4; };
+
+constexpr int kSimtComputeWarps = 8;
+constexpr int kSimtThreads = (kSimtComputeWarps + 1) * 32;
+
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int N = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int N = 2; };
+
+template <typename T>
+__device__ __forceinline__ void lds16(const uint8_t* p, T (&v)[Vec16<T>::N]) {
+    const typename Vec16<T>::type x = *reinterpret_cast<const typename Vec16<T>::type*>(p);
+    if constexpr (Vec16<T>::N == 4) {
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+        v[0] = x.x; v[1] = x.y;
+    }
+}
+
+template <typename T>
+constexpr int simt_smem_bytes() {
+    using Cfg = SimtCfg<T>;
+    return Cfg::STAGES * (Cfg::BM + Cfg::BN) * Cfg::BK * (int)sizeof(T) + 2 * Cfg::STAGES * 8 + 1024;
+}
+
+// Byte offsets of the A and B tiles inside a stage.
+template <typename T>
+__host__ __device__ constexpr int simt_a_bytes() { return SimtCfg<T>::BM * SimtCfg<T>::BK * (int)sizeof(T); }
+template <typename T>
+__host__ __device__ constexpr int simt_stage_bytes() {
+    return (SimtCfg<T>::BM + SimtCfg<T>::BN) * SimtCfg<T>::BK * (int)sizeof(T);
+}
+
+// Producer lane: issue the num_kt K-tile loads of the tile at (m0, n0) on
+// ring iterations it, it+1, ... Returns false (after letting its own copies
+// land) if a wait gave up.
+template <typename T, bool A_K, bool B_K>
+__device__ __forceinline__ bool simt_produce(const CUtensorMap* tmA, const CUtensorMap* tmB, int m0, int n0,
+                                             int num_kt, uint8_t* smem, int stage_stride, uint64_t* full,
+                                             uint64_t* empty, uint32_t& it, uint32_t* err) {
+    using Cfg = SimtCfg<T>;
+    constexpr int ST = Cfg::STAGES, BK = Cfg::BK;
+    constexpr int A_BYTES = simt_a_bytes<T>();
+    constexpr uint32_t TX = simt_stage_bytes<T>();
+    for (int kt = 0; kt < num_kt; ++kt, ++it) {
+        const int s = it % ST;
+        if (it >= ST && !mbar_wait(&empty[s], ((it / ST) - 1) & 1, err, 0x101)) {
+            const uint32_t first = it > (uint32_t)ST ? it - ST : 0;
+            for (uint32_t j = first; j < it; ++j) mbar_wait_drain(&full[j % ST], (j / ST) & 1);
+            return false;
+        }
+        uint8_t* sa = smem + s * stage_stride;
+        uint8_t* sb = sa + A_BYTES;
+        mbar_arrive_expect_tx(&full[s], TX);
+        const int k0 = kt * BK;
+        if (A_K) tma_load_2d(sa, tmA, &full[s], k0, m0);
+        else     tma_load_2d(sa, tmA, &full[s], m0, k0);
+        if (B_K) tma_load_2d(sb, tmB, &full[s], k0, n0);
+        else     tma_load_2d(sb, tmB, &full[s], n0, k0);
+    }
+    return true;
+}
+
+// Epilogue data of one tile: C = alpha*acc + beta*Cin, written to c (cin
+// may equal c).
+template <typename T>
+struct SimtOut {
+    T* c;
+    size_t ldc;
+    const T* cin;
+    size_t ldcin;
+    int m, n;
+    T alpha, beta;
+    int beta_mode;  // 0: beta == 0 (C not read), 1: beta == 1, 2: general
+    int tri;        // 0 full C; 1 upper triangle only (row <= col); 2 lower (row >= col)
+};
+
+// Compute warps: consume num_kt stages from ring iteration it, then write
+// C = alpha*acc + beta*C for this tile. Returns false if a wait gave up.
+template <typename T, bool A_K, bool B_K>
+__device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0, int num_kt, uint8_t* smem,
+                                             int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
+                                             uint32_t* err, int warp, int lane) {
+    using Cfg = SimtCfg<T>;
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, TN = Cfg::TN, ST = Cfg::STAGES;
+    constexpr int VEC = Vec16<T>::N;  // elements per 16-byte load
+    constexpr int A_BYTES = simt_a_bytes<T>();
+    static_assert(BK * sizeof(T) == 128, "a K-major tile row must be one 128-byte swizzle row");
+    static_assert(A_BYTES % 1024 == 0, "swizzled tiles need 1 KiB alignment");
+    const int wm = warp & 1, wn = warp >> 1;          // 2 x 4 warps
+    const int lane_m = lane & 7, lane_n = lane >> 3;  // 8 x 4 lanes
+    const int wm0 = wm * 64, wn0 = wn * (4 * TN);
+
+    T acc[8][TN];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+    for (int kt = 0; kt < num_kt; ++kt, ++it) {
+        const int s = it % ST;
+        if (!mbar_wait(&full[s], (it / ST) & 1, err, 0x102)) return false;
+        const uint8_t* sa = smem + s * stage_stride;
+        const uint8_t* sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += VEC) {
+            T a[VEC][8];
+            T b[VEC][TN];
+            const int chunk = kk / VEC;  // 16-byte chunk along k within a 128-byte row
+            if constexpr (A_K) {
+                // [m][k] swizzled: a quarter-warp (same lane_n, lane_m 0..7)
+                // touches 8 rows whose swizzled chunks chunk^lane_m differ.
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int row = wm0 + lane_m + 8 * r;
+                    T v[VEC];
+                    lds16<T>(sa + row * 128 + ((chunk ^ (row & 7)) << 4), v);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) a[q][r] = v[q];
+                }
+            } else {
+                // [k][m]: a quarter-warp reads 8 consecutive 16-byte chunks of one row.
+#pragma unroll
+                for (int q = 0; q < VEC; ++q)
+#pragma unroll
+                    for (int g = 0; g < 8 / VEC; ++g) {
+                        const int col = wm0 + g * 8 * VEC + lane_m * VEC;
+                        T v[VEC];
+                        lds16<T>(sa + ((kk + q) * BM + col) * sizeof(T), v);
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) a[q][g * VEC + e] = v[e];
+                    }
+            }
+            if constexpr (B_K) {
+                // [n][k] swizzled: a quarter-warp shares lane_n -> one address (broadcast).
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    const int row = wn0 + lane_n * TN + j;
+                    T v[VEC];
+                    lds16<T>(sb + row * 128 + ((chunk ^ (row & 7)) << 4), v);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) b[q][j] = v[q];
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q)
+#pragma unroll
+                    for (int g = 0; g < TN / VEC; ++g) {
+                        const int col = wn0 + g * 4 * VEC + lane_n * VEC;
+                        T v[VEC];
+                        lds16<T>(sb + ((kk + q) * BN + col) * sizeof(T), v);
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) b[q][g * VEC + e] = v[e];
+                    }
+            }
+#pragma unroll
+            for (int q = 0; q < VEC; ++q)
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[q][i], b[q][j], acc[i][j]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+
+    // ---------------- epilogue: C = alpha*acc + beta*C ----------------
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = m0 + (A_K ? (wm0 + lane_m + 8 * i)
+                                : (wm0 + (i / VEC) * 8 * VEC + lane_m * VEC + (i % VEC)));
+        if (r >= o.m) continue;
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int cidx = n0 + (B_K ? (wn0 + lane_n * TN + j)
+                                       : (wn0 + (j / VEC) * 4 * VEC + lane_n * VEC + (j % VEC)));
+            if (cidx >= o.n) continue;
+            if ((o.tri == 1 && r > cidx) || (o.tri == 2 && r < cidx)) continue;
+            T* cp = o.c + r + static_cast<size_t>(cidx) * o.ldc;
+            T t = T(0);
+            if (o.beta_mode != 0) {
+                const T cv = o.cin[r + static_cast<size_t>(cidx) * o.ldcin];
+                t = (o.beta_mode == 1) ? cv : o.beta * cv;
+            }
+            *cp = fma(o.alpha, acc[i][j], t);
+        }
+    }
+    return true;
+}
+
+}  // namespace rb

@@ -1,0 +1,112 @@
+"""Batching and serving forms of rblas's gemm (level3::gemm, src/level3.rs:32-62)
+on device-resident operands: the grouped persistent kernel and the serving
+loop of librblas_b200.so (rb_gemm_grouped_dev, rb_server_*)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .types import Layout, Transpose
+
+__all__ = ["Problem", "grouped_gemm", "Server"]
+
+
+@dataclass
+class Problem:
+    """C := alpha*op(A)*op(B) + beta*C with device pointers (ints)."""
+    dtype: object  # np.float32 / np.float64
+    layout: int
+    transa: int
+    transb: int
+    m: int
+    n: int
+    k: int
+    alpha: float
+    a: int
+    lda: int
+    b: int
+    ldb: int
+    beta: float
+    c: int
+    ldc: int
+
+    def to_c(self) -> _lib.RbGemmProblem:
+        return _lib.RbGemmProblem(
+            0 if np.dtype(self.dtype) == np.float32 else 1, int(Layout(self.layout)),
+            int(Transpose(self.transa)), int(Transpose(self.transb)), self.m, self.n, self.k,
+            float(self.alpha), float(self.beta), C.c_void_p(self.a), self.lda, C.c_void_p(self.b),
+            self.ldb, C.c_void_p(self.c), self.ldc)
+
+
+def _array(problems):
+    arr = (_lib.RbGemmProblem * len(problems))()
+    for i, p in enumerate(problems):
+        arr[i] = p.to_c() if isinstance(p, Problem) else p
+    return arr
+
+
+def grouped_gemm(problems, stream=0):
+    """Run every problem in one grouped launch on `stream`."""
+    arr = _array(problems)
+    err = _lib.RbError()
+    st = _lib.load().rb_gemm_grouped_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
+                                         C.byref(err))
+    _lib.check(st, err)
+
+
+class Server:
+    """The library's serving loop (rb_server_*): requests on device-resident
+    inputs, results in server-owned HBM under a budget, continuous batching
+    into grouped launches (grouped=True) or one launch per request."""
+
+    def __init__(self, budget_bytes: int, max_batch: int = 256, grouped: bool = True):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        st = self._lib.rb_server_create(budget_bytes, max_batch, int(grouped), C.byref(h))
+        if st != 0:
+            raise RuntimeError(f"rb_server_create failed: {self._lib.rb_status_string(st).decode()}")
+        self._h = h
+
+    def submit(self, p: Problem) -> int:
+        rid = C.c_uint64()
+        q = p.to_c()
+        st = self._lib.rb_server_submit(self._h, C.byref(q), C.byref(rid))
+        if st != 0:
+            raise RuntimeError(f"submit failed: {self._lib.rb_status_string(st).decode()}")
+        return rid.value
+
+    def wait(self, rid: int, timeout_us: int = -1):
+        """-> (status, result_ptr, ldd, (enqueue_ns, admit_ns, finish_ns))."""
+        d = C.c_void_p()
+        ldd = C.c_size_t()
+        t = _lib.RbRequestTimes()
+        st = self._lib.rb_server_wait(self._h, rid, timeout_us, C.byref(d), C.byref(ldd), C.byref(t))
+        return st, d.value, ldd.value, (t.enqueue_ns, t.admit_ns, t.finish_ns)
+
+    def release(self, rid: int) -> int:
+        return self._lib.rb_server_release(self._h, rid)
+
+    def run_trace(self, problems, arrival_ns):
+        """Replay a trace natively; returns an (n, 3) uint64 array of
+        (enqueue, admit, finish) ns and the status."""
+        arr = _array(problems)
+        arrivals = np.ascontiguousarray(arrival_ns, dtype=np.uint64)
+        times = (_lib.RbRequestTimes * len(problems))()
+        st = self._lib.rb_server_run_trace(self._h, arr, arrivals.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                           len(problems), times)
+        out = np.array([(t.enqueue_ns, t.admit_ns, t.finish_ns) for t in times], dtype=np.uint64)
+        return st, out
+
+    def close(self):
+        if self._h:
+            self._lib.rb_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
