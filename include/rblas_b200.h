@@ -247,6 +247,11 @@ typedef struct {
  * err->got is the index of the offending problem. Enqueued on `stream`. */
 rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, void* stream,
                               rb_error* err);
+/* The number of K ranges (split-K factor) the grouped kernel cuts this
+ * problem into. It depends on the problem's own shape alone, and the K
+ * partials are summed in a fixed order, so a problem's result is the same
+ * whatever else shares the launch. 0 for an invalid problem. */
+int rb_gemm_grouped_splits(const rb_gemm_problem* p);
 
 /* Per-request timestamps (CLOCK_MONOTONIC ns): submitted, admitted into a
  * batch (result memory reserved), finished (batch completion observed). */

@@ -3,18 +3,27 @@
 //
 // The host builds a device-side problem table: per problem two TMA tensor
 // maps (in global memory, 64-byte aligned), the epilogue description, the
-// tile grid and the problem's first index in the concatenated tile space.
-// A persistent grid (one CTA per SM) walks that space round-robin; each
-// CTA's producer lane and compute warps follow the same tile sequence, find
-// the problem by binary search, and run the same tile pipeline as the
-// single-problem kernel (simt_tile.cuh) through one continuous mbarrier ring,
-// so tiles of different problems stream back to back without a launch.
+// tile grid, the split-K factor and the problem's first index in the
+// concatenated work-item space (item = one K range of one C tile). Problems
+// are ordered longest item first. A persistent grid (one CTA per SM) takes
+// items from an atomic counter (greedy longest-first scheduling); the
+// producer lane claims each item and hands it to the compute warps through a
+// two-slot mbarrier ring, then all of them run the same tile pipeline as the
+// single-problem kernel (simt_tile.cuh) through one continuous stage ring, so
+// tiles of different problems stream back to back without a launch.
+//
+// Split-K is deterministic: each of a tile's S items stores its partial
+// accumulator to a 64 KiB workspace slot; the item that arrives last on the
+// tile's counter sums the S slots in index order and runs the epilogue, so a
+// problem's result depends only on its own shape (which fixes S), never on
+// the other problems in the launch or on timing.
 // Work per problem: 2mnk flop.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "../../include/rblas_b200.h"
@@ -27,8 +36,15 @@ namespace rb {
 namespace {
 
 constexpr int kGroupStage = 32768;  // max(f32 32 KiB, f64 24 KiB) stage
-constexpr int kGroupSmem = SimtCfg<float>::STAGES * kGroupStage + 2 * SimtCfg<float>::STAGES * 8 + 1024;
+constexpr int kGroupST = SimtCfg<float>::STAGES;
+// stages, then full/empty stage barriers, item ring barriers, compute barrier, item slots, reduce flag
+constexpr int kGroupCtl = 2 * kGroupST * 8 + 4 * 8 + 8 + 2 * 4 + 4;
+constexpr int kGroupSmem = kGroupST * kGroupStage + 128 + 1024;
+static_assert(kGroupCtl <= 128, "control block");
 static_assert(SimtCfg<float>::STAGES == SimtCfg<double>::STAGES, "one ring for both dtypes");
+constexpr int kSlotElems = SimtCfg<float>::BM * SimtCfg<float>::BN;  // per-slot f32 elements (64 KiB)
+static_assert(kSlotElems * 4 == SimtCfg<double>::BM * SimtCfg<double>::BN * 8, "one slot size for both dtypes");
+constexpr size_t kSlotBytes = kSlotElems * 4;
 
 struct alignas(64) GroupProblem {
     CUtensorMap tmA;
@@ -41,7 +57,10 @@ struct alignas(64) GroupProblem {
     int variant;  // dtype * 4 + a_kmajor * 2 + b_kmajor
     int tiles_m, tiles_n;
     int beta_mode;
-    int pad;
+    int splits;       // S: items per C tile
+    int kt_per_split; // K-tiles per item (the last item of a tile may have fewer)
+    int ws_slot;      // first workspace slot (S > 1)
+    int sem;          // first tile counter (S > 1)
 };
 
 __device__ __forceinline__ int find_problem(const int* __restrict__ starts, int nprob, int t) {
@@ -54,70 +73,170 @@ __device__ __forceinline__ int find_problem(const int* __restrict__ starts, int 
     return lo;
 }
 
-template <typename T, bool A_K, bool B_K>
-__device__ __noinline__ bool produce_v(const GroupProblem* p, int tm, int tn, uint8_t* smem, uint64_t* full,
-                                          uint64_t* empty, uint32_t& it, uint32_t* err) {
-    return simt_produce<T, A_K, B_K>(&p->tmA, &p->tmB, tm * SimtCfg<T>::BM, tn * SimtCfg<T>::BN, p->num_kt, smem,
-                                     kGroupStage, full, empty, it, err);
+// An item's tile and K range.
+struct Item {
+    int tm, tn, tile, split, kt0, nkt;
+};
+
+__device__ __forceinline__ Item decode_item(const GroupProblem* p, int r) {
+    Item w;
+    w.tile = r / p->splits;
+    w.split = r - w.tile * p->splits;
+    raster_tile(w.tile, p->tiles_m, p->tiles_n, w.tm, w.tn);
+    w.kt0 = w.split * p->kt_per_split;
+    w.nkt = min(p->kt_per_split, p->num_kt - w.kt0);
+    return w;
+}
+
+// Barrier of the 8 compute warps on an mbarrier (count 8, one arrival per
+// warp), so that the wait is bounded like every other wait in the kernel.
+__device__ __forceinline__ bool compute_sync(uint64_t* cbar, uint32_t& cph, uint32_t* err, int lane) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(cbar);
+    const bool ok = mbar_wait(cbar, cph & 1, err, 0x113);
+    ++cph;
+    return ok;
 }
 
 template <typename T, bool A_K, bool B_K>
-__device__ __noinline__ bool consume_v(const GroupProblem* p, int tm, int tn, uint8_t* smem, uint64_t* full,
-                                          uint64_t* empty, uint32_t& it, uint32_t* err, int warp, int lane) {
+__device__ __noinline__ bool produce_v(const GroupProblem* p, int r, uint8_t* smem, uint64_t* full,
+                                       uint64_t* empty, uint32_t& it, uint32_t* err) {
+    const Item w = decode_item(p, r);
+    return simt_produce<T, A_K, B_K>(&p->tmA, &p->tmB, w.tm * SimtCfg<T>::BM, w.tn * SimtCfg<T>::BN, w.kt0, w.nkt,
+                                     smem, kGroupStage, full, empty, it, err);
+}
+
+template <typename T, bool A_K, bool B_K>
+__device__ __noinline__ bool consume_v(const GroupProblem* p, int r, uint8_t* smem, uint64_t* full, uint64_t* empty,
+                                       uint32_t& it, uint32_t* err, int warp, int lane, float* ws, int* sems,
+                                       volatile int* red_flag, uint64_t* cbar, uint32_t& cph) {
+    constexpr int TN = SimtCfg<T>::TN;
+    const Item w = decode_item(p, r);
+    T acc[8][TN];
+    if (!simt_mainloop<T, A_K, B_K>(acc, w.nkt, smem, kGroupStage, full, empty, it, err, warp, lane)) return false;
     const SimtOut<T> o{static_cast<T*>(p->c), p->ldc, static_cast<const T*>(p->cin), p->ldcin, p->m, p->n,
                        static_cast<T>(p->alpha), static_cast<T>(p->beta), p->beta_mode, 0};
-    return simt_consume<T, A_K, B_K>(o, tm * SimtCfg<T>::BM, tn * SimtCfg<T>::BN, p->num_kt, smem, kGroupStage,
-                                     full, empty, it, err, warp, lane);
+    const int m0 = w.tm * SimtCfg<T>::BM, n0 = w.tn * SimtCfg<T>::BN;
+    if (p->splits == 1) {
+        simt_epilogue<T, A_K, B_K>(o, acc, m0, n0, warp, lane);
+        return true;
+    }
+    // split-K: partial to this item's slot, element (i, j) of thread t at
+    // [(i * TN + j) * 256 + t] so every warp store is 32 consecutive values
+    constexpr int NT = kSimtComputeWarps * 32;
+    const int t = warp * 32 + lane;
+    T* base = reinterpret_cast<T*>(ws + static_cast<size_t>(p->ws_slot + w.tile * p->splits) * kSlotElems);
+    T* mine = base + static_cast<size_t>(w.split) * (kSlotBytes / sizeof(T));
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) __stcg(mine + (i * TN + j) * NT + t, acc[i][j]);
+    __threadfence();
+    if (!compute_sync(cbar, cph, err, lane)) return false;
+    if (t == 0) *red_flag = (atomicAdd(sems + p->sem + w.tile, 1) == p->splits - 1);
+    if (!compute_sync(cbar, cph, err, lane)) return false;
+    const bool last = *red_flag;
+    // every thread has read the flag before the next item may rewrite it
+    if (!compute_sync(cbar, cph, err, lane)) return false;
+    if (!last) return true;
+    __threadfence();
+    // the last item of the tile sums the S partials in slot order
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = __ldcg(base + (i * TN + j) * NT + t);
+    for (int s = 1; s < p->splits; ++s) {
+        const T* src = base + static_cast<size_t>(s) * (kSlotBytes / sizeof(T));
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < TN; ++j) acc[i][j] += __ldcg(src + (i * TN + j) * NT + t);
+    }
+    simt_epilogue<T, A_K, B_K>(o, acc, m0, n0, warp, lane);
+    return true;
 }
 
+// ctl layout: [0] item counter, then one counter per split tile (zeroed by
+// the host with the table upload).
 __global__ void __launch_bounds__(kSimtThreads, 1)
     grouped_gemm_kernel(const GroupProblem* __restrict__ probs, const int* __restrict__ starts, int nprob,
-                        int total_tiles, uint32_t* err) {
-    constexpr int ST = SimtCfg<float>::STAGES;
+                        int total_items, int* ctl, float* ws, uint32_t* err) {
+    constexpr int ST = kGroupST;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * kGroupStage);
     uint64_t* empty = full + ST;
+    uint64_t* item_full = empty + ST;
+    uint64_t* item_empty = item_full + 2;
+    uint64_t* cbar = item_empty + 2;
+    volatile int* item_slot = reinterpret_cast<volatile int*>(cbar + 1);
+    volatile int* red_flag = item_slot + 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], kSimtComputeWarps);
         }
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&item_full[s], 1);
+            mbar_init(&item_empty[s], kSimtComputeWarps);
+        }
+        mbar_init(cbar, kSimtComputeWarps);
         fence_barrier_init();
     }
     __syncthreads();
-    uint32_t it = 0;
+    uint32_t it = 0, cph = 0;
     const bool producer = (warp == kSimtComputeWarps);
     if (producer && lane != 0) return;
-    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-        const int pi = find_problem(starts, nprob, t);
+    int* sems = ctl + 1;
+    for (uint32_t q = 0;; ++q) {
+        const int slot = q & 1;
+        int item;
+        if (producer) {
+            item = atomicAdd(ctl, 1);
+            if (item >= total_items) item = -1;
+            if (q >= 2 && !mbar_wait(&item_empty[slot], ((q >> 1) - 1) & 1, err, 0x111)) {
+                const uint32_t first = it > (uint32_t)ST ? it - ST : 0;
+                for (uint32_t j = first; j < it; ++j) mbar_wait_drain(&full[j % ST], (j / ST) & 1);
+                return;
+            }
+            item_slot[slot] = item;
+            mbar_arrive(&item_full[slot]);
+        } else {
+            if (!mbar_wait(&item_full[slot], (q >> 1) & 1, err, 0x112)) return;
+            item = item_slot[slot];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&item_empty[slot]);
+        }
+        if (item < 0) return;
+        const int pi = find_problem(starts, nprob, item);
         const GroupProblem* p = probs + pi;
-        int tm, tn;
-        raster_tile(t - __ldg(starts + pi), p->tiles_m, p->tiles_n, tm, tn);
+        const int r = item - __ldg(starts + pi);
         bool ok;
         if (producer) {
             switch (p->variant) {
-                case 0: ok = produce_v<float, false, false>(p, tm, tn, smem, full, empty, it, err); break;
-                case 1: ok = produce_v<float, false, true>(p, tm, tn, smem, full, empty, it, err); break;
-                case 2: ok = produce_v<float, true, false>(p, tm, tn, smem, full, empty, it, err); break;
-                case 3: ok = produce_v<float, true, true>(p, tm, tn, smem, full, empty, it, err); break;
-                case 4: ok = produce_v<double, false, false>(p, tm, tn, smem, full, empty, it, err); break;
-                case 5: ok = produce_v<double, false, true>(p, tm, tn, smem, full, empty, it, err); break;
-                case 6: ok = produce_v<double, true, false>(p, tm, tn, smem, full, empty, it, err); break;
-                default: ok = produce_v<double, true, true>(p, tm, tn, smem, full, empty, it, err); break;
+                case 0: ok = produce_v<float, false, false>(p, r, smem, full, empty, it, err); break;
+                case 1: ok = produce_v<float, false, true>(p, r, smem, full, empty, it, err); break;
+                case 2: ok = produce_v<float, true, false>(p, r, smem, full, empty, it, err); break;
+                case 3: ok = produce_v<float, true, true>(p, r, smem, full, empty, it, err); break;
+                case 4: ok = produce_v<double, false, false>(p, r, smem, full, empty, it, err); break;
+                case 5: ok = produce_v<double, false, true>(p, r, smem, full, empty, it, err); break;
+                case 6: ok = produce_v<double, true, false>(p, r, smem, full, empty, it, err); break;
+                default: ok = produce_v<double, true, true>(p, r, smem, full, empty, it, err); break;
             }
         } else {
+#define RB_CONSUME(T, AK, BK) consume_v<T, AK, BK>(p, r, smem, full, empty, it, err, warp, lane, ws, sems, red_flag, cbar, cph)
             switch (p->variant) {
-                case 0: ok = consume_v<float, false, false>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 1: ok = consume_v<float, false, true>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 2: ok = consume_v<float, true, false>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 3: ok = consume_v<float, true, true>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 4: ok = consume_v<double, false, false>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 5: ok = consume_v<double, false, true>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                case 6: ok = consume_v<double, true, false>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
-                default: ok = consume_v<double, true, true>(p, tm, tn, smem, full, empty, it, err, warp, lane); break;
+                case 0: ok = RB_CONSUME(float, false, false); break;
+                case 1: ok = RB_CONSUME(float, false, true); break;
+                case 2: ok = RB_CONSUME(float, true, false); break;
+                case 3: ok = RB_CONSUME(float, true, true); break;
+                case 4: ok = RB_CONSUME(double, false, false); break;
+                case 5: ok = RB_CONSUME(double, false, true); break;
+                case 6: ok = RB_CONSUME(double, true, false); break;
+                default: ok = RB_CONSUME(double, true, true); break;
             }
+#undef RB_CONSUME
         }
         if (!ok) return;
     }
@@ -148,44 +267,121 @@ int validate_problem(const rb_gemm_problem& q) {
     return RB_OK;
 }
 
-size_t grouped_table_bytes(size_t count) { return count * (sizeof(GroupProblem) + sizeof(int)); }
+namespace {
+
+// Split-K policy: a function of the problem's own shape only, so a result
+// never depends on what else shares the launch. A problem with fewer C tiles
+// than SMs and a long K is cut into up to kMaxSplit K ranges of at least
+// kMinSplitKt K-tiles, aiming at about one wave of items for the problem.
+constexpr int kMinSplitKt = 16;
+constexpr int kMaxSplit = 16;
+constexpr int kWaveItems = 148;
+
+struct Plan {
+    size_t m, n, k;  // column-major (normalised)
+    bool ta, tb;
+    int tiles_m, tiles_n, num_kt, splits, kt_per_split;
+};
+
+Plan plan_problem(const rb_gemm_problem& q) {
+    Plan pl{};
+    const bool ta = q.transa != RB_NO_TRANS, tb = q.transb != RB_NO_TRANS;
+    const bool col = q.layout == RB_COL_MAJOR;
+    pl.m = col ? q.m : q.n;
+    pl.n = col ? q.n : q.m;
+    pl.k = q.k;
+    pl.ta = col ? ta : tb;
+    pl.tb = col ? tb : ta;
+    const bool f64 = q.dtype == 1;
+    const int BN = f64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+    const int BK = f64 ? SimtCfg<double>::BK : SimtCfg<float>::BK;
+    pl.tiles_m = static_cast<int>((pl.m + 127) / 128);
+    pl.tiles_n = static_cast<int>((pl.n + BN - 1) / BN);
+    const bool skip_ab = (pl.k == 0 || q.alpha == 0.0);
+    pl.num_kt = skip_ab ? 0 : static_cast<int>((pl.k + BK - 1) / BK);
+    pl.splits = 1;
+    pl.kt_per_split = std::max(pl.num_kt, 1);
+    const long tiles = static_cast<long>(pl.tiles_m) * pl.tiles_n;
+    if (pl.m && pl.n && tiles < kWaveItems && pl.num_kt >= 2 * kMinSplitKt) {
+        int s = std::min<long>({static_cast<long>(pl.num_kt / kMinSplitKt), static_cast<long>(kMaxSplit),
+                                (kWaveItems + tiles - 1) / tiles});
+        if (s > 1) {
+            pl.kt_per_split = (pl.num_kt + s - 1) / s;
+            pl.splits = (pl.num_kt + pl.kt_per_split - 1) / pl.kt_per_split;
+        }
+    }
+    return pl;
+}
+
+size_t plan_slots(const Plan& pl) {
+    return pl.splits > 1 ? static_cast<size_t>(pl.tiles_m) * pl.tiles_n * pl.splits : 0;
+}
+
+}  // namespace
+
+size_t grouped_table_bytes(size_t count, size_t sems) {
+    return rup(count * sizeof(GroupProblem) + count * sizeof(int) + (1 + sems) * sizeof(int), 256);
+}
+
+size_t grouped_ws_slots(const rb_gemm_problem& q) {
+    if (validate_problem(q) != RB_OK) return 0;
+    return plan_slots(plan_problem(q));
+}
+
+size_t grouped_slot_bytes() { return kSlotBytes; }
+
+int grouped_splits(const rb_gemm_problem& q) {
+    if (validate_problem(q) != RB_OK) return 0;
+    return plan_problem(q).splits;
+}
 
 int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
                      cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging) {
-    std::vector<GroupProblem> table;
-    std::vector<int> starts;
-    table.reserve(count);
-    size_t scratch = 0;
-    int total = 0;
-    // first pass: validate and normalise (row-major -> column-major by swapping the operands)
-    struct Norm { bool ta, tb; size_t m, n, k; const void* a; size_t lda; const void* b; size_t ldb; };
-    std::vector<Norm> norm(count);
+    // first pass: validate and plan (row-major -> column-major by swapping the operands)
+    std::vector<Plan> plan(count);
     for (size_t i = 0; i < count; ++i) {
-        const rb_gemm_problem& q = probs[i];
-        const int v = validate_problem(q);
+        const int v = validate_problem(probs[i]);
         if (v != RB_OK) {
             if (bad_index) *bad_index = i;
             return v;
         }
-        const bool ta = q.transa != RB_NO_TRANS, tb = q.transb != RB_NO_TRANS;
-        if (q.layout == RB_COL_MAJOR) norm[i] = {ta, tb, q.m, q.n, q.k, q.a, q.lda, q.b, q.ldb};
-        else norm[i] = {tb, ta, q.n, q.m, q.k, q.b, q.ldb, q.a, q.lda};
+        plan[i] = plan_problem(probs[i]);
     }
+    // order: longest item first (greedy longest-processing-time scheduling
+    // through the kernel's atomic item counter); estimated time per K-tile
+    // of an item, f32 : f64 about 15 : 8
+    std::vector<size_t> order;
+    order.reserve(count);
+    for (size_t i = 0; i < count; ++i)
+        if (plan[i].m && plan[i].n) order.push_back(i);
+    auto cost = [&](size_t i) {
+        return static_cast<long>(std::min(plan[i].kt_per_split, std::max(plan[i].num_kt, 1))) *
+               (probs[i].dtype ? 8 : 15);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost(x) > cost(y); });
+    if (order.empty()) return RB_OK;
+
     // second pass: scratch for operands TMA cannot address directly
     const size_t elem_of[2] = {4, 8};
+    size_t scratch = 0;
     std::vector<std::pair<size_t, size_t>> rp_a(count, {SIZE_MAX, 0}), rp_b(count, {SIZE_MAX, 0});
-    for (size_t i = 0; i < count; ++i) {
-        const Norm& nm = norm[i];
-        const size_t el = elem_of[probs[i].dtype];
-        if (nm.m == 0 || nm.n == 0 || nm.k == 0 || probs[i].alpha == 0.0) continue;
+    for (size_t i : order) {
+        const Plan& pl = plan[i];
+        const rb_gemm_problem& q = probs[i];
+        const size_t el = elem_of[q.dtype];
+        if (pl.num_kt == 0) continue;
+        const bool col = q.layout == RB_COL_MAJOR;
+        const void* a = col ? q.a : q.b;
+        const void* b = col ? q.b : q.a;
+        const size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
         const size_t vec = 16 / el;
-        if (!tma_aligned(nm.a, nm.lda, el)) {
-            const size_t rows = nm.ta ? nm.k : nm.m, cols = nm.ta ? nm.m : nm.k, ld2 = rup(rows, vec);
+        if (!tma_aligned(a, lda, el)) {
+            const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k, ld2 = rup(rows, vec);
             rp_a[i] = {scratch, ld2};
             scratch += rup(ld2 * cols * el, 256);
         }
-        if (!tma_aligned(nm.b, nm.ldb, el)) {
-            const size_t rows = nm.tb ? nm.n : nm.k, cols = nm.tb ? nm.k : nm.n, ld2 = rup(rows, vec);
+        if (!tma_aligned(b, ldb, el)) {
+            const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n, ld2 = rup(rows, vec);
             rp_b[i] = {scratch, ld2};
             scratch += rup(ld2 * cols * el, 256);
         }
@@ -196,41 +392,48 @@ int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* con
         e = cudaMallocAsync(reinterpret_cast<void**>(&sbuf), scratch, st);
         if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
     }
-    for (size_t i = 0; i < count; ++i) {
+    std::vector<GroupProblem> table;
+    std::vector<int> starts;
+    table.reserve(order.size());
+    starts.reserve(order.size());
+    size_t total = 0, slots = 0, sems = 0;
+    for (size_t i : order) {
         const rb_gemm_problem& q = probs[i];
-        Norm nm = norm[i];
-        if (nm.m == 0 || nm.n == 0) continue;
+        const Plan& pl = plan[i];
         const size_t el = elem_of[q.dtype];
         const bool f64 = q.dtype == 1;
-        const bool skip_ab = (nm.k == 0 || q.alpha == 0.0);
+        const bool col = q.layout == RB_COL_MAJOR;
+        const void* a = col ? q.a : q.b;
+        const void* b = col ? q.b : q.a;
+        size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
         if (rp_a[i].first != SIZE_MAX) {
-            const size_t rows = nm.ta ? nm.k : nm.m, cols = nm.ta ? nm.m : nm.k;
-            e = cudaMemcpy2DAsync(sbuf + rp_a[i].first, rp_a[i].second * el, nm.a, nm.lda * el, rows * el, cols,
+            const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k;
+            e = cudaMemcpy2DAsync(sbuf + rp_a[i].first, rp_a[i].second * el, a, lda * el, rows * el, cols,
                                   cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) { if (ce) *ce = e; cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-            nm.a = sbuf + rp_a[i].first;
-            nm.lda = rp_a[i].second;
+            a = sbuf + rp_a[i].first;
+            lda = rp_a[i].second;
         }
         if (rp_b[i].first != SIZE_MAX) {
-            const size_t rows = nm.tb ? nm.n : nm.k, cols = nm.tb ? nm.k : nm.n;
-            e = cudaMemcpy2DAsync(sbuf + rp_b[i].first, rp_b[i].second * el, nm.b, nm.ldb * el, rows * el, cols,
+            const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n;
+            e = cudaMemcpy2DAsync(sbuf + rp_b[i].first, rp_b[i].second * el, b, ldb * el, rows * el, cols,
                                   cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) { if (ce) *ce = e; cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-            nm.b = sbuf + rp_b[i].first;
-            nm.ldb = rp_b[i].second;
+            b = sbuf + rp_b[i].first;
+            ldb = rp_b[i].second;
         }
         GroupProblem g{};
         const int BM = 128, BN = f64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
         const int BK = f64 ? SimtCfg<double>::BK : SimtCfg<float>::BK;
         const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        const bool a_k = nm.ta, b_k = !nm.tb;
+        const bool a_k = pl.ta, b_k = !pl.tb;
         CUresult r = CUDA_SUCCESS;
-        if (!skip_ab) {
-            r = a_k ? make_tmap_2d(&g.tmA, nm.a, dt, el, nm.k, nm.m, nm.lda, BK, BM, true)
-                    : make_tmap_2d(&g.tmA, nm.a, dt, el, nm.m, nm.k, nm.lda, BM, BK, false);
+        if (pl.num_kt > 0) {
+            r = a_k ? make_tmap_2d(&g.tmA, a, dt, el, pl.k, pl.m, lda, BK, BM, true)
+                    : make_tmap_2d(&g.tmA, a, dt, el, pl.m, pl.k, lda, BM, BK, false);
             if (r == CUDA_SUCCESS)
-                r = b_k ? make_tmap_2d(&g.tmB, nm.b, dt, el, nm.k, nm.n, nm.ldb, BK, BN, true)
-                        : make_tmap_2d(&g.tmB, nm.b, dt, el, nm.n, nm.k, nm.ldb, BN, BK, false);
+                r = b_k ? make_tmap_2d(&g.tmB, b, dt, el, pl.k, pl.n, ldb, BK, BN, true)
+                        : make_tmap_2d(&g.tmB, b, dt, el, pl.n, pl.k, ldb, BN, BK, false);
         }
         if (r != CUDA_SUCCESS) {
             if (ce) *ce = static_cast<int32_t>(r);
@@ -242,42 +445,61 @@ int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* con
         g.ldc = q.ldc;
         g.cin = cin ? cin[i] : q.c;
         g.ldcin = ldcin ? ldcin[i] : q.ldc;
-        g.alpha = q.alpha;
+        // k == 0 or alpha == 0: C = beta*Cin exactly (alpha*0 would turn an inf alpha into NaN)
+        g.alpha = pl.num_kt ? q.alpha : 0.0;
         g.beta = q.beta;
-        g.m = static_cast<int>(nm.m);
-        g.n = static_cast<int>(nm.n);
-        g.num_kt = skip_ab ? 0 : static_cast<int>((nm.k + BK - 1) / BK);  // k == 0 || alpha == 0: C = beta*Cin
+        g.m = static_cast<int>(pl.m);
+        g.n = static_cast<int>(pl.n);
+        g.num_kt = pl.num_kt;
         g.variant = (f64 ? 4 : 0) + (a_k ? 2 : 0) + (b_k ? 1 : 0);
-        g.tiles_m = static_cast<int>((nm.m + BM - 1) / BM);
-        g.tiles_n = static_cast<int>((nm.n + BN - 1) / BN);
+        g.tiles_m = pl.tiles_m;
+        g.tiles_n = pl.tiles_n;
         g.beta_mode = (q.beta == 0.0) ? 0 : (q.beta == 1.0 ? 1 : 2);
-        starts.push_back(total);
-        total += g.tiles_m * g.tiles_n;
+        g.splits = pl.splits;
+        g.kt_per_split = pl.kt_per_split;
+        g.ws_slot = static_cast<int>(slots);
+        g.sem = static_cast<int>(sems);
+        if (pl.splits > 1) {
+            slots += plan_slots(pl);
+            sems += static_cast<size_t>(pl.tiles_m) * pl.tiles_n;
+        }
+        starts.push_back(static_cast<int>(total));
+        total += static_cast<size_t>(pl.tiles_m) * pl.tiles_n * pl.splits;
         table.push_back(g);
     }
-    if (table.empty()) {
+    if (total > 0x7fffffff || slots > 0x7fffffff) {
         if (sbuf) cudaFreeAsync(sbuf, st);
-        return RB_OK;
+        return RB_ERR_INVALID_ARG;
     }
-    const size_t tbytes = table.size() * sizeof(GroupProblem);
-    const size_t all_bytes = tbytes + starts.size() * sizeof(int);
+    // device layout: [table][starts][item counter][tile counters], zeroed counters uploaded with the table
+    const size_t n = table.size();
+    const size_t tbytes = n * sizeof(GroupProblem);
+    const size_t ctl_off = tbytes + n * sizeof(int);
+    const size_t all_bytes = grouped_table_bytes(n, sems);
+    const size_t ws_bytes = slots * kSlotBytes;
+    const bool staged = staging && staging->host && staging->dev && all_bytes <= staging->bytes &&
+                        (ws_bytes == 0 || (staging->ws && ws_bytes <= staging->ws_bytes));
+    uint8_t* host = nullptr;
+    std::vector<uint8_t> pageable;
     void* dev = nullptr;
-    const bool staged = staging && staging->host && staging->dev && all_bytes <= staging->bytes;
+    float* ws = nullptr;
     if (staged) {
-        // pinned source: one truly asynchronous copy, no allocation
-        std::memcpy(staging->host, table.data(), tbytes);
-        std::memcpy(static_cast<uint8_t*>(staging->host) + tbytes, starts.data(), starts.size() * sizeof(int));
+        host = static_cast<uint8_t*>(staging->host);
         dev = staging->dev;
-        e = cudaMemcpyAsync(dev, staging->host, all_bytes, cudaMemcpyHostToDevice, st);
+        ws = static_cast<float*>(staging->ws);
     } else {
-        e = cudaMallocAsync(&dev, all_bytes, st);
+        pageable.resize(all_bytes);
+        host = pageable.data();
+        e = cudaMallocAsync(&dev, all_bytes + ws_bytes, st);
         if (e != cudaSuccess) { if (ce) *ce = e; if (sbuf) cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-        // pageable sources: the copies are staged before the calls return
-        e = cudaMemcpyAsync(dev, table.data(), tbytes, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(static_cast<uint8_t*>(dev) + tbytes, starts.data(), starts.size() * sizeof(int),
-                                cudaMemcpyHostToDevice, st);
+        if (ws_bytes) ws = reinterpret_cast<float*>(static_cast<uint8_t*>(dev) + all_bytes);
     }
+    std::memcpy(host, table.data(), tbytes);
+    std::memcpy(host + tbytes, starts.data(), n * sizeof(int));
+    std::memset(host + ctl_off, 0, all_bytes - ctl_off);
+    // a pinned source copies asynchronously; a pageable one is staged by the
+    // driver before the call returns
+    e = cudaMemcpyAsync(dev, host, all_bytes, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         static bool attr = false;
         if (!attr) {
@@ -290,12 +512,13 @@ int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* con
         cudaGetDevice(&dev_id);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
         double work = 0;
-        for (size_t i = 0; i < count; ++i) work += 2.0 * probs[i].m * probs[i].n * static_cast<double>(probs[i].k);
+        for (size_t i : order) work += 2.0 * probs[i].m * probs[i].n * static_cast<double>(probs[i].k);
         KernelTimer tmr;
         kernel_timing_begin("grouped_gemm", work, st, &tmr);
-        grouped_gemm_kernel<<<std::min(total, sms), kSimtThreads, kGroupSmem, st>>>(
-            static_cast<const GroupProblem*>(dev),
-            reinterpret_cast<const int*>(static_cast<uint8_t*>(dev) + tbytes), static_cast<int>(table.size()), total,
+        uint8_t* d8 = static_cast<uint8_t*>(dev);
+        grouped_gemm_kernel<<<static_cast<int>(std::min<size_t>(total, sms)), kSimtThreads, kGroupSmem, st>>>(
+            reinterpret_cast<const GroupProblem*>(d8), reinterpret_cast<const int*>(d8 + tbytes),
+            static_cast<int>(n), static_cast<int>(total), reinterpret_cast<int*>(d8 + ctl_off), ws,
             device_error_word());
         kernel_timing_end(&tmr, st);
         count_launch();

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         if (lane == 0) {
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            simt_produce<T, A_K, B_K>(&tmA, &tmB, m0, n0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err);
+            simt_produce<T, A_K, B_K>(&tmA, &tmB, m0, n0, 0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err);
         }
         return;
     }

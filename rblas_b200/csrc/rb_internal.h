@@ -114,16 +114,24 @@ template <typename T, bool CX>
 int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A,
              size_t lda, T* B, size_t ldb, cudaStream_t st, int32_t* ce);
 
-// Staging for the grouped kernel's problem table: a pinned host buffer and a
-// device buffer of `bytes` each, owned by the caller, reused once the
-// previous launch that used them has finished (the serving loop keeps one
-// per stream). Without it every launch allocates its table stream-ordered.
+// Staging for the grouped kernel: a pinned host buffer and a device buffer
+// of `bytes` each for the problem table and its counters, and a split-K
+// workspace of ws_bytes, owned by the caller and reused once the previous
+// launch that used them has finished (the serving loop keeps one set per
+// stream). Without it every launch allocates stream-ordered.
 struct GroupStaging {
     void* host;
     void* dev;
     size_t bytes;
+    void* ws;
+    size_t ws_bytes;
 };
-size_t grouped_table_bytes(size_t count);
+// Table bytes for `count` problems of which split ones hold `sems` C tiles.
+size_t grouped_table_bytes(size_t count, size_t sems);
+// Split-K workspace slots (grouped_slot_bytes() each) one problem needs.
+size_t grouped_ws_slots(const rb_gemm_problem& q);
+size_t grouped_slot_bytes();
+int grouped_splits(const rb_gemm_problem& q);
 
 // rblas's argument checks for one table entry (dtype, layout, transposes,
 // leading dimensions) plus the 32-bit tile-index limit; an rb_status value.

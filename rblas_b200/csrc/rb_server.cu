@@ -12,8 +12,9 @@
 //      released results makes room for the next ones);
 //   3. launches the admitted set as one grouped kernel on the next of two
 //      streams, so a batch starts while the previous one drains.
-// In per-request mode (grouped = 0) every request is its own launch on the
-// same two streams -- the baseline the grouped mode is measured against.
+// In per-request mode (grouped = 0) every admitted request is launched at
+// once as its own single-problem kernel, alternating between the two
+// streams -- the baseline the grouped mode is measured against.
 #include <cuda_runtime.h>
 #include <time.h>
 
@@ -107,6 +108,7 @@ struct Request {
     uint64_t id;
     rb_gemm_problem prob;  // prob.c = C0 (input); the output D is server-owned
     size_t d_bytes, ldd;
+    size_t ws_slots;       // split-K workspace slots of the grouped kernel
     void* d = nullptr;
     int status = -1;  // -1 queued, -2 in flight, else rb_status
     rb_request_times t{};
@@ -126,15 +128,18 @@ public:
     int device = 0;
     Pool pool;
     cudaStream_t streams[2] = {nullptr, nullptr};
-    // per stream: pinned host + device problem table of max_batch entries,
-    // rewritten only after that stream's previous batch has retired
-    GroupStaging staging[2] = {{nullptr, nullptr, 0}, {nullptr, nullptr, 0}};
+    // per stream: pinned host + device problem table of max_batch entries and
+    // a split-K workspace, rewritten only after that stream's previous batch
+    // has retired (grouped mode keeps at most one batch per stream in flight)
+    static constexpr size_t kWsBytes = size_t(256) << 20;
+    GroupStaging staging[2] = {{nullptr, nullptr, 0, nullptr, 0}, {nullptr, nullptr, 0, nullptr, 0}};
+    size_t ws_slot_cap = 0;
     std::vector<cudaEvent_t> free_events;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request*> queue;
     std::unordered_map<uint64_t, Request*> reqs;
-    std::deque<Batch> inflight;
+    std::deque<Batch> inflight[2];  // per stream, in launch order
     std::vector<uint64_t> completed;  // ids finished since the trace player last looked
     bool track_completed = false;
     std::atomic<uint64_t> next_id{1};
@@ -151,13 +156,16 @@ public:
             if (*e != cudaSuccess) return RB_ERR_CUDA;
         }
         if (grouped) {
-            const size_t tb = grouped_table_bytes(static_cast<size_t>(max_batch));
+            ws_slot_cap = kWsBytes / grouped_slot_bytes();
+            const size_t tb = grouped_table_bytes(static_cast<size_t>(max_batch), ws_slot_cap);
             for (auto& g : staging) {
                 *e = cudaMallocHost(&g.host, tb);
                 if (*e != cudaSuccess) return RB_ERR_ALLOC;
-                *e = cudaMalloc(&g.dev, tb);
+                *e = cudaMalloc(&g.dev, tb + kWsBytes);
                 if (*e != cudaSuccess) return RB_ERR_ALLOC;
                 g.bytes = tb;
+                g.ws = static_cast<uint8_t*>(g.dev) + tb;
+                g.ws_bytes = kWsBytes;
             }
         }
         worker = std::thread([this] { loop(); });
@@ -173,14 +181,15 @@ public:
         if (worker.joinable()) worker.join();
         for (auto& s : streams)
             if (s) cudaStreamSynchronize(s);
-        for (auto& b : inflight) cudaEventDestroy(b.done);
+        for (auto& q : inflight)
+            for (auto& b : q) cudaEventDestroy(b.done);
         for (auto ev : free_events) cudaEventDestroy(ev);
         for (auto& s : streams)
             if (s) cudaStreamDestroy(s);
         for (auto& g : staging) {
             if (g.host) cudaFreeHost(g.host);
             if (g.dev) cudaFree(g.dev);
-            g = GroupStaging{nullptr, nullptr, 0};
+            g = GroupStaging{nullptr, nullptr, 0, nullptr, 0};
         }
         for (auto& kv : reqs) delete kv.second;
         pool.release_all();
@@ -197,20 +206,24 @@ public:
         return e;
     }
 
-    // retire finished batches (caller holds mu)
+    size_t inflight_count() const { return inflight[0].size() + inflight[1].size(); }
+
+    // retire finished batches, in order per stream (caller holds mu)
     bool retire() {
         bool any = false;
-        while (!inflight.empty() && cudaEventQuery(inflight.front().done) == cudaSuccess) {
-            Batch& b = inflight.front();
-            const uint64_t t = now_ns();
-            for (Request* r : b.reqs) {
-                if (r->status < 0) r->status = RB_OK;
-                r->t.finish_ns = t;
-                if (track_completed) completed.push_back(r->id);
+        for (auto& q : inflight) {
+            while (!q.empty() && cudaEventQuery(q.front().done) == cudaSuccess) {
+                Batch& b = q.front();
+                const uint64_t t = now_ns();
+                for (Request* r : b.reqs) {
+                    if (r->status < 0) r->status = RB_OK;
+                    r->t.finish_ns = t;
+                    if (track_completed) completed.push_back(r->id);
+                }
+                free_events.push_back(b.done);
+                q.pop_front();
+                any = true;
             }
-            free_events.push_back(b.done);
-            inflight.pop_front();
-            any = true;
         }
         return any;
     }
@@ -248,32 +261,67 @@ public:
         std::unique_lock<std::mutex> lk(mu);
         while (!stop) {
             if (retire()) cv_done.notify_all();
-            std::vector<Request*> batch;
-            // keep two batches in flight: one running, one queued behind it
-            if (!queue.empty() && inflight.size() < 2) {
-                while (!queue.empty() && static_cast<int>(batch.size()) < max_batch) {
+            if (grouped) {
+                // continuous batching: one batch running, one queued behind it;
+                // everything that arrived meanwhile forms the next batch
+                std::vector<Request*> batch;
+                // a stream whose previous batch has retired (its staging is free)
+                const int s = inflight[next_stream].empty() ? next_stream
+                              : (inflight[next_stream ^ 1].empty() ? (next_stream ^ 1) : -1);
+                if (!queue.empty() && s >= 0) {
+                    size_t slots = 0;
+                    while (!queue.empty() && static_cast<int>(batch.size()) < max_batch) {
+                        Request* r = queue.front();
+                        if (slots + r->ws_slots > ws_slot_cap) break;  // next batch
+                        void* d = pool.alloc(r->d_bytes);
+                        if (!d) break;  // wait for results to be released
+                        r->d = d;
+                        r->status = -2;
+                        r->t.admit_ns = now_ns();
+                        slots += r->ws_slots;
+                        queue.pop_front();
+                        batch.push_back(r);
+                    }
+                }
+                if (!batch.empty()) {
+                    inflight[s].push_back(Batch{std::move(batch), get_event(), s});
+                    next_stream = s ^ 1;
+                    const Batch& b = inflight[s].back();
+                    lk.unlock();
+                    const int rc = launch(b);
+                    lk.lock();
+                    if (rc != RB_OK)
+                        for (Request* r : b.reqs) r->status = rc;
+                    continue;
+                }
+            } else {
+                // per request: launch every admitted request at once
+                std::vector<Batch*> fresh;
+                while (!queue.empty() && inflight_count() < kMaxInflightRequests) {
                     Request* r = queue.front();
                     void* d = pool.alloc(r->d_bytes);
-                    if (!d) break;  // wait for results to be released
+                    if (!d) break;
                     r->d = d;
                     r->status = -2;
                     r->t.admit_ns = now_ns();
                     queue.pop_front();
-                    batch.push_back(r);
+                    const int s = next_stream;
+                    next_stream ^= 1;
+                    inflight[s].push_back(Batch{std::vector<Request*>{r}, get_event(), s});
+                    fresh.push_back(&inflight[s].back());
+                }
+                if (!fresh.empty()) {
+                    // only this thread changes `inflight`, so the entries stay put while unlocked
+                    lk.unlock();
+                    std::vector<int> rcs(fresh.size());
+                    for (size_t i = 0; i < fresh.size(); ++i) rcs[i] = launch(*fresh[i]);
+                    lk.lock();
+                    for (size_t i = 0; i < fresh.size(); ++i)
+                        if (rcs[i] != RB_OK) fresh[i]->reqs[0]->status = rcs[i];
+                    continue;
                 }
             }
-            if (!batch.empty()) {
-                inflight.push_back(Batch{std::move(batch), get_event(), next_stream});
-                next_stream ^= 1;
-                const Batch& b = inflight.back();
-                lk.unlock();
-                const int rc = launch(b);
-                lk.lock();
-                if (rc != RB_OK)
-                    for (Request* r : b.reqs) r->status = rc;
-                continue;
-            }
-            if (!inflight.empty()) {
+            if (inflight_count()) {
                 lk.unlock();
                 std::this_thread::sleep_for(std::chrono::microseconds(10));
                 lk.lock();
@@ -282,6 +330,7 @@ public:
             }
         }
     }
+    static constexpr size_t kMaxInflightRequests = 4096;
 };
 
 }  // namespace
@@ -308,6 +357,8 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
     }
     return static_cast<rb_status>(rc);
 }
+
+int rb_gemm_grouped_splits(const rb_gemm_problem* p) { return p ? grouped_splits(*p) : 0; }
 
 rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void** server) {
     if (!server || max_batch < 1 || budget_bytes < 256) return RB_ERR_INVALID_ARG;
@@ -339,6 +390,7 @@ rb_status rb_server_submit(void* server, const rb_gemm_problem* p, uint64_t* id)
     const size_t cols = (p->layout == RB_COL_MAJOR) ? p->n : p->m;
     r->ldd = std::max<size_t>(rup(rows, 16 / el), 16 / el);
     r->d_bytes = r->ldd * std::max<size_t>(cols, 1) * el;
+    r->ws_slots = s->grouped ? grouped_ws_slots(*p) : 0;
     if (r->d_bytes > s->pool.capacity()) {
         delete r;
         return RB_ERR_BUSY;  // can never be admitted under this budget

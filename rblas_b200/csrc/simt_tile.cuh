@@ -55,12 +55,12 @@ __host__ __device__ constexpr int simt_stage_bytes() {
     return (SimtCfg<T>::BM + SimtCfg<T>::BN) * SimtCfg<T>::BK * (int)sizeof(T);
 }
 
-// Producer lane: issue the num_kt K-tile loads of the tile at (m0, n0) on
-// ring iterations it, it+1, ... Returns false (after letting its own copies
-// land) if a wait gave up.
+// Producer lane: issue the num_kt K-tile loads (starting at K-tile kt0) of
+// the tile at (m0, n0) on ring iterations it, it+1, ... Returns false (after
+// letting its own copies land) if a wait gave up.
 template <typename T, bool A_K, bool B_K>
 __device__ __forceinline__ bool simt_produce(const CUtensorMap* tmA, const CUtensorMap* tmB, int m0, int n0,
-                                             int num_kt, uint8_t* smem, int stage_stride, uint64_t* full,
+                                             int kt0, int num_kt, uint8_t* smem, int stage_stride, uint64_t* full,
                                              uint64_t* empty, uint32_t& it, uint32_t* err) {
     using Cfg = SimtCfg<T>;
     constexpr int ST = Cfg::STAGES, BK = Cfg::BK;
@@ -76,7 +76,7 @@ __device__ __forceinline__ bool simt_produce(const CUtensorMap* tmA, const CUten
         uint8_t* sa = smem + s * stage_stride;
         uint8_t* sb = sa + A_BYTES;
         mbar_arrive_expect_tx(&full[s], TX);
-        const int k0 = kt * BK;
+        const int k0 = (kt0 + kt) * BK;
         if (A_K) tma_load_2d(sa, tmA, &full[s], k0, m0);
         else     tma_load_2d(sa, tmA, &full[s], m0, k0);
         if (B_K) tma_load_2d(sb, tmB, &full[s], k0, n0);
@@ -99,12 +99,12 @@ struct SimtOut {
     int tri;        // 0 full C; 1 upper triangle only (row <= col); 2 lower (row >= col)
 };
 
-// Compute warps: consume num_kt stages from ring iteration it, then write
-// C = alpha*acc + beta*C for this tile. Returns false if a wait gave up.
+// Compute warps: consume num_kt stages from ring iteration it into the
+// thread's 8 x TN accumulator. Returns false if a wait gave up.
 template <typename T, bool A_K, bool B_K>
-__device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0, int num_kt, uint8_t* smem,
-                                             int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
-                                             uint32_t* err, int warp, int lane) {
+__device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T>::TN], int num_kt, const uint8_t* smem,
+                                              int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
+                                              uint32_t* err, int warp, int lane) {
     using Cfg = SimtCfg<T>;
     constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, TN = Cfg::TN, ST = Cfg::STAGES;
     constexpr int VEC = Vec16<T>::N;  // elements per 16-byte load
@@ -115,7 +115,6 @@ __device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0
     const int lane_m = lane & 7, lane_n = lane >> 3;  // 8 x 4 lanes
     const int wm0 = wm * 64, wn0 = wn * (4 * TN);
 
-    T acc[8][TN];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -187,8 +186,18 @@ __device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
+    return true;
+}
 
-    // ---------------- epilogue: C = alpha*acc + beta*C ----------------
+// Compute warps: C = alpha*acc + beta*Cin for the tile at (m0, n0).
+template <typename T, bool A_K, bool B_K>
+__device__ __forceinline__ void simt_epilogue(const SimtOut<T>& o, const T (&acc)[8][SimtCfg<T>::TN], int m0,
+                                              int n0, int warp, int lane) {
+    constexpr int TN = SimtCfg<T>::TN;
+    constexpr int VEC = Vec16<T>::N;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int lane_m = lane & 7, lane_n = lane >> 3;
+    const int wm0 = wm * 64, wn0 = wn * (4 * TN);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int r = m0 + (A_K ? (wm0 + lane_m + 8 * i)
@@ -209,6 +218,16 @@ __device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0
             *cp = fma(o.alpha, acc[i][j], t);
         }
     }
+}
+
+// Mainloop then epilogue: one whole tile.
+template <typename T, bool A_K, bool B_K>
+__device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0, int num_kt, uint8_t* smem,
+                                             int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
+                                             uint32_t* err, int warp, int lane) {
+    T acc[8][SimtCfg<T>::TN];
+    if (!simt_mainloop<T, A_K, B_K>(acc, num_kt, smem, stage_stride, full, empty, it, err, warp, lane)) return false;
+    simt_epilogue<T, A_K, B_K>(o, acc, m0, n0, warp, lane);
     return true;
 }
 

@@ -11,7 +11,7 @@ import numpy as np
 from . import _lib
 from .types import Layout, Transpose
 
-__all__ = ["Problem", "grouped_gemm", "Server"]
+__all__ = ["Problem", "grouped_gemm", "grouped_splits", "Server"]
 
 
 @dataclass
@@ -55,6 +55,12 @@ def grouped_gemm(problems, stream=0):
     st = _lib.load().rb_gemm_grouped_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
                                          C.byref(err))
     _lib.check(st, err)
+
+
+def grouped_splits(p: Problem) -> int:
+    """Split-K factor the grouped kernel uses for p (shape-only; 0 if invalid)."""
+    q = p.to_c()
+    return _lib.load().rb_gemm_grouped_splits(C.byref(q))
 
 
 class Server:

@@ -15,7 +15,7 @@ import pytest
 
 import oracle
 from rblas_b200 import level3
-from rblas_b200.serving import Problem, Server, grouped_gemm
+from rblas_b200.serving import Problem, Server, grouped_gemm, grouped_splits
 from rblas_b200.types import Layout
 
 pytestmark = pytest.mark.gpu
@@ -70,6 +70,10 @@ def random_mix(rng, count, max_dim=700):
 def test_grouped_matches_restatement_and_single_calls():
     rng = np.random.default_rng(60)
     probs = random_mix(rng, 48)
+    # split-K cases: few C tiles, long K (f32 and f64, both transposes)
+    probs.append(make_problem(rng, np.float32, Layout.ColMajor, 0, 0, 100, 90, 3000, 1.25, 0.5))
+    probs.append(make_problem(rng, np.float64, Layout.RowMajor, 1, 2, 130, 70, 2500, -0.75, 1.0))
+    probs.append(make_problem(rng, np.float64, Layout.ColMajor, 2, 1, 257, 129, 1111, 0.5, 0.0))
     # edge cases: k == 0, alpha == 0, a 1 x 1 x 1 problem, beta == 0 with NaN C
     probs.append(make_problem(rng, np.float64, Layout.ColMajor, 0, 0, 33, 17, 0, 1.5, -0.5))
     probs.append(make_problem(rng, np.float32, Layout.RowMajor, 1, 0, 40, 21, 13, 0.0, 2.0))
@@ -88,12 +92,34 @@ def test_grouped_matches_restatement_and_single_calls():
     torch.cuda.synchronize()
     for i, ((p, (A, B, Cc)), c0, single) in enumerate(zip(probs, c0s, singles)):
         got = Cc.cpu().numpy()
-        assert np.array_equal(got, single.cpu().numpy(), equal_nan=True), f"problem {i} differs from single call"
+        if grouped_splits(p) == 1:
+            # the same tile code with the same K order as the single-problem kernel
+            assert np.array_equal(got, single.cpu().numpy(), equal_nan=True), f"problem {i} differs from single call"
         if p.beta == 0.0:
             assert not np.any(np.isnan(got))
         ref = restatement(p, A, B, c0)
         tol = 4 * max(p.k, 1) * (2.0 ** -24 if p.dtype == np.float32 else 2.0 ** -53)
         assert normwise(p, got, ref, A, B, c0) <= tol, f"problem {i}"
+
+
+def test_grouped_split_results_independent_of_the_mix():
+    """A split problem gives bit-identical results alone and in a launch
+    with many others (the split factor is shape-only, the K partials are
+    summed in a fixed order)."""
+    rng = np.random.default_rng(64)
+    target, (A, B, C0) = make_problem(rng, np.float32, Layout.ColMajor, 0, 1, 150, 200, 4000, 1.5, -1.0)
+    assert grouped_splits(target) > 1
+    c0 = C0.clone()
+    grouped_gemm([target])
+    torch.cuda.synchronize()
+    alone = C0.clone()
+    C0.copy_(c0)
+    mix = random_mix(rng, 40)
+    grouped_gemm([p for p, _ in mix[:20]] + [target] + [p for p, _ in mix[20:]])
+    torch.cuda.synchronize()
+    assert torch.equal(alone, C0)
+    ref = restatement(target, A, B, c0)
+    assert normwise(target, alone.cpu().numpy(), ref, A, B, c0) <= 4 * 4000 * 2.0 ** -24
 
 
 def test_server_result_same_alone_and_in_a_mix():
