@@ -253,6 +253,33 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
  * whatever else shares the launch. 0 for an invalid problem. */
 int rb_gemm_grouped_splits(const rb_gemm_problem* p);
 
+/* A grouped launch frozen into a CUDA graph: the problem table (with its
+ * TMA descriptors), the split-K workspace and any repack scratch are built
+ * and allocated once; rb_gemm_grouped_plan_launch replays the graph on
+ * `stream` (counter reset, repacks, the grouped kernel) with no host-side
+ * table work. The problems' pointers are fixed at creation; the data they
+ * point to may change between launches. Launches of one plan must not
+ * overlap on the device (they share the workspace). On a validation error
+ * err->got is the index of the offending problem. */
+rb_status rb_gemm_grouped_plan_create(const rb_gemm_problem* problems, size_t count, void** plan,
+                                      rb_error* err);
+rb_status rb_gemm_grouped_plan_launch(void* plan, void* stream, rb_error* err);
+rb_status rb_gemm_grouped_plan_destroy(void* plan);
+
+/* Split-K autotuner of the grouped kernel. Times the candidate split
+ * factors of every shape bucket (floor(log2) of m, n, k in 32..4096, per
+ * dtype) on the current device, installs the winners process-wide and, if
+ * cache_path is not NULL, writes them there; *buckets_tuned = buckets timed.
+ * Takes seconds and about 1.5 GB of device memory while it runs. Launches
+ * planned after the call use the table, so a problem's result depends on its
+ * shape and the installed table only. */
+rb_status rb_autotune_grouped(const char* cache_path, int* buckets_tuned);
+/* Install a table written by rb_autotune_grouped on the same device model
+ * (RB_ERR_INVALID_ARG if the file or its device line does not match). */
+rb_status rb_autotune_load(const char* cache_path);
+/* Back to the built-in split rule. */
+rb_status rb_autotune_reset(void);
+
 /* Per-request timestamps (CLOCK_MONOTONIC ns): submitted, admitted into a
  * batch (result memory reserved), finished (batch completion observed). */
 typedef struct {

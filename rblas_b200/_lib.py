@@ -75,6 +75,12 @@ SIGNATURES = {
     "rb_dgemm_ozaki_noalloc": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _vp, _perr]),
     "rb_gemm_grouped_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _vp, _perr]),
     "rb_gemm_grouped_splits": (_i, [C.POINTER(RbGemmProblem)]),
+    "rb_gemm_grouped_plan_create": (_i, [C.POINTER(RbGemmProblem), _sz, C.POINTER(C.c_void_p), _perr]),
+    "rb_gemm_grouped_plan_launch": (_i, [_vp, _vp, _perr]),
+    "rb_gemm_grouped_plan_destroy": (_i, [_vp]),
+    "rb_autotune_grouped": (_i, [C.c_char_p, C.POINTER(C.c_int)]),
+    "rb_autotune_load": (_i, [C.c_char_p]),
+    "rb_autotune_reset": (_i, []),
     "rb_server_create": (_i, [_sz, _i, _i, C.POINTER(C.c_void_p)]),
     "rb_server_submit": (_i, [_vp, C.POINTER(RbGemmProblem), C.POINTER(C.c_uint64)]),
     "rb_server_wait": (_i, [_vp, C.c_uint64, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),

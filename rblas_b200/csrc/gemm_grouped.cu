@@ -23,6 +23,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -283,7 +286,45 @@ struct Plan {
     int tiles_m, tiles_n, num_kt, splits, kt_per_split;
 };
 
-Plan plan_problem(const rb_gemm_problem& q) {
+// Tuned split factors per shape bucket (floor(log2) of the column-major m, n
+// and of k, per dtype), installed by the autotuner or from its cache file.
+// Readers take a snapshot; a problem's split depends on its shape and on the
+// table installed when its launch was planned.
+std::mutex g_tune_mu;
+std::shared_ptr<const std::map<uint32_t, int>> g_tuned;
+thread_local int t_forced_splits = 0;  // autotuner candidates
+
+int log2_bucket(size_t x) {
+    int b = 0;
+    while (x > 1 && b < 31) {
+        x >>= 1;
+        ++b;
+    }
+    return b;
+}
+
+}  // namespace
+
+uint32_t tune_key(int dtype, size_t m, size_t n, size_t k) {
+    return (static_cast<uint32_t>(dtype & 1) << 24) | (static_cast<uint32_t>(log2_bucket(m)) << 16) |
+           (static_cast<uint32_t>(log2_bucket(n)) << 8) | static_cast<uint32_t>(log2_bucket(k));
+}
+
+void set_tuned_splits(std::shared_ptr<const std::map<uint32_t, int>> table) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned = std::move(table);
+}
+
+void force_grouped_splits(int s) { t_forced_splits = s; }
+
+namespace {
+
+std::shared_ptr<const std::map<uint32_t, int>> tuned_snapshot() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return g_tuned;
+}
+
+Plan plan_problem(const rb_gemm_problem& q, const std::map<uint32_t, int>* tuned = nullptr) {
     Plan pl{};
     const bool ta = q.transa != RB_NO_TRANS, tb = q.transb != RB_NO_TRANS;
     const bool col = q.layout == RB_COL_MAJOR;
@@ -302,13 +343,23 @@ Plan plan_problem(const rb_gemm_problem& q) {
     pl.splits = 1;
     pl.kt_per_split = std::max(pl.num_kt, 1);
     const long tiles = static_cast<long>(pl.tiles_m) * pl.tiles_n;
-    if (pl.m && pl.n && tiles < kWaveItems && pl.num_kt >= 2 * kMinSplitKt) {
-        int s = std::min<long>({static_cast<long>(pl.num_kt / kMinSplitKt), static_cast<long>(kMaxSplit),
-                                (kWaveItems + tiles - 1) / tiles});
-        if (s > 1) {
-            pl.kt_per_split = (pl.num_kt + s - 1) / s;
-            pl.splits = (pl.num_kt + pl.kt_per_split - 1) / pl.kt_per_split;
+    if (!pl.m || !pl.n || pl.num_kt < 2) return pl;
+    int s = 1;
+    if (t_forced_splits > 0) {
+        s = t_forced_splits;
+    } else {
+        auto it = tuned ? tuned->find(tune_key(q.dtype, pl.m, pl.n, pl.k)) : std::map<uint32_t, int>::const_iterator();
+        if (tuned && it != tuned->end()) {
+            s = it->second;
+        } else if (tiles < kWaveItems && pl.num_kt >= 2 * kMinSplitKt) {
+            s = static_cast<int>(std::min<long>({static_cast<long>(pl.num_kt / kMinSplitKt),
+                                                 static_cast<long>(kMaxSplit), (kWaveItems + tiles - 1) / tiles}));
         }
+    }
+    s = std::max(1, std::min({s, kMaxSplit, pl.num_kt}));
+    if (s > 1) {
+        pl.kt_per_split = (pl.num_kt + s - 1) / s;
+        pl.splits = (pl.num_kt + pl.kt_per_split - 1) / pl.kt_per_split;
     }
     return pl;
 }
@@ -325,210 +376,334 @@ size_t grouped_table_bytes(size_t count, size_t sems) {
 
 size_t grouped_ws_slots(const rb_gemm_problem& q) {
     if (validate_problem(q) != RB_OK) return 0;
-    return plan_slots(plan_problem(q));
+    return plan_slots(plan_problem(q, tuned_snapshot().get()));
 }
 
 size_t grouped_slot_bytes() { return kSlotBytes; }
 
 int grouped_splits(const rb_gemm_problem& q) {
     if (validate_problem(q) != RB_OK) return 0;
-    return plan_problem(q).splits;
+    return plan_problem(q, tuned_snapshot().get()).splits;
 }
 
-int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
-                     cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging) {
-    // first pass: validate and plan (row-major -> column-major by swapping the operands)
-    std::vector<Plan> plan(count);
-    for (size_t i = 0; i < count; ++i) {
-        const int v = validate_problem(probs[i]);
-        if (v != RB_OK) {
-            if (bad_index) *bad_index = i;
-            return v;
-        }
-        plan[i] = plan_problem(probs[i]);
-    }
-    // order: longest item first (greedy longest-processing-time scheduling
-    // through the kernel's atomic item counter); estimated time per K-tile
-    // of an item, f32 : f64 about 15 : 8
-    std::vector<size_t> order;
-    order.reserve(count);
-    for (size_t i = 0; i < count; ++i)
-        if (plan[i].m && plan[i].n) order.push_back(i);
-    auto cost = [&](size_t i) {
-        return static_cast<long>(std::min(plan[i].kt_per_split, std::max(plan[i].num_kt, 1))) *
-               (probs[i].dtype ? 8 : 15);
-    };
-    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost(x) > cost(y); });
-    if (order.empty()) return RB_OK;
+namespace {
 
-    // second pass: scratch for operands TMA cannot address directly
-    const size_t elem_of[2] = {4, 8};
-    size_t scratch = 0;
-    std::vector<std::pair<size_t, size_t>> rp_a(count, {SIZE_MAX, 0}), rp_b(count, {SIZE_MAX, 0});
-    for (size_t i : order) {
-        const Plan& pl = plan[i];
-        const rb_gemm_problem& q = probs[i];
-        const size_t el = elem_of[q.dtype];
-        if (pl.num_kt == 0) continue;
-        const bool col = q.layout == RB_COL_MAJOR;
-        const void* a = col ? q.a : q.b;
-        const void* b = col ? q.b : q.a;
-        const size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
-        const size_t vec = 16 / el;
-        if (!tma_aligned(a, lda, el)) {
-            const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k, ld2 = rup(rows, vec);
-            rp_a[i] = {scratch, ld2};
-            scratch += rup(ld2 * cols * el, 256);
+// Host side of one grouped launch: validation, ordering, the split plan,
+// the repacks of operands TMA cannot address, and the device image (table,
+// item starts, zeroed counters). Used by the one-shot path and by plans.
+class GroupBuilder {
+public:
+    struct Repack {
+        const void* src;
+        size_t spitch, dst_off, dpitch, width, height;
+    };
+    size_t n = 0, total = 0, slots = 0, sems = 0, tbytes = 0, ctl_off = 0, all_bytes = 0, scratch = 0;
+    double work = 0;
+    std::vector<Repack> repacks;
+
+    // validate and size everything; *bad = first invalid problem
+    int plan(const rb_gemm_problem* probs, size_t count, size_t* bad) {
+        probs_ = probs;
+        plan_.resize(count);
+        const auto tuned = tuned_snapshot();
+        for (size_t i = 0; i < count; ++i) {
+            const int v = validate_problem(probs[i]);
+            if (v != RB_OK) {
+                if (bad) *bad = i;
+                return v;
+            }
+            plan_[i] = plan_problem(probs[i], tuned.get());
         }
-        if (!tma_aligned(b, ldb, el)) {
-            const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n, ld2 = rup(rows, vec);
-            rp_b[i] = {scratch, ld2};
-            scratch += rup(ld2 * cols * el, 256);
+        // order: longest item first (greedy longest-processing-time
+        // scheduling through the kernel's atomic item counter); estimated
+        // time per K-tile of an item, f32 : f64 about 15 : 8
+        order_.clear();
+        for (size_t i = 0; i < count; ++i)
+            if (plan_[i].m && plan_[i].n) order_.push_back(i);
+        auto cost = [&](size_t i) {
+            return static_cast<long>(std::min(plan_[i].kt_per_split, std::max(plan_[i].num_kt, 1))) *
+                   (probs[i].dtype ? 8 : 15);
+        };
+        std::stable_sort(order_.begin(), order_.end(), [&](size_t x, size_t y) { return cost(x) > cost(y); });
+        rp_a_.assign(count, {SIZE_MAX, 0});
+        rp_b_.assign(count, {SIZE_MAX, 0});
+        scratch = slots = sems = total = 0;
+        work = 0;
+        for (size_t i : order_) {
+            const Plan& pl = plan_[i];
+            const rb_gemm_problem& q = probs[i];
+            const size_t el = q.dtype ? 8 : 4, vec = 16 / el;
+            work += 2.0 * q.m * q.n * static_cast<double>(q.k);
+            if (pl.splits > 1) {
+                slots += plan_slots(pl);
+                sems += static_cast<size_t>(pl.tiles_m) * pl.tiles_n;
+            }
+            total += static_cast<size_t>(pl.tiles_m) * pl.tiles_n * pl.splits;
+            if (pl.num_kt == 0) continue;
+            const bool col = q.layout == RB_COL_MAJOR;
+            if (!tma_aligned(col ? q.a : q.b, col ? q.lda : q.ldb, el)) {
+                const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k, ld2 = rup(rows, vec);
+                rp_a_[i] = {scratch, ld2};
+                scratch += rup(ld2 * cols * el, 256);
+            }
+            if (!tma_aligned(col ? q.b : q.a, col ? q.ldb : q.lda, el)) {
+                const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n, ld2 = rup(rows, vec);
+                rp_b_[i] = {scratch, ld2};
+                scratch += rup(ld2 * cols * el, 256);
+            }
         }
+        if (total > 0x7fffffff || slots > 0x7fffffff) return RB_ERR_INVALID_ARG;
+        n = order_.size();
+        tbytes = n * sizeof(GroupProblem);
+        ctl_off = tbytes + n * sizeof(int);
+        all_bytes = grouped_table_bytes(n, sems);
+        return RB_OK;
     }
-    uint8_t* sbuf = nullptr;
-    cudaError_t e;
-    if (scratch) {
-        e = cudaMallocAsync(reinterpret_cast<void**>(&sbuf), scratch, st);
-        if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
+
+    // write the device image (all_bytes) into `image`, tensor maps pointing
+    // at `scratch_base` for repacked operands; fills `repacks`
+    int encode(const void* const* cin, const size_t* ldcin, uint8_t* scratch_base, uint8_t* image, size_t* bad,
+               int32_t* ce) {
+        repacks.clear();
+        std::vector<int> starts;
+        starts.reserve(n);
+        size_t slot = 0, sem = 0, item = 0, row = 0;
+        for (size_t i : order_) {
+            const rb_gemm_problem& q = probs_[i];
+            const Plan& pl = plan_[i];
+            const size_t el = q.dtype ? 8 : 4;
+            const bool f64 = q.dtype == 1;
+            const bool col = q.layout == RB_COL_MAJOR;
+            const void* a = col ? q.a : q.b;
+            const void* b = col ? q.b : q.a;
+            size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
+            if (rp_a_[i].first != SIZE_MAX) {
+                const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k;
+                repacks.push_back({a, lda * el, rp_a_[i].first, rp_a_[i].second * el, rows * el, cols});
+                a = scratch_base + rp_a_[i].first;
+                lda = rp_a_[i].second;
+            }
+            if (rp_b_[i].first != SIZE_MAX) {
+                const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n;
+                repacks.push_back({b, ldb * el, rp_b_[i].first, rp_b_[i].second * el, rows * el, cols});
+                b = scratch_base + rp_b_[i].first;
+                ldb = rp_b_[i].second;
+            }
+            GroupProblem g{};
+            const int BM = 128, BN = f64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+            const int BK = f64 ? SimtCfg<double>::BK : SimtCfg<float>::BK;
+            const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+            const bool a_k = pl.ta, b_k = !pl.tb;
+            CUresult r = CUDA_SUCCESS;
+            if (pl.num_kt > 0) {
+                r = a_k ? make_tmap_2d(&g.tmA, a, dt, el, pl.k, pl.m, lda, BK, BM, true)
+                        : make_tmap_2d(&g.tmA, a, dt, el, pl.m, pl.k, lda, BM, BK, false);
+                if (r == CUDA_SUCCESS)
+                    r = b_k ? make_tmap_2d(&g.tmB, b, dt, el, pl.k, pl.n, ldb, BK, BN, true)
+                            : make_tmap_2d(&g.tmB, b, dt, el, pl.n, pl.k, ldb, BN, BK, false);
+            }
+            if (r != CUDA_SUCCESS) {
+                if (ce) *ce = static_cast<int32_t>(r);
+                if (bad) *bad = i;
+                return RB_ERR_CUDA;
+            }
+            g.c = q.c;
+            g.ldc = q.ldc;
+            g.cin = cin ? cin[i] : q.c;
+            g.ldcin = ldcin ? ldcin[i] : q.ldc;
+            // k == 0 or alpha == 0: C = beta*Cin exactly (alpha*0 would turn an inf alpha into NaN)
+            g.alpha = pl.num_kt ? q.alpha : 0.0;
+            g.beta = q.beta;
+            g.m = static_cast<int>(pl.m);
+            g.n = static_cast<int>(pl.n);
+            g.num_kt = pl.num_kt;
+            g.variant = (f64 ? 4 : 0) + (a_k ? 2 : 0) + (b_k ? 1 : 0);
+            g.tiles_m = pl.tiles_m;
+            g.tiles_n = pl.tiles_n;
+            g.beta_mode = (q.beta == 0.0) ? 0 : (q.beta == 1.0 ? 1 : 2);
+            g.splits = pl.splits;
+            g.kt_per_split = pl.kt_per_split;
+            g.ws_slot = static_cast<int>(slot);
+            g.sem = static_cast<int>(sem);
+            if (pl.splits > 1) {
+                slot += plan_slots(pl);
+                sem += static_cast<size_t>(pl.tiles_m) * pl.tiles_n;
+            }
+            starts.push_back(static_cast<int>(item));
+            item += static_cast<size_t>(pl.tiles_m) * pl.tiles_n * pl.splits;
+            std::memcpy(image + row * sizeof(GroupProblem), &g, sizeof(GroupProblem));
+            ++row;
+        }
+        std::memcpy(image + tbytes, starts.data(), n * sizeof(int));
+        std::memset(image + ctl_off, 0, all_bytes - ctl_off);
+        return RB_OK;
     }
-    std::vector<GroupProblem> table;
-    std::vector<int> starts;
-    table.reserve(order.size());
-    starts.reserve(order.size());
-    size_t total = 0, slots = 0, sems = 0;
-    for (size_t i : order) {
-        const rb_gemm_problem& q = probs[i];
-        const Plan& pl = plan[i];
-        const size_t el = elem_of[q.dtype];
-        const bool f64 = q.dtype == 1;
-        const bool col = q.layout == RB_COL_MAJOR;
-        const void* a = col ? q.a : q.b;
-        const void* b = col ? q.b : q.a;
-        size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
-        if (rp_a[i].first != SIZE_MAX) {
-            const size_t rows = pl.ta ? pl.k : pl.m, cols = pl.ta ? pl.m : pl.k;
-            e = cudaMemcpy2DAsync(sbuf + rp_a[i].first, rp_a[i].second * el, a, lda * el, rows * el, cols,
-                                  cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) { if (ce) *ce = e; cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-            a = sbuf + rp_a[i].first;
-            lda = rp_a[i].second;
+
+    cudaError_t enqueue_repacks(uint8_t* scratch_base, cudaStream_t st) const {
+        for (const Repack& r : repacks) {
+            const cudaError_t e = cudaMemcpy2DAsync(scratch_base + r.dst_off, r.dpitch, r.src, r.spitch, r.width,
+                                                    r.height, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
         }
-        if (rp_b[i].first != SIZE_MAX) {
-            const size_t rows = pl.tb ? pl.n : pl.k, cols = pl.tb ? pl.k : pl.n;
-            e = cudaMemcpy2DAsync(sbuf + rp_b[i].first, rp_b[i].second * el, b, ldb * el, rows * el, cols,
-                                  cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) { if (ce) *ce = e; cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-            b = sbuf + rp_b[i].first;
-            ldb = rp_b[i].second;
-        }
-        GroupProblem g{};
-        const int BM = 128, BN = f64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-        const int BK = f64 ? SimtCfg<double>::BK : SimtCfg<float>::BK;
-        const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        const bool a_k = pl.ta, b_k = !pl.tb;
-        CUresult r = CUDA_SUCCESS;
-        if (pl.num_kt > 0) {
-            r = a_k ? make_tmap_2d(&g.tmA, a, dt, el, pl.k, pl.m, lda, BK, BM, true)
-                    : make_tmap_2d(&g.tmA, a, dt, el, pl.m, pl.k, lda, BM, BK, false);
-            if (r == CUDA_SUCCESS)
-                r = b_k ? make_tmap_2d(&g.tmB, b, dt, el, pl.k, pl.n, ldb, BK, BN, true)
-                        : make_tmap_2d(&g.tmB, b, dt, el, pl.n, pl.k, ldb, BN, BK, false);
-        }
-        if (r != CUDA_SUCCESS) {
-            if (ce) *ce = static_cast<int32_t>(r);
-            if (bad_index) *bad_index = i;
-            if (sbuf) cudaFreeAsync(sbuf, st);
-            return RB_ERR_CUDA;
-        }
-        g.c = q.c;
-        g.ldc = q.ldc;
-        g.cin = cin ? cin[i] : q.c;
-        g.ldcin = ldcin ? ldcin[i] : q.ldc;
-        // k == 0 or alpha == 0: C = beta*Cin exactly (alpha*0 would turn an inf alpha into NaN)
-        g.alpha = pl.num_kt ? q.alpha : 0.0;
-        g.beta = q.beta;
-        g.m = static_cast<int>(pl.m);
-        g.n = static_cast<int>(pl.n);
-        g.num_kt = pl.num_kt;
-        g.variant = (f64 ? 4 : 0) + (a_k ? 2 : 0) + (b_k ? 1 : 0);
-        g.tiles_m = pl.tiles_m;
-        g.tiles_n = pl.tiles_n;
-        g.beta_mode = (q.beta == 0.0) ? 0 : (q.beta == 1.0 ? 1 : 2);
-        g.splits = pl.splits;
-        g.kt_per_split = pl.kt_per_split;
-        g.ws_slot = static_cast<int>(slots);
-        g.sem = static_cast<int>(sems);
-        if (pl.splits > 1) {
-            slots += plan_slots(pl);
-            sems += static_cast<size_t>(pl.tiles_m) * pl.tiles_n;
-        }
-        starts.push_back(static_cast<int>(total));
-        total += static_cast<size_t>(pl.tiles_m) * pl.tiles_n * pl.splits;
-        table.push_back(g);
+        return cudaSuccess;
     }
-    if (total > 0x7fffffff || slots > 0x7fffffff) {
-        if (sbuf) cudaFreeAsync(sbuf, st);
-        return RB_ERR_INVALID_ARG;
-    }
-    // device layout: [table][starts][item counter][tile counters], zeroed counters uploaded with the table
-    const size_t n = table.size();
-    const size_t tbytes = n * sizeof(GroupProblem);
-    const size_t ctl_off = tbytes + n * sizeof(int);
-    const size_t all_bytes = grouped_table_bytes(n, sems);
-    const size_t ws_bytes = slots * kSlotBytes;
-    const bool staged = staging && staging->host && staging->dev && all_bytes <= staging->bytes &&
-                        (ws_bytes == 0 || (staging->ws && ws_bytes <= staging->ws_bytes));
-    uint8_t* host = nullptr;
-    std::vector<uint8_t> pageable;
-    void* dev = nullptr;
-    float* ws = nullptr;
-    if (staged) {
-        host = static_cast<uint8_t*>(staging->host);
-        dev = staging->dev;
-        ws = static_cast<float*>(staging->ws);
-    } else {
-        pageable.resize(all_bytes);
-        host = pageable.data();
-        e = cudaMallocAsync(&dev, all_bytes + ws_bytes, st);
-        if (e != cudaSuccess) { if (ce) *ce = e; if (sbuf) cudaFreeAsync(sbuf, st); return RB_ERR_CUDA; }
-        if (ws_bytes) ws = reinterpret_cast<float*>(static_cast<uint8_t*>(dev) + all_bytes);
-    }
-    std::memcpy(host, table.data(), tbytes);
-    std::memcpy(host + tbytes, starts.data(), n * sizeof(int));
-    std::memset(host + ctl_off, 0, all_bytes - ctl_off);
-    // a pinned source copies asynchronously; a pageable one is staged by the
-    // driver before the call returns
-    e = cudaMemcpyAsync(dev, host, all_bytes, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) {
+
+    // the kernel over a device image already in place (counters zeroed)
+    cudaError_t launch(uint8_t* dev_image, float* ws, cudaStream_t st, bool timed) const {
         static bool attr = false;
         if (!attr) {
-            e = cudaFuncSetAttribute(grouped_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
-            attr = (e == cudaSuccess);
+            const cudaError_t e =
+                cudaFuncSetAttribute(grouped_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
+            if (e != cudaSuccess) return e;
+            attr = true;
         }
-    }
-    if (e == cudaSuccess) {
         int dev_id = 0, sms = 148;
         cudaGetDevice(&dev_id);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
-        double work = 0;
-        for (size_t i : order) work += 2.0 * probs[i].m * probs[i].n * static_cast<double>(probs[i].k);
         KernelTimer tmr;
-        kernel_timing_begin("grouped_gemm", work, st, &tmr);
-        uint8_t* d8 = static_cast<uint8_t*>(dev);
+        if (timed) kernel_timing_begin("grouped_gemm", work, st, &tmr);
         grouped_gemm_kernel<<<static_cast<int>(std::min<size_t>(total, sms)), kSimtThreads, kGroupSmem, st>>>(
-            reinterpret_cast<const GroupProblem*>(d8), reinterpret_cast<const int*>(d8 + tbytes),
-            static_cast<int>(n), static_cast<int>(total), reinterpret_cast<int*>(d8 + ctl_off), ws,
+            reinterpret_cast<const GroupProblem*>(dev_image), reinterpret_cast<const int*>(dev_image + tbytes),
+            static_cast<int>(n), static_cast<int>(total), reinterpret_cast<int*>(dev_image + ctl_off), ws,
             device_error_word());
-        kernel_timing_end(&tmr, st);
-        count_launch();
-        e = cudaGetLastError();
+        if (timed) kernel_timing_end(&tmr, st);
+        if (timed) count_launch();  // a captured launch is counted at each replay
+        return cudaGetLastError();
     }
-    if (!staged) cudaFreeAsync(dev, st);
-    if (sbuf) cudaFreeAsync(sbuf, st);
-    if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
+
+private:
+    const rb_gemm_problem* probs_ = nullptr;
+    std::vector<Plan> plan_;
+    std::vector<size_t> order_;
+    std::vector<std::pair<size_t, size_t>> rp_a_, rp_b_;
+};
+
+}  // namespace
+
+int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
+                     cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging) {
+    GroupBuilder gb;
+    int rc = gb.plan(probs, count, bad_index);
+    if (rc != RB_OK || gb.n == 0) return rc;
+    if (!device_error_word()) return RB_ERR_ALLOC;
+    const size_t ws_bytes = gb.slots * kSlotBytes;
+    const bool staged = staging && staging->host && staging->dev && gb.all_bytes <= staging->bytes &&
+                        (ws_bytes == 0 || (staging->ws && ws_bytes <= staging->ws_bytes));
+    uint8_t* host = nullptr;
+    std::vector<uint8_t> pageable;
+    uint8_t* dev = nullptr;
+    float* ws = nullptr;
+    cudaError_t e;
+    // one stream-ordered allocation for what staging does not cover: [image][workspace][repack scratch]
+    const size_t own = (staged ? 0 : gb.all_bytes + ws_bytes) + gb.scratch;
+    uint8_t* mem = nullptr;
+    if (own) {
+        e = cudaMallocAsync(reinterpret_cast<void**>(&mem), own, st);
+        if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
+    }
+    if (staged) {
+        host = static_cast<uint8_t*>(staging->host);
+        dev = static_cast<uint8_t*>(staging->dev);
+        ws = static_cast<float*>(staging->ws);
+    } else {
+        pageable.resize(gb.all_bytes);
+        host = pageable.data();
+        dev = mem;
+        if (ws_bytes) ws = reinterpret_cast<float*>(mem + gb.all_bytes);
+    }
+    uint8_t* scratch = gb.scratch ? mem + (staged ? 0 : gb.all_bytes + ws_bytes) : nullptr;
+    rc = gb.encode(cin, ldcin, scratch, host, bad_index, ce);
+    if (rc == RB_OK) {
+        // a pinned source copies asynchronously; a pageable one is staged by
+        // the driver before the call returns
+        e = gb.enqueue_repacks(scratch, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dev, host, gb.all_bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = gb.launch(dev, ws, st, true);
+        if (e != cudaSuccess) {
+            if (ce) *ce = e;
+            rc = RB_ERR_CUDA;
+        }
+    }
+    if (mem) cudaFreeAsync(mem, st);
+    return rc;
+}
+
+// A grouped launch frozen into a CUDA graph: table, workspace and repack
+// scratch allocated once; each replay re-zeroes the counters, redoes the
+// repacks (operand contents may change between replays) and runs the kernel.
+struct GroupedPlan {
+    uint8_t* mem = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GroupedPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (mem) cudaFree(mem);
+    }
+};
+
+int grouped_plan_create(const rb_gemm_problem* probs, size_t count, void** out, int32_t* ce, size_t* bad) {
+    GroupBuilder gb;
+    int rc = gb.plan(probs, count, bad);
+    if (rc != RB_OK) return rc;
+    if (!device_error_word()) return RB_ERR_ALLOC;
+    GroupedPlan* pl = new GroupedPlan();
+    const size_t ws_bytes = gb.slots * kSlotBytes;
+    const size_t total = rup(gb.all_bytes, 256) + ws_bytes + gb.scratch;
+    cudaError_t e = cudaSuccess;
+    if (total) e = cudaMalloc(&pl->mem, total);
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        delete pl;
+        return RB_ERR_ALLOC;
+    }
+    uint8_t* dev = pl->mem;
+    float* ws = ws_bytes ? reinterpret_cast<float*>(pl->mem + rup(gb.all_bytes, 256)) : nullptr;
+    uint8_t* scratch = gb.scratch ? pl->mem + rup(gb.all_bytes, 256) + ws_bytes : nullptr;
+    std::vector<uint8_t> image(gb.all_bytes);
+    if (gb.n) rc = gb.encode(nullptr, nullptr, scratch, image.data(), bad, ce);
+    if (rc == RB_OK && gb.n) e = cudaMemcpy(dev, image.data(), gb.all_bytes, cudaMemcpyHostToDevice);
+    cudaStream_t cs = nullptr;
+    if (rc == RB_OK && e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (rc == RB_OK && e == cudaSuccess) {
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t e2 = cudaSuccess;
+            if (gb.n) {
+                e2 = cudaMemsetAsync(dev + gb.ctl_off, 0, gb.all_bytes - gb.ctl_off, cs);
+                if (e2 == cudaSuccess) e2 = gb.enqueue_repacks(scratch, cs);
+                if (e2 == cudaSuccess) e2 = gb.launch(dev, ws, cs, false);
+            }
+            e = cudaStreamEndCapture(cs, &pl->graph);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+    }
+    if (cs) cudaStreamDestroy(cs);
+    if (rc == RB_OK && e != cudaSuccess) {
+        if (ce) *ce = e;
+        rc = RB_ERR_CUDA;
+    }
+    if (rc != RB_OK) {
+        delete pl;
+        return rc;
+    }
+    *out = pl;
     return RB_OK;
 }
+
+int grouped_plan_launch(void* plan, cudaStream_t st, int32_t* ce) {
+    GroupedPlan* pl = static_cast<GroupedPlan*>(plan);
+    const cudaError_t e = cudaGraphLaunch(pl->exec, st);
+    count_launch();
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        return RB_ERR_CUDA;
+    }
+    return RB_OK;
+}
+
+void grouped_plan_destroy(void* plan) { delete static_cast<GroupedPlan*>(plan); }
 
 int single_gemm_dev(const rb_gemm_problem* prob, const void* cin, size_t ldcin, cudaStream_t st, int32_t* ce) {
     const rb_gemm_problem& q = *prob;

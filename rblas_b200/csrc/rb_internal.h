@@ -8,6 +8,8 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <map>
+#include <memory>
 #include <mutex>
 
 #include "../../include/rblas_b200.h"
@@ -132,6 +134,13 @@ size_t grouped_table_bytes(size_t count, size_t sems);
 size_t grouped_ws_slots(const rb_gemm_problem& q);
 size_t grouped_slot_bytes();
 int grouped_splits(const rb_gemm_problem& q);
+// Split-K autotuning: bucket key of a (column-major) shape, the installed
+// table of tuned factors (nullptr: the built-in rule), and a per-thread
+// forced factor for timing candidates (0: off).
+uint32_t tune_key(int dtype, size_t m, size_t n, size_t k);
+void set_tuned_splits(std::shared_ptr<const std::map<uint32_t, int>> table);
+void force_grouped_splits(int s);
+constexpr int kGroupedMaxSplit = 16;
 
 // rblas's argument checks for one table entry (dtype, layout, transposes,
 // leading dimensions) plus the 32-bit tile-index limit; an rb_status value.
@@ -142,6 +151,11 @@ int validate_problem(const rb_gemm_problem& q);
 // while the result goes to problems[i].c. *bad_index: first invalid problem.
 int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
                      cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging = nullptr);
+
+// Grouped launch frozen into a CUDA graph (rb_gemm_grouped_plan_*).
+int grouped_plan_create(const rb_gemm_problem* probs, size_t count, void** plan, int32_t* ce, size_t* bad);
+int grouped_plan_launch(void* plan, cudaStream_t st, int32_t* ce);
+void grouped_plan_destroy(void* plan);
 
 // One problem of the serving loop's per-request mode: the single-problem
 // plain kernel (one launch), result to probs->c, C0 read from cin.

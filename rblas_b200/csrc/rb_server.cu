@@ -360,6 +360,44 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
 
 int rb_gemm_grouped_splits(const rb_gemm_problem* p) { return p ? grouped_splits(*p) : 0; }
 
+rb_status rb_gemm_grouped_plan_create(const rb_gemm_problem* problems, size_t count, void** plan, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if (!plan || (count && !problems)) {
+        if (err) err->code = RB_ERR_INVALID_ARG;
+        return RB_ERR_INVALID_ARG;
+    }
+    int32_t ce = 0;
+    size_t bad = 0;
+    const int rc = grouped_plan_create(problems, count, plan, &ce, &bad);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->got = bad;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
+
+rb_status rb_gemm_grouped_plan_launch(void* plan, void* stream, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if (!plan) {
+        if (err) err->code = RB_ERR_INVALID_ARG;
+        return RB_ERR_INVALID_ARG;
+    }
+    int32_t ce = 0;
+    const int rc = grouped_plan_launch(plan, static_cast<cudaStream_t>(stream), &ce);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
+
+rb_status rb_gemm_grouped_plan_destroy(void* plan) {
+    if (!plan) return RB_ERR_INVALID_ARG;
+    grouped_plan_destroy(plan);
+    return RB_OK;
+}
+
 rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void** server) {
     if (!server || max_batch < 1 || budget_bytes < 256) return RB_ERR_INVALID_ARG;
     Server* s = new Server();

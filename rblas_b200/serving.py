@@ -11,7 +11,8 @@ import numpy as np
 from . import _lib
 from .types import Layout, Transpose
 
-__all__ = ["Problem", "grouped_gemm", "grouped_splits", "Server"]
+__all__ = ["Problem", "grouped_gemm", "grouped_splits", "GroupedPlan", "Server", "autotune", "autotune_load",
+           "autotune_reset"]
 
 
 @dataclass
@@ -55,6 +56,60 @@ def grouped_gemm(problems, stream=0):
     st = _lib.load().rb_gemm_grouped_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
                                          C.byref(err))
     _lib.check(st, err)
+
+
+class GroupedPlan:
+    """A grouped launch frozen into a CUDA graph (rb_gemm_grouped_plan_*):
+    built once, replayed with launch(stream)."""
+
+    def __init__(self, problems):
+        self._lib = _lib.load()
+        arr = _array(problems)
+        h = C.c_void_p()
+        err = _lib.RbError()
+        st = self._lib.rb_gemm_grouped_plan_create(arr, len(problems), C.byref(h), C.byref(err))
+        _lib.check(st, err)
+        self._h = h
+
+    def launch(self, stream=0):
+        err = _lib.RbError()
+        st = self._lib.rb_gemm_grouped_plan_launch(self._h, C.c_void_p(stream) if stream else None, C.byref(err))
+        _lib.check(st, err)
+
+    def close(self):
+        if self._h:
+            self._lib.rb_gemm_grouped_plan_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _check(st):
+    err = _lib.RbError()
+    err.code = st
+    _lib.check(st, err)
+
+
+def autotune(cache_path: str | None = None) -> int:
+    """Run the grouped kernel's split-K autotuner (rb_autotune_grouped) and
+    install its table; returns the number of shape buckets timed."""
+    n = C.c_int()
+    st = _lib.load().rb_autotune_grouped(cache_path.encode() if cache_path else None, C.byref(n))
+    _check(st)
+    return n.value
+
+
+def autotune_load(cache_path: str) -> None:
+    st = _lib.load().rb_autotune_load(cache_path.encode())
+    _check(st)
+
+
+def autotune_reset() -> None:
+    _lib.load().rb_autotune_reset()
 
 
 def grouped_splits(p: Problem) -> int:
