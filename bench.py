@@ -358,6 +358,70 @@ def run_ours(args):
         del SA, SB, SC
         torch.cuda.empty_cache()
 
+    # ---- the other configurations: SGEMM 1024^3 (C1), tall-skinny SGEMM
+    # 65536x128x8192 (C3), complex 2048^3 ConjTrans/NoTrans (C4) and the
+    # batched f64 trsm 512^2 x 64 right-hand sides x 1024 (C4)
+    others = {}
+    if not args.no_configs:
+        from rblas_b200 import complex3
+
+        def form_times(fn_for, work, forms, reps):
+            res = {}
+            for name, prec in forms:
+                ms, launches, kr3 = timed(fn_for(prec), reps, 2)
+                res[name] = {"tflops": work / (ms * 1e-3) / 1e12, "ms": ms, "launches_per_call": launches / reps,
+                             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in kr3.items()}}
+            return res
+
+        g2 = torch.Generator(device=dev)
+        g2.manual_seed(1234)
+        # C1: f32 col-major NN 1024^3, alpha = 1, beta = 0
+        n1 = 1024
+        X1 = [torch.rand(n1 * n1, dtype=torch.float32, device=dev, generator=g2) * 2 - 1 for _ in range(3)]
+        others["c1_sgemm_1024"] = form_times(
+            lambda prec: (lambda: level3.gemm_dev(Layout.ColMajor, 0, 0, n1, n1, n1, 1.0, X1[0].data_ptr(), n1,
+                                                  X1[1].data_ptr(), n1, 0.0, X1[2].data_ptr(), n1, np.float32,
+                                                  prec=prec, stream=sh)),
+            2.0 * n1 ** 3, (("plain", Precision.Plain), ("bf16x3", Precision.Bf16x3), ("bf16x6", Precision.Bf16x6)), 20)
+        del X1
+        # C3 tall-skinny: 65536 x 128 x 8192, alpha = beta = 1
+        m3, n3, k3 = 65536, 128, 8192
+        A3 = torch.rand(m3 * k3, dtype=torch.float32, device=dev, generator=g2) * 2 - 1
+        B3 = torch.rand(k3 * n3, dtype=torch.float32, device=dev, generator=g2) * 2 - 1
+        C3 = torch.rand(m3 * n3, dtype=torch.float32, device=dev, generator=g2) * 2 - 1
+        others["c3_sgemm_65536x128x8192"] = form_times(
+            lambda prec: (lambda: level3.gemm_dev(Layout.ColMajor, 0, 0, m3, n3, k3, 1.0, A3.data_ptr(), m3,
+                                                  B3.data_ptr(), k3, 1.0, C3.data_ptr(), m3, np.float32,
+                                                  prec=prec, stream=sh)),
+            2.0 * m3 * n3 * k3, (("plain", Precision.Plain), ("bf16x3", Precision.Bf16x3), ("bf16x6", Precision.Bf16x6)), 5)
+        others["c3_sgemm_65536x128x8192"]["min_bytes"] = 4 * (m3 * k3 + k3 * n3 + 2 * m3 * n3)
+        del A3, B3, C3
+        # C4 complex: ConjTrans/NoTrans 2048^3, alpha = (1, 0.5), beta = 0; 8mnk real flop (4M)
+        n4 = 2048
+        for cdt, tdt, cforms in ((np.complex128, torch.float64, (("plain", Precision.Plain), ("ozaki", Precision.Ozaki))),
+                                 (np.complex64, torch.float32, (("plain", Precision.Plain), ("bf16x3", Precision.Bf16x3),
+                                                                ("bf16x6", Precision.Bf16x6)))):
+            Xc = [torch.randn(2 * n4 * n4, dtype=tdt, device=dev, generator=g2) for _ in range(3)]
+            others["c4_%s_2048_CN" % ("zgemm" if cdt == np.complex128 else "cgemm")] = form_times(
+                lambda prec: (lambda: complex3.gemm_dev(2, 0, n4, n4, n4, 1.0 + 0.5j, Xc[0].data_ptr(), n4,
+                                                        Xc[1].data_ptr(), n4, 0.0, Xc[2].data_ptr(), n4, cdt,
+                                                        prec=prec, stream=sh)),
+                8.0 * n4 ** 3, cforms, 4)
+            del Xc
+        # C4 batched trsm: 1024 x (512 x 512 lower, 64 RHS), f64; m^2 n flop each
+        qb, nb_, batch = 512, 64, 1024
+        At = torch.randn(qb * qb * batch, dtype=torch.float64, device=dev, generator=g2) * (0.1 / qb ** 0.5)
+        At.view(batch, qb, qb).diagonal(dim1=1, dim2=2).uniform_(1.0, 2.0)
+        Bt = torch.rand(qb * nb_ * batch, dtype=torch.float64, device=dev, generator=g2) * 2 - 1
+        ms, launches, kr4 = timed(lambda: level3.trsm_batched_dev(0, 1, 0, 0, qb, nb_, 1.0, At.data_ptr(), qb,
+                                                                  qb * qb, Bt.data_ptr(), qb, qb * nb_, batch,
+                                                                  np.float64, stream=sh), 5, 2)
+        others["c4_dtrsm_batched_512x64x1024"] = {
+            "tflops": qb * qb * nb_ * batch / (ms * 1e-3) / 1e12, "ms": ms, "launches_per_call": launches / 5,
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in kr4.items()}}
+        del At, Bt
+        torch.cuda.empty_cache()
+
     # ---- e2e through the public host API (pinned host buffers) -------------
     e2e = None
     if not args.no_e2e:
@@ -427,7 +491,8 @@ def run_ours(args):
             "form": headline_name, "config": config_block(args), "forms": forms,
             "clocks": clocks, "e2e": e2e, "gpu_launches": hl["gpu_launches"],
             "roofline": roofline, "cpu_baseline": cpu, "peaks_measured": peaks,
-            "sgemm_8192": sgemm, "serving": serving, "device_error": err_status[0],
+            "sgemm_8192": sgemm, "configs": others, "serving": serving,
+            "device_error": {"after_headline": err_status[0], "end_of_run": rb.device_error()[0]},
         }
         print(json.dumps(line))
     if dist:
@@ -564,6 +629,35 @@ def run_kernel_only(args):
                       "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}))
 
 
+def run_trsm_batched_only(args):
+    """The batched f64 trsm of the C4 configuration (512 x 512 lower, 64
+    right-hand sides) on `--trsm-batched BATCH` members, launched warmup +
+    steps times (for ncu captures on a bounded batch)."""
+    import torch
+
+    from rblas_b200 import level3
+
+    q, nrhs, batch = 512, 64, args.trsm_batched
+    g = torch.Generator(device="cuda")
+    g.manual_seed(8)
+    A = torch.randn(q * q * batch, dtype=torch.float64, device="cuda", generator=g) * (0.1 / q ** 0.5)
+    A.view(batch, q, q).diagonal(dim1=1, dim2=2).uniform_(1.0, 2.0)
+    B = torch.rand(q * nrhs * batch, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    sh = torch.cuda.current_stream().cuda_stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            e0.record()
+        level3.trsm_batched_dev(0, 1, 0, 0, q, nrhs, 1.0, A.data_ptr(), q, q * q, B.data_ptr(), q, q * nrhs,
+                                batch, np.float64, stream=sh)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"trsm_batched": [q, nrhs, batch], "ms": ms,
+                      "tflops": q * q * nrhs * batch / (ms * 1e-3) / 1e12}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,16 +671,21 @@ def main():
     ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,
                     metavar=("M", "N", "K"), help="time one column-major GEMM shape only")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--trsm-batched", type=int, default=0, metavar="BATCH",
+                    help="time the batched f64 trsm (512 x 512, 64 RHS) on BATCH members only")
     ap.add_argument("--serve", action="store_true", help="serving sweep (request stream replay)")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rates", default="1000,2000,5000,8000,10000,12500,15000,17500,20000,25000,30000,50000")
     ap.add_argument("--no-autotune", action="store_true", help="serving: keep the built-in split-K rule")
     ap.add_argument("--no-serve", action="store_true", help="default run: skip the serving summary")
+    ap.add_argument("--no-configs", action="store_true", help="default run: skip the C1/C3/C4 measurements")
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--ta", type=int, default=0)
     ap.add_argument("--tb", type=int, default=0)
     args = ap.parse_args()
-    if args.serve:
+    if args.trsm_batched:
+        run_trsm_batched_only(args)
+    elif args.serve:
         run_serve_mode(args)
     elif args.shape:
         run_kernel_only(args)

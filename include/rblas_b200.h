@@ -219,6 +219,23 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                        size_t n, double alpha, const double* a, size_t lda, double* b, size_t ldb,
                        void* stream, rb_error* err);
 
+/* Batched trsm on device pointers (no counterpart in the reference, which
+ * solves one problem per call: trsm, src/level3.rs:390-520). Problem i solves
+ * with A_i = a + i*stride_a and B_i = b + i*stride_b (elements), all sharing
+ * side, uplo, trans, diag, m, n, alpha, lda, ldb; column-major like rblas.
+ * One launch for the batch: each CTA keeps a slice of B_i's right-hand sides
+ * in shared memory for the whole solve (32 right-hand sides per CTA up to
+ * order 652 f64 / 1560 f32, 16 or 8 up to 2608 f64 / 6240 f32; larger orders
+ * fall back to the single-problem path per member). The B_i must not
+ * overlap. Enqueued on `stream`. */
+rb_status rb_strsm_batched_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                               size_t n, float alpha, const float* a, size_t lda, size_t stride_a, float* b,
+                               size_t ldb, size_t stride_b, size_t batch, void* stream, rb_error* err);
+rb_status rb_dtrsm_batched_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,
+                               size_t n, double alpha, const double* a, size_t lda, size_t stride_a,
+                               double* b, size_t ldb, size_t stride_b, size_t batch, void* stream,
+                               rb_error* err);
+
 /* ---------------------------------------------------------------------------
  * Grouped GEMM and the serving loop (no counterpart in the reference: rblas
  * is a synchronous library; these are the batching and serving forms of its

@@ -72,6 +72,9 @@ SIGNATURES = {
     "rb_ctrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_dtrsm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_strsm_batched_dev": (_i, [_i, _i, _i, _i, _sz, _sz, C.c_float, _vp, _sz, _sz, _vp, _sz, _sz, _sz, _vp,
+                                  _perr]),
+    "rb_dtrsm_batched_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _sz, _vp, _perr]),
     "rb_dgemm_ozaki_noalloc": (_i, [_i, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _vp, _perr]),
     "rb_gemm_grouped_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _vp, _perr]),
     "rb_gemm_grouped_splits": (_i, [C.POINTER(RbGemmProblem)]),

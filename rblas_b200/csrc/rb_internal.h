@@ -152,6 +152,12 @@ int validate_problem(const rb_gemm_problem& q);
 int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
                      cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging = nullptr);
 
+// Batched triangular solve over uniformly strided A_i / B_i (rb_?trsm_batched_dev).
+template <typename T>
+int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T alpha, const T* A, size_t lda,
+                     size_t stride_a, T* B, size_t ldb, size_t stride_b, size_t batch, cudaStream_t st,
+                     int32_t* ce, rb_error* err);
+
 // Grouped launch frozen into a CUDA graph (rb_gemm_grouped_plan_*).
 int grouped_plan_create(const rb_gemm_problem* probs, size_t count, void** plan, int32_t* ce, size_t* bad);
 int grouped_plan_launch(void* plan, cudaStream_t st, int32_t* ce);

@@ -1,0 +1,359 @@
+// trsm_batched.cu -- batched triangular solve, one launch for the batch.
+//
+// rblas's trsm (src/level3.rs:390-520) solves op(A) X = alpha*B (Left) or
+// X op(A) = alpha*B (Right) for one problem by substitution. For a batch of
+// same-shaped problems (uniform strides between the A_i and between the
+// B_i) each problem is small -- the C4 case is 512 x 512 lower with 64
+// right-hand sides, 16.8 Mflop -- so the single-problem path's blocked
+// algorithm (a diagonal-block launch plus a GEMM launch per 64-row block)
+// would pay ~15 launches per problem. Here every CTA owns RB right-hand
+// sides of one problem: it keeps its q x RB slice of alpha*B in shared
+// memory and runs a right-looking blocked forward substitution on it
+// entirely on chip:
+//   for each 64-row block: substitution inside the block, staged in shared
+//   memory (each warp solves its own columns, rows in order, with a division
+//   by the diagonal unless Unit), then
+//   the trailing rows -= A[trailing, block] * X[block] as a register-tiled
+//   SIMT GEMM (4 x 4 outputs per thread) over 128-row panels of A staged in
+//   shared memory.
+// Right side is the transposed problem (B read through swapped strides);
+// an upper-triangular op(A) is solved as a lower one with rows and columns
+// reversed. Work per problem: q^2 * nrhs flop (q = order of A).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "../../include/rblas_b200.h"
+#include "rb_device.cuh"
+#include "rb_internal.h"
+
+namespace rb {
+
+namespace {
+
+constexpr int kTbNB = 64;      // diagonal block
+constexpr int kTbPanel = 128;  // trailing rows per staged A panel
+constexpr int kTbThreads = 256;
+
+struct TbParams {
+    int q, nrhs;
+    int rev;    // solve the reversed (upper -> lower) system (B rows reversed)
+    int unit;   // unit diagonal
+    // op'(A)[r][c] (reversed when rev) at A_i + a_off + r*a_dr + c*a_dc
+    long long a_off, a_dr, a_dc;
+    size_t stride_a, ldb_rs, ldb_cs, stride_b;  // B element (i, j) of the solve at i*rs + j*cs
+};
+
+template <typename T>
+__device__ __forceinline__ const T* a_ptr(const T* __restrict__ A, const TbParams& p, int r, int c) {
+    return A + (p.a_off + static_cast<long long>(r) * p.a_dr + static_cast<long long>(c) * p.a_dc);
+}
+
+// Asynchronous element copies global -> shared (cp.async, 4 or 8 bytes), so
+// a thread's copies are all in flight at once instead of one load latency
+// each; cp_wait() completes this thread's copies (a barrier must follow).
+template <typename T>
+__device__ __forceinline__ void cp_elem(T* dst, const T* src) {
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// N consecutive elements from 16-byte-aligned shared memory in 16-byte loads.
+template <typename T, int N>
+__device__ __forceinline__ void ld_vec(const T* src, T (&v)[N]) {
+    if constexpr (sizeof(T) == 8 && N % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i += 2) {
+            const double2 x = *reinterpret_cast<const double2*>(src + i);
+            v[i] = x.x;
+            v[i + 1] = x.y;
+        }
+    } else if constexpr (sizeof(T) == 4 && N % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i += 4) {
+            const float4 x = *reinterpret_cast<const float4*>(src + i);
+            v[i] = x.x;
+            v[i + 1] = x.y;
+            v[i + 2] = x.z;
+            v[i + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = src[i];
+    }
+}
+
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(kTbThreads)
+    trsm_batched_kernel(const T* __restrict__ A0, T* __restrict__ B0, T alpha, TbParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* Y = reinterpret_cast<T*>(smem_raw);  // [q][RB]
+    T* P = Y + static_cast<size_t>(p.q) * RB;  // [kTbNB][kTbPanel]
+    const int tid = threadIdx.x;
+    const T* A = A0 + static_cast<size_t>(blockIdx.y) * p.stride_a;
+    T* B = B0 + static_cast<size_t>(blockIdx.y) * p.stride_b;
+    const int c0 = blockIdx.x * RB;
+    const int ncols = min(RB, p.nrhs - c0);
+    const int q = p.q;
+
+    // Y = alpha * B slice (rows reversed when rev); consecutive threads walk
+    // the unit-stride direction of B
+    const bool rows_fast = p.ldb_rs == 1;
+    for (int idx = tid; idx < q * RB; idx += kTbThreads) {
+        const int i = rows_fast ? idx % q : idx / RB;
+        const int j = rows_fast ? idx / q : idx % RB;
+        T* dst = Y + (p.rev ? q - 1 - i : i) * RB + j;
+        if (j < ncols) cp_elem(dst, B + (static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs));
+        else *dst = T(0);
+    }
+    cp_wait();
+    __syncthreads();
+    if (alpha != T(1))  // B := alpha*B first (src/level3.rs:403-409)
+        for (int idx = tid; idx < q * RB; idx += kTbThreads) Y[idx] = alpha * Y[idx];
+    __syncthreads();
+
+    const int tr = (tid / 8) * 4;       // panel rows of this thread (32 groups of 4)
+    const int tc = (tid % 8) * (RB / 8);  // columns (8 groups of RB/8)
+    constexpr int CW = RB / 8;
+    for (int o = 0; o < q; o += kTbNB) {
+        const int nb = min(kTbNB, q - o);
+        // substitution inside the diagonal block, staged in shared memory
+        // transposed (Dt[c][r] = op'(A)[o+r][o+c], r >= c). Each warp solves
+        // RB/8 columns on its own, lane l holding rows l and l+32 of them:
+        // at step t the lane owning row t divides it by the diagonal (unless
+        // Unit), broadcasts it, and every lane folds it into its later rows.
+        T* Dt = P;
+        for (int idx = tid; idx < nb * nb; idx += kTbThreads) {
+            const int r = idx % nb, c = idx / nb;
+            if (r >= c) cp_elem(Dt + c * kTbNB + r, a_ptr(A, p, o + r, o + c));
+        }
+        cp_wait();
+        __syncthreads();
+        {
+            constexpr int CWD = RB / 8;  // columns per warp
+            const int warp = tid >> 5, lane = tid & 31;
+            const int col0 = warp * CWD;
+            T y0[CWD], y1[CWD];
+#pragma unroll
+            for (int c = 0; c < CWD; ++c) {
+                y0[c] = (lane < nb) ? Y[(o + lane) * RB + col0 + c] : T(0);
+                y1[c] = (lane + 32 < nb) ? Y[(o + lane + 32) * RB + col0 + c] : T(0);
+            }
+            for (int t = 0; t < nb; ++t) {
+                const int owner = t & 31;
+                const bool hi = t >= 32;  // warp-uniform
+                T xt[CWD];
+#pragma unroll
+                for (int c = 0; c < CWD; ++c) xt[c] = __shfl_sync(0xffffffffu, hi ? y1[c] : y0[c], owner);
+                if (!p.unit) {
+                    // lane c divides column c's value, then broadcasts it
+                    const T d = Dt[t * kTbNB + t];
+                    T mine = xt[0];
+#pragma unroll
+                    for (int c = 1; c < CWD; ++c)
+                        if (lane == c) mine = xt[c];
+                    if (lane < CWD) mine = mine / d;
+#pragma unroll
+                    for (int c = 0; c < CWD; ++c) xt[c] = __shfl_sync(0xffffffffu, mine, c);
+                    if (lane == owner) {
+#pragma unroll
+                        for (int c = 0; c < CWD; ++c) {
+                            if (hi) y1[c] = xt[c];
+                            else y0[c] = xt[c];
+                        }
+                    }
+                }
+                const T d0 = Dt[t * kTbNB + lane], d1 = Dt[t * kTbNB + lane + 32];
+#pragma unroll
+                for (int c = 0; c < CWD; ++c) {
+                    if (lane > t) y0[c] = y0[c] - d0 * xt[c];
+                    if (lane + 32 > t) y1[c] = y1[c] - d1 * xt[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CWD; ++c) {
+                if (lane < nb) Y[(o + lane) * RB + col0 + c] = y0[c];
+                if (lane + 32 < nb) Y[(o + lane + 32) * RB + col0 + c] = y1[c];
+            }
+        }
+        __syncthreads();
+        // trailing update over 128-row panels
+        for (int r0 = o + nb; r0 < q; r0 += kTbPanel) {
+            const int pr = min(kTbPanel, q - r0);
+            for (int idx = tid; idx < nb * kTbPanel; idx += kTbThreads) {
+                const int r = idx % kTbPanel, s = idx / kTbPanel;
+                if (r < pr) cp_elem(P + s * kTbPanel + r, a_ptr(A, p, r0 + r, o + s));
+                else P[s * kTbPanel + r] = T(0);
+            }
+            cp_wait();
+            __syncthreads();
+            T acc[4][CW];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < CW; ++j) acc[i][j] = T(0);
+#pragma unroll 4
+            for (int s = 0; s < nb; ++s) {
+                T a[4], y[CW];
+                ld_vec<T, 4>(P + s * kTbPanel + tr, a);
+                ld_vec<T, CW>(Y + (o + s) * RB + tc, y);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < CW; ++j) acc[i][j] = fma(a[i], y[j], acc[i][j]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (tr + i < pr)
+#pragma unroll
+                    for (int j = 0; j < CW; ++j) Y[(r0 + tr + i) * RB + tc + j] -= acc[i][j];
+            __syncthreads();
+        }
+    }
+
+    for (int idx = tid; idx < q * RB; idx += kTbThreads) {
+        const int i = rows_fast ? idx % q : idx / RB;
+        const int j = rows_fast ? idx / q : idx % RB;
+        if (j < ncols)
+            B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs] =
+                Y[(p.rev ? q - 1 - i : i) * RB + j];
+    }
+}
+
+template <typename T, int RB>
+size_t tb_smem(int q) {
+    return (static_cast<size_t>(q) * RB + static_cast<size_t>(kTbNB) * kTbPanel) * sizeof(T);
+}
+
+template <typename T, int RB>
+cudaError_t tb_launch(const T* A, T* B, T alpha, const TbParams& p, size_t batch, cudaStream_t st) {
+    const size_t smem = tb_smem<T, RB>(p.q);
+    cudaError_t e = cudaFuncSetAttribute(trsm_batched_kernel<T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const dim3 grid((p.nrhs + RB - 1) / RB, static_cast<unsigned>(batch));
+    KernelTimer tmr;
+    kernel_timing_begin(sizeof(T) == 8 ? "trsm_batched_d" : "trsm_batched_s",
+                        static_cast<double>(p.q) * p.q * p.nrhs * static_cast<double>(batch), st, &tmr);
+    trsm_batched_kernel<T, RB><<<grid, kTbThreads, smem, st>>>(A, B, alpha, p);
+    kernel_timing_end(&tmr, st);
+    count_launch();
+    return cudaGetLastError();
+}
+
+constexpr size_t kTbSmemMax = 227 * 1024;
+
+}  // namespace
+
+template <typename T>
+int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T alpha, const T* A, size_t lda,
+                     size_t stride_a, T* B, size_t ldb, size_t stride_b, size_t batch, cudaStream_t st,
+                     int32_t* ce, rb_error* err) {
+    if ((side != RB_LEFT && side != RB_RIGHT) || (uplo != RB_UPPER && uplo != RB_LOWER) || trans < 0 || trans > 2 ||
+        (diag != RB_NON_UNIT && diag != RB_UNIT))
+        return RB_ERR_INVALID_ARG;
+    const size_t q = (side == RB_LEFT) ? m : n, nrhs = (side == RB_LEFT) ? n : m;
+    // leading dimensions (check_matrix for a q x q A and an m x n B, column-major)
+    if (q > 0 && lda < q) {
+        if (err) *err = rb_error{RB_ERR_INVALID_LEADING_DIM, 'a', lda, q, 0};
+        return RB_ERR_INVALID_LEADING_DIM;
+    }
+    if (m > 0 && n > 0 && ldb < m) {
+        if (err) *err = rb_error{RB_ERR_INVALID_LEADING_DIM, 'b', ldb, m, 0};
+        return RB_ERR_INVALID_LEADING_DIM;
+    }
+    if (m == 0 || n == 0 || batch == 0) return RB_OK;
+    if (q > 0x7fffffff || nrhs > 0x7fffffff) return RB_ERR_INVALID_ARG;
+    if (batch > 65535) {  // grid.y limit: launch in chunks
+        for (size_t b0 = 0; b0 < batch; b0 += 65535) {
+            const int rc = trsm_batched_dev<T>(side, uplo, trans, diag, m, n, alpha, A + b0 * stride_a, lda, stride_a,
+                                               B + b0 * stride_b, ldb, stride_b, std::min<size_t>(65535, batch - b0),
+                                               st, ce, err);
+            if (rc != RB_OK) return rc;
+        }
+        return RB_OK;
+    }
+    const bool tr = trans != RB_NO_TRANS;
+    // solve op'(A) Y = alpha Z: Left op' = op, Right op' = op^T (Z = B^T)
+    const bool eff_tr = (side == RB_LEFT) ? tr : !tr;
+    const bool eff_upper = (uplo == RB_UPPER) != eff_tr;
+    TbParams p{};
+    p.q = static_cast<int>(q);
+    p.nrhs = static_cast<int>(nrhs);
+    p.rev = eff_upper;
+    p.unit = diag == RB_UNIT;
+    // op'(A)[r][c] = eff_tr ? A[c + r*lda] : A[r + c*lda]; reversed: r -> q-1-r, c -> q-1-c
+    const long long ld = static_cast<long long>(lda), qm = static_cast<long long>(q) - 1;
+    const long long sr = eff_tr ? ld : 1, sc = eff_tr ? 1 : ld;
+    p.a_off = eff_upper ? qm * (sr + sc) : 0;
+    p.a_dr = eff_upper ? -sr : sr;
+    p.a_dc = eff_upper ? -sc : sc;
+    p.stride_a = stride_a;
+    p.ldb_rs = (side == RB_LEFT) ? 1 : ldb;
+    p.ldb_cs = (side == RB_LEFT) ? ldb : 1;
+    p.stride_b = stride_b;
+    cudaError_t e;
+    if (tb_smem<T, 32>(p.q) <= kTbSmemMax) e = tb_launch<T, 32>(A, B, alpha, p, batch, st);
+    else if (tb_smem<T, 16>(p.q) <= kTbSmemMax) e = tb_launch<T, 16>(A, B, alpha, p, batch, st);
+    else if (tb_smem<T, 8>(p.q) <= kTbSmemMax) e = tb_launch<T, 8>(A, B, alpha, p, batch, st);
+    else {
+        // too large for one CTA's shared memory: the single-problem path per member
+        for (size_t i = 0; i < batch; ++i) {
+            const int rc = trsm_dev<T, false>(side, uplo, trans, diag, m, n, alpha, T(0), A + i * stride_a, lda,
+                                              B + i * stride_b, ldb, st, ce);
+            if (rc != RB_OK) return rc;
+        }
+        return RB_OK;
+    }
+    if (e != cudaSuccess) {
+        if (ce) *ce = static_cast<int32_t>(e);
+        return RB_ERR_CUDA;
+    }
+    return RB_OK;
+}
+
+template int trsm_batched_dev<float>(int, int, int, int, size_t, size_t, float, const float*, size_t, size_t, float*,
+                                     size_t, size_t, size_t, cudaStream_t, int32_t*, rb_error*);
+template int trsm_batched_dev<double>(int, int, int, int, size_t, size_t, double, const double*, size_t, size_t,
+                                      double*, size_t, size_t, size_t, cudaStream_t, int32_t*, rb_error*);
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+rb_status rb_strsm_batched_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                               float alpha, const float* a, size_t lda, size_t stride_a, float* b, size_t ldb,
+                               size_t stride_b, size_t batch, void* stream, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    int32_t ce = 0;
+    const int rc = trsm_batched_dev<float>(side, uplo, trans, diag, m, n, alpha, a, lda, stride_a, b, ldb, stride_b,
+                                           batch, static_cast<cudaStream_t>(stream), &ce, err);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
+
+rb_status rb_dtrsm_batched_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                               double alpha, const double* a, size_t lda, size_t stride_a, double* b, size_t ldb,
+                               size_t stride_b, size_t batch, void* stream, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    int32_t ce = 0;
+    const int rc = trsm_batched_dev<double>(side, uplo, trans, diag, m, n, alpha, a, lda, stride_a, b, ldb, stride_b,
+                                            batch, static_cast<cudaStream_t>(stream), &ce, err);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
+
+}  // extern "C"

@@ -128,3 +128,19 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
                                    int(Diag(diag)), m, n, alpha, _ptr(a), lda, a.size, _ptr(b), ldb,
                                    b.size, C.byref(err))
     _lib.check(st, err)
+
+
+def trsm_batched_dev(side, uplo, trans, diag, m, n, alpha, a_ptr, lda, stride_a, b_ptr, ldb, stride_b,
+                     batch, dtype, stream=0):
+    """Batched trsm on device pointers (rb_?trsm_batched_dev): problem i is
+    trsm(side, uplo, trans, diag, m, n, alpha, A_i, lda, B_i, ldb) with
+    A_i = a + i*stride_a, B_i = b + i*stride_b (elements). Enqueued on
+    `stream`, no synchronisation."""
+    from .types import Diag, Side, Uplo
+    lib = _lib.load()
+    err = _lib.RbError()
+    fn = lib.rb_strsm_batched_dev if np.dtype(dtype) == np.float32 else lib.rb_dtrsm_batched_dev
+    st = fn(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)), int(Diag(diag)), m, n, alpha,
+            C.c_void_p(a_ptr), lda, stride_a, C.c_void_p(b_ptr), ldb, stride_b, batch,
+            C.c_void_p(stream) if stream else None, C.byref(err))
+    _lib.check(st, err)
