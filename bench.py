@@ -330,8 +330,15 @@ def run_ours(args):
     else:
         peak, unit, bound = peaks["fp64_fma_tflops"], "TFLOP/s", "fp64"
         psrc = "FP64 DFMA throughput measured in-run by rb_probe_fma_peak_tflops; not in MEASURED_PEAKS.json"
+    # DRAM bytes per launch of the dominant kernel, measured by ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
+    # the step's shapes: 2.562 GB at 4096^3 (x4 per step), 1.268 GB at
+    # 3000x5000x2048 (x1)
+    traffic = (4 * 2.562e9 + 1.268e9) / 5 if kname == "umma_ozaki_i8" else None
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over "
+                                   "the step's launch shapes") if traffic else None,
                 "kernel": kname, "launches": cnt, "avg_launch_ms": kms / cnt,
                 "work_per_launch": work / cnt, "peak_source": psrc,
                 "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in kr.items()}}
@@ -629,6 +636,53 @@ def run_kernel_only(args):
                       "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}))
 
 
+def run_grouped_only(args):
+    """The first `--grouped-batch N` requests of the serving stream as one
+    grouped launch (device-resident operands), launched warmup + steps times
+    (for ncu captures of the grouped kernel on a bounded batch)."""
+    import torch
+
+    from rblas_b200.serving import Problem, grouped_gemm
+
+    tr = serving_trace(args.grouped_batch)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(6)
+    big = 4096 * 4096 + (1 << 22)
+    pools = {0: torch.randn(big, dtype=torch.float32, device="cuda", generator=g),
+             1: torch.randn(big, dtype=torch.float64, device="cuda", generator=g)}
+    outs, probs, flops = [], [], 0.0
+    for i in range(args.grouped_batch):
+        m, n, k = (int(x) for x in tr["mnk"][i])
+        dt = int(tr["dtype"][i])
+        layout, ta, tb = int(tr["layout"][i]), int(tr["ta"][i]), int(tr["tb"][i])
+        ar, ac = (k, m) if ta else (m, k)
+        br, bc = (n, k) if tb else (k, n)
+        lda = ar if layout == 1 else ac
+        ldb = br if layout == 1 else bc
+        ldc = m if layout == 1 else n
+        es = 4 if dt == 0 else 8
+        base = pools[dt].data_ptr()
+        offs = [int(o) // 16 * 16 for o in tr["offs"][i]]
+        c = torch.empty(m * n, dtype=torch.float32 if dt == 0 else torch.float64, device="cuda").normal_()
+        outs.append(c)
+        probs.append(Problem(np.float32 if dt == 0 else np.float64, layout, ta, tb, m, n, k, float(tr["alpha"][i]),
+                             base + offs[0] * es, lda, base + offs[1] * es, ldb, float(tr["beta"][i]),
+                             c.data_ptr(), ldc))
+        flops += 2.0 * m * n * k
+    sh = torch.cuda.current_stream().cuda_stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            e0.record()
+        grouped_gemm(probs, sh)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"grouped_batch": args.grouped_batch, "flop": flops, "ms": ms,
+                      "tflops": flops / (ms * 1e-3) / 1e12}))
+
+
 def run_trsm_batched_only(args):
     """The batched f64 trsm of the C4 configuration (512 x 512 lower, 64
     right-hand sides) on `--trsm-batched BATCH` members, launched warmup +
@@ -671,6 +725,8 @@ def main():
     ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,
                     metavar=("M", "N", "K"), help="time one column-major GEMM shape only")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--grouped-batch", type=int, default=0, metavar="N",
+                    help="time one grouped launch of the first N serving requests only")
     ap.add_argument("--trsm-batched", type=int, default=0, metavar="BATCH",
                     help="time the batched f64 trsm (512 x 512, 64 RHS) on BATCH members only")
     ap.add_argument("--serve", action="store_true", help="serving sweep (request stream replay)")
@@ -685,6 +741,8 @@ def main():
     args = ap.parse_args()
     if args.trsm_batched:
         run_trsm_batched_only(args)
+    elif args.grouped_batch:
+        run_grouped_only(args)
     elif args.serve:
         run_serve_mode(args)
     elif args.shape:

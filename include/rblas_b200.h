@@ -225,7 +225,7 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
  * side, uplo, trans, diag, m, n, alpha, lda, ldb; column-major like rblas.
  * One launch for the batch: each CTA keeps a slice of B_i's right-hand sides
  * in shared memory for the whole solve (32 right-hand sides per CTA up to
- * order 652 f64 / 1560 f32, 16 or 8 up to 2608 f64 / 6240 f32; larger orders
+ * order 632 f64 / 1512 f32, 16 or 8 up to 2318 f64 / 5546 f32; larger orders
  * fall back to the single-problem path per member). The B_i must not
  * overlap. Enqueued on `stream`. */
 rb_status rb_strsm_batched_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m,

@@ -14,8 +14,8 @@
 //   memory (each warp solves its own columns, rows in order, with a division
 //   by the diagonal unless Unit), then
 //   the trailing rows -= A[trailing, block] * X[block] as a register-tiled
-//   SIMT GEMM (4 x 4 outputs per thread) over 128-row panels of A staged in
-//   shared memory.
+//   SIMT GEMM (4 rows x RB/8 columns per thread) over 128-row panels of A
+//   staged in shared memory.
 // Right side is the transposed problem (B read through swapped strides);
 // an upper-triangular op(A) is solved as a lower one with rows and columns
 // reversed. Work per problem: q^2 * nrhs flop (q = order of A).
@@ -92,8 +92,12 @@ template <typename T, int RB>
 __global__ void __launch_bounds__(kTbThreads)
     trsm_batched_kernel(const T* __restrict__ A0, T* __restrict__ B0, T alpha, TbParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Y = reinterpret_cast<T*>(smem_raw);  // [q][RB]
-    T* P = Y + static_cast<size_t>(p.q) * RB;  // [kTbNB][kTbPanel]
+    // Y: [q][YS], rows padded by one element so that a warp reading one
+    // column down 32 rows touches distinct banks
+    constexpr int YS = RB + 1;
+    T* Y = reinterpret_cast<T*>(smem_raw);
+    // P: [kTbNB][kTbPanel], 16-byte aligned for the vector loads (q*YS may be odd)
+    T* P = Y + ((static_cast<size_t>(p.q) * YS + 3) & ~static_cast<size_t>(3));
     const int tid = threadIdx.x;
     const T* A = A0 + static_cast<size_t>(blockIdx.y) * p.stride_a;
     T* B = B0 + static_cast<size_t>(blockIdx.y) * p.stride_b;
@@ -107,18 +111,18 @@ __global__ void __launch_bounds__(kTbThreads)
     for (int idx = tid; idx < q * RB; idx += kTbThreads) {
         const int i = rows_fast ? idx % q : idx / RB;
         const int j = rows_fast ? idx / q : idx % RB;
-        T* dst = Y + (p.rev ? q - 1 - i : i) * RB + j;
+        T* dst = Y + (p.rev ? q - 1 - i : i) * YS + j;
         if (j < ncols) cp_elem(dst, B + (static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs));
         else *dst = T(0);
     }
     cp_wait();
     __syncthreads();
     if (alpha != T(1))  // B := alpha*B first (src/level3.rs:403-409)
-        for (int idx = tid; idx < q * RB; idx += kTbThreads) Y[idx] = alpha * Y[idx];
+        for (int idx = tid; idx < q * RB; idx += kTbThreads) Y[(idx / RB) * YS + idx % RB] *= alpha;
     __syncthreads();
 
-    const int tr = (tid / 8) * 4;       // panel rows of this thread (32 groups of 4)
-    const int tc = (tid % 8) * (RB / 8);  // columns (8 groups of RB/8)
+    const int tr = (tid / 8) * 4;  // panel rows of this thread (32 groups of 4)
+    const int tc = tid % 8;        // columns tc, tc+8, ... (RB/8 of them)
     constexpr int CW = RB / 8;
     for (int o = 0; o < q; o += kTbNB) {
         const int nb = min(kTbNB, q - o);
@@ -141,8 +145,8 @@ __global__ void __launch_bounds__(kTbThreads)
             T y0[CWD], y1[CWD];
 #pragma unroll
             for (int c = 0; c < CWD; ++c) {
-                y0[c] = (lane < nb) ? Y[(o + lane) * RB + col0 + c] : T(0);
-                y1[c] = (lane + 32 < nb) ? Y[(o + lane + 32) * RB + col0 + c] : T(0);
+                y0[c] = (lane < nb) ? Y[(o + lane) * YS + col0 + c] : T(0);
+                y1[c] = (lane + 32 < nb) ? Y[(o + lane + 32) * YS + col0 + c] : T(0);
             }
             for (int t = 0; t < nb; ++t) {
                 const int owner = t & 31;
@@ -177,8 +181,8 @@ __global__ void __launch_bounds__(kTbThreads)
             }
 #pragma unroll
             for (int c = 0; c < CWD; ++c) {
-                if (lane < nb) Y[(o + lane) * RB + col0 + c] = y0[c];
-                if (lane + 32 < nb) Y[(o + lane + 32) * RB + col0 + c] = y1[c];
+                if (lane < nb) Y[(o + lane) * YS + col0 + c] = y0[c];
+                if (lane + 32 < nb) Y[(o + lane + 32) * YS + col0 + c] = y1[c];
             }
         }
         __syncthreads();
@@ -201,7 +205,8 @@ __global__ void __launch_bounds__(kTbThreads)
             for (int s = 0; s < nb; ++s) {
                 T a[4], y[CW];
                 ld_vec<T, 4>(P + s * kTbPanel + tr, a);
-                ld_vec<T, CW>(Y + (o + s) * RB + tc, y);
+#pragma unroll
+                for (int j = 0; j < CW; ++j) y[j] = Y[(o + s) * YS + tc + 8 * j];
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(kTbThreads)
             for (int i = 0; i < 4; ++i)
                 if (tr + i < pr)
 #pragma unroll
-                    for (int j = 0; j < CW; ++j) Y[(r0 + tr + i) * RB + tc + j] -= acc[i][j];
+                    for (int j = 0; j < CW; ++j) Y[(r0 + tr + i) * YS + tc + 8 * j] -= acc[i][j];
             __syncthreads();
         }
     }
@@ -221,13 +226,14 @@ __global__ void __launch_bounds__(kTbThreads)
         const int j = rows_fast ? idx / q : idx % RB;
         if (j < ncols)
             B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs] =
-                Y[(p.rev ? q - 1 - i : i) * RB + j];
+                Y[(p.rev ? q - 1 - i : i) * YS + j];
     }
 }
 
 template <typename T, int RB>
 size_t tb_smem(int q) {
-    return (static_cast<size_t>(q) * RB + static_cast<size_t>(kTbNB) * kTbPanel) * sizeof(T);
+    return (((static_cast<size_t>(q) * (RB + 1) + 3) & ~static_cast<size_t>(3)) +
+            static_cast<size_t>(kTbNB) * kTbPanel) * sizeof(T);
 }
 
 template <typename T, int RB>
