@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "../../include/rblas_b200.h"
 #include "rb_device.cuh"
@@ -528,6 +529,7 @@ __global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, 
     if (r >= R) return;
     const int p0 = blockIdx.y * 1024, p1 = min(K, p0 + 1024);
     int best = kExpSentinel;
+#pragma unroll 8
     for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) {
         const double v = x[static_cast<size_t>(r) * rs + q];
         if (v != 0.0) best = max(best, frexp_exp(v));
@@ -543,6 +545,7 @@ __global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, 
     if (r >= R) return;
     const int p0 = blockIdx.y * 32, p1 = min(K, p0 + 32);
     int best = kExpSentinel;
+#pragma unroll 8
     for (int q = p0; q < p1; ++q) {
         const double v = x[r + static_cast<size_t>(q) * ps];
         if (v != 0.0) best = max(best, frexp_exp(v));
@@ -553,79 +556,119 @@ __global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, 
 constexpr int kTile = 64;
 
 // Load a 64 x 64 tile of the R x K view into shared memory (coalesced along
-// the view's contiguous dimension); out-of-range elements read as 0.
+// the view's contiguous dimension); out-of-range elements read as 0. Blocks
+// of 256 threads: each thread issues its 16 loads before the first store, so
+// the loads are in flight together instead of one latency each.
+constexpr int kTileThreads = 256;
 template <typename T>
 __device__ __forceinline__ void load_tile(const T* __restrict__ x, size_t rs, size_t ps, int R, int K,
                                           int r0, int p0, T (*tile)[kTile + 1]) {
+    constexpr int PER = kTile * kTile / kTileThreads;
     const bool kcontig = (ps == 1);
-    for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+    T v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
         const int a = idx % kTile, b = idx / kTile;
         const int r = kcontig ? b : a;
         const int q = kcontig ? a : b;
-        T v = T(0);
-        if (r0 + r < R && p0 + q < K) v = x[static_cast<size_t>(r0 + r) * rs + static_cast<size_t>(p0 + q) * ps];
-        tile[r][q] = v;
+        v[i] = (r0 + r < R && p0 + q < K) ? x[static_cast<size_t>(r0 + r) * rs + static_cast<size_t>(p0 + q) * ps]
+                                          : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
+        const int a = idx % kTile, b = idx / kTile;
+        tile[kcontig ? b : a][kcontig ? a : b] = v[i];
     }
 }
 
 // Ozaki slicing. With e[r] the row exponent (|x| < 2^e), y = x * 2^-(e+1)
-// lies in (-1/2, 1/2). Digits are extracted exactly in FP64,
-//   d_0 = floor(y * 2^7) in [-64, 63],  d_t = floor(rem * 2^8) in [0, 255],
-// then balanced from the least significant up: d_t >= 128 becomes
-// d_t - 256 with a carry of 1 into d_{t-1} (d_0 <= 64 after the carry).
-// The result: signed 8-bit digits with y = sum_t d_t 2^-(7+8t) + rem,
-// 0 <= rem < 2^-(7+8(s-1)), and tail digits that are symmetric about zero,
-// so the dropped cross products do not accumulate a bias along K.
+// lies in (-1/2, 1/2). For s slices let N = 7 + 8(s-1) and
+//   Y = floor(y * 2^N) = floor(x * 2^(N-e-1)),
+// computed exactly from x's bits (x = m * 2^q with an integer m of at most
+// 53 bits: Y = m << (q+N-e-1), or an arithmetic right shift -- a floor --
+// when that exponent is negative; |Y| < 2^(N-1) <= 2^94 fits an __int128).
+// Its base-256 digits, the top one signed, are
+//   d_0 = floor(y * 2^7) in [-64, 63],  d_t = floor(y * 2^(7+8t)) mod 256,
+// which are then balanced from the least significant up: d_t >= 128 becomes
+// d_t - 256 with a carry of 1 into d_{t-1} (d_0 <= 64 after the carry). The
+// result: signed 8-bit digits with y = sum_t d_t 2^-(7+8t) + rem,
+// 0 <= rem < 2^-N, and tail digits symmetric about zero, so the dropped cross
+// products do not accumulate a bias along K. No floating-point rounding
+// occurs anywhere in the extraction.
 constexpr int kMaxSlices = 12;
+
+// floor(x * 2^n) for |x * 2^n| < 2^94 (Int = __int128) or < 2^62 (long long)
+template <typename Int>
+__device__ __forceinline__ Int floor_scaled(double x, int n) {
+    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
+    const int ex = static_cast<int>((bits >> 52) & 0x7FF);
+    long long m = static_cast<long long>(bits & ((1ull << 52) - 1));
+    if (ex != 0) m |= (1ll << 52);
+    if (m == 0) return 0;
+    if (bits >> 63) m = -m;
+    const int sh = (ex == 0 ? 1 : ex) - 1075 + n;  // x = m * 2^((ex|1) - 1075)
+    if (sh >= 0) return static_cast<Int>(m) << sh;
+    if (sh <= -63) return m < 0 ? -1 : 0;
+    return static_cast<Int>(m >> (-sh));  // arithmetic shift: floor
+}
+
+// S slices known at compile time: up to 8 digits the integer fits 64 bits.
+template <int S>
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
                                                           int R, int K, const int* __restrict__ e,
-                                                          int slices, int8_t* __restrict__ out, size_t kp,
-                                                          size_t plane) {
+                                                          int8_t* __restrict__ out, size_t kp, size_t plane) {
+    using Int = typename std::conditional<(S <= 8), long long, __int128>::type;
+    constexpr int slices = S;
     __shared__ double tile[kTile][kTile + 1];
     const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
     load_tile<double>(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;  // 64 rows x 4 chunks of 16
     if (r0 + r >= R) return;
+    if (p0 + c * 16 >= static_cast<int>(kp)) return;
     const int er = e[r0 + r];
-    uint32_t w[kMaxSlices][4];
+    const int n = 7 + 8 * (slices - 1) - er - 1;  // Y = floor(x * 2^n)
+    uint32_t w[S][4];
 #pragma unroll
-    for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
-#pragma unroll 1
+    for (int t = 0; t < S; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
+#pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const double y = (er == kExpSentinel) ? 0.0 : scalbn(tile[r][c * 16 + i], -(er + 1));
-        int d[kMaxSlices];
-        double v = y * 128.0;
-        double f = floor(v);
-        d[0] = static_cast<int>(f);
-        double rem = v - f;
+        const Int Y = (er == kExpSentinel) ? Int(0) : floor_scaled<Int>(tile[r][c * 16 + i], n);
+        int d[S];
 #pragma unroll
-        for (int t = 1; t < kMaxSlices; ++t) {
-            if (t < slices) {
-                v = rem * 256.0;
-                f = floor(v);
-                d[t] = static_cast<int>(f);
-                rem = v - f;
-            } else {
-                d[t] = 0;
-            }
+        for (int t = 0; t < S; ++t) {
+            const int sh = 8 * (S - 1 - t);
+            d[t] = (t == 0) ? static_cast<int>(Y >> sh) : static_cast<int>((Y >> sh) & 0xFF);
         }
 #pragma unroll
-        for (int t = kMaxSlices - 1; t >= 1; --t) {
+        for (int t = S - 1; t >= 1; --t) {
             if (d[t] >= 128) {
                 d[t] -= 256;
                 d[t - 1] += 1;
             }
         }
 #pragma unroll
-        for (int t = 0; t < kMaxSlices; ++t)
-            w[t][i >> 2] |= (static_cast<uint32_t>(d[t]) & 0xFFu) << (8 * (i & 3));
+        for (int t = 0; t < S; ++t) w[t][i >> 2] |= (static_cast<uint32_t>(d[t]) & 0xFFu) << (8 * (i & 3));
     }
-    if (p0 + c * 16 >= static_cast<int>(kp)) return;
     const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
 #pragma unroll
-    for (int t = 0; t < kMaxSlices; ++t)
-        if (t < slices) *reinterpret_cast<uint4*>(out + t * plane + off) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+    for (int t = 0; t < S; ++t)
+        *reinterpret_cast<uint4*>(out + t * plane + off) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+}
+
+// Host dispatch on the slice count (2 .. kMaxSlices).
+void launch_ozaki_slices(dim3 grid, cudaStream_t st, const double* x, size_t rs, size_t ps, int R, int K,
+                         const int* e, int slices, int8_t* out, size_t kp, size_t plane) {
+    switch (slices) {
+#define RB_SLICES(S) \
+    case S: ozaki_slice_kernel<S><<<grid, 256, 0, st>>>(x, rs, ps, R, K, e, out, kp, plane); break;
+        RB_SLICES(2) RB_SLICES(3) RB_SLICES(4) RB_SLICES(5) RB_SLICES(6) RB_SLICES(7) RB_SLICES(8)
+        RB_SLICES(9) RB_SLICES(10) RB_SLICES(11) RB_SLICES(12)
+#undef RB_SLICES
+        default: break;
+    }
 }
 
 // BF16 split into `planes` (2 or 3) planes: out[0] = bf16(x),
@@ -839,8 +882,8 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     else          row_exp_rcontig_kernel<<<dim3((n + 255) / 256, k32), 256, 0, st>>>(B, bps, n, k, eb);
     const dim3 ga((kp + kTile - 1) / kTile, (m + kTile - 1) / kTile);
     const dim3 gb((kp + kTile - 1) / kTile, (n + kTile - 1) / kTile);
-    ozaki_slice_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, ea, slices, sla, kp, pa);
-    ozaki_slice_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, eb, slices, slb, kp, pb);
+    launch_ozaki_slices(ga, st, A, ars, aps, m, k, ea, slices, sla, kp, pa);
+    launch_ozaki_slices(gb, st, B, brs, bps, n, k, eb, slices, slb, kp, pb);
     count_launch(5);
     CUtensorMap tma, tmb;
     CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, m, slices, kp, kUM);
@@ -1008,8 +1051,8 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         else          row_exp_rcontig_kernel<<<dim3((N + 255) / 256, k32), 256, 0, st>>>(cb, bps, N, K, eb);
         const dim3 ga((kp + kTile - 1) / kTile, (M + kTile - 1) / kTile);
         const dim3 gb((kp + kTile - 1) / kTile, (N + kTile - 1) / kTile);
-        ozaki_slice_kernel<<<ga, 256, 0, st>>>(ca, ars, aps, M, K, ea, slices, sla, kp, pa);
-        ozaki_slice_kernel<<<gb, 256, 0, st>>>(cb, brs, bps, N, K, eb, slices, slb, kp, pb);
+        launch_ozaki_slices(ga, st, ca, ars, aps, M, K, ea, slices, sla, kp, pa);
+        launch_ozaki_slices(gb, st, cb, brs, bps, N, K, eb, slices, slb, kp, pb);
         count_launch(5);
         CUtensorMap tma, tmb;
         CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, K, M, slices, kp, kUM);
