@@ -479,7 +479,8 @@ def run_ours(args):
     if not args.no_serve and rank == 0 and ws == 1:
         from rblas_b200.serving import autotune
         tuned = autotune()
-        serving = run_serving(torch, [5000.0, 10000.0, 15000.0, 20000.0, 50000.0], 5000, 60 << 30)
+        serving = run_serving(torch, [5000.0, 10000.0, 15000.0, 20000.0, 50000.0], 5000, 60 << 30,
+                              with_forms=False)
         serving["autotuned_buckets"] = tuned
         serving["note"] = ("5000-request slice of the serving stream; operands resident in HBM; "
                            "latency = enqueue -> completion observed by the server")
@@ -524,7 +525,13 @@ def serving_trace(n_req, seed=5):
                 offs=rng.integers(0, 1 << 20, (n_req, 3)))
 
 
-def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5):
+# precision forms for large serving requests (each within 2x of plain's
+# error against the FP64 oracle): f32 >= 5e8 flop in BF16X6, f64 >= 4e9 flop
+# in Ozaki; smaller requests stay on the grouped plain kernel
+SERVE_FORMS = {"f32_form": 3, "f64_form": 2, "f32_min_flop": 5e8, "f64_min_flop": 4e9}
+
+
+def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=True):
     """Replay a Poisson stream of n_req requests at each rate through the
     server in grouped mode and in per-request mode. Operands are standard
     normal values resident in HBM (pools the requests point into)."""
@@ -561,10 +568,17 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5):
     for rate in rates:
         arrivals = (np.cumsum(gaps) / rate * 1e9).astype(np.uint64)
         row = {"rate_req_s": rate}
-        for mode, grouped in (("grouped", True), ("per_request", False)):
-            # both modes admit the same sets; per-request mode launches the
-            # single-problem kernel once per request, grouped mode once per set
+        modes = [("grouped", True, False), ("per_request", False, False)]
+        if with_forms:
+            modes.append(("grouped_forms", True, True))
+        for mode, grouped, forms in modes:
+            # all modes admit the same sets; per-request mode launches the
+            # single-problem plain kernel once per request, grouped mode one
+            # grouped plain launch per set, grouped_forms runs the large
+            # requests of each set in the precision forms
             with Server(budget_bytes=budget, max_batch=max_batch, grouped=grouped) as srv:
+                if forms:
+                    srv.set_forms(**SERVE_FORMS)
                 st, times = srv.run_trace(problems, arrivals)
             lat = (times[:, 2].astype(np.int64) - times[:, 0].astype(np.int64)) / 1e6
             span = (int(times[:, 2].max()) - int(times[:, 0].min())) / 1e9
@@ -576,17 +590,25 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5):
     slo = []
     for bound in (2.0, 5.0, 10.0, 20.0, 50.0, 100.0):
         best = {}
-        for mode in ("grouped", "per_request"):
-            ok = [r[mode]["tflops"] for r in out["rates"] if r[mode]["p99_ms"] <= bound]
+        for mode in ("grouped", "per_request", "grouped_forms"):
+            ok = [r[mode]["tflops"] for r in out["rates"] if mode in r and r[mode]["p99_ms"] <= bound]
             best[mode] = max(ok) if ok else None
-        ratio = (best["grouped"] / best["per_request"]) if best["grouped"] and best["per_request"] else None
-        slo.append({"p99_bound_ms": bound, "grouped_tflops": best["grouped"],
-                    "per_request_tflops": best["per_request"], "ratio": ratio})
+        pr = best["per_request"]
+        slo.append({"p99_bound_ms": bound, "grouped_tflops": best["grouped"], "per_request_tflops": pr,
+                    "grouped_forms_tflops": best["grouped_forms"],
+                    "ratio": (best["grouped"] / pr) if best["grouped"] and pr else None,
+                    "ratio_forms": (best["grouped_forms"] / pr) if best["grouped_forms"] and pr else None})
     out["at_equal_p99"] = slo
+    if with_forms:
+        out["forms"] = dict(SERVE_FORMS, note="grouped_forms: requests at or above the flop thresholds run alone "
+                                              "in BF16X6 (f32) / Ozaki (f64), the rest grouped plain")
     sat = max(out["rates"], key=lambda r: r["rate_req_s"])
     out["saturated"] = {"rate_req_s": sat["rate_req_s"], "grouped_tflops": sat["grouped"]["tflops"],
                         "per_request_tflops": sat["per_request"]["tflops"],
                         "ratio": sat["grouped"]["tflops"] / sat["per_request"]["tflops"]}
+    if with_forms:
+        out["saturated"]["grouped_forms_tflops"] = sat["grouped_forms"]["tflops"]
+        out["saturated"]["ratio_forms"] = sat["grouped_forms"]["tflops"] / sat["per_request"]["tflops"]
     del pools
     torch.cuda.empty_cache()
     return out

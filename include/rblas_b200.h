@@ -309,6 +309,15 @@ typedef struct {
  * grouped = 1 packs each admitted set into one grouped launch; grouped = 0
  * launches every request on its own (the per-request baseline). */
 rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void** server);
+/* Arithmetic forms for large requests: an f32 request of at least
+ * f32_min_flop flop (2mnk) runs on its own in f32_form (RB_PREC_PLAIN,
+ * RB_PREC_BF16X3 or RB_PREC_BF16X6), an f64 request of at least f64_min_flop
+ * in f64_form (RB_PREC_PLAIN or RB_PREC_OZAKI); all other requests take the
+ * plain path (grouped or one launch each). Applies to batches formed after
+ * the call; default plain. The precision forms take their scratch (digit or
+ * split planes) stream-ordered, outside the result budget. */
+rb_status rb_server_set_forms(void* server, int f32_form, int f64_form, double f32_min_flop,
+                              double f64_min_flop);
 /* Queue D = alpha*op(A)*op(B) + beta*C0 where p->c is the device-resident
  * C0 (read only when beta != 0) and D is allocated by the server with C's
  * layout. Returns at once; RB_ERR_BUSY if D could never fit the budget. */

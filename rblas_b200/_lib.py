@@ -85,6 +85,7 @@ SIGNATURES = {
     "rb_autotune_load": (_i, [C.c_char_p]),
     "rb_autotune_reset": (_i, []),
     "rb_server_create": (_i, [_sz, _i, _i, C.POINTER(C.c_void_p)]),
+    "rb_server_set_forms": (_i, [_vp, _i, _i, _d, _d]),
     "rb_server_submit": (_i, [_vp, C.POINTER(RbGemmProblem), C.POINTER(C.c_uint64)]),
     "rb_server_wait": (_i, [_vp, C.c_uint64, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                             C.POINTER(RbRequestTimes)]),

@@ -118,6 +118,8 @@ struct Batch {
     std::vector<Request*> reqs;
     cudaEvent_t done;
     int stream;
+    int form[2];         // forms and thresholds in force when the batch formed
+    double min_flop[2];
 };
 
 class Server {
@@ -125,6 +127,11 @@ public:
     size_t budget;
     int max_batch;
     int grouped;
+    // arithmetic forms for large requests (rb_server_set_forms): requests of
+    // at least min_flop[dtype] flop run alone in form[dtype]; the rest take
+    // the plain path (grouped or single)
+    int form[2] = {RB_PREC_PLAIN, RB_PREC_PLAIN};
+    double min_flop[2] = {0.0, 0.0};
     int device = 0;
     Pool pool;
     cudaStream_t streams[2] = {nullptr, nullptr};
@@ -245,15 +252,65 @@ public:
             probs.push_back(q);
         }
         int rc = RB_OK;
-        if (grouped) {
-            rc = grouped_gemm_dev(probs.data(), probs.size(), cin.data(), ldcin.data(), st, &ce, nullptr,
-                                  &staging[b.stream]);
-        } else {
-            for (size_t i = 0; i < probs.size() && rc == RB_OK; ++i)
-                rc = single_gemm_dev(&probs[i], cin[i], ldcin[i], st, &ce);
+        // large requests in a precision form run on their own; the rest stay plain
+        std::vector<size_t> alone;
+        std::vector<rb_gemm_problem> plain;
+        std::vector<const void*> plain_cin;
+        std::vector<size_t> plain_ldcin;
+        for (size_t i = 0; i < probs.size(); ++i) {
+            const rb_gemm_problem& q = probs[i];
+            const int f = b.form[q.dtype & 1];
+            const double flop = 2.0 * q.m * q.n * static_cast<double>(q.k);
+            if (f != RB_PREC_PLAIN && flop >= b.min_flop[q.dtype & 1] && flop > 0 && q.alpha != 0.0) {
+                alone.push_back(i);
+            } else {
+                plain.push_back(q);
+                plain_cin.push_back(cin[i]);
+                plain_ldcin.push_back(ldcin[i]);
+            }
         }
+        if (grouped) {
+            if (!plain.empty())
+                rc = grouped_gemm_dev(plain.data(), plain.size(), plain_cin.data(), plain_ldcin.data(), st, &ce,
+                                      nullptr, &staging[b.stream]);
+        } else {
+            for (size_t i = 0; i < plain.size() && rc == RB_OK; ++i)
+                rc = single_gemm_dev(&plain[i], plain_cin[i], plain_ldcin[i], st, &ce);
+        }
+        for (size_t i = 0; i < alone.size() && rc == RB_OK; ++i)
+            rc = precision_request(probs[alone[i]], cin[alone[i]], ldcin[alone[i]],
+                                   b.form[probs[alone[i]].dtype & 1], st, &ce);
         cudaEventRecord(b.done, st);
         return rc;
+    }
+
+    // D = alpha*op(A)op(B) + beta*C0 in a precision form: C0 copied into D
+    // (beta != 0), then the library's in-place column-major GEMM on D
+    static int precision_request(const rb_gemm_problem& q, const void* c0, size_t ldc0, int prec, cudaStream_t st,
+                                 int32_t* ce) {
+        const bool col = q.layout == RB_COL_MAJOR;
+        const size_t el = q.dtype ? 8 : 4;
+        const size_t m = col ? q.m : q.n, n = col ? q.n : q.m;  // column-major view
+        if (q.beta != 0.0) {
+            const cudaError_t e = cudaMemcpy2DAsync(q.c, q.ldc * el, c0, ldc0 * el, m * el, n,
+                                                    cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) {
+                if (ce) *ce = e;
+                return RB_ERR_CUDA;
+            }
+        }
+        const bool ta = (col ? q.transa : q.transb) != RB_NO_TRANS;
+        const bool tb = (col ? q.transb : q.transa) != RB_NO_TRANS;
+        const void* a = col ? q.a : q.b;
+        const void* b = col ? q.b : q.a;
+        const size_t lda = col ? q.lda : q.ldb, ldb = col ? q.ldb : q.lda;
+        if (q.dtype)
+            return gemm_colmajor_dev<double>(ta, tb, m, n, q.k, q.alpha, static_cast<const double*>(a), lda,
+                                             static_cast<const double*>(b), ldb, q.beta, static_cast<double*>(q.c),
+                                             q.ldc, prec, st, 0, ce);
+        return gemm_colmajor_dev<float>(ta, tb, m, n, q.k, static_cast<float>(q.alpha), static_cast<const float*>(a),
+                                        lda, static_cast<const float*>(b), ldb, static_cast<float>(q.beta),
+                                        static_cast<float*>(q.c), q.ldc, prec, st, 0, ce);
     }
 
     void loop() {
@@ -284,7 +341,8 @@ public:
                     }
                 }
                 if (!batch.empty()) {
-                    inflight[s].push_back(Batch{std::move(batch), get_event(), s});
+                    inflight[s].push_back(Batch{std::move(batch), get_event(), s, {form[0], form[1]},
+                                                {min_flop[0], min_flop[1]}});
                     next_stream = s ^ 1;
                     const Batch& b = inflight[s].back();
                     lk.unlock();
@@ -307,7 +365,8 @@ public:
                     queue.pop_front();
                     const int s = next_stream;
                     next_stream ^= 1;
-                    inflight[s].push_back(Batch{std::vector<Request*>{r}, get_event(), s});
+                    inflight[s].push_back(Batch{std::vector<Request*>{r}, get_event(), s, {form[0], form[1]},
+                                                {min_flop[0], min_flop[1]}});
                     fresh.push_back(&inflight[s].back());
                 }
                 if (!fresh.empty()) {
@@ -412,6 +471,19 @@ rb_status rb_server_create(size_t budget_bytes, int max_batch, int grouped, void
         return st;
     }
     *server = s;
+    return RB_OK;
+}
+
+rb_status rb_server_set_forms(void* server, int f32_form, int f64_form, double f32_min_flop, double f64_min_flop) {
+    Server* s = static_cast<Server*>(server);
+    if (!s || (f32_form != RB_PREC_PLAIN && f32_form != RB_PREC_BF16X3 && f32_form != RB_PREC_BF16X6) ||
+        (f64_form != RB_PREC_PLAIN && f64_form != RB_PREC_OZAKI) || !(f32_min_flop >= 0) || !(f64_min_flop >= 0))
+        return RB_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->form[0] = f32_form;
+    s->form[1] = f64_form;
+    s->min_flop[0] = f32_min_flop;
+    s->min_flop[1] = f64_min_flop;
     return RB_OK;
 }
 

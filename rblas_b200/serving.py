@@ -131,6 +131,15 @@ class Server:
             raise RuntimeError(f"rb_server_create failed: {self._lib.rb_status_string(st).decode()}")
         self._h = h
 
+    def set_forms(self, f32_form=0, f64_form=0, f32_min_flop=0.0, f64_min_flop=0.0):
+        """Run large requests in a precision form (rb_server_set_forms):
+        f32 requests of >= f32_min_flop flop in f32_form (Precision.Bf16x3 /
+        Bf16x6), f64 requests of >= f64_min_flop in f64_form (Precision.Ozaki)."""
+        st = self._lib.rb_server_set_forms(self._h, int(f32_form), int(f64_form), float(f32_min_flop),
+                                           float(f64_min_flop))
+        if st != 0:
+            raise RuntimeError(f"rb_server_set_forms failed: {self._lib.rb_status_string(st).decode()}")
+
     def submit(self, p: Problem) -> int:
         rid = C.c_uint64()
         q = p.to_c()

@@ -203,6 +203,47 @@ def _read(ptr, m, n, ld, dt, layout):
     return mat.T.copy() if layout == Layout.ColMajor else mat.copy()
 
 
+def test_server_precision_forms_for_large_requests():
+    """With set_forms, large requests run alone in the precision form (bit-
+    identical to the single-call path in that form) while small ones stay on
+    the grouped plain path; both in one serving run."""
+    from rblas_b200.types import Precision
+    rng = np.random.default_rng(66)
+    bigs = [make_problem(rng, np.float32, Layout.RowMajor, 1, 0, 600, 500, 700, 1.5, -0.5),
+            make_problem(rng, np.float64, Layout.ColMajor, 0, 1, 520, 610, 650, -0.75, 1.25),
+            make_problem(rng, np.float64, Layout.RowMajor, 2, 2, 300, 900, 800, 0.5, 0.0)]
+    small = random_mix(rng, 20, max_dim=200)
+    for grouped in (True, False):
+        with Server(budget_bytes=512 << 20, max_batch=32, grouped=grouped) as srv:
+            srv.set_forms(Precision.Bf16x6, Precision.Ozaki, 1e8, 1e8)
+            order = small[:10] + bigs + small[10:]
+            ids = [srv.submit(p) for p, _ in order]
+            got = []
+            for rid, (p, _) in zip(ids, order):
+                st, d, ldd, _ = srv.wait(rid)
+                assert st == 0
+                got.append(_read(d, p.m, p.n, ldd, p.dtype, p.layout))
+                srv.release(rid)
+        for (p, (A, B, C0)), g in zip(order, got):
+            flop = 2.0 * p.m * p.n * p.k
+            if flop >= 1e8:
+                prec = Precision.Bf16x6 if p.dtype == np.float32 else Precision.Ozaki
+                c = C0.clone()
+                level3.gemm_dev(p.layout, p.transa, p.transb, p.m, p.n, p.k, p.alpha, p.a, p.lda, p.b, p.ldb,
+                                p.beta, c.data_ptr(), p.ldc, p.dtype, prec=prec)
+                torch.cuda.synchronize()
+                h = c.cpu().numpy()
+                exp = h.reshape(p.m, p.n) if p.layout == Layout.RowMajor else h.reshape(p.n, p.m).T
+                assert np.array_equal(g, exp), (grouped, p.m, p.n, p.k)
+            else:
+                ref = restatement(p, A, B, C0)
+                ref = ref.reshape(p.m, p.n) if p.layout == Layout.RowMajor else ref.reshape(p.n, p.m).T
+                den = abs(p.alpha) * float(A.double().norm()) * float(B.double().norm()) + \
+                    (abs(p.beta) * float(C0.double().norm()) if p.beta != 0.0 else 0.0)
+                tol = 4 * max(p.k, 1) * (2.0 ** -24 if p.dtype == np.float32 else 2.0 ** -53)
+                assert np.linalg.norm(g.astype(np.float64) - ref) / den <= tol
+
+
 def test_server_budget_admission_and_busy():
     rng = np.random.default_rng(62)
     mix = random_mix(rng, 40, max_dim=300)
