@@ -242,15 +242,24 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
                 if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
             }
             if (ok && row_ok) {
+                // C read 16 values at a time, all requested before use, so
+                // the loads' latencies overlap instead of adding up
 #pragma unroll
-                for (int j = 0; j < UN; ++j) {
-                    const int col = n0 + j;
-                    if (col >= p.n) break;
-                    float* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
-                    float tb = 0.f;
-                    if (p.beta_mode == 1) tb = *cp;
-                    else if (p.beta_mode == 2) tb = p.beta_f * *cp;
-                    *cp = fmaf(p.alpha_f, sum[j], tb);
+                for (int g = 0; g < UN / 16; ++g) {
+                    float cv[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int col = n0 + g * 16 + jj;
+                        cv[jj] = (p.beta_mode != 0 && col < p.n) ? p.c[r + static_cast<size_t>(col) * p.ldc] : 0.f;
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int col = n0 + g * 16 + jj;
+                        if (col < p.n) {
+                            const float tb = (p.beta_mode == 2) ? p.beta_f * cv[jj] : cv[jj];
+                            p.c[r + static_cast<size_t>(col) * p.ldc] = fmaf(p.alpha_f, sum[g * 16 + jj], tb);
+                        }
+                    }
                 }
             }
         }
@@ -300,6 +309,14 @@ struct OzParams {
     const int* col_exp;
     uint32_t* err;
 };
+
+// v * 2^x: one multiply by an exactly representable power of two (the same
+// single rounding as scalbn), scalbn only where 2^x is not a double.
+__device__ __forceinline__ double scale_pow2(double v, int x) {
+    if (x >= -1022 && x <= 1023) return v * __longlong_as_double(static_cast<long long>(x + 1023) << 52);
+    if (x >= -1074 && x < -1022) return v * __longlong_as_double(1LL << (x + 1074));
+    return scalbn(v, x);
+}
 
 // unit u (0-based) of a chunk covers diagonals d0 and d1 = d0 + 1 (d1 < 0
 // when absent); units go from the highest diagonals down.
@@ -454,36 +471,40 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 const bool first_unit = (u == 0);
                 // digits of both operands are scaled by 2^-(e+1): weight 2^-(14+8d) per diagonal
                 const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0) - 2;
+                // C is read (beta*C0 on the first unit, the running sum after)
+                const bool read_c = !first_unit || p.beta_mode != 0;
+                const bool live = row_ok && !(er == kExpSentinel && !first_unit);
 #pragma unroll 1
-                for (int ch = 0; ch < 4; ++ch) {
-                    const int col0 = half * 128 + ch * 32;
-                    uint32_t v0[32], v1[32];
-                    tmem_ld32(lanebase + col0, v0);
-                    if (d1 >= 0) tmem_ld32(lanebase + UN + col0, v1);
-                    tmem_ld_wait();
-                    if (!row_ok || (er == kExpSentinel && !first_unit)) continue;
+                for (int ch = 0; ch < 8; ++ch) {
+                    // 16 columns at a time; the chunk's C values are requested
+                    // before the TMEM wait, so their latencies overlap
+                    const int col0 = half * 128 + ch * 16;
                     const int cbase = n0 + col0;
+                    double cv[16];
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) {
+                    for (int jj = 0; jj < 16; ++jj)
+                        cv[jj] = (live && read_c && cbase + jj < p.n)
+                                     ? p.c[r + static_cast<size_t>(cbase + jj) * p.ldc] : 0.0;
+                    uint32_t v0[16], v1[16];
+                    tmem_ld16(lanebase + col0, v0);
+                    if (d1 >= 0) tmem_ld16(lanebase + UN + col0, v1);
+                    tmem_ld_wait();
+                    if (!live) continue;
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
                         const int col = cbase + jj;
-                        if (col >= p.n) break;
-                        double* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
-                        const int fc = __ldg(p.col_exp + col);
-                        double term = 0.0;
-                        if (er != kExpSentinel && fc != kExpSentinel) {
-                            double sv = static_cast<double>(static_cast<int32_t>(v0[jj]));
-                            if (d1 >= 0) sv = fma(sv, 256.0, static_cast<double>(static_cast<int32_t>(v1[jj])));
-                            term = scalbn(sv, er + fc - wexp);
+                        if (col < p.n) {
+                            const int fc = __ldg(p.col_exp + col);
+                            double term = 0.0;
+                            if (er != kExpSentinel && fc != kExpSentinel) {
+                                double sv = static_cast<double>(static_cast<int32_t>(v0[jj]));
+                                if (d1 >= 0) sv = fma(sv, 256.0, static_cast<double>(static_cast<int32_t>(v1[jj])));
+                                term = scale_pow2(sv, er + fc - wexp);
+                            }
+                            double acc = cv[jj];
+                            if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
+                            p.c[r + static_cast<size_t>(col) * p.ldc] = fma(p.alpha, term, acc);
                         }
-                        double acc;
-                        if (first_unit) {
-                            acc = 0.0;
-                            if (p.beta_mode == 1) acc = *cp;
-                            else if (p.beta_mode == 2) acc = p.beta * *cp;
-                        } else {
-                            acc = *cp;
-                        }
-                        *cp = fma(p.alpha, term, acc);
                     }
                 }
                 tc_fence_before();
