@@ -397,8 +397,13 @@ rb_status rb_device_error(int clear, uint32_t* detail);
 void rb_kernel_timing_enable(int on);
 int rb_kernel_timing_report(char* buf, size_t buf_len);
 
-/* Releases the cached device/pinned staging buffers of the current device. */
+/* Releases the cached device/pinned staging buffers of the current device
+ * and returns the scratch pool's free blocks to the driver. */
 void rb_release_cached_memory(void);
+/* Freed scratch (split/digit planes, repacks, problem tables) stays mapped
+ * in the library's per-device pool up to this many bytes (default 8 GiB), so
+ * that calls after a synchronisation do not map memory again. */
+void rb_set_scratch_cache_bytes(size_t bytes);
 
 /* Measures the current GPU's FMA throughput in TFLOP/s (is_f64: FP64 DFMA,
  * else FP32 FFMA; iters <= 0 picks a default). The roofline denominator of

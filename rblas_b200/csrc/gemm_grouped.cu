@@ -598,7 +598,7 @@ int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* con
     const size_t own = (staged ? 0 : gb.all_bytes + ws_bytes) + gb.scratch;
     uint8_t* mem = nullptr;
     if (own) {
-        e = cudaMallocAsync(reinterpret_cast<void**>(&mem), own, st);
+        e = scratch_alloc(reinterpret_cast<void**>(&mem), own, st);
         if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
     }
     if (staged) {

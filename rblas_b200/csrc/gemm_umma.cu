@@ -843,7 +843,7 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
     void* buf = nullptr;
     const size_t a_bytes = round_up(planes * pa * sizeof(__nv_bfloat16), 256);
-    cudaError_t e = cudaMallocAsync(&buf, a_bytes + planes * pb * sizeof(__nv_bfloat16), st);
+    cudaError_t e = scratch_alloc(&buf, a_bytes + planes * pb * sizeof(__nv_bfloat16), st);
     if (e != cudaSuccess) return e;
     __nv_bfloat16* sa = static_cast<__nv_bfloat16*>(buf);
     __nv_bfloat16* sb = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(buf) + a_bytes);
@@ -887,7 +887,7 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     void* buf = nullptr;
     const size_t exps = round_up((static_cast<size_t>(m) + n) * sizeof(int), 256);
     const size_t a_bytes = round_up(slices * pa, 256);
-    cudaError_t e = cudaMallocAsync(&buf, exps + a_bytes + slices * pb, st);
+    cudaError_t e = scratch_alloc(&buf, exps + a_bytes + slices * pb, st);
     if (e != cudaSuccess) return e;
     int* ea = static_cast<int*>(buf);
     int* eb = ea + m;

@@ -304,7 +304,7 @@ int complex_gemm_dev(int transa, int transb, size_t m, size_t n, size_t k, T ar,
     const size_t b_bytes = expand_b ? rup(ldb2 * n * sizeof(T), 256) : 0;
     const size_t p_bytes = ldp * n * sizeof(T);
     void* buf = nullptr;
-    cudaError_t e = cudaMallocAsync(&buf, a_bytes + b_bytes + p_bytes, st);
+    cudaError_t e = scratch_alloc(&buf, a_bytes + b_bytes + p_bytes, st);
     if (e != cudaSuccess) return fail(e, ce);
     T* Ap = static_cast<T*>(buf);
     T* Bp = expand_b ? reinterpret_cast<T*>(static_cast<uint8_t*>(buf) + a_bytes) : const_cast<T*>(B);
@@ -360,7 +360,7 @@ int symm_dev(int side, int uplo, size_t m, size_t n, T alpha, const T* A, size_t
     if (m == 0 || n == 0) return RB_OK;
     const size_t ldf = rup(q, 16 / sizeof(T));
     void* full = nullptr;
-    cudaError_t e = cudaMallocAsync(&full, ldf * q * sizeof(T), st);
+    cudaError_t e = scratch_alloc(&full, ldf * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
     sym_expand_kernel<T, false><<<grid_for(q * q), 256, 0, st>>>(A, lda, (int)q, uplo, 0, static_cast<T*>(full), ldf);
     count_launch();
@@ -382,7 +382,7 @@ int hesy_dev(int herm, int side, int uplo, size_t m, size_t n, T ar, T ai, const
     if (m == 0 || n == 0) return RB_OK;  // src/complex3.rs:184-186
     const size_t q = (side == RB_LEFT) ? m : n;
     void* full = nullptr;
-    cudaError_t e = cudaMallocAsync(&full, 2 * q * q * sizeof(T), st);
+    cudaError_t e = scratch_alloc(&full, 2 * q * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
     sym_expand_kernel<T, true><<<grid_for(q * q), 256, 0, st>>>(A, lda, (int)q, uplo, herm, static_cast<T*>(full), q);
     count_launch();

@@ -23,6 +23,60 @@
 
 namespace rb {
 
+// ---- library scratch pool (one per device) ---------------------------------
+namespace {
+std::mutex g_pool_mu;
+constexpr int kPoolDevices = 64;
+cudaMemPool_t g_pools[kPoolDevices] = {};
+std::atomic<uint64_t> g_scratch_cache{uint64_t(8) << 30};
+
+cudaMemPool_t pool_for_current(cudaError_t* err) {
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess || dev < 0 || dev >= kPoolDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        *err = cudaMemPoolCreate(&g_pools[dev], &props);
+        if (*err != cudaSuccess) {
+            g_pools[dev] = nullptr;
+            return nullptr;
+        }
+        uint64_t thr = g_scratch_cache.load();
+        cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    return g_pools[dev];
+}
+}  // namespace
+
+cudaError_t scratch_alloc_raw(void** p, size_t bytes, cudaStream_t st) {
+    cudaError_t e;
+    cudaMemPool_t pool = pool_for_current(&e);
+    if (!pool) return e == cudaSuccess ? cudaErrorMemoryAllocation : e;
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+void scratch_trim() {
+    cudaError_t e;
+    cudaMemPool_t pool = pool_for_current(&e);
+    if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+
+void set_scratch_cache_bytes(size_t bytes) {
+    g_scratch_cache.store(bytes);
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    uint64_t thr = bytes;
+    for (auto& pl : g_pools)
+        if (pl) cudaMemPoolSetAttribute(pl, cudaMemPoolAttrReleaseThreshold, &thr);
+}
+
+}  // namespace rb
+
+namespace rb {
+
 std::atomic<uint64_t> g_launches{0};
 
 // ---- kernel timing registry ---------------------------------------------------
@@ -252,7 +306,7 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
     const size_t b_rows = p.tb ? p.n : p.k, b_cols = p.tb ? p.k : p.n;
     if (!tma_ok(A, lda)) {
         const size_t ld2 = (a_rows + vec - 1) / vec * vec;
-        e = cudaMallocAsync(&scratch[0], ld2 * a_cols * sizeof(T), st);
+        e = scratch_alloc(&scratch[0], ld2 * a_cols * sizeof(T), st);
         if (e != cudaSuccess) return cuda_fail(err, e);
         e = cudaMemcpy2DAsync(scratch[0], ld2 * sizeof(T), A, lda * sizeof(T), a_rows * sizeof(T),
                               a_cols, cudaMemcpyDeviceToDevice, st);
@@ -262,7 +316,7 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
     }
     if (!tma_ok(B, ldb)) {
         const size_t ld2 = (b_rows + vec - 1) / vec * vec;
-        e = cudaMallocAsync(&scratch[1], ld2 * b_cols * sizeof(T), st);
+        e = scratch_alloc(&scratch[1], ld2 * b_cols * sizeof(T), st);
         if (e != cudaSuccess) return cuda_fail(err, e);
         e = cudaMemcpy2DAsync(scratch[1], ld2 * sizeof(T), B, ldb * sizeof(T), b_rows * sizeof(T),
                               b_cols, cudaMemcpyDeviceToDevice, st);
@@ -631,7 +685,10 @@ void rb_release_cached_memory(void) {
         c->buf[i] = nullptr;
         c->cap[i] = 0;
     }
+    scratch_trim();
 }
+
+void rb_set_scratch_cache_bytes(size_t bytes) { rb::set_scratch_cache_bytes(bytes); }
 
 }  // extern "C"
 

@@ -51,6 +51,19 @@ bool kernel_timing_on();
 void kernel_timing_begin(const char* name, double work, cudaStream_t st, KernelTimer* t);
 void kernel_timing_end(KernelTimer* t, cudaStream_t st);
 
+// Stream-ordered scratch (split and digit planes, repacks, tables) from the
+// library's own per-device memory pool. Freed blocks stay mapped in the pool
+// up to a release threshold (default 8 GiB, rb_set_scratch_cache_bytes), so
+// a call after a synchronisation does not map fresh memory again; free with
+// cudaFreeAsync on the stream.
+cudaError_t scratch_alloc_raw(void** p, size_t bytes, cudaStream_t st);
+template <typename T>
+inline cudaError_t scratch_alloc(T** p, size_t bytes, cudaStream_t st) {
+    return scratch_alloc_raw(reinterpret_cast<void**>(p), bytes, st);
+}
+void scratch_trim();
+void set_scratch_cache_bytes(size_t bytes);
+
 // Per-device error word (device memory, zero when healthy).
 uint32_t* device_error_word();
 
