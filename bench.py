@@ -479,8 +479,7 @@ def run_ours(args):
     if not args.no_serve and rank == 0 and ws == 1:
         from rblas_b200.serving import autotune
         tuned = autotune()
-        serving = run_serving(torch, [5000.0, 10000.0, 15000.0, 20000.0, 50000.0], 5000, 60 << 30,
-                              with_forms=False)
+        serving = run_serving(torch, [10000.0, 15000.0, 20000.0, 25000.0, 30000.0, 50000.0], 5000, 60 << 30)
         serving["autotuned_buckets"] = tuned
         serving["note"] = ("5000-request slice of the serving stream; operands resident in HBM; "
                            "latency = enqueue -> completion observed by the server")
@@ -526,9 +525,9 @@ def serving_trace(n_req, seed=5):
 
 
 # precision forms for large serving requests (each within 2x of plain's
-# error against the FP64 oracle): f32 >= 5e8 flop in BF16X6, f64 >= 4e9 flop
+# error against the FP64 oracle): f32 >= 2e8 flop in BF16X6, f64 >= 1e9 flop
 # in Ozaki; smaller requests stay on the grouped plain kernel
-SERVE_FORMS = {"f32_form": 3, "f64_form": 2, "f32_min_flop": 5e8, "f64_min_flop": 4e9}
+SERVE_FORMS = {"f32_form": 3, "f64_form": 2, "f32_min_flop": 2e8, "f64_min_flop": 1e9}
 
 
 def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=True):
@@ -617,6 +616,9 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
 def run_serve_mode(args):
     import torch
     torch.cuda.set_device(0)
+    if args.serve_thresholds:
+        f32_min, f64_min = (float(x) for x in args.serve_thresholds.split(","))
+        SERVE_FORMS.update(f32_min_flop=f32_min, f64_min_flop=f64_min)
     if not args.no_autotune:
         from rblas_b200.serving import autotune
         autotune()
@@ -755,6 +757,8 @@ def main():
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rates", default="1000,2000,5000,8000,10000,12500,15000,17500,20000,25000,30000,50000")
     ap.add_argument("--no-autotune", action="store_true", help="serving: keep the built-in split-K rule")
+    ap.add_argument("--serve-thresholds", default="", metavar="F32,F64",
+                    help="serving: flop thresholds for the precision forms (default 2e8,1e9)")
     ap.add_argument("--no-serve", action="store_true", help="default run: skip the serving summary")
     ap.add_argument("--no-configs", action="store_true", help="default run: skip the C1/C3/C4 measurements")
     ap.add_argument("--budget-gb", type=float, default=120.0)

@@ -59,6 +59,18 @@ cudaError_t scratch_alloc_raw(void** p, size_t bytes, cudaStream_t st) {
     return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
 
+void scratch_reserve(size_t bytes) {
+    cudaError_t e;
+    cudaMemPool_t pool = pool_for_current(&e);
+    if (!pool || bytes == 0) return;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return;
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, bytes, pool, st) == cudaSuccess) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+}
+
 void scratch_trim() {
     cudaError_t e;
     cudaMemPool_t pool = pool_for_current(&e);

@@ -62,6 +62,9 @@ inline cudaError_t scratch_alloc(T** p, size_t bytes, cudaStream_t st) {
     return scratch_alloc_raw(reinterpret_cast<void**>(p), bytes, st);
 }
 void scratch_trim();
+// Map `bytes` into the scratch pool now (allocated and freed at once), so
+// that later allocations within the release threshold find it mapped.
+void scratch_reserve(size_t bytes);
 void set_scratch_cache_bytes(size_t bytes);
 
 // Per-device error word (device memory, zero when healthy).

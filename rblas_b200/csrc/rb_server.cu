@@ -135,6 +135,12 @@ public:
     int device = 0;
     Pool pool;
     cudaStream_t streams[2] = {nullptr, nullptr};
+    // requests that run alone in a precision form go round-robin over these,
+    // so medium-sized ones share the GPU instead of running one after another
+    static constexpr int kFormStreams = 4;
+    cudaStream_t form_streams[kFormStreams] = {};
+    cudaEvent_t form_events[kFormStreams] = {};  // re-recorded per use; a wait takes the latest record
+    int next_form_stream = 0;
     // per stream: pinned host + device problem table of max_batch entries and
     // a split-K workspace, rewritten only after that stream's previous batch
     // has retired (grouped mode keeps at most one batch per stream in flight)
@@ -160,6 +166,11 @@ public:
         if (!pool.init(budget, e)) return RB_ERR_ALLOC;
         for (auto& s : streams) {
             *e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (*e != cudaSuccess) return RB_ERR_CUDA;
+        }
+        for (int i = 0; i < kFormStreams; ++i) {
+            *e = cudaStreamCreateWithFlags(&form_streams[i], cudaStreamNonBlocking);
+            if (*e == cudaSuccess) *e = cudaEventCreateWithFlags(&form_events[i], cudaEventDisableTiming);
             if (*e != cudaSuccess) return RB_ERR_CUDA;
         }
         if (grouped) {
@@ -188,11 +199,17 @@ public:
         if (worker.joinable()) worker.join();
         for (auto& s : streams)
             if (s) cudaStreamSynchronize(s);
+        for (auto& s : form_streams)
+            if (s) cudaStreamSynchronize(s);
         for (auto& q : inflight)
             for (auto& b : q) cudaEventDestroy(b.done);
         for (auto ev : free_events) cudaEventDestroy(ev);
         for (auto& s : streams)
             if (s) cudaStreamDestroy(s);
+        for (int i = 0; i < kFormStreams; ++i) {
+            if (form_streams[i]) cudaStreamDestroy(form_streams[i]);
+            if (form_events[i]) cudaEventDestroy(form_events[i]);
+        }
         for (auto& g : staging) {
             if (g.host) cudaFreeHost(g.host);
             if (g.dev) cudaFree(g.dev);
@@ -277,9 +294,18 @@ public:
             for (size_t i = 0; i < plain.size() && rc == RB_OK; ++i)
                 rc = single_gemm_dev(&plain[i], plain_cin[i], plain_ldcin[i], st, &ce);
         }
-        for (size_t i = 0; i < alone.size() && rc == RB_OK; ++i)
+        for (size_t i = 0; i < alone.size() && rc == RB_OK; ++i) {
+            // on a form stream; the batch's stream then waits for it, so the
+            // batch's completion event covers the request
+            const int f = next_form_stream;
+            next_form_stream = (next_form_stream + 1) % kFormStreams;
             rc = precision_request(probs[alone[i]], cin[alone[i]], ldcin[alone[i]],
-                                   b.form[probs[alone[i]].dtype & 1], st, &ce);
+                                   b.form[probs[alone[i]].dtype & 1], form_streams[f], &ce);
+            if (rc == RB_OK) {
+                cudaEventRecord(form_events[f], form_streams[f]);
+                cudaStreamWaitEvent(st, form_events[f], 0);
+            }
+        }
         cudaEventRecord(b.done, st);
         return rc;
     }
@@ -479,6 +505,13 @@ rb_status rb_server_set_forms(void* server, int f32_form, int f64_form, double f
     if (!s || (f32_form != RB_PREC_PLAIN && f32_form != RB_PREC_BF16X3 && f32_form != RB_PREC_BF16X6) ||
         (f64_form != RB_PREC_PLAIN && f64_form != RB_PREC_OZAKI) || !(f32_min_flop >= 0) || !(f64_min_flop >= 0))
         return RB_ERR_INVALID_ARG;
+    // precision requests take their planes from the scratch pool on several
+    // streams at once: map its working set now rather than in the middle of
+    // a run (growing a pool under load stalled the serving loop)
+    if (f32_form != RB_PREC_PLAIN || f64_form != RB_PREC_PLAIN) {
+        cudaSetDevice(s->device);
+        scratch_reserve(size_t(6) << 30);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     s->form[0] = f32_form;
     s->form[1] = f64_form;
