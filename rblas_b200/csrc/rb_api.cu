@@ -131,10 +131,14 @@ constexpr int kMaxDevices = 64;
 
 // Per-device state for host-slice calls: an internal stream, grow-only
 // staging buffers for A, B, C, and the device error word.
+constexpr int kHostPanels = 4;  // column panels of a large host-slice GEMM
+
 struct DeviceCtx {
     std::mutex mu;
     bool init = false;
     cudaStream_t stream = nullptr;
+    cudaStream_t pstream[kHostPanels] = {};  // one per panel of a pipelined host call
+    cudaEvent_t a_ready = nullptr, pdone[kHostPanels] = {};
     uint32_t* err_word = nullptr;
     void* buf[3] = {nullptr, nullptr, nullptr};
     size_t cap[3] = {0, 0, 0};
@@ -162,6 +166,12 @@ DeviceCtx* ctx_for_current(cudaError_t* e) {
         *e = cudaMalloc(&c.err_word, 64);
         if (*e != cudaSuccess) return nullptr;
         *e = cudaMemset(c.err_word, 0, 64);
+        if (*e != cudaSuccess) return nullptr;
+        *e = cudaEventCreateWithFlags(&c.a_ready, cudaEventDisableTiming);
+        for (int i = 0; i < kHostPanels && *e == cudaSuccess; ++i) {
+            *e = cudaStreamCreateWithFlags(&c.pstream[i], cudaStreamNonBlocking);
+            if (*e == cudaSuccess) *e = cudaEventCreateWithFlags(&c.pdone[i], cudaEventDisableTiming);
+        }
         if (*e != cudaSuccess) return nullptr;
         c.init = true;
     }
@@ -416,6 +426,64 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
     T* dB = static_cast<T*>(ctx->buf[1]);
     T* dC = static_cast<T*>(ctx->buf[2]);
     cudaStream_t st = ctx->stream;
+
+    // Large calls run as column panels of C (and of op(B)), each on its own
+    // stream, after A has been uploaded once: one panel's upload, GEMM and
+    // download overlap the others' (host-to-device and device-to-host copies
+    // use separate engines). Every element of C is computed from the same
+    // operands in the same order as in one whole call, so results are the
+    // same bit for bit. Panels are multiples of 256 columns (every kernel's
+    // tile width divides 256, and the offsets stay 16-byte aligned).
+    const size_t el = sizeof(T);
+    const size_t total_bytes = (need_ab ? (a_rows * a_cols + b_rows * b_cols) * el : 0) +
+                               p.m * p.n * el * (read_c ? 2 : 1);
+    if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256) {
+        const size_t width = std::max<size_t>(256, (p.n + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
+        if (need_ab) {
+            e = cudaMemcpy2DAsync(dA, lda_d * el, p.a, p.lda * el, a_rows * el, a_cols, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(err, e);
+        }
+        if ((e = cudaEventRecord(ctx->a_ready, st)) != cudaSuccess) return cuda_fail(err, e);
+        rb_status ps = RB_OK;
+        int used = 0;
+        for (size_t j0 = 0; j0 < p.n && ps == RB_OK; j0 += width, ++used) {
+            const size_t jn = std::min(width, p.n - j0);
+            cudaStream_t sp = ctx->pstream[used];
+            e = cudaStreamWaitEvent(sp, ctx->a_ready, 0);
+            if (e == cudaSuccess && need_ab) {
+                if (p.tb)  // op(B) columns j0.. are rows j0.. of the stored n x k B
+                    e = cudaMemcpy2DAsync(dB + j0, ldb_d * el, p.b + j0, p.ldb * el, jn * el, b_cols,
+                                          cudaMemcpyHostToDevice, sp);
+                else
+                    e = cudaMemcpy2DAsync(dB + j0 * ldb_d, ldb_d * el, p.b + j0 * p.ldb, p.ldb * el, b_rows * el, jn,
+                                          cudaMemcpyHostToDevice, sp);
+            }
+            if (e == cudaSuccess && read_c)
+                e = cudaMemcpy2DAsync(dC + j0 * ldc_d, ldc_d * el, p.c + j0 * p.ldc, p.ldc * el, p.m * el, jn,
+                                      cudaMemcpyHostToDevice, sp);
+            if (e != cudaSuccess) {
+                ps = cuda_fail(err, e);
+                break;
+            }
+            ColProblem<T> q = p;
+            q.n = jn;
+            q.a = dA; q.lda = lda_d;
+            q.b = p.tb ? dB + j0 : dB + j0 * ldb_d; q.ldb = ldb_d;
+            q.c = dC + j0 * ldc_d; q.ldc = ldc_d;
+            ps = run_dev<T>(q, prec, sp, err);
+            if (ps != RB_OK) break;
+            e = cudaMemcpy2DAsync(p.c + j0 * p.ldc, p.ldc * el, dC + j0 * ldc_d, ldc_d * el, p.m * el, jn,
+                                  cudaMemcpyDeviceToHost, sp);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->pdone[used], sp);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->pdone[used], 0);
+            if (e != cudaSuccess) ps = cuda_fail(err, e);
+        }
+        if (ps != RB_OK) {
+            for (int i = 0; i < used + 1 && i < kHostPanels; ++i) cudaStreamSynchronize(ctx->pstream[i]);
+            return ps;
+        }
+        return check_device_word(ctx, err);
+    }
 
     if (need_ab) {
         e = cudaMemcpy2DAsync(dA, lda_d * sizeof(T), p.a, p.lda * sizeof(T), a_rows * sizeof(T), a_cols,

@@ -141,3 +141,33 @@ def test_launch_counter_advances():
     p = Problem(Layout.ColMajor, 0, 0, 64, 64, 64, np.float32, seed=12)
     _gpu_gemm(p)
     assert rb.launch_count() > before
+
+
+@pytest.mark.parametrize("dtype,prec", [(np.float64, 0), (np.float64, 2), (np.float32, 0), (np.float32, 3)])
+@pytest.mark.parametrize("layout,ta,tb,m,n,k", [(Layout.ColMajor, 0, 0, 2600, 1300, 2600),
+                                                 (Layout.RowMajor, 1, 1, 2400, 1536, 2600),
+                                                 (Layout.ColMajor, 1, 0, 3072, 2304, 1400)])
+def test_pipelined_host_call_matches_device_call_exactly(dtype, prec, layout, ta, tb, m, n, k):
+    """Host-slice calls of at least 64 MB run as column panels on several
+    streams; every element is computed as in one whole call, so the result
+    equals the device-pointer call on the same data bit for bit (ragged last
+    panel, transposes, both layouts, plain and precision forms)."""
+    torch = pytest.importorskip("torch")
+    from rblas_b200.types import Precision
+    rng = np.random.default_rng(120 + m)
+    ar, ac = (k, m) if ta else (m, k)
+    br, bc = (n, k) if tb else (k, n)
+    contig = (lambda r, c: r) if layout == Layout.ColMajor else (lambda r, c: c)
+    lda, ldb, ldc = contig(ar, ac), contig(br, bc), contig(m, n)
+    a = rng.standard_normal(ar * ac).astype(dtype)
+    b = rng.standard_normal(br * bc).astype(dtype)
+    c0 = rng.standard_normal(m * n).astype(dtype)
+    assert (a.nbytes + b.nbytes + 2 * c0.nbytes) >= 64 << 20
+    host = c0.copy()
+    level3.gemm(layout, ta, tb, m, n, k, 1.25, a, lda, b, ldb, -0.5, host, ldc, prec=Precision(prec))
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    A, B, Cd = (torch.tensor(x, dtype=tdt, device="cuda") for x in (a, b, c0))
+    level3.gemm_dev(layout, ta, tb, m, n, k, 1.25, A.data_ptr(), lda, B.data_ptr(), ldb, -0.5, Cd.data_ptr(), ldc,
+                    dtype, prec=Precision(prec))
+    torch.cuda.synchronize()
+    assert np.array_equal(host, Cd.cpu().numpy())
