@@ -60,6 +60,48 @@ def dist_info():
     return ws, rank, local
 
 
+class Replicas:
+    """One replica of the step per rank: GEMM has no exchange step, so the
+    ranks share only the barrier before each timed region and the max over
+    ranks of each time (every rank takes the same collective steps in the
+    same order). `device` holds the reduction tensor: the rank's GPU for
+    nccl, the CPU for gloo."""
+
+    def __init__(self, backend, device):
+        import torch
+        self.torch = torch
+        self.ws, self.rank, _ = dist_info()
+        self.device = device
+        self.dist = None
+        if self.ws > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x):
+        if not self.dist:
+            return float(x)
+        t = self.torch.tensor([float(x)], device=self.device, dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    @staticmethod
+    def value(work_per_rank, seconds, ws):
+        """Whole-job throughput (TFLOP/s): every rank's work over the slowest rank's time."""
+        return work_per_rank * ws / seconds / 1e12
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # --------------------------------------------------------------------------
 # clocks
 # --------------------------------------------------------------------------
@@ -232,11 +274,7 @@ def run_ours(args):
 
     ws, rank, local = dist_info()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    rep = Replicas("nccl", torch.device("cuda", local))
 
     lib = rb.load_library()
     dev = torch.device("cuda", local)
@@ -265,8 +303,7 @@ def run_ours(args):
     def timed(fn, steps, warmup):
         for _ in range(warmup):
             fn()
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -281,11 +318,7 @@ def run_ours(args):
         lib.rb_kernel_timing_enable(0)
         kr = kernel_report()
         launches = rb.launch_count() - l0
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = rep.max(e0.elapsed_time(e1))
         return ms / steps, launches, kr
 
     # ---- pipe peaks measured in this run (roofline denominators) ----------
@@ -310,7 +343,7 @@ def run_ours(args):
             continue
         with ClockSampler(local) as cs:
             ms, launches, kr = timed(lambda: dev_step(prec), args.steps, args.warmup)
-        forms[name] = {"tflops": step_flops() * ws / (ms * 1e-3) / 1e12, "ms_per_step": ms,
+        forms[name] = {"tflops": Replicas.value(step_flops(), ms * 1e-3, ws), "ms_per_step": ms,
                        "gpu_launches": launches, "clocks": cs.summary()}
         kreports[name] = kr
         if name == "plain" or args.form != "plain":
@@ -456,20 +489,15 @@ def run_ours(args):
 
         for _ in range(max(1, args.warmup)):
             host_step()
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
         k_e2e = max(2, args.steps // 2)
         t0 = time.perf_counter()
         for _ in range(k_e2e):
             h2d, d2h = host_step()
         torch.cuda.synchronize()
-        dt = (time.perf_counter() - t0) / k_e2e
-        if dist:
-            t = torch.tensor([dt], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
-        e2e = {"value": step_flops() * ws / dt / 1e12, "unit": "TFLOP/s",
+        dt = rep.max((time.perf_counter() - t0) / k_e2e)
+        e2e = {"value": Replicas.value(step_flops(), dt, ws), "unit": "TFLOP/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": k_e2e,
                "timing": "host wall clock around synchronous host-API calls (pinned buffers)"}
 
@@ -502,9 +530,7 @@ def run_ours(args):
             "device_error": {"after_headline": err_status[0], "end_of_run": rb.device_error()[0]},
         }
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 # --------------------------------------------------------------------------
