@@ -219,6 +219,86 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                        size_t n, double alpha, const double* a, size_t lda, double* b, size_t ldb,
                        void* stream, rb_error* err);
 
+/* ---------------------------------------------------------------------------
+ * Level 2: gemv and rank-1 updates (level2::gemv / ger, src/level2.rs:11-88;
+ * complex2::gemv / geru / gerc, src/complex2.rs:11-145). x and y are strided
+ * (incx, incy in elements; incx may be 0). Host-slice forms check A like
+ * check_matrix and each vector against its slice length ('x', 'y'), then
+ * return RB_ERR_ZERO_STRIDE for incy == 0 with more than one output (rblas
+ * would update one element serially; there is no parallel form). The beta
+ * pass follows rblas: real beta == 1 leaves y, beta == 0 writes 0 without
+ * reading y; complex always runs it (src/complex2.rs:31-40). alpha == 0
+ * stops after the beta pass (gemv) or writes nothing (rank-1 updates).
+ * ------------------------------------------------------------------------- */
+
+/* y := alpha*op(A)*x + beta*y; A is m x n in `layout`; op(A) is A for
+ * RB_NO_TRANS (x has n elements, y m), A^T for RB_TRANS (x m, y n), A^H for
+ * RB_CONJ_TRANS (complex). Replaces level2::gemv (src/level2.rs:11-62) and
+ * complex2::gemv (src/complex2.rs:11-77). */
+rb_status rb_sgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, float alpha, const float* a,
+                   size_t lda, size_t a_len, const float* x, size_t incx, size_t x_len, float beta, float* y,
+                   size_t incy, size_t y_len, rb_error* err);
+rb_status rb_dgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, double alpha, const double* a,
+                   size_t lda, size_t a_len, const double* x, size_t incx, size_t x_len, double beta, double* y,
+                   size_t incy, size_t y_len, rb_error* err);
+rb_status rb_cgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex32 alpha,
+                   const rb_complex32* a, size_t lda, size_t a_len, const rb_complex32* x, size_t incx,
+                   size_t x_len, rb_complex32 beta, rb_complex32* y, size_t incy, size_t y_len, rb_error* err);
+rb_status rb_zgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex64 alpha,
+                   const rb_complex64* a, size_t lda, size_t a_len, const rb_complex64* x, size_t incx,
+                   size_t x_len, rb_complex64 beta, rb_complex64* y, size_t incy, size_t y_len, rb_error* err);
+/* A := alpha*x*y^T + A (A m x n in `layout`, x m elements, y n).
+ * Replaces level2::ger (src/level2.rs:65-88); each element is computed as
+ * rblas does (fma(alpha*x_i, y_j, a_ij)). */
+rb_status rb_sger(rb_layout layout, size_t m, size_t n, float alpha, const float* x, size_t incx, size_t x_len,
+                  const float* y, size_t incy, size_t y_len, float* a, size_t lda, size_t a_len, rb_error* err);
+rb_status rb_dger(rb_layout layout, size_t m, size_t n, double alpha, const double* x, size_t incx, size_t x_len,
+                  const double* y, size_t incy, size_t y_len, double* a, size_t lda, size_t a_len, rb_error* err);
+/* A := alpha*x*y^T + A (geru) or alpha*x*y^H + A (gerc): complex2::geru /
+ * gerc (src/complex2.rs:80-145), each element as rblas computes it. */
+rb_status rb_cgeru(rb_layout layout, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* x, size_t incx,
+                   size_t x_len, const rb_complex32* y, size_t incy, size_t y_len, rb_complex32* a, size_t lda,
+                   size_t a_len, rb_error* err);
+rb_status rb_zgeru(rb_layout layout, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* x, size_t incx,
+                   size_t x_len, const rb_complex64* y, size_t incy, size_t y_len, rb_complex64* a, size_t lda,
+                   size_t a_len, rb_error* err);
+rb_status rb_cgerc(rb_layout layout, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* x, size_t incx,
+                   size_t x_len, const rb_complex32* y, size_t incy, size_t y_len, rb_complex32* a, size_t lda,
+                   size_t a_len, rb_error* err);
+rb_status rb_zgerc(rb_layout layout, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* x, size_t incx,
+                   size_t x_len, const rb_complex64* y, size_t incy, size_t y_len, rb_complex64* a, size_t lda,
+                   size_t a_len, rb_error* err);
+/* Device-pointer twins of the above, enqueued on `stream` (lda checked;
+ * buffer lengths are the caller's responsibility). */
+rb_status rb_sgemv_dev(rb_layout layout, rb_transpose trans, size_t m, size_t n, float alpha, const float* a,
+                       size_t lda, const float* x, size_t incx, float beta, float* y, size_t incy, void* stream,
+                       rb_error* err);
+rb_status rb_dgemv_dev(rb_layout layout, rb_transpose trans, size_t m, size_t n, double alpha, const double* a,
+                       size_t lda, const double* x, size_t incx, double beta, double* y, size_t incy, void* stream,
+                       rb_error* err);
+rb_status rb_cgemv_dev(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex32 alpha,
+                       const rb_complex32* a, size_t lda, const rb_complex32* x, size_t incx, rb_complex32 beta,
+                       rb_complex32* y, size_t incy, void* stream, rb_error* err);
+rb_status rb_zgemv_dev(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex64 alpha,
+                       const rb_complex64* a, size_t lda, const rb_complex64* x, size_t incx, rb_complex64 beta,
+                       rb_complex64* y, size_t incy, void* stream, rb_error* err);
+rb_status rb_sger_dev(rb_layout layout, size_t m, size_t n, float alpha, const float* x, size_t incx,
+                      const float* y, size_t incy, float* a, size_t lda, void* stream, rb_error* err);
+rb_status rb_dger_dev(rb_layout layout, size_t m, size_t n, double alpha, const double* x, size_t incx,
+                      const double* y, size_t incy, double* a, size_t lda, void* stream, rb_error* err);
+rb_status rb_cgeru_dev(rb_layout layout, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* x,
+                       size_t incx, const rb_complex32* y, size_t incy, rb_complex32* a, size_t lda, void* stream,
+                       rb_error* err);
+rb_status rb_zgeru_dev(rb_layout layout, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* x,
+                       size_t incx, const rb_complex64* y, size_t incy, rb_complex64* a, size_t lda, void* stream,
+                       rb_error* err);
+rb_status rb_cgerc_dev(rb_layout layout, size_t m, size_t n, rb_complex32 alpha, const rb_complex32* x,
+                       size_t incx, const rb_complex32* y, size_t incy, rb_complex32* a, size_t lda, void* stream,
+                       rb_error* err);
+rb_status rb_zgerc_dev(rb_layout layout, size_t m, size_t n, rb_complex64 alpha, const rb_complex64* x,
+                       size_t incx, const rb_complex64* y, size_t incy, rb_complex64* a, size_t lda, void* stream,
+                       rb_error* err);
+
 /* Batched trsm on device pointers (no counterpart in the reference, which
  * solves one problem per call: trsm, src/level3.rs:390-520). Problem i solves
  * with A_i = a + i*stride_a and B_i = b + i*stride_b (elements), all sharing

@@ -80,6 +80,14 @@ def _declare(L):
     L.or_lcg_fill_f32.argtypes = [C.c_uint64, _i, _sz, _pf]
     L.or_lcg_fill_f32.restype = C.c_uint64
     L.or_set_force_scalar.argtypes = [_i]
+    L.or_sgemv.argtypes = [_i, _i, _sz, _sz, _f, _pf, _sz, _pf, _sz, _f, _pf, _sz]
+    L.or_dgemv.argtypes = [_i, _i, _sz, _sz, _d, _pd, _sz, _pd, _sz, _d, _pd, _sz]
+    L.or_sger.argtypes = [_i, _sz, _sz, _f, _pf, _sz, _pf, _sz, _pf, _sz]
+    L.or_dger.argtypes = [_i, _sz, _sz, _d, _pd, _sz, _pd, _sz, _pd, _sz]
+    L.or_cgemv.argtypes = [_i, _i, _sz, _sz, _f, _f, _pf, _sz, _pf, _sz, _f, _f, _pf, _sz]
+    L.or_zgemv.argtypes = [_i, _i, _sz, _sz, _d, _d, _pd, _sz, _pd, _sz, _d, _d, _pd, _sz]
+    L.or_cger.argtypes = [_i, _sz, _sz, _f, _f, _pf, _sz, _pf, _sz, _pf, _sz, _i]
+    L.or_zger.argtypes = [_i, _sz, _sz, _d, _d, _pd, _sz, _pd, _sz, _pd, _sz, _i]
     L.or_have_avx2_fma.restype = _i
 
 
@@ -174,6 +182,41 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     else:
         lib().or_ztrsm(side, uplo, trans, diag, m, n, float(np.real(alpha)), float(np.imag(alpha)),
                        _ptr(a, C.c_double), lda, _ptr(b, C.c_double), ldb)
+
+
+def gemv(layout, trans, m, n, alpha, a, lda, x, incx, beta, y, incy):
+    """level2::gemv / complex2::gemv (src/level2.rs:11-62, src/complex2.rs:11-77), y in place."""
+    if y.dtype == np.float32:
+        lib().or_sgemv(layout, trans, m, n, float(alpha), _ptr(a, C.c_float), lda, _ptr(x, C.c_float), incx,
+                       float(beta), _ptr(y, C.c_float), incy)
+    elif y.dtype == np.float64:
+        lib().or_dgemv(layout, trans, m, n, float(alpha), _ptr(a, C.c_double), lda, _ptr(x, C.c_double), incx,
+                       float(beta), _ptr(y, C.c_double), incy)
+    elif y.dtype == np.complex64:
+        lib().or_cgemv(layout, trans, m, n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(a, C.c_float), lda,
+                       _ptr(x, C.c_float), incx, float(np.real(beta)), float(np.imag(beta)), _ptr(y, C.c_float),
+                       incy)
+    else:
+        lib().or_zgemv(layout, trans, m, n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(a, C.c_double),
+                       lda, _ptr(x, C.c_double), incx, float(np.real(beta)), float(np.imag(beta)),
+                       _ptr(y, C.c_double), incy)
+
+
+def ger(layout, m, n, alpha, x, incx, y, incy, a, lda, conj=False):
+    """level2::ger (src/level2.rs:65-88); complex: complex2::geru / gerc
+    (src/complex2.rs:80-145, conj=True conjugates y). A in place."""
+    if a.dtype == np.float32:
+        lib().or_sger(layout, m, n, float(alpha), _ptr(x, C.c_float), incx, _ptr(y, C.c_float), incy,
+                      _ptr(a, C.c_float), lda)
+    elif a.dtype == np.float64:
+        lib().or_dger(layout, m, n, float(alpha), _ptr(x, C.c_double), incx, _ptr(y, C.c_double), incy,
+                      _ptr(a, C.c_double), lda)
+    elif a.dtype == np.complex64:
+        lib().or_cger(layout, m, n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(x, C.c_float), incx,
+                      _ptr(y, C.c_float), incy, _ptr(a, C.c_float), lda, int(conj))
+    else:
+        lib().or_zger(layout, m, n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(x, C.c_double), incx,
+                      _ptr(y, C.c_double), incy, _ptr(a, C.c_double), lda, int(conj))
 
 
 def set_force_scalar(on: bool):

@@ -681,6 +681,121 @@ void dd_gemm_any(int layout, int transa, int transb, size_t m, size_t n, size_t 
 
 }  // namespace
 
+// ---- Level 2 (src/level2.rs, src/complex2.rs) -------------------------------
+// (rs, cs) = layout.strides(lda): RowMajor (lda, 1), ColMajor (1, lda)  src/types.rs:20-25
+
+// src/level2.rs:91-104 (scale_y), 11-62 (gemv)
+template <typename T>
+void gemv_impl(int layout, int trans, size_t m, size_t n, T alpha, const T* a, size_t lda, const T* x,
+               size_t incx, T beta, T* y, size_t incy) {
+    const size_t rs = layout == 0 ? lda : 1, cs = layout == 0 ? 1 : lda;
+    const bool tr = trans != 0;
+    const size_t leny = tr ? n : m;
+    if (beta != T(1)) {
+        size_t iy = 0;
+        for (size_t q = 0; q < leny; ++q) {
+            y[iy] = (beta == T(0)) ? T(0) : beta * y[iy];
+            iy += incy;
+        }
+    }
+    if (alpha == T(0)) return;
+    if (!tr) {
+        for (size_t i = 0; i < m; ++i) {
+            T acc = T(0);
+            size_t jx = 0;
+            for (size_t j = 0; j < n; ++j) {
+                acc = fmaT(a[i * rs + j * cs], x[jx], acc);
+                jx += incx;
+            }
+            y[i * incy] = fmaT(alpha, acc, y[i * incy]);
+        }
+    } else {
+        for (size_t i = 0; i < m; ++i) {
+            const T xi = alpha * x[i * incx];
+            for (size_t j = 0; j < n; ++j) {
+                const size_t yj = j * incy;
+                y[yj] = fmaT(a[i * rs + j * cs], xi, y[yj]);
+            }
+        }
+    }
+}
+
+// src/level2.rs:65-88
+template <typename T>
+void ger_impl(int layout, size_t m, size_t n, T alpha, const T* x, size_t incx, const T* y, size_t incy, T* a,
+              size_t lda) {
+    if (alpha == T(0)) return;
+    const size_t rs = layout == 0 ? lda : 1, cs = layout == 0 ? 1 : lda;
+    for (size_t i = 0; i < m; ++i) {
+        const T axi = alpha * x[i * incx];
+        for (size_t j = 0; j < n; ++j) {
+            const size_t idx = i * rs + j * cs;
+            a[idx] = fmaT(axi, y[j * incy], a[idx]);
+        }
+    }
+}
+
+// src/complex2.rs:11-77. The beta pass runs whenever beta is zero or not one,
+// which is always ("!is_zero || != one"): beta == 1 still multiplies.
+template <typename T>
+void cgemv_impl(int layout, int trans, size_t m, size_t n, Cx<T> alpha, const Cx<T>* a, size_t lda, const Cx<T>* x,
+                size_t incx, Cx<T> beta, Cx<T>* y, size_t incy) {
+    const size_t rs = layout == 0 ? lda : 1, cs = layout == 0 ? 1 : lda;
+    const bool conj = trans == 2, tr = trans != 0;
+    const size_t leny = tr ? n : m;
+    const bool beta_zero = beta.re == T(0) && beta.im == T(0);
+    const bool beta_one = beta.re == T(1) && beta.im == T(0);
+    if (!beta_zero || !beta_one) {
+        size_t iy = 0;
+        for (size_t q = 0; q < leny; ++q) {
+            y[iy] = beta_zero ? Cx<T>{T(0), T(0)} : cmul(beta, y[iy]);
+            iy += incy;
+        }
+    }
+    if (alpha.re == T(0) && alpha.im == T(0)) return;
+    auto aval = [&](size_t i, size_t j) {
+        const Cx<T> v = a[i * rs + j * cs];
+        return conj ? cconj(v) : v;
+    };
+    if (!tr) {
+        for (size_t i = 0; i < m; ++i) {
+            Cx<T> acc{T(0), T(0)};
+            size_t jx = 0;
+            for (size_t j = 0; j < n; ++j) {
+                acc = cadd(acc, cmul(aval(i, j), x[jx]));
+                jx += incx;
+            }
+            y[i * incy] = cadd(y[i * incy], cmul(alpha, acc));
+        }
+    } else {
+        for (size_t j = 0; j < n; ++j) {
+            Cx<T> acc{T(0), T(0)};
+            size_t ix = 0;
+            for (size_t i = 0; i < m; ++i) {
+                acc = cadd(acc, cmul(aval(i, j), x[ix]));
+                ix += incx;
+            }
+            y[j * incy] = cadd(y[j * incy], cmul(alpha, acc));
+        }
+    }
+}
+
+// src/complex2.rs:80-145 (geru conj = false, gerc conj = true)
+template <typename T>
+void crank1_impl(int layout, size_t m, size_t n, Cx<T> alpha, const Cx<T>* x, size_t incx, const Cx<T>* y,
+                 size_t incy, Cx<T>* a, size_t lda, bool conj) {
+    if (alpha.re == T(0) && alpha.im == T(0)) return;
+    const size_t rs = layout == 0 ? lda : 1, cs = layout == 0 ? 1 : lda;
+    for (size_t i = 0; i < m; ++i) {
+        const Cx<T> axi = cmul(alpha, x[i * incx]);
+        for (size_t j = 0; j < n; ++j) {
+            const Cx<T> yj = conj ? cconj(y[j * incy]) : y[j * incy];
+            const size_t idx = i * rs + j * cs;
+            a[idx] = cadd(a[idx], cmul(axi, yj));
+        }
+    }
+}
+
 // ============================================================================
 // extern "C" surface used by the test harness (ctypes). Integer enums follow
 // the product header: layout 0=RowMajor 1=ColMajor; trans 0=None 1=Trans
@@ -846,6 +961,45 @@ void or_dd_dgemm(int layout, int transa, int transb, size_t m, size_t n, size_t 
 void or_dd_core(size_t nrows, size_t n, size_t k, double alpha, const double* am, const double* bm,
                 double beta, const double* c0, double* hi, double* lo, int threads) {
     dd_gemm_core(nrows, n, k, alpha, am, bm, beta, c0, hi, lo, threads);
+}
+
+void or_sgemv(int layout, int trans, size_t m, size_t n, float alpha, const float* a, size_t lda,
+              const float* x, size_t incx, float beta, float* y, size_t incy) {
+    gemv_impl<float>(layout, trans, m, n, alpha, a, lda, x, incx, beta, y, incy);
+}
+void or_dgemv(int layout, int trans, size_t m, size_t n, double alpha, const double* a, size_t lda,
+              const double* x, size_t incx, double beta, double* y, size_t incy) {
+    gemv_impl<double>(layout, trans, m, n, alpha, a, lda, x, incx, beta, y, incy);
+}
+void or_sger(int layout, size_t m, size_t n, float alpha, const float* x, size_t incx, const float* y, size_t incy,
+             float* a, size_t lda) {
+    ger_impl<float>(layout, m, n, alpha, x, incx, y, incy, a, lda);
+}
+void or_dger(int layout, size_t m, size_t n, double alpha, const double* x, size_t incx, const double* y,
+             size_t incy, double* a, size_t lda) {
+    ger_impl<double>(layout, m, n, alpha, x, incx, y, incy, a, lda);
+}
+void or_cgemv(int layout, int trans, size_t m, size_t n, float ar, float ai, const float* a, size_t lda,
+              const float* x, size_t incx, float br, float bi, float* y, size_t incy) {
+    cgemv_impl<float>(layout, trans, m, n, {ar, ai}, reinterpret_cast<const Cx<float>*>(a), lda,
+                      reinterpret_cast<const Cx<float>*>(x), incx, {br, bi}, reinterpret_cast<Cx<float>*>(y), incy);
+}
+void or_zgemv(int layout, int trans, size_t m, size_t n, double ar, double ai, const double* a, size_t lda,
+              const double* x, size_t incx, double br, double bi, double* y, size_t incy) {
+    cgemv_impl<double>(layout, trans, m, n, {ar, ai}, reinterpret_cast<const Cx<double>*>(a), lda,
+                       reinterpret_cast<const Cx<double>*>(x), incx, {br, bi}, reinterpret_cast<Cx<double>*>(y),
+                       incy);
+}
+void or_cger(int layout, size_t m, size_t n, float ar, float ai, const float* x, size_t incx, const float* y,
+             size_t incy, float* a, size_t lda, int conj) {
+    crank1_impl<float>(layout, m, n, {ar, ai}, reinterpret_cast<const Cx<float>*>(x), incx,
+                       reinterpret_cast<const Cx<float>*>(y), incy, reinterpret_cast<Cx<float>*>(a), lda, conj != 0);
+}
+void or_zger(int layout, size_t m, size_t n, double ar, double ai, const double* x, size_t incx, const double* y,
+             size_t incy, double* a, size_t lda, int conj) {
+    crank1_impl<double>(layout, m, n, {ar, ai}, reinterpret_cast<const Cx<double>*>(x), incx,
+                        reinterpret_cast<const Cx<double>*>(y), incy, reinterpret_cast<Cx<double>*>(a), lda,
+                        conj != 0);
 }
 
 }  // extern "C"

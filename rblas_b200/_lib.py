@@ -71,6 +71,26 @@ SIGNATURES = {
     "rb_dtrsm": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ctrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_sgemv": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _f, _vp, _sz, _sz, _perr]),
+    "rb_sgemv_dev": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz, _vp, _perr]),
+    "rb_dgemv": (_i, [_i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _perr]),
+    "rb_dgemv_dev": (_i, [_i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz, _vp, _perr]),
+    "rb_cgemv": (_i, [_i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex32, _vp, _sz, _sz, _perr]),
+    "rb_cgemv_dev": (_i, [_i, _i, _sz, _sz, RbComplex32, _vp, _sz, _vp, _sz, RbComplex32, _vp, _sz, _vp, _perr]),
+    "rb_zgemv": (_i, [_i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, RbComplex64, _vp, _sz, _sz, _perr]),
+    "rb_zgemv_dev": (_i, [_i, _i, _sz, _sz, RbComplex64, _vp, _sz, _vp, _sz, RbComplex64, _vp, _sz, _vp, _perr]),
+    "rb_sger": (_i, [_i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_sger_dev": (_i, [_i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_dger": (_i, [_i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_dger_dev": (_i, [_i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_cgeru": (_i, [_i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_cgeru_dev": (_i, [_i, _sz, _sz, RbComplex32, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_zgeru": (_i, [_i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_zgeru_dev": (_i, [_i, _sz, _sz, RbComplex64, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_cgerc": (_i, [_i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_cgerc_dev": (_i, [_i, _sz, _sz, RbComplex32, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
+    "rb_zgerc": (_i, [_i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_zgerc_dev": (_i, [_i, _sz, _sz, RbComplex64, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _perr]),
     "rb_dtrsm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
     "rb_strsm_batched_dev": (_i, [_i, _i, _i, _i, _sz, _sz, C.c_float, _vp, _sz, _sz, _vp, _sz, _sz, _sz, _vp,
                                   _perr]),

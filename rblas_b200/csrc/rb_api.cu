@@ -871,6 +871,76 @@ rb_status dev_status(int rc, int32_t ce, rb_error* err) {
     return static_cast<rb_status>(rc);
 }
 
+
+// ---- Level 2 host slices (src/level2.rs, src/complex2.rs) --------------------
+
+// A strided vector of len elements must reach element (len-1)*inc.
+rb_status check_vector(char which, size_t len, size_t inc, size_t buf_len, rb_error* err) {
+    if (len == 0) return RB_OK;
+    const size_t need = (len - 1) * inc + 1;
+    if (buf_len < need) {
+        set_err(err, RB_ERR_BUFFER_TOO_SMALL, which, buf_len, need);
+        return RB_ERR_BUFFER_TOO_SMALL;
+    }
+    return RB_OK;
+}
+
+// A vector staged as a 1 x len block with pitch inc (inc 0: one element).
+HostMat vec_mat(const void* src, void* dst, size_t len, size_t inc, size_t elem, bool in, bool out) {
+    return HostMat{src, dst, 1, inc == 0 ? (len ? 1 : 0) : len, inc == 0 ? 1 : inc, elem, in, out};
+}
+
+template <typename T, bool CX>
+rb_status gemv_host(rb_layout layout, rb_transpose trans, size_t m, size_t n, T ar, T ai, const T* a, size_t lda,
+                    size_t a_len, const T* x, size_t incx, size_t x_len, T br, T bi, T* y, size_t incy, size_t y_len,
+                    rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_layout(layout) || !valid_trans(trans)) return invalid(err);
+    const bool tr = trans != RB_NO_TRANS;
+    const size_t lenx = tr ? m : n, leny = tr ? n : m;
+    rb_status s;
+    if ((s = check_matrix(layout, 'a', m, n, lda, a_len, true, err)) != RB_OK) return s;
+    if ((s = check_vector('x', lenx, incx, x_len, err)) != RB_OK) return s;
+    if ((s = check_vector('y', leny, incy, y_len, err)) != RB_OK) return s;
+    if (incy == 0 && leny > 1) {  // every output on one element: no parallel form
+        set_err(err, RB_ERR_ZERO_STRIDE, 'y', 0, 0);
+        return RB_ERR_ZERO_STRIDE;
+    }
+    if (leny == 0) return RB_OK;
+    const size_t el = sizeof(T) * (CX ? 2 : 1);
+    const bool col = layout == RB_COL_MAJOR;
+    HostMat mats[3] = {{a, nullptr, col ? m : n, col ? n : m, lda, el, m > 0 && n > 0, false},
+                       vec_mat(x, nullptr, lenx, incx, el, lenx > 0, false),
+                       vec_mat(y, y, leny, incy, el, true, true)};
+    return host_run(mats, 3, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return gemv_dev<T, CX>(layout, trans, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
+                               static_cast<const T*>(d[1]), incx == 0 ? 0 : static_cast<long long>(ld[1]), br, bi,
+                               static_cast<T*>(d[2]), static_cast<long long>(ld[2]), st, ce);
+    });
+}
+
+template <typename T, bool CX>
+rb_status ger_host(rb_layout layout, size_t m, size_t n, T ar, T ai, const T* x, size_t incx, size_t x_len,
+                   const T* y, size_t incy, size_t y_len, T* a, size_t lda, size_t a_len, int conj, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_layout(layout)) return invalid(err);
+    rb_status s;
+    if ((s = check_vector('x', m, incx, x_len, err)) != RB_OK) return s;
+    if ((s = check_vector('y', n, incy, y_len, err)) != RB_OK) return s;
+    if ((s = check_matrix(layout, 'a', m, n, lda, a_len, true, err)) != RB_OK) return s;
+    if (m == 0 || n == 0 || (ar == T(0) && (!CX || ai == T(0)))) return RB_OK;  // nothing is written
+    const size_t el = sizeof(T) * (CX ? 2 : 1);
+    const bool col = layout == RB_COL_MAJOR;
+    HostMat mats[3] = {vec_mat(x, nullptr, m, incx, el, true, false), vec_mat(y, nullptr, n, incy, el, true, false),
+                       {a, a, col ? m : n, col ? n : m, lda, el, true, true}};
+    return host_run(mats, 3, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return ger_dev<T, CX>(layout, m, n, ar, ai, static_cast<const T*>(d[0]),
+                              incx == 0 ? 0 : static_cast<long long>(ld[0]), static_cast<const T*>(d[1]),
+                              incy == 0 ? 0 : static_cast<long long>(ld[1]), static_cast<T*>(d[2]), ld[2], conj, st,
+                              ce);
+    });
+}
+
 }  // namespace
 }  // namespace rb
 
@@ -1001,5 +1071,54 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                                            static_cast<cudaStream_t>(stream), &ce);
     return dev_status(rc, ce, err);
 }
+
+
+// ---- Level 2 (src/level2.rs:11-88, src/complex2.rs:11-145) ------------------
+rb_status rb_sgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, float alpha, const float* a, size_t lda,
+                   size_t a_len, const float* x, size_t incx, size_t x_len, float beta, float* y, size_t incy,
+                   size_t y_len, rb_error* err) {
+    return gemv_host<float, false>(layout, trans, m, n, alpha, 0.f, a, lda, a_len, x, incx, x_len, beta, 0.f, y, incy,
+                                   y_len, err);
+}
+rb_status rb_dgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, double alpha, const double* a,
+                   size_t lda, size_t a_len, const double* x, size_t incx, size_t x_len, double beta, double* y,
+                   size_t incy, size_t y_len, rb_error* err) {
+    return gemv_host<double, false>(layout, trans, m, n, alpha, 0.0, a, lda, a_len, x, incx, x_len, beta, 0.0, y,
+                                    incy, y_len, err);
+}
+rb_status rb_cgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex32 alpha,
+                   const rb_complex32* a, size_t lda, size_t a_len, const rb_complex32* x, size_t incx, size_t x_len,
+                   rb_complex32 beta, rb_complex32* y, size_t incy, size_t y_len, rb_error* err) {
+    return gemv_host<float, true>(layout, trans, m, n, alpha.re, alpha.im, reinterpret_cast<const float*>(a), lda,
+                                  a_len, reinterpret_cast<const float*>(x), incx, x_len, beta.re, beta.im,
+                                  reinterpret_cast<float*>(y), incy, y_len, err);
+}
+rb_status rb_zgemv(rb_layout layout, rb_transpose trans, size_t m, size_t n, rb_complex64 alpha,
+                   const rb_complex64* a, size_t lda, size_t a_len, const rb_complex64* x, size_t incx, size_t x_len,
+                   rb_complex64 beta, rb_complex64* y, size_t incy, size_t y_len, rb_error* err) {
+    return gemv_host<double, true>(layout, trans, m, n, alpha.re, alpha.im, reinterpret_cast<const double*>(a), lda,
+                                   a_len, reinterpret_cast<const double*>(x), incx, x_len, beta.re, beta.im,
+                                   reinterpret_cast<double*>(y), incy, y_len, err);
+}
+rb_status rb_sger(rb_layout layout, size_t m, size_t n, float alpha, const float* x, size_t incx, size_t x_len,
+                  const float* y, size_t incy, size_t y_len, float* a, size_t lda, size_t a_len, rb_error* err) {
+    return ger_host<float, false>(layout, m, n, alpha, 0.f, x, incx, x_len, y, incy, y_len, a, lda, a_len, 0, err);
+}
+rb_status rb_dger(rb_layout layout, size_t m, size_t n, double alpha, const double* x, size_t incx, size_t x_len,
+                  const double* y, size_t incy, size_t y_len, double* a, size_t lda, size_t a_len, rb_error* err) {
+    return ger_host<double, false>(layout, m, n, alpha, 0.0, x, incx, x_len, y, incy, y_len, a, lda, a_len, 0, err);
+}
+#define RB_CGER(NAME, T, CT, CONJ)                                                                                  \
+    rb_status NAME(rb_layout layout, size_t m, size_t n, CT alpha, const CT* x, size_t incx, size_t x_len,          \
+                   const CT* y, size_t incy, size_t y_len, CT* a, size_t lda, size_t a_len, rb_error* err) {       \
+        return ger_host<T, true>(layout, m, n, alpha.re, alpha.im, reinterpret_cast<const T*>(x), incx, x_len,      \
+                                 reinterpret_cast<const T*>(y), incy, y_len, reinterpret_cast<T*>(a), lda, a_len,   \
+                                 CONJ, err);                                                                        \
+    }
+RB_CGER(rb_cgeru, float, rb_complex32, 0)
+RB_CGER(rb_zgeru, double, rb_complex64, 0)
+RB_CGER(rb_cgerc, float, rb_complex32, 1)
+RB_CGER(rb_zgerc, double, rb_complex64, 1)
+#undef RB_CGER
 
 }  // extern "C"

@@ -168,6 +168,16 @@ int validate_problem(const rb_gemm_problem& q);
 int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
                      cudaStream_t st, int32_t* ce, size_t* bad_index, const GroupStaging* staging = nullptr);
 
+// Level 2 on device pointers (rb_?gemv_dev, rb_?ger*_dev): complex arrays
+// are interleaved {re, im}; alpha/beta given as (re, im) (im ignored for
+// real). conj (rank-1 update) conjugates y. incx/incy in elements.
+template <typename T, bool CX>
+int gemv_dev(int layout, int trans, size_t m, size_t n, T ar, T ai, const T* A, size_t lda, const T* x,
+             long long incx, T br, T bi, T* y, long long incy, cudaStream_t st, int32_t* ce);
+template <typename T, bool CX>
+int ger_dev(int layout, size_t m, size_t n, T ar, T ai, const T* x, long long incx, const T* y, long long incy, T* A,
+            size_t lda, int conj, cudaStream_t st, int32_t* ce);
+
 // Batched triangular solve over uniformly strided A_i / B_i (rb_?trsm_batched_dev).
 template <typename T>
 int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T alpha, const T* A, size_t lda,
