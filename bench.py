@@ -53,6 +53,16 @@ def step_flops():
     return sum(2.0 * m * n * k for _, _, m, n, k in step_gemms())
 
 
+def measured_peaks():
+    """The pool's measured peaks (MEASURED_PEAKS.json beside this file), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -461,6 +471,29 @@ def run_ours(args):
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in kr4.items()}}
         del At, Bt
         torch.cuda.empty_cache()
+        # Level 2 (HBM-bound): dgemv 16384^2 col-major N and T (m*n*8 bytes of
+        # A per call), dger 16384^2 (A read and written: 2*m*n*8 bytes)
+        from rblas_b200 import level2
+        n2l = 16384
+        AL = torch.randn(n2l * n2l, dtype=torch.float64, device=dev, generator=g2)
+        xl = torch.randn(n2l, dtype=torch.float64, device=dev, generator=g2)
+        yl = torch.randn(n2l, dtype=torch.float64, device=dev, generator=g2)
+        hbm = (measured_peaks() or {}).get("hbm_gbs")
+        lv2 = {"hbm_peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm else None}
+        for name, fn, nbytes in (
+                ("dgemv_N", lambda: level2.gemv_dev(1, 0, n2l, n2l, 1.0, AL.data_ptr(), n2l, xl.data_ptr(), 1, 0.5,
+                                                    yl.data_ptr(), 1, np.float64, stream=sh), 8.0 * n2l * n2l),
+                ("dgemv_T", lambda: level2.gemv_dev(1, 1, n2l, n2l, 1.0, AL.data_ptr(), n2l, xl.data_ptr(), 1, 0.5,
+                                                    yl.data_ptr(), 1, np.float64, stream=sh), 8.0 * n2l * n2l),
+                ("dger", lambda: level2.ger_dev(1, n2l, n2l, 1e-3, xl.data_ptr(), 1, yl.data_ptr(), 1, AL.data_ptr(),
+                                                n2l, np.float64, stream=sh), 16.0 * n2l * n2l)):
+            ms, launches, _ = timed(fn, 10, 2)
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            lv2[name] = {"ms": ms, "gb_s": gbs, "frac_of_hbm": gbs / hbm if hbm else None,
+                         "launches_per_call": launches / 10}
+        others["level2_16384"] = lv2
+        del AL, xl, yl
+        torch.cuda.empty_cache()
 
     # ---- e2e through the public host API (pinned host buffers) -------------
     e2e = None
@@ -686,6 +719,41 @@ def run_kernel_only(args):
                       "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}))
 
 
+def run_level2_only(args):
+    """dgemv (N and T) and dger on an n x n column-major f64 matrix, each
+    launched warmup + steps times (for ncu captures on a bounded case)."""
+    import torch
+
+    from rblas_b200 import level2
+
+    n = args.level2
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    A = torch.randn(n * n, dtype=torch.float64, device="cuda", generator=g)
+    x = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    sh = torch.cuda.current_stream().cuda_stream
+    out = {"level2": n}
+    for name, fn, nbytes in (
+            ("dgemv_N", lambda: level2.gemv_dev(1, 0, n, n, 1.0, A.data_ptr(), n, x.data_ptr(), 1, 0.5, y.data_ptr(),
+                                                1, np.float64, stream=sh), 8.0 * n * n),
+            ("dgemv_T", lambda: level2.gemv_dev(1, 1, n, n, 1.0, A.data_ptr(), n, x.data_ptr(), 1, 0.5, y.data_ptr(),
+                                                1, np.float64, stream=sh), 8.0 * n * n),
+            ("dger", lambda: level2.ger_dev(1, n, n, 1e-3, x.data_ptr(), 1, y.data_ptr(), 1, A.data_ptr(), n,
+                                            np.float64, stream=sh), 16.0 * n * n)):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for i in range(args.warmup + args.steps):
+            if i == args.warmup:
+                e0.record()
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(args.steps, 1)
+        out[name] = {"ms": ms, "gb_s": nbytes / (ms * 1e-3) / 1e9}
+    print(json.dumps(out))
+
+
 def run_grouped_only(args):
     """The first `--grouped-batch N` requests of the serving stream as one
     grouped launch (device-resident operands), launched warmup + steps times
@@ -775,6 +843,8 @@ def main():
     ap.add_argument("--kernel-only", dest="shape", type=int, nargs=3, default=None,
                     metavar=("M", "N", "K"), help="time one column-major GEMM shape only")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
+    ap.add_argument("--level2", type=int, default=0, metavar="N",
+                    help="time dgemv (N, T) and dger on an N x N f64 matrix only")
     ap.add_argument("--grouped-batch", type=int, default=0, metavar="N",
                     help="time one grouped launch of the first N serving requests only")
     ap.add_argument("--trsm-batched", type=int, default=0, metavar="BATCH",
@@ -795,6 +865,8 @@ def main():
         run_trsm_batched_only(args)
     elif args.grouped_batch:
         run_grouped_only(args)
+    elif args.level2:
+        run_level2_only(args)
     elif args.serve:
         run_serve_mode(args)
     elif args.shape:

@@ -92,24 +92,43 @@ __device__ __forceinline__ C2<T> shfl_el(C2<T> v, int o) {
 
 constexpr int kL2Threads = 256;
 
-// y_r partial over columns [c0, c1) of range s: ws[s * R + r]
+// y_r partial over columns [c0, c1) of range s: ws[s * R + r]. A CTA covers
+// kSweepRows consecutive rows (each thread kRowsPerThread of them, 256 apart,
+// so every warp load stays one contiguous 256-byte run and the CTA reads
+// 8 KB contiguous per f64 column); the accumulators are independent.
+constexpr int kRowsPerThread = 4;
+constexpr int kSweepRows = kL2Threads * kRowsPerThread;
+
 template <typename E>
 __global__ void __launch_bounds__(kL2Threads)
     gemv_sweep_kernel(const E* __restrict__ A, size_t ld, int R, int C, const E* __restrict__ x, long long incx,
                       int conj, int cchunk, E* __restrict__ ws) {
-    const int r = blockIdx.x * kL2Threads + threadIdx.x;
-    if (r >= R) return;
+    const int rbase = blockIdx.x * kSweepRows + threadIdx.x;
     const int s = blockIdx.y;
     const int c0 = s * cchunk, c1 = min(C, c0 + cchunk);
-    E acc = zero_el(static_cast<E*>(nullptr));
-    const E* a = A + r;
-#pragma unroll 8
-    for (int c = c0; c < c1; ++c) {
-        E v = ld_el(a + static_cast<size_t>(c) * ld);
-        if (conj) v = conj_el(v);
-        acc = mac(acc, v, ld_el(x + static_cast<long long>(c) * incx));
+    E acc[kRowsPerThread];
+    bool live[kRowsPerThread];
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        acc[q] = zero_el(static_cast<E*>(nullptr));
+        live[q] = rbase + q * kL2Threads < R;
     }
-    ws[static_cast<size_t>(s) * R + r] = acc;
+#pragma unroll 4
+    for (int c = c0; c < c1; ++c) {
+        const E xc = ld_el(x + static_cast<long long>(c) * incx);
+        const E* col = A + static_cast<size_t>(c) * ld + rbase;
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) {
+            if (live[q]) {
+                E v = ld_el(col + q * kL2Threads);
+                if (conj) v = conj_el(v);
+                acc[q] = mac(acc[q], v, xc);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q)
+        if (live[q]) ws[static_cast<size_t>(s) * R + rbase + q * kL2Threads] = acc[q];
 }
 
 // y_c partial over rows [r0, r1) of range s: ws[s * C + c]
@@ -191,17 +210,24 @@ __global__ void gemv_finalize_cplx(C2<T>* y, long long incy, int len, const C2<T
 
 // A[r, c] (column-major view) += alpha*x (.) y: the x index is the view's
 // row when x_on_rows, else its column; y likewise on the other index.
+// A CTA covers kSweepRows consecutive rows of a range of columns (each
+// thread kRowsPerThread rows, 256 apart), the columns strided by gridDim.y.
 template <typename T>
 __global__ void __launch_bounds__(kL2Threads)
     ger_real_kernel(T* A, size_t ld, int R, int C, const T* __restrict__ x, long long incx, const T* __restrict__ y,
                     long long incy, T alpha, int x_on_rows) {
-    const int r = blockIdx.x * kL2Threads + threadIdx.x;
-    if (r >= R) return;
+    const int rbase = blockIdx.x * kSweepRows + threadIdx.x;
     for (int c = blockIdx.y; c < C; c += gridDim.y) {
-        const int xi = x_on_rows ? r : c, yj = x_on_rows ? c : r;
-        const T axi = mul_rn(alpha, __ldg(x + static_cast<long long>(xi) * incx));  // src/level2.rs:83
-        T* p = A + r + static_cast<size_t>(c) * ld;
-        *p = fma(axi, __ldg(y + static_cast<long long>(yj) * incy), *p);          // src/level2.rs:86
+        T* col = A + static_cast<size_t>(c) * ld;
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) {
+            const int r = rbase + q * kL2Threads;
+            if (r < R) {
+                const int xi = x_on_rows ? r : c, yj = x_on_rows ? c : r;
+                const T axi = mul_rn(alpha, __ldg(x + static_cast<long long>(xi) * incx));  // src/level2.rs:83
+                col[r] = fma(axi, __ldg(y + static_cast<long long>(yj) * incy), col[r]);     // src/level2.rs:86
+            }
+        }
     }
 }
 
@@ -209,15 +235,20 @@ template <typename T>
 __global__ void __launch_bounds__(kL2Threads)
     ger_cplx_kernel(C2<T>* A, size_t ld, int R, int C, const C2<T>* __restrict__ x, long long incx,
                     const C2<T>* __restrict__ y, long long incy, C2<T> alpha, int x_on_rows, int conj) {
-    const int r = blockIdx.x * kL2Threads + threadIdx.x;
-    if (r >= R) return;
+    const int rbase = blockIdx.x * kSweepRows + threadIdx.x;
     for (int c = blockIdx.y; c < C; c += gridDim.y) {
-        const int xi = x_on_rows ? r : c, yj = x_on_rows ? c : r;
-        const C2<T> axi = cmul(alpha, ld_el(x + static_cast<long long>(xi) * incx));  // src/complex2.rs:135
-        C2<T> yv = ld_el(y + static_cast<long long>(yj) * incy);
-        if (conj) yv = cconj(yv);                                                      // src/complex2.rs:137-141
-        C2<T>* p = A + r + static_cast<size_t>(c) * ld;
-        *p = cadd(*p, cmul(axi, yv));                                                  // src/complex2.rs:143
+        C2<T>* col = A + static_cast<size_t>(c) * ld;
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) {
+            const int r = rbase + q * kL2Threads;
+            if (r < R) {
+                const int xi = x_on_rows ? r : c, yj = x_on_rows ? c : r;
+                const C2<T> axi = cmul(alpha, ld_el(x + static_cast<long long>(xi) * incx));  // src/complex2.rs:135
+                C2<T> yv = ld_el(y + static_cast<long long>(yj) * incy);
+                if (conj) yv = cconj(yv);                                              // src/complex2.rs:137-141
+                col[r] = cadd(col[r], cmul(axi, yv));                                  // src/complex2.rs:143
+            }
+        }
     }
 }
 
@@ -250,7 +281,7 @@ int gemv_dev(int layout, int trans, size_t m, size_t n, T ar, T ai, const T* A, 
     bool have_work = !alpha_zero && R > 0 && Cc > 0;
     if (have_work) {
         if (sweep) {
-            const int rb = blocks_for(R);
+            const int rb = (R + kSweepRows - 1) / kSweepRows;
             S = std::max(1, std::min((target + rb - 1) / rb, std::max(1, Cc / 16)));
             chunk = (Cc + S - 1) / S;
             S = (Cc + chunk - 1) / chunk;
@@ -267,8 +298,8 @@ int gemv_dev(int layout, int trans, size_t m, size_t n, T ar, T ai, const T* A, 
         const E* Av = reinterpret_cast<const E*>(A);
         const E* xv = reinterpret_cast<const E*>(x);
         if (sweep)
-            gemv_sweep_kernel<E><<<dim3(blocks_for(R), S), kL2Threads, 0, st>>>(Av, lda, R, Cc, xv, incx, conj, chunk,
-                                                                                  ws);
+            gemv_sweep_kernel<E><<<dim3((R + kSweepRows - 1) / kSweepRows, S), kL2Threads, 0, st>>>(
+                Av, lda, R, Cc, xv, incx, conj, chunk, ws);
         else
             gemv_dot_kernel<E><<<dim3(Cc, S), kL2Threads, 0, st>>>(Av, lda, R, Cc, xv, incx, conj, chunk, ws);
         count_launch();
@@ -297,7 +328,9 @@ int ger_dev(int layout, size_t m, size_t n, T ar, T ai, const T* x, long long in
     if (m > 0x7fffffff || n > 0x7fffffff) return RB_ERR_INVALID_ARG;
     const bool col = layout == RB_COL_MAJOR;
     const int R = static_cast<int>(col ? m : n), Cc = static_cast<int>(col ? n : m);
-    const dim3 grid(blocks_for(R), std::min(Cc, 65535));
+    // about 8 CTAs per SM over the row blocks, each walking a slice of columns
+    const int rblocks = (R + kSweepRows - 1) / kSweepRows;
+    const dim3 grid(rblocks, std::max(1, std::min({Cc, 65535, (148 * 8 * 4 + rblocks - 1) / rblocks})));
     if constexpr (CX)
         ger_cplx_kernel<T><<<grid, kL2Threads, 0, st>>>(reinterpret_cast<C2<T>*>(A), lda, R, Cc,
                                                         reinterpret_cast<const C2<T>*>(x), incx,
