@@ -186,3 +186,43 @@ def test_config_sizes_error_report():
         with open(path, "w") as f:
             json.dump(report, f, indent=1)
     print(json.dumps(report, indent=1))
+
+
+@pytest.mark.parametrize("layout,ta,tb,m,n,k", [(Layout.ColMajor, 0, 0, 300, 257, 513),
+                                                 (Layout.RowMajor, 1, 1, 1000, 900, 700),
+                                                 (Layout.ColMajor, 1, 0, 64, 64, 4096)])
+def test_ozaki_unit_parallel_matches_fused_epilogue_exactly(layout, ta, tb, m, n, k):
+    """Problems with fewer tiles than SMs run one diagonal-pair unit per CTA
+    and fold the units' exact terms in unit order afterwards; that is the
+    fused epilogue's arithmetic, so the result equals the fused path's (run
+    here through the allocation-free entry point, which always fuses) bit
+    for bit -- including a zero row, a zero column and beta = 0 with NaN C."""
+    import ctypes as C
+    torch = pytest.importorskip("torch")
+    from rblas_b200 import _lib
+    g = torch.Generator(device="cuda")
+    g.manual_seed(m + n)
+    ar, ac = (k, m) if ta else (m, k)
+    br, bc = (n, k) if tb else (k, n)
+    lda = ar if layout == Layout.ColMajor else ac
+    ldb = br if layout == Layout.ColMajor else bc
+    ldc = m if layout == Layout.ColMajor else n
+    A = torch.randn(ar * ac, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(br * bc, dtype=torch.float64, device="cuda", generator=g)
+    # a zero row of op(A): row 3 of A (stored rows when NoTrans col-major)
+    if layout == Layout.ColMajor and not ta:
+        A.view(ac, ar)[:, 3] = 0.0
+    for beta, fill in ((-0.5, None), (0.0, float("nan"))):
+        C0 = torch.randn(m * n, dtype=torch.float64, device="cuda", generator=g)
+        if fill is not None:
+            C0.fill_(fill)
+        got, ref = C0.clone(), C0.clone()
+        level3.gemm_dev(layout, ta, tb, m, n, k, 1.25, A.data_ptr(), lda, B.data_ptr(), ldb, beta, got.data_ptr(),
+                        ldc, np.float64, prec=Precision.Ozaki)
+        err = _lib.RbError()
+        st = _lib.load().rb_dgemm_ozaki_noalloc(int(layout), ta, tb, m, n, k, 1.25, C.c_void_p(A.data_ptr()), lda,
+                                                C.c_void_p(B.data_ptr()), ldb, beta, C.c_void_p(ref.data_ptr()), ldc,
+                                                None, C.byref(err))
+        assert st == 0
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref) or torch.allclose(got, ref, rtol=0, atol=0, equal_nan=True)
