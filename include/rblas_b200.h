@@ -299,6 +299,28 @@ rb_status rb_zgerc_dev(rb_layout layout, size_t m, size_t n, rb_complex64 alpha,
                        size_t incx, const rb_complex64* y, size_t incy, rb_complex64* a, size_t lda, void* stream,
                        rb_error* err);
 
+/* Triangular multiply, B := alpha*op(A)*B (Left, A m x m) or alpha*B*op(A)
+ * (Right, A n x n); A triangular (uplo, diag), column-major like trsm.
+ * No counterpart in the reference: rblas lists trmm among its remaining
+ * Level-3 routines (README.md roadmap); the arguments follow its trsm
+ * (src/level3.rs:390-402) and standard BLAS trmm. op(A) is expanded to a
+ * full matrix and multiplied in one plain GEMM. */
+rb_status rb_strmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   float alpha, const float* a, size_t lda, size_t a_len, float* b, size_t ldb, size_t b_len,
+                   rb_error* err);
+rb_status rb_dtrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   double alpha, const double* a, size_t lda, size_t a_len, double* b, size_t ldb, size_t b_len,
+                   rb_error* err);
+rb_status rb_ctrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex32 alpha, const rb_complex32* a, size_t lda, size_t a_len, rb_complex32* b,
+                   size_t ldb, size_t b_len, rb_error* err);
+rb_status rb_ztrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex64 alpha, const rb_complex64* a, size_t lda, size_t a_len, rb_complex64* b,
+                   size_t ldb, size_t b_len, rb_error* err);
+rb_status rb_dtrmm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                       double alpha, const double* a, size_t lda, double* b, size_t ldb, void* stream,
+                       rb_error* err);
+
 /* Batched trsm on device pointers (no counterpart in the reference, which
  * solves one problem per call: trsm, src/level3.rs:390-520). Problem i solves
  * with A_i = a + i*stride_a and B_i = b + i*stride_b (elements), all sharing

@@ -80,6 +80,8 @@ def _declare(L):
     L.or_lcg_fill_f32.argtypes = [C.c_uint64, _i, _sz, _pf]
     L.or_lcg_fill_f32.restype = C.c_uint64
     L.or_set_force_scalar.argtypes = [_i]
+    L.or_strmm.argtypes = [_i, _i, _i, _i, _sz, _sz, _f, _pf, _sz, _pf, _sz]
+    L.or_dtrmm.argtypes = [_i, _i, _i, _i, _sz, _sz, _d, _pd, _sz, _pd, _sz]
     L.or_sgemv.argtypes = [_i, _i, _sz, _sz, _f, _pf, _sz, _pf, _sz, _f, _pf, _sz]
     L.or_dgemv.argtypes = [_i, _i, _sz, _sz, _d, _pd, _sz, _pd, _sz, _d, _pd, _sz]
     L.or_sger.argtypes = [_i, _sz, _sz, _f, _pf, _sz, _pf, _sz, _pf, _sz]
@@ -182,6 +184,15 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     else:
         lib().or_ztrsm(side, uplo, trans, diag, m, n, float(np.real(alpha)), float(np.imag(alpha)),
                        _ptr(a, C.c_double), lda, _ptr(b, C.c_double), ldb)
+
+
+def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    """The textbook trmm (rblas has none), B in place; real types."""
+    if b.dtype == np.float32:
+        lib().or_strmm(side, uplo, trans, diag, m, n, float(alpha), _ptr(a, C.c_float), lda, _ptr(b, C.c_float), ldb)
+    else:
+        lib().or_dtrmm(side, uplo, trans, diag, m, n, float(alpha), _ptr(a, C.c_double), lda, _ptr(b, C.c_double),
+                       ldb)
 
 
 def gemv(layout, trans, m, n, alpha, a, lda, x, incx, beta, y, incy):

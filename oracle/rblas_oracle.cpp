@@ -681,6 +681,34 @@ void dd_gemm_any(int layout, int transa, int transb, size_t m, size_t n, size_t 
 
 }  // namespace
 
+// ---- trmm (no rblas counterpart: the textbook definition) ---------------------
+// out = alpha * op(A) * B (Left) or alpha * B * op(A) (Right), op(A) the
+// triangle of A (unit diagonal when diag), each output accumulated in index
+// order with fma (real) or acc + a*b (complex); then B = out.
+template <typename T>
+inline T tri_at(const T* a, size_t lda, int uplo, int trans, int diag, size_t i, size_t j) {
+    const size_t r = trans ? j : i, c = trans ? i : j;
+    if (r == c && diag) return T(1);
+    const bool stored = uplo == 0 ? r <= c : r >= c;
+    return stored ? a[r + c * lda] : T(0);
+}
+template <typename T>
+void trmm_impl(int side, int uplo, int trans, int diag, size_t m, size_t n, T alpha, const T* a, size_t lda, T* b,
+               size_t ldb) {
+    std::vector<T> out(m * n);
+    for (size_t j = 0; j < n; ++j)
+        for (size_t i = 0; i < m; ++i) {
+            T acc = T(0);
+            if (side == 0)
+                for (size_t k = 0; k < m; ++k) acc = fmaT(tri_at(a, lda, uplo, trans, diag, i, k), b[k + j * ldb], acc);
+            else
+                for (size_t k = 0; k < n; ++k) acc = fmaT(b[i + k * ldb], tri_at(a, lda, uplo, trans, diag, k, j), acc);
+            out[i + j * m] = alpha * acc;
+        }
+    for (size_t j = 0; j < n; ++j)
+        for (size_t i = 0; i < m; ++i) b[i + j * ldb] = out[i + j * m];
+}
+
 // ---- Level 2 (src/level2.rs, src/complex2.rs) -------------------------------
 // (rs, cs) = layout.strides(lda): RowMajor (lda, 1), ColMajor (1, lda)  src/types.rs:20-25
 
@@ -1000,6 +1028,15 @@ void or_zger(int layout, size_t m, size_t n, double ar, double ai, const double*
     crank1_impl<double>(layout, m, n, {ar, ai}, reinterpret_cast<const Cx<double>*>(x), incx,
                         reinterpret_cast<const Cx<double>*>(y), incy, reinterpret_cast<Cx<double>*>(a), lda,
                         conj != 0);
+}
+
+void or_dtrmm(int side, int uplo, int trans, int diag, size_t m, size_t n, double alpha, const double* a,
+              size_t lda, double* b, size_t ldb) {
+    trmm_impl<double>(side, uplo, trans != 0, diag, m, n, alpha, a, lda, b, ldb);
+}
+void or_strmm(int side, int uplo, int trans, int diag, size_t m, size_t n, float alpha, const float* a, size_t lda,
+              float* b, size_t ldb) {
+    trmm_impl<float>(side, uplo, trans != 0, diag, m, n, alpha, a, lda, b, ldb);
 }
 
 }  // extern "C"

@@ -71,6 +71,11 @@ SIGNATURES = {
     "rb_dtrsm": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ctrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
     "rb_ztrsm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_strmm": (_i, [_i, _i, _i, _i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_dtrmm": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_ctrmm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex32, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_ztrmm": (_i, [_i, _i, _i, _i, _sz, _sz, RbComplex64, _vp, _sz, _sz, _vp, _sz, _sz, _perr]),
+    "rb_dtrmm_dev": (_i, [_i, _i, _i, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _perr]),
     "rb_sgemv": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _sz, _vp, _sz, _sz, _f, _vp, _sz, _sz, _perr]),
     "rb_sgemv_dev": (_i, [_i, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz, _vp, _perr]),
     "rb_dgemv": (_i, [_i, _i, _sz, _sz, _d, _vp, _sz, _sz, _vp, _sz, _sz, _d, _vp, _sz, _sz, _perr]),

@@ -12,7 +12,7 @@ from . import _lib
 from .level3 import _as_slice, _ptr
 from .types import Diag, Precision, Side, Transpose, Uplo
 
-__all__ = ["gemm", "gemm_dev", "symm", "hemm", "trsm"]
+__all__ = ["gemm", "gemm_dev", "symm", "hemm", "trsm", "trmm"]
 
 
 def _kind(c):
@@ -91,4 +91,17 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     st = getattr(lib, f"rb_{p}trsm")(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)),
                                       int(Diag(diag)), m, n, _cx(ct, alpha), _ptr(a), lda, a.size,
                                       _ptr(b), ldb, b.size, C.byref(err))
+    _lib.check(st, err)
+
+
+def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    """Complex triangular multiply in place of B (no rblas counterpart):
+    B := alpha*op(A)*B (Left) or alpha*B*op(A) (Right); ConjTrans conjugates A."""
+    dt, p, ct = _kind(b)
+    a = _as_slice(a, dt, "a")
+    b = _as_slice(b, dt, "b", writable=True)
+    err = _lib.RbError()
+    st = getattr(_lib.load(), f"rb_{p}trmm")(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)),
+                                             int(Diag(diag)), m, n, _cx(ct, alpha), _ptr(a), lda, a.size, _ptr(b),
+                                             ldb, b.size, C.byref(err))
     _lib.check(st, err)

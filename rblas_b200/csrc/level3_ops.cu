@@ -191,6 +191,31 @@ __global__ void scale_b_kernel(T* __restrict__ b, size_t ldb, int m, int n, T ar
     }
 }
 
+// op(A) of a triangular A expanded to a full q x q column-major matrix:
+// the referenced triangle of A (transposed for Trans / ConjTrans, conjugated
+// for ConjTrans), zeros outside it, ones on the diagonal for Unit.
+template <typename T, bool CX>
+__global__ void tri_expand_kernel(const T* __restrict__ a, size_t lda, int q, int uplo, int trans, int diag,
+                                  T* __restrict__ full, size_t ldf) {
+    constexpr int W = CX ? 2 : 1;
+    const size_t total = static_cast<size_t>(q) * q;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t j = idx / q, i = idx - j * q;
+        const size_t r = trans ? j : i, c = trans ? i : j;  // stored position of op(A)[i, j]
+        const bool stored = (uplo == RB_UPPER) ? (r <= c) : (r >= c);
+        T re = T(0), im = T(0);
+        if (r == c && diag == RB_UNIT) {
+            re = T(1);
+        } else if (stored) {
+            re = a[W * (r + c * lda)];
+            if constexpr (CX) im = (trans == RB_CONJ_TRANS) ? T(0) - a[W * (r + c * lda) + 1] : a[W * (r + c * lda) + 1];
+        }
+        full[W * (i + j * ldf)] = re;
+        if constexpr (CX) full[W * (i + j * ldf) + 1] = im;
+    }
+}
+
 constexpr int kNbReal = 64, kNbCplx = 32;
 
 // Solve one diagonal block by substitution for `nvec` independent vectors,
@@ -482,6 +507,59 @@ int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, 
     }
     return RB_OK;
 }
+
+// B := alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular: op(A)
+// expanded to a full matrix, one GEMM into scratch, copied back into B.
+template <typename T, bool CX>
+int trmm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A, size_t lda, T* B,
+             size_t ldb, cudaStream_t st, int32_t* ce) {
+    if (m == 0 || n == 0) return RB_OK;
+    constexpr int W = CX ? 2 : 1;
+    const size_t q = (side == RB_LEFT) ? m : n;
+    const size_t vec = 16 / (W * sizeof(T)) > 0 ? 16 / (W * sizeof(T)) : 1;
+    const size_t ldf = rup(q, vec), ldo = rup(m, vec);
+    const size_t full_bytes = rup(W * ldf * q * sizeof(T), 256);
+    void* buf = nullptr;
+    cudaError_t e = scratch_alloc(&buf, full_bytes + W * ldo * n * sizeof(T), st);
+    if (e != cudaSuccess) return fail(e, ce);
+    T* full = static_cast<T*>(buf);
+    T* out = reinterpret_cast<T*>(static_cast<uint8_t*>(buf) + full_bytes);
+    tri_expand_kernel<T, CX><<<grid_for(q * q), 256, 0, st>>>(A, lda, static_cast<int>(q), uplo, trans, diag, full,
+                                                               ldf);
+    count_launch();
+    int rc;
+    if constexpr (CX) {
+        if (side == RB_LEFT)
+            rc = complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, n, m, ar, ai, full, ldf, B, ldb, T(0), T(0), out, ldo,
+                                     RB_PREC_PLAIN, st, ce);
+        else
+            rc = complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, n, n, ar, ai, B, ldb, full, ldf, T(0), T(0), out, ldo,
+                                     RB_PREC_PLAIN, st, ce);
+    } else {
+        if (side == RB_LEFT)
+            rc = gemm_colmajor_dev<T>(false, false, m, n, m, ar, full, ldf, B, ldb, T(0), out, ldo, RB_PREC_PLAIN, st,
+                                      0, ce);
+        else
+            rc = gemm_colmajor_dev<T>(false, false, m, n, n, ar, B, ldb, full, ldf, T(0), out, ldo, RB_PREC_PLAIN, st,
+                                      0, ce);
+    }
+    if (rc == RB_OK) {
+        e = cudaMemcpy2DAsync(B, W * ldb * sizeof(T), out, W * ldo * sizeof(T), W * m * sizeof(T), n,
+                              cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) rc = fail(e, ce);
+    }
+    cudaFreeAsync(buf, st);
+    return rc;
+}
+
+template int trmm_dev<float, false>(int, int, int, int, size_t, size_t, float, float, const float*, size_t, float*,
+                                    size_t, cudaStream_t, int32_t*);
+template int trmm_dev<double, false>(int, int, int, int, size_t, size_t, double, double, const double*, size_t,
+                                     double*, size_t, cudaStream_t, int32_t*);
+template int trmm_dev<float, true>(int, int, int, int, size_t, size_t, float, float, const float*, size_t, float*,
+                                   size_t, cudaStream_t, int32_t*);
+template int trmm_dev<double, true>(int, int, int, int, size_t, size_t, double, double, const double*, size_t,
+                                    double*, size_t, cudaStream_t, int32_t*);
 
 template int complex_gemm_dev<float>(int, int, size_t, size_t, size_t, float, float, const float*, size_t,
                                      const float*, size_t, float, float, float*, size_t, int, cudaStream_t,

@@ -866,6 +866,26 @@ rb_status trsm_host(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag
     });
 }
 
+// trmm: no rblas counterpart (its README lists trmm as remaining Level 3);
+// the argument checks follow trsm's (src/level3.rs:390-402 shapes).
+template <typename T, bool CX>
+rb_status trmm_host(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, T ar, T ai,
+                    const T* a, size_t lda, size_t a_len, T* b, size_t ldb, size_t b_len, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_side(side) || !valid_uplo(uplo) || !valid_trans(trans) || !valid_diag(diag)) return invalid(err);
+    const size_t q = (side == RB_LEFT) ? m : n;
+    rb_status s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'a', q, q, lda, a_len, true, err))) return s;
+    if ((s = check_matrix(RB_COL_MAJOR, 'b', m, n, ldb, b_len, true, err))) return s;
+    if (m == 0 || n == 0) return RB_OK;
+    const size_t el = (CX ? 2 : 1) * sizeof(T);
+    HostMat mats[2] = {{a, nullptr, q, q, lda, el, true, false}, {b, b, m, n, ldb, el, true, true}};
+    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+        return trmm_dev<T, CX>(side, uplo, trans, diag, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
+                               static_cast<T*>(d[1]), ld[1], st, ce);
+    });
+}
+
 rb_status dev_status(int rc, int32_t ce, rb_error* err) {
     if (rc != RB_OK) set_err(err, rc, 0, 0, 0, ce);
     return static_cast<rb_status>(rc);
@@ -1120,5 +1140,38 @@ RB_CGER(rb_zgeru, double, rb_complex64, 0)
 RB_CGER(rb_cgerc, float, rb_complex32, 1)
 RB_CGER(rb_zgerc, double, rb_complex64, 1)
 #undef RB_CGER
+
+
+// ---- trmm (no rblas counterpart) ----------------------------------------------
+rb_status rb_strmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, float alpha,
+                   const float* a, size_t lda, size_t a_len, float* b, size_t ldb, size_t b_len, rb_error* err) {
+    return trmm_host<float, false>(side, uplo, trans, diag, m, n, alpha, 0.f, a, lda, a_len, b, ldb, b_len, err);
+}
+rb_status rb_dtrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n, double alpha,
+                   const double* a, size_t lda, size_t a_len, double* b, size_t ldb, size_t b_len, rb_error* err) {
+    return trmm_host<double, false>(side, uplo, trans, diag, m, n, alpha, 0.0, a, lda, a_len, b, ldb, b_len, err);
+}
+rb_status rb_ctrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex32 alpha, const rb_complex32* a, size_t lda, size_t a_len, rb_complex32* b, size_t ldb,
+                   size_t b_len, rb_error* err) {
+    return trmm_host<float, true>(side, uplo, trans, diag, m, n, alpha.re, alpha.im, reinterpret_cast<const float*>(a),
+                                  lda, a_len, reinterpret_cast<float*>(b), ldb, b_len, err);
+}
+rb_status rb_ztrmm(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                   rb_complex64 alpha, const rb_complex64* a, size_t lda, size_t a_len, rb_complex64* b, size_t ldb,
+                   size_t b_len, rb_error* err) {
+    return trmm_host<double, true>(side, uplo, trans, diag, m, n, alpha.re, alpha.im,
+                                   reinterpret_cast<const double*>(a), lda, a_len, reinterpret_cast<double*>(b), ldb,
+                                   b_len, err);
+}
+rb_status rb_dtrmm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag, size_t m, size_t n,
+                       double alpha, const double* a, size_t lda, double* b, size_t ldb, void* stream, rb_error* err) {
+    set_err(err, RB_OK);
+    if (!valid_side(side) || !valid_uplo(uplo) || !valid_trans(trans) || !valid_diag(diag)) return invalid(err);
+    int32_t ce = 0;
+    const int rc = trmm_dev<double, false>(side, uplo, trans, diag, m, n, alpha, 0.0, a, lda, b, ldb,
+                                           static_cast<cudaStream_t>(stream), &ce);
+    return dev_status(rc, ce, err);
+}
 
 }  // extern "C"

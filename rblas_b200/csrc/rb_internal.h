@@ -178,6 +178,11 @@ template <typename T, bool CX>
 int ger_dev(int layout, size_t m, size_t n, T ar, T ai, const T* x, long long incx, const T* y, long long incy, T* A,
             size_t lda, int conj, cudaStream_t st, int32_t* ce);
 
+// Triangular multiply B := alpha*op(A)*B (Left) / alpha*B*op(A) (Right) through one GEMM.
+template <typename T, bool CX>
+int trmm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A, size_t lda, T* B,
+             size_t ldb, cudaStream_t st, int32_t* ce);
+
 // Batched triangular solve over uniformly strided A_i / B_i (rb_?trsm_batched_dev).
 template <typename T>
 int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T alpha, const T* A, size_t lda,

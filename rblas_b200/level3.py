@@ -144,3 +144,18 @@ def trsm_batched_dev(side, uplo, trans, diag, m, n, alpha, a_ptr, lda, stride_a,
             C.c_void_p(a_ptr), lda, stride_a, C.c_void_p(b_ptr), ldb, stride_b, batch,
             C.c_void_p(stream) if stream else None, C.byref(err))
     _lib.check(st, err)
+
+
+def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+    """Triangular multiply in place of B: B := alpha*op(A)*B (Left) or
+    alpha*B*op(A) (Right), A triangular. No rblas counterpart (its README
+    lists trmm as remaining Level 3); arguments as level3::trsm."""
+    from .types import Diag, Side, Uplo
+    dt = _dtype_of(b)
+    a = _as_slice(a, dt, "a")
+    b = _as_slice(b, dt, "b", writable=True)
+    err = _lib.RbError()
+    st = _real_fn(_lib.load(), dt, "trmm")(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)),
+                                           int(Diag(diag)), m, n, alpha, _ptr(a), lda, a.size, _ptr(b), ldb, b.size,
+                                           C.byref(err))
+    _lib.check(st, err)
