@@ -224,6 +224,27 @@ def cpu_baseline(threads, reps=2):
                       f"1 warm-up; rblas threads-feature gemm restated in C++ (oracle/)"}
 
 
+def level1_cpu_baseline(n=1 << 24, reps=3):
+    """rblas's ddot and daxpy restated in C++ (oracle/: its AVX2 dot order and
+    fused axpy), single thread as rblas's Level 1 is, on 2^24 f64 (128 MiB per
+    vector, above the host caches), in the same bytes-per-call terms."""
+    import oracle
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n)
+    y = rng.standard_normal(n)
+    out = {"cores": 1, "kind": "port", "sample": f"n = {n} f64, median of {reps} after 1 warm-up"}
+    for name, fn, nbytes in (("ddot", lambda: oracle.dot(n, x, 1, y, 1), 16.0 * n),
+                             ("daxpy", lambda: oracle.axpy(n, 1e-3, x, 1, y, 1), 24.0 * n)):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        out[name + "_gb_s"] = nbytes / statistics.median(ts) / 1e9
+    return out
+
+
 def run_reference(args):
     ws, rank, _ = dist_info()
     if rank != 0:
@@ -494,6 +515,31 @@ def run_ours(args):
         others["level2_16384"] = lv2
         del AL, xl, yl
         torch.cuda.empty_cache()
+        # Level 1 (HBM-bound): 2^27 f64 per vector (1 GiB each, above L2, so
+        # every call streams from HBM); f32 and complex forms over the same bytes
+        n1 = 1 << 27
+        keep1, cases1 = level1_cases(torch, n1, dev, sh)
+        lv1 = {"hbm_peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm else None,
+               "vector_bytes": 8 * n1}
+        for name, fn, nbytes in cases1:
+            ms, launches, _ = timed(fn, 10, 3)
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            lv1[name] = {"ms": ms, "gb_s": gbs, "frac_of_hbm": gbs / hbm if hbm else None,
+                         "launches_per_call": launches / 10}
+        # launch-bound end: rblas's own bench sizes (1M f32, src benches/level1.rs)
+        small = torch.ones(2 << 20, dtype=torch.float32, device=dev)
+        from rblas_b200 import level1 as l1mod
+        for name, fn in (("saxpy_1M_us", lambda: l1mod.axpy_dev(1 << 20, 3.0, small.data_ptr(), 1,
+                                                                  small[1 << 20:].data_ptr(), 1, np.float32, sh)),
+                         ("sdot_1M_us", lambda: l1mod.dot_dev(1 << 20, small.data_ptr(), 1, small[1 << 20:].data_ptr(),
+                                                              1, keep1[2].data_ptr(), np.float32, sh))):
+            ms, _, _ = timed(fn, 200, 20)
+            lv1[name] = ms * 1e3
+        if rank == 0 and ws == 1 and not args.no_cpu:
+            lv1["cpu_baseline"] = level1_cpu_baseline()
+        others["level1_2^27_f64"] = lv1
+        del keep1, cases1, small
+        torch.cuda.empty_cache()
 
     # ---- e2e through the public host API (pinned host buffers) -------------
     e2e = None
@@ -719,6 +765,62 @@ def run_kernel_only(args):
                       "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}))
 
 
+def level1_cases(torch, n, dev, sh, seed=11):
+    """Level-1 calls on device vectors of n scalars (f64 / f32 views of the
+    same 8n-byte buffers; complex over n/2 elements), each with its
+    algorithmic HBM bytes per call: axpy reads x, y and writes y (3 vectors),
+    dot reads 2, asum / nrm2 read 1, scal reads and writes 1, copy reads 1 and
+    writes 1, swap reads and writes 2."""
+    from rblas_b200 import complex1, level1
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    x = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    y = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    r = torch.zeros(4, dtype=torch.float64, device=dev)
+    xs, ys = x.view(torch.float32), y.view(torch.float32)  # 2n f32 over the same bytes
+    px, py, pr, B = x.data_ptr(), y.data_ptr(), r.data_ptr(), 8.0 * n
+    f64, f32, c128 = np.float64, np.float32, np.complex128
+    return (x, y, r), [
+        ("daxpy", lambda: level1.axpy_dev(n, 1e-3, px, 1, py, 1, f64, sh), 3 * B),
+        ("ddot", lambda: level1.dot_dev(n, px, 1, py, 1, pr, f64, sh), 2 * B),
+        ("dnrm2", lambda: level1.nrm2_dev(n, px, 1, pr, f64, sh), B),
+        ("dasum", lambda: level1.asum_dev(n, px, 1, pr, f64, sh), B),
+        ("dscal", lambda: level1.scal_dev(n, 1.0 - 1e-9, py, 1, f64, sh), 2 * B),
+        ("dcopy", lambda: level1.copy_dev(n, px, 1, py, 1, f64, sh), 2 * B),
+        ("dswap", lambda: level1.swap_dev(n, px, 1, py, 1, f64, sh), 4 * B),
+        ("saxpy", lambda: level1.axpy_dev(2 * n, 1e-3, xs.data_ptr(), 1, ys.data_ptr(), 1, f32, sh), 3 * B),
+        ("sdot", lambda: level1.dot_dev(2 * n, xs.data_ptr(), 1, ys.data_ptr(), 1, pr, f32, sh), 2 * B),
+        ("snrm2", lambda: level1.nrm2_dev(2 * n, xs.data_ptr(), 1, pr, f32, sh), B),
+        ("zaxpy", lambda: complex1.axpy_dev(n // 2, 1e-3 + 1e-3j, px, 1, py, 1, c128, sh), 3 * B),
+        ("zdotc", lambda: complex1.dotc_dev(n // 2, px, 1, py, 1, pr, c128, sh), 2 * B),
+        ("dznrm2", lambda: complex1.nrm2_dev(n // 2, px, 1, pr, c128, sh), B),
+        ("daxpy_incx2", lambda: level1.axpy_dev(n // 2, 1e-3, px, 2, py, 2, f64, sh), 3 * B / 2),
+    ]
+
+
+def run_level1_only(args):
+    """The Level-1 calls of `level1_cases` on n-scalar f64 vectors, each
+    launched warmup + steps times (for ncu captures on a bounded case)."""
+    import torch
+
+    n = args.level1
+    sh = torch.cuda.current_stream().cuda_stream
+    keep, cases = level1_cases(torch, n, "cuda", sh)
+    out = {"level1": n}
+    for name, fn, nbytes in cases:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for i in range(args.warmup + args.steps):
+            if i == args.warmup:
+                e0.record()
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(args.steps, 1)
+        out[name] = {"ms": ms, "gb_s": nbytes / (ms * 1e-3) / 1e9}
+    print(json.dumps(out))
+
+
 def run_level2_only(args):
     """dgemv (N and T) and dger on an n x n column-major f64 matrix, each
     launched warmup + steps times (for ncu captures on a bounded case)."""
@@ -845,6 +947,8 @@ def main():
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f64")
     ap.add_argument("--level2", type=int, default=0, metavar="N",
                     help="time dgemv (N, T) and dger on an N x N f64 matrix only")
+    ap.add_argument("--level1", type=int, default=0, metavar="N",
+                    help="Level-1 calls on N-scalar f64 vectors only (bounded ncu captures)")
     ap.add_argument("--grouped-batch", type=int, default=0, metavar="N",
                     help="time one grouped launch of the first N serving requests only")
     ap.add_argument("--trsm-batched", type=int, default=0, metavar="BATCH",
@@ -867,6 +971,8 @@ def main():
         run_grouped_only(args)
     elif args.level2:
         run_level2_only(args)
+    elif args.level1:
+        run_level1_only(args)
     elif args.serve:
         run_serve_mode(args)
     elif args.shape:

@@ -220,6 +220,114 @@ rb_status rb_dtrsm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                        void* stream, rb_error* err);
 
 /* ---------------------------------------------------------------------------
+ * Level 1: vector-vector routines (level1::axpy / dot / scal / nrm2 / asum /
+ * copy / swap, src/level1.rs:17-163; complex1::axpy / dotu / dotc / scal /
+ * nrm2, src/complex1.rs:8-112). Vectors are strided (incx, incy in
+ * elements). The argument rules follow rblas in its order: n == 0, real axpy
+ * with alpha == 0 and real scal with alpha == 1 return at once (reductions
+ * give 0); a zero stride is RB_ERR_ZERO_STRIDE where rblas asserts a positive
+ * one (axpy, dot, scal, nrm2; src/level1.rs:31,53,78,100, src/complex1.rs:
+ * 19,75,90) and is accepted where rblas's loop accepts it (asum, copy, dotu,
+ * dotc; copy with incy == 0 leaves x's last element in y[0]); swap with a
+ * zero stride and n > 1 is RB_ERR_ZERO_STRIDE (rblas would rotate elements
+ * one at a time). Host-slice forms then check each vector reaches its last
+ * strided element (RB_ERR_BUFFER_TOO_SMALL, which 'x' / 'y'), where rblas's
+ * indexing panics. axpy, scal, copy and swap compute every element exactly
+ * as rblas does; dot, dotu, dotc, asum and nrm2 sum in a fixed parallel
+ * order (the same result on every call) and agree with rblas's sequential
+ * sum within rounding; nrm2 keeps the scaled sum of squares, so it neither
+ * overflows nor underflows where rblas does not.
+ * ------------------------------------------------------------------------- */
+
+/* y := alpha*x + y. Replaces level1::axpy (src/level1.rs:17-41),
+ * complex1::axpy (src/complex1.rs:8-27). */
+rb_status rb_saxpy(size_t n, float alpha, const float* x, size_t incx, size_t x_len, float* y, size_t incy,
+                   size_t y_len, rb_error* err);
+rb_status rb_daxpy(size_t n, double alpha, const double* x, size_t incx, size_t x_len, double* y, size_t incy,
+                   size_t y_len, rb_error* err);
+rb_status rb_caxpy(size_t n, rb_complex32 alpha, const rb_complex32* x, size_t incx, size_t x_len,
+                   rb_complex32* y, size_t incy, size_t y_len, rb_error* err);
+rb_status rb_zaxpy(size_t n, rb_complex64 alpha, const rb_complex64* x, size_t incx, size_t x_len,
+                   rb_complex64* y, size_t incy, size_t y_len, rb_error* err);
+/* x := alpha*x. Replaces level1::scal (src/level1.rs:70-86), complex1::scal
+ * (src/complex1.rs:71-81). */
+rb_status rb_sscal(size_t n, float alpha, float* x, size_t incx, size_t x_len, rb_error* err);
+rb_status rb_dscal(size_t n, double alpha, double* x, size_t incx, size_t x_len, rb_error* err);
+rb_status rb_cscal(size_t n, rb_complex32 alpha, rb_complex32* x, size_t incx, size_t x_len, rb_error* err);
+rb_status rb_zscal(size_t n, rb_complex64 alpha, rb_complex64* x, size_t incx, size_t x_len, rb_error* err);
+/* y := x; x <-> y. Replace level1::copy / swap (src/level1.rs:139-163). */
+rb_status rb_scopy(size_t n, const float* x, size_t incx, size_t x_len, float* y, size_t incy, size_t y_len,
+                   rb_error* err);
+rb_status rb_dcopy(size_t n, const double* x, size_t incx, size_t x_len, double* y, size_t incy, size_t y_len,
+                   rb_error* err);
+rb_status rb_sswap(size_t n, float* x, size_t incx, size_t x_len, float* y, size_t incy, size_t y_len,
+                   rb_error* err);
+rb_status rb_dswap(size_t n, double* x, size_t incx, size_t x_len, double* y, size_t incy, size_t y_len,
+                   rb_error* err);
+/* *result := x^T y. Replaces level1::dot (src/level1.rs:45-66). */
+rb_status rb_sdot(size_t n, const float* x, size_t incx, size_t x_len, const float* y, size_t incy, size_t y_len,
+                  float* result, rb_error* err);
+rb_status rb_ddot(size_t n, const double* x, size_t incx, size_t x_len, const double* y, size_t incy,
+                  size_t y_len, double* result, rb_error* err);
+/* *result := sum x_i y_i (dotu) or sum conj(x_i) y_i (dotc). Replace
+ * complex1::dotu / dotc (src/complex1.rs:31-67). */
+rb_status rb_cdotu(size_t n, const rb_complex32* x, size_t incx, size_t x_len, const rb_complex32* y, size_t incy,
+                   size_t y_len, rb_complex32* result, rb_error* err);
+rb_status rb_zdotu(size_t n, const rb_complex64* x, size_t incx, size_t x_len, const rb_complex64* y, size_t incy,
+                   size_t y_len, rb_complex64* result, rb_error* err);
+rb_status rb_cdotc(size_t n, const rb_complex32* x, size_t incx, size_t x_len, const rb_complex32* y, size_t incy,
+                   size_t y_len, rb_complex32* result, rb_error* err);
+rb_status rb_zdotc(size_t n, const rb_complex64* x, size_t incx, size_t x_len, const rb_complex64* y, size_t incy,
+                   size_t y_len, rb_complex64* result, rb_error* err);
+/* *result := sum |x_i|. Replaces level1::asum (src/level1.rs:127-135). */
+rb_status rb_sasum(size_t n, const float* x, size_t incx, size_t x_len, float* result, rb_error* err);
+rb_status rb_dasum(size_t n, const double* x, size_t incx, size_t x_len, double* result, rb_error* err);
+/* *result := ||x||_2 by the scaled sum of squares. Replaces level1::nrm2
+ * (src/level1.rs:96-123), complex1::nrm2 (src/complex1.rs:86-112). */
+rb_status rb_snrm2(size_t n, const float* x, size_t incx, size_t x_len, float* result, rb_error* err);
+rb_status rb_dnrm2(size_t n, const double* x, size_t incx, size_t x_len, double* result, rb_error* err);
+rb_status rb_scnrm2(size_t n, const rb_complex32* x, size_t incx, size_t x_len, float* result, rb_error* err);
+rb_status rb_dznrm2(size_t n, const rb_complex64* x, size_t incx, size_t x_len, double* result, rb_error* err);
+/* Device-pointer twins, enqueued on `stream` (strides checked; lengths are
+ * the caller's). Reductions write their result to device memory. */
+rb_status rb_saxpy_dev(size_t n, float alpha, const float* x, size_t incx, float* y, size_t incy, void* stream,
+                       rb_error* err);
+rb_status rb_daxpy_dev(size_t n, double alpha, const double* x, size_t incx, double* y, size_t incy, void* stream,
+                       rb_error* err);
+rb_status rb_caxpy_dev(size_t n, rb_complex32 alpha, const rb_complex32* x, size_t incx, rb_complex32* y,
+                       size_t incy, void* stream, rb_error* err);
+rb_status rb_zaxpy_dev(size_t n, rb_complex64 alpha, const rb_complex64* x, size_t incx, rb_complex64* y,
+                       size_t incy, void* stream, rb_error* err);
+rb_status rb_sscal_dev(size_t n, float alpha, float* x, size_t incx, void* stream, rb_error* err);
+rb_status rb_dscal_dev(size_t n, double alpha, double* x, size_t incx, void* stream, rb_error* err);
+rb_status rb_cscal_dev(size_t n, rb_complex32 alpha, rb_complex32* x, size_t incx, void* stream, rb_error* err);
+rb_status rb_zscal_dev(size_t n, rb_complex64 alpha, rb_complex64* x, size_t incx, void* stream, rb_error* err);
+rb_status rb_scopy_dev(size_t n, const float* x, size_t incx, float* y, size_t incy, void* stream, rb_error* err);
+rb_status rb_dcopy_dev(size_t n, const double* x, size_t incx, double* y, size_t incy, void* stream,
+                       rb_error* err);
+rb_status rb_sswap_dev(size_t n, float* x, size_t incx, float* y, size_t incy, void* stream, rb_error* err);
+rb_status rb_dswap_dev(size_t n, double* x, size_t incx, double* y, size_t incy, void* stream, rb_error* err);
+rb_status rb_sdot_dev(size_t n, const float* x, size_t incx, const float* y, size_t incy, float* result,
+                      void* stream, rb_error* err);
+rb_status rb_ddot_dev(size_t n, const double* x, size_t incx, const double* y, size_t incy, double* result,
+                      void* stream, rb_error* err);
+rb_status rb_cdotu_dev(size_t n, const rb_complex32* x, size_t incx, const rb_complex32* y, size_t incy,
+                       rb_complex32* result, void* stream, rb_error* err);
+rb_status rb_zdotu_dev(size_t n, const rb_complex64* x, size_t incx, const rb_complex64* y, size_t incy,
+                       rb_complex64* result, void* stream, rb_error* err);
+rb_status rb_cdotc_dev(size_t n, const rb_complex32* x, size_t incx, const rb_complex32* y, size_t incy,
+                       rb_complex32* result, void* stream, rb_error* err);
+rb_status rb_zdotc_dev(size_t n, const rb_complex64* x, size_t incx, const rb_complex64* y, size_t incy,
+                       rb_complex64* result, void* stream, rb_error* err);
+rb_status rb_sasum_dev(size_t n, const float* x, size_t incx, float* result, void* stream, rb_error* err);
+rb_status rb_dasum_dev(size_t n, const double* x, size_t incx, double* result, void* stream, rb_error* err);
+rb_status rb_snrm2_dev(size_t n, const float* x, size_t incx, float* result, void* stream, rb_error* err);
+rb_status rb_dnrm2_dev(size_t n, const double* x, size_t incx, double* result, void* stream, rb_error* err);
+rb_status rb_scnrm2_dev(size_t n, const rb_complex32* x, size_t incx, float* result, void* stream, rb_error* err);
+rb_status rb_dznrm2_dev(size_t n, const rb_complex64* x, size_t incx, double* result, void* stream,
+                        rb_error* err);
+
+/* ---------------------------------------------------------------------------
  * Level 2: gemv and rank-1 updates (level2::gemv / ger, src/level2.rs:11-88;
  * complex2::gemv / geru / gerc, src/complex2.rs:11-145). x and y are strided
  * (incx, incy in elements; incx may be 0). Host-slice forms check A like

@@ -2,9 +2,11 @@
 
 ctypes bindings to ``liboracle.so`` (built from ``rblas_oracle.cpp`` by the
 Makefile beside it): a CPU restatement of rblas's Level-3 GEMM path
-(src/level3.rs, src/kernel/gemm.rs, src/kernel/gemm_avx2.rs, src/complex3.rs)
-and a compensated double-double accuracy oracle, plus numpy helpers for the
-normwise error metric.
+(src/level3.rs, src/kernel/gemm.rs, src/kernel/gemm_avx2.rs, src/complex3.rs),
+of its Level-1 and Level-2 routines (src/level1.rs, src/complex1.rs,
+src/kernel/avx2.rs, src/level2.rs, src/complex2.rs), a compensated
+double-double accuracy oracle, and numpy helpers for the normwise error
+metric.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package; the product library never does.
@@ -80,6 +82,23 @@ def _declare(L):
     L.or_lcg_fill_f32.argtypes = [C.c_uint64, _i, _sz, _pf]
     L.or_lcg_fill_f32.restype = C.c_uint64
     L.or_set_force_scalar.argtypes = [_i]
+    for P, t, pt in (("s", _f, _pf), ("d", _d, _pd)):
+        getattr(L, f"or_{P}axpy").argtypes = [_sz, t, pt, _sz, pt, _sz]
+        getattr(L, f"or_{P}dot").argtypes = [_sz, pt, _sz, pt, _sz]
+        getattr(L, f"or_{P}dot").restype = t
+        getattr(L, f"or_{P}scal").argtypes = [_sz, t, pt, _sz]
+        getattr(L, f"or_{P}nrm2").argtypes = [_sz, pt, _sz]
+        getattr(L, f"or_{P}nrm2").restype = t
+        getattr(L, f"or_{P}asum").argtypes = [_sz, pt, _sz]
+        getattr(L, f"or_{P}asum").restype = t
+        getattr(L, f"or_{P}copy").argtypes = [_sz, pt, _sz, pt, _sz]
+        getattr(L, f"or_{P}swap").argtypes = [_sz, pt, _sz, pt, _sz]
+    for P, t, pt in (("c", _f, _pf), ("z", _d, _pd)):
+        getattr(L, f"or_{P}axpy").argtypes = [_sz, t, t, pt, _sz, pt, _sz]
+        getattr(L, f"or_{P}dot").argtypes = [_sz, pt, _sz, pt, _sz, _i, pt]
+        getattr(L, f"or_{P}scal").argtypes = [_sz, t, t, pt, _sz]
+        getattr(L, f"or_{P}nrm2").argtypes = [_sz, pt, _sz]
+        getattr(L, f"or_{P}nrm2").restype = t
     L.or_strmm.argtypes = [_i, _i, _i, _i, _sz, _sz, _f, _pf, _sz, _pf, _sz]
     L.or_dtrmm.argtypes = [_i, _i, _i, _i, _sz, _sz, _d, _pd, _sz, _pd, _sz]
     L.or_sgemv.argtypes = [_i, _i, _sz, _sz, _f, _pf, _sz, _pf, _sz, _f, _pf, _sz]
@@ -184,6 +203,68 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     else:
         lib().or_ztrsm(side, uplo, trans, diag, m, n, float(np.real(alpha)), float(np.imag(alpha)),
                        _ptr(a, C.c_double), lda, _ptr(b, C.c_double), ldb)
+
+
+def _l1(x):
+    dt = np.dtype(x.dtype)
+    p = {np.dtype(np.float32): "s", np.dtype(np.float64): "d", np.dtype(np.complex64): "c",
+         np.dtype(np.complex128): "z"}[dt]
+    ct = C.c_float if p in "sc" else C.c_double
+    return p, ct
+
+
+def axpy(n, alpha, x, incx, y, incy):
+    """level1::axpy / complex1::axpy (src/level1.rs:17-42, src/complex1.rs:8-28), y in place."""
+    p, ct = _l1(y)
+    if p in "sd":
+        getattr(lib(), f"or_{p}axpy")(n, float(alpha), _ptr(x, ct), incx, _ptr(y, ct), incy)
+    else:
+        getattr(lib(), f"or_{p}axpy")(n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(x, ct), incx,
+                                      _ptr(y, ct), incy)
+
+
+def dot(n, x, incx, y, incy, conj=False):
+    """level1::dot (src/level1.rs:45-66, contiguous through the AVX2 or scalar
+    kernel of src/kernel/); complex1::dotu / dotc (src/complex1.rs:31-68)."""
+    p, ct = _l1(x)
+    if p in "sd":
+        return float(getattr(lib(), f"or_{p}dot")(n, _ptr(x, ct), incx, _ptr(y, ct), incy))
+    out = np.zeros(2, dtype=np.float32 if p == "c" else np.float64)
+    getattr(lib(), f"or_{p}dot")(n, _ptr(x, ct), incx, _ptr(y, ct), incy, int(conj), _ptr(out, ct))
+    return complex(out[0], out[1])
+
+
+def scal(n, alpha, x, incx):
+    """level1::scal / complex1::scal (src/level1.rs:70-93, src/complex1.rs:71-83), x in place."""
+    p, ct = _l1(x)
+    if p in "sd":
+        getattr(lib(), f"or_{p}scal")(n, float(alpha), _ptr(x, ct), incx)
+    else:
+        getattr(lib(), f"or_{p}scal")(n, float(np.real(alpha)), float(np.imag(alpha)), _ptr(x, ct), incx)
+
+
+def nrm2(n, x, incx):
+    """level1::nrm2 / complex1::nrm2 (scaled sum of squares)."""
+    p, ct = _l1(x)
+    return float(getattr(lib(), f"or_{p}nrm2")(n, _ptr(x, ct), incx))
+
+
+def asum(n, x, incx):
+    """level1::asum (src/level1.rs:127-136)."""
+    p, ct = _l1(x)
+    return float(getattr(lib(), f"or_{p}asum")(n, _ptr(x, ct), incx))
+
+
+def copy(n, x, incx, y, incy):
+    """level1::copy (src/level1.rs:139-151), y in place."""
+    p, ct = _l1(y)
+    getattr(lib(), f"or_{p}copy")(n, _ptr(x, ct), incx, _ptr(y, ct), incy)
+
+
+def swap(n, x, incx, y, incy):
+    """level1::swap (src/level1.rs:155-163), x and y in place."""
+    p, ct = _l1(y)
+    getattr(lib(), f"or_{p}swap")(n, _ptr(x, ct), incx, _ptr(y, ct), incy)
 
 
 def trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):

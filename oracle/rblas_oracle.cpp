@@ -40,6 +40,8 @@
 #include <string.h>
 #include <math.h>
 #include <atomic>
+#include <cmath>
+#include <utility>
 #include <vector>
 #include <thread>
 #include <algorithm>
@@ -681,6 +683,79 @@ void dd_gemm_any(int layout, int transa, int transb, size_t m, size_t n, size_t 
 
 }  // namespace
 
+// ---- Level 1 (src/level1.rs, src/complex1.rs, src/kernel/{avx2,scalar}.rs) ----
+
+// src/kernel/avx2.rs:30-56 / 104-130: two W-lane fma accumulators over
+// blocks of 2W, then W, hsum of acc0+acc1 (hsum256_ps / hsum256_pd order),
+// then the tail with scalar fma. src/kernel/scalar.rs: 4 accumulators.
+template <typename T>
+T dot_contig(size_t n, const T* x, const T* y) {
+    if (have_avx2_fma()) {
+        constexpr size_t W = sizeof(T) == 4 ? 8 : 4;
+        T a0[W] = {}, a1[W] = {};
+        size_t i = 0;
+        for (; i + 2 * W <= n; i += 2 * W)
+            for (size_t l = 0; l < W; ++l) {
+                a0[l] = fmaT(x[i + l], y[i + l], a0[l]);
+                a1[l] = fmaT(x[i + W + l], y[i + W + l], a1[l]);
+            }
+        for (; i + W <= n; i += W)
+            for (size_t l = 0; l < W; ++l) a0[l] = fmaT(x[i + l], y[i + l], a0[l]);
+        T v[W];
+        for (size_t l = 0; l < W; ++l) v[l] = a0[l] + a1[l];
+        T acc;
+        if (W == 8) {  // lo + hi, then movehl, then lane 1
+            T t[4];
+            for (int k = 0; k < 4; ++k) t[k] = v[k] + v[k + 4];
+            const T u0 = t[0] + t[2], u1 = t[1] + t[3];
+            acc = u0 + u1;
+        } else {
+            const T t0 = v[0] + v[2], t1 = v[1] + v[3];
+            acc = t0 + t1;
+        }
+        for (; i < n; ++i) acc = fmaT(x[i], y[i], acc);
+        return acc;
+    }
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    const size_t chunks = n / 4;
+    for (size_t k = 0; k < chunks; ++k) {
+        const size_t i = k * 4;
+        a0 = fmaT(x[i], y[i], a0);
+        a1 = fmaT(x[i + 1], y[i + 1], a1);
+        a2 = fmaT(x[i + 2], y[i + 2], a2);
+        a3 = fmaT(x[i + 3], y[i + 3], a3);
+    }
+    T acc = (a0 + a1) + (a2 + a3);
+    for (size_t i = chunks * 4; i < n; ++i) acc = fmaT(x[i], y[i], acc);
+    return acc;
+}
+
+// src/level1.rs:45-66
+template <typename T>
+T dot_impl(size_t n, const T* x, size_t incx, const T* y, size_t incy) {
+    if (n == 0) return T(0);
+    if (incx == 1 && incy == 1) return dot_contig(n, x, y);
+    T acc = T(0);
+    for (size_t q = 0; q < n; ++q) acc = fmaT(x[q * incx], y[q * incy], acc);
+    return acc;
+}
+
+// src/level1.rs:96-124 (scaled sum of squares); complex: both components (src/complex1.rs:86-118)
+template <typename T>
+void nrm2_step(T xi, T& scale, T& ssq) {
+    if (xi != T(0)) {
+        const T a = std::fabs(xi);
+        if (scale < a) {
+            const T r = scale / a;
+            ssq = T(1) + ssq * (r * r);
+            scale = a;
+        } else {
+            const T r = a / scale;
+            ssq = ssq + r * r;
+        }
+    }
+}
+
 // ---- trmm (no rblas counterpart: the textbook definition) ---------------------
 // out = alpha * op(A) * B (Left) or alpha * B * op(A) (Right), op(A) the
 // triangle of A (unit diagonal when diag), each output accumulated in index
@@ -1038,5 +1113,73 @@ void or_strmm(int side, int uplo, int trans, int diag, size_t m, size_t n, float
               float* b, size_t ldb) {
     trmm_impl<float>(side, uplo, trans != 0, diag, m, n, alpha, a, lda, b, ldb);
 }
+
+// Level 1, real (src/level1.rs)
+#define OR_L1_REAL(P, T)                                                                                           \
+    void or_##P##axpy(size_t n, T alpha, const T* x, size_t incx, T* y, size_t incy) {                             \
+        if (n == 0 || alpha == T(0)) return;                                                                       \
+        for (size_t q = 0; q < n; ++q) y[q * incy] = fmaT(alpha, x[q * incx], y[q * incy]);                        \
+    }                                                                                                              \
+    T or_##P##dot(size_t n, const T* x, size_t incx, const T* y, size_t incy) { return dot_impl(n, x, incx, y, incy); } \
+    void or_##P##scal(size_t n, T alpha, T* x, size_t incx) {                                                      \
+        if (n == 0 || alpha == T(1)) return;                                                                       \
+        for (size_t q = 0; q < n; ++q) x[q * incx] = alpha * x[q * incx];                                          \
+    }                                                                                                              \
+    T or_##P##nrm2(size_t n, const T* x, size_t incx) {                                                            \
+        if (n == 0) return T(0);                                                                                   \
+        T scale = T(0), ssq = T(1);                                                                                \
+        for (size_t q = 0; q < n; ++q) nrm2_step(x[q * incx], scale, ssq);                                         \
+        return scale * std::sqrt(ssq);                                                                             \
+    }                                                                                                              \
+    T or_##P##asum(size_t n, const T* x, size_t incx) {                                                            \
+        T acc = T(0);                                                                                              \
+        for (size_t q = 0; q < n; ++q) acc = acc + std::fabs(x[q * incx]);                                         \
+        return acc;                                                                                                \
+    }                                                                                                              \
+    /* src/level1.rs:139-163: element by element in order (zero strides included) */                             \
+    void or_##P##copy(size_t n, const T* x, size_t incx, T* y, size_t incy) {                                      \
+        for (size_t q = 0; q < n; ++q) y[q * incy] = x[q * incx];                                                  \
+    }                                                                                                              \
+    void or_##P##swap(size_t n, T* x, size_t incx, T* y, size_t incy) {                                            \
+        for (size_t q = 0; q < n; ++q) std::swap(x[q * incx], y[q * incy]);                                        \
+    }
+OR_L1_REAL(s, float)
+OR_L1_REAL(d, double)
+#undef OR_L1_REAL
+
+// Level 1, complex (src/complex1.rs); results returned through out[2]
+#define OR_L1_CPLX(P, T)                                                                                           \
+    void or_##P##axpy(size_t n, T ar, T ai, const T* x, size_t incx, T* y, size_t incy) {                          \
+        if (n == 0 || (ar == T(0) && ai == T(0))) return;                                                          \
+        const Cx<T> al{ar, ai};                                                                                    \
+        auto X = reinterpret_cast<const Cx<T>*>(x);                                                                \
+        auto Y = reinterpret_cast<Cx<T>*>(y);                                                                      \
+        for (size_t q = 0; q < n; ++q) Y[q * incy] = cadd(cmul(al, X[q * incx]), Y[q * incy]);                     \
+    }                                                                                                              \
+    void or_##P##dot(size_t n, const T* x, size_t incx, const T* y, size_t incy, int conj, T* out) {               \
+        auto X = reinterpret_cast<const Cx<T>*>(x);                                                                \
+        auto Y = reinterpret_cast<const Cx<T>*>(y);                                                                \
+        Cx<T> acc{T(0), T(0)};                                                                                     \
+        for (size_t q = 0; q < n; ++q) acc = cadd(acc, cmul(conj ? cconj(X[q * incx]) : X[q * incx], Y[q * incy])); \
+        out[0] = acc.re;                                                                                           \
+        out[1] = acc.im;                                                                                           \
+    }                                                                                                              \
+    void or_##P##scal(size_t n, T ar, T ai, T* x, size_t incx) {                                                   \
+        const Cx<T> al{ar, ai};                                                                                    \
+        auto X = reinterpret_cast<Cx<T>*>(x);                                                                      \
+        for (size_t q = 0; q < n; ++q) X[q * incx] = cmul(al, X[q * incx]);                                        \
+    }                                                                                                              \
+    T or_##P##nrm2(size_t n, const T* x, size_t incx) {                                                            \
+        if (n == 0) return T(0);                                                                                   \
+        T scale = T(0), ssq = T(1);                                                                                \
+        for (size_t q = 0; q < n; ++q) {                                                                           \
+            nrm2_step(x[2 * q * incx], scale, ssq);                                                                \
+            nrm2_step(x[2 * q * incx + 1], scale, ssq);                                                            \
+        }                                                                                                          \
+        return scale * std::sqrt(ssq);                                                                             \
+    }
+OR_L1_CPLX(c, float)
+OR_L1_CPLX(z, double)
+#undef OR_L1_CPLX
 
 }  // extern "C"

@@ -131,6 +131,39 @@ SIGNATURES = {
 }
 
 
+def _level1_signatures():
+    """Level 1 (include/rblas_b200.h): host slices carry a length after each
+    vector; the _dev forms take a stream instead. Reductions write *result."""
+    sig = {}
+    for p, t in (("s", _f), ("d", _d)):
+        sig[f"rb_{p}axpy"] = (_i, [_sz, t, _vp, _sz, _sz, _vp, _sz, _sz, _perr])
+        sig[f"rb_{p}axpy_dev"] = (_i, [_sz, t, _vp, _sz, _vp, _sz, _vp, _perr])
+        sig[f"rb_{p}scal"] = (_i, [_sz, t, _vp, _sz, _sz, _perr])
+        sig[f"rb_{p}scal_dev"] = (_i, [_sz, t, _vp, _sz, _vp, _perr])
+        for name in ("copy", "swap"):
+            sig[f"rb_{p}{name}"] = (_i, [_sz, _vp, _sz, _sz, _vp, _sz, _sz, _perr])
+            sig[f"rb_{p}{name}_dev"] = (_i, [_sz, _vp, _sz, _vp, _sz, _vp, _perr])
+        sig[f"rb_{p}dot"] = (_i, [_sz, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _perr])
+        sig[f"rb_{p}dot_dev"] = (_i, [_sz, _vp, _sz, _vp, _sz, _vp, _vp, _perr])
+        for name in ("asum", "nrm2"):
+            sig[f"rb_{p}{name}"] = (_i, [_sz, _vp, _sz, _sz, _vp, _perr])
+            sig[f"rb_{p}{name}_dev"] = (_i, [_sz, _vp, _sz, _vp, _vp, _perr])
+    for p, n, ct in (("c", "sc", RbComplex32), ("z", "dz", RbComplex64)):
+        sig[f"rb_{p}axpy"] = (_i, [_sz, ct, _vp, _sz, _sz, _vp, _sz, _sz, _perr])
+        sig[f"rb_{p}axpy_dev"] = (_i, [_sz, ct, _vp, _sz, _vp, _sz, _vp, _perr])
+        sig[f"rb_{p}scal"] = (_i, [_sz, ct, _vp, _sz, _sz, _perr])
+        sig[f"rb_{p}scal_dev"] = (_i, [_sz, ct, _vp, _sz, _vp, _perr])
+        for name in ("dotu", "dotc"):
+            sig[f"rb_{p}{name}"] = (_i, [_sz, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _perr])
+            sig[f"rb_{p}{name}_dev"] = (_i, [_sz, _vp, _sz, _vp, _sz, _vp, _vp, _perr])
+        sig[f"rb_{n}nrm2"] = (_i, [_sz, _vp, _sz, _sz, _vp, _perr])
+        sig[f"rb_{n}nrm2_dev"] = (_i, [_sz, _vp, _sz, _vp, _vp, _perr])
+    return sig
+
+
+SIGNATURES.update(_level1_signatures())
+
+
 def load():
     """Load (once) and return the CDLL. Raises if the library is absent."""
     global _lib

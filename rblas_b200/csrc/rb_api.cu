@@ -961,6 +961,46 @@ rb_status ger_host(rb_layout layout, size_t m, size_t n, T ar, T ai, const T* x,
     });
 }
 
+// ---- Level 1 host slices (src/level1.rs, src/complex1.rs) --------------------
+// Each vector travels as the contiguous span from its first to its last
+// strided element (one copy at full speed; the kernels keep the stride), so
+// elements between the strided ones come back unchanged. scal's vector is x;
+// reductions write *result (T, or {re, im} for dotu / dotc).
+template <typename T, bool CX>
+rb_status l1_host(int op, size_t n, T ar, T ai, const T* x, size_t incx, size_t x_len, T* y, size_t incy,
+                  size_t y_len, T* result, rb_error* err) {
+    set_err(err, RB_OK);
+    bool noop = false;
+    const rb_status s = l1_check(op, CX, n, ar == T(0) && ai == T(0), ar == T(1) && ai == T(0), incx, x_len, incy,
+                                 y_len, true, &noop, err);
+    if (s != RB_OK) return s;
+    const bool red = op >= L1_DOT;
+    const size_t nres = red ? ((op == L1_DOTU || op == L1_DOTC) ? 2 : 1) : 0;
+    if (red && !result) return invalid(err);
+    if (noop) {
+        for (size_t r = 0; r < nres; ++r) result[r] = T(0);
+        return RB_OK;
+    }
+    const bool uses_y = op == L1_AXPY || op == L1_COPY || op == L1_SWAP || op == L1_DOT || op == L1_DOTU ||
+                        op == L1_DOTC;
+    if (!x || (uses_y && !y)) return invalid(err);
+    const size_t el = sizeof(T) * (CX ? 2 : 1);
+    const size_t sx = incx == 0 ? 1 : (n - 1) * incx + 1, sy = incy == 0 ? 1 : (n - 1) * incy + 1;
+    const bool x_out = op == L1_SCAL || op == L1_SWAP, y_out = op == L1_AXPY || op == L1_COPY || op == L1_SWAP;
+    HostMat mats[3];
+    int nm = 0;
+    mats[nm++] = HostMat{x, x_out ? const_cast<T*>(x) : nullptr, sx, 1, sx, el, true, x_out};
+    if (uses_y) mats[nm++] = HostMat{y, y_out ? y : nullptr, sy, 1, sy, el, op != L1_COPY || incy > 1, y_out};
+    if (red) mats[nm++] = HostMat{nullptr, result, nres, 1, nres, sizeof(T), false, true};
+    return host_run(mats, nm, err, [&](void** d, size_t*, cudaStream_t st, int32_t* ce) {
+        T* dx = static_cast<T*>(d[0]);
+        T* dy = uses_y ? static_cast<T*>(d[1]) : nullptr;
+        T* dr = red ? static_cast<T*>(d[nm - 1]) : nullptr;
+        if (op == L1_SCAL) return l1_dev<T, CX>(op, n, ar, ai, nullptr, 0, dx, incx, nullptr, st, ce);
+        return l1_dev<T, CX>(op, n, ar, ai, dx, incx, dy, incy, dr, st, ce);
+    });
+}
+
 }  // namespace
 }  // namespace rb
 
@@ -1173,5 +1213,68 @@ rb_status rb_dtrmm_dev(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag d
                                            static_cast<cudaStream_t>(stream), &ce);
     return dev_status(rc, ce, err);
 }
+
+// Level 1 over host slices, real (src/level1.rs)
+#define RB_L1_REAL_HOST(P, T)                                                                                      \
+    rb_status rb_##P##axpy(size_t n, T alpha, const T* x, size_t incx, size_t x_len, T* y, size_t incy,            \
+                           size_t y_len, rb_error* err) {                                                          \
+        return l1_host<T, false>(L1_AXPY, n, alpha, T(0), x, incx, x_len, y, incy, y_len, nullptr, err);           \
+    }                                                                                                              \
+    rb_status rb_##P##scal(size_t n, T alpha, T* x, size_t incx, size_t x_len, rb_error* err) {                    \
+        return l1_host<T, false>(L1_SCAL, n, alpha, T(0), x, incx, x_len, nullptr, 0, 0, nullptr, err);            \
+    }                                                                                                              \
+    rb_status rb_##P##copy(size_t n, const T* x, size_t incx, size_t x_len, T* y, size_t incy, size_t y_len,       \
+                           rb_error* err) {                                                                        \
+        return l1_host<T, false>(L1_COPY, n, T(0), T(0), x, incx, x_len, y, incy, y_len, nullptr, err);            \
+    }                                                                                                              \
+    rb_status rb_##P##swap(size_t n, T* x, size_t incx, size_t x_len, T* y, size_t incy, size_t y_len,             \
+                           rb_error* err) {                                                                        \
+        return l1_host<T, false>(L1_SWAP, n, T(0), T(0), x, incx, x_len, y, incy, y_len, nullptr, err);            \
+    }                                                                                                              \
+    rb_status rb_##P##dot(size_t n, const T* x, size_t incx, size_t x_len, const T* y, size_t incy, size_t y_len,  \
+                          T* result, rb_error* err) {                                                              \
+        return l1_host<T, false>(L1_DOT, n, T(0), T(0), x, incx, x_len, const_cast<T*>(y), incy, y_len, result,    \
+                                 err);                                                                             \
+    }                                                                                                              \
+    rb_status rb_##P##asum(size_t n, const T* x, size_t incx, size_t x_len, T* result, rb_error* err) {            \
+        return l1_host<T, false>(L1_ASUM, n, T(0), T(0), x, incx, x_len, nullptr, 0, 0, result, err);              \
+    }                                                                                                              \
+    rb_status rb_##P##nrm2(size_t n, const T* x, size_t incx, size_t x_len, T* result, rb_error* err) {            \
+        return l1_host<T, false>(L1_NRM2, n, T(0), T(0), x, incx, x_len, nullptr, 0, 0, result, err);              \
+    }
+RB_L1_REAL_HOST(s, float)
+RB_L1_REAL_HOST(d, double)
+#undef RB_L1_REAL_HOST
+
+// Level 1 over host slices, complex (src/complex1.rs)
+#define RB_L1_CPLX_HOST(P, N, T, CT)                                                                               \
+    rb_status rb_##P##axpy(size_t n, CT alpha, const CT* x, size_t incx, size_t x_len, CT* y, size_t incy,         \
+                           size_t y_len, rb_error* err) {                                                          \
+        return l1_host<T, true>(L1_AXPY, n, alpha.re, alpha.im, reinterpret_cast<const T*>(x), incx, x_len,        \
+                                reinterpret_cast<T*>(y), incy, y_len, nullptr, err);                               \
+    }                                                                                                              \
+    rb_status rb_##P##scal(size_t n, CT alpha, CT* x, size_t incx, size_t x_len, rb_error* err) {                  \
+        return l1_host<T, true>(L1_SCAL, n, alpha.re, alpha.im, reinterpret_cast<T*>(x), incx, x_len, nullptr, 0,  \
+                                0, nullptr, err);                                                                  \
+    }                                                                                                              \
+    rb_status rb_##P##dotu(size_t n, const CT* x, size_t incx, size_t x_len, const CT* y, size_t incy,             \
+                           size_t y_len, CT* result, rb_error* err) {                                              \
+        return l1_host<T, true>(L1_DOTU, n, T(0), T(0), reinterpret_cast<const T*>(x), incx, x_len,                \
+                                reinterpret_cast<T*>(const_cast<CT*>(y)), incy, y_len,                             \
+                                reinterpret_cast<T*>(result), err);                                                \
+    }                                                                                                              \
+    rb_status rb_##P##dotc(size_t n, const CT* x, size_t incx, size_t x_len, const CT* y, size_t incy,             \
+                           size_t y_len, CT* result, rb_error* err) {                                              \
+        return l1_host<T, true>(L1_DOTC, n, T(0), T(0), reinterpret_cast<const T*>(x), incx, x_len,                \
+                                reinterpret_cast<T*>(const_cast<CT*>(y)), incy, y_len,                             \
+                                reinterpret_cast<T*>(result), err);                                                \
+    }                                                                                                              \
+    rb_status rb_##N##nrm2(size_t n, const CT* x, size_t incx, size_t x_len, T* result, rb_error* err) {           \
+        return l1_host<T, true>(L1_NRM2, n, T(0), T(0), reinterpret_cast<const T*>(x), incx, x_len, nullptr, 0, 0, \
+                                result, err);                                                                      \
+    }
+RB_L1_CPLX_HOST(c, sc, float, rb_complex32)
+RB_L1_CPLX_HOST(z, dz, double, rb_complex64)
+#undef RB_L1_CPLX_HOST
 
 }  // extern "C"

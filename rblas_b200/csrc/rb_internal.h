@@ -178,6 +178,17 @@ template <typename T, bool CX>
 int ger_dev(int layout, size_t m, size_t n, T ar, T ai, const T* x, long long incx, const T* y, long long incy, T* A,
             size_t lda, int conj, cudaStream_t st, int32_t* ce);
 
+// Level 1 (rb_?axpy ... rb_?nrm2 and their _dev forms). Reductions come
+// after L1_DOT; scal's vector is passed as y.
+enum L1Op : int { L1_AXPY = 0, L1_SCAL, L1_COPY, L1_SWAP, L1_DOT, L1_ASUM, L1_NRM2, L1_DOTU, L1_DOTC };
+// Device pointers; out (reductions) receives T, or {re, im} for dotu / dotc.
+template <typename T, bool CX>
+int l1_dev(int op, size_t n, T ar, T ai, const T* x, size_t incx, T* y, size_t incy, T* out, cudaStream_t st,
+           int32_t* ce);
+// rblas's argument rules for op; *noop when the call writes nothing.
+rb_status l1_check(int op, bool cx, size_t n, bool alpha_zero, bool alpha_one, size_t incx, size_t x_len,
+                   size_t incy, size_t y_len, bool have_len, bool* noop, rb_error* err);
+
 // Triangular multiply B := alpha*op(A)*B (Left) / alpha*B*op(A) (Right) through one GEMM.
 template <typename T, bool CX>
 int trmm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A, size_t lda, T* B,
