@@ -35,7 +35,9 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
+#include <vector>
 #include <type_traits>
 
 #include "../../include/rblas_b200.h"
@@ -308,15 +310,19 @@ struct OzParams {
     const int* row_exp;
     const int* col_exp;
     uint32_t* err;
-    // unit-parallel mode (unit_parallel != 0): a work item is one unit of
-    // one tile; its epilogue writes the unit's exact FP64 terms to plane u
-    // of ws (element (r, c) at r + c * ldw) and ozaki_reduce_kernel folds
-    // the planes into C in unit order, the same operations as the fused
-    // epilogue. Used when a problem has too few tiles to fill the GPU.
+    // Split tail: the last tail_tiles tiles (in raster order) run as one work
+    // item per (tile, unit). Such an item's epilogue writes the unit's exact
+    // FP64 terms to its own plane of ws (kOzTileElems doubles per tile and
+    // unit, element (row, col) of the tile at row + col * kUM), and
+    // ozaki_reduce_kernel folds the planes into C in unit order afterwards:
+    // the same operations as the fused epilogue, so the same bits. Used where
+    // whole tiles would leave SMs idle (a partial last wave, or fewer tiles
+    // than SMs). 0: every tile fused.
     double* ws;
-    size_t ldw, ws_plane;
-    int unit_parallel;
+    int tail_tiles;
 };
+
+constexpr int kOzTileElems = kUM * 256;
 
 // v * 2^x: one multiply by an exactly representable power of two (the same
 // single rounding as scalbn), scalbn only where 2^x is not a double.
@@ -328,10 +334,41 @@ __device__ __forceinline__ double scale_pow2(double v, int x) {
 
 // unit u (0-based) of a chunk covers diagonals d0 and d1 = d0 + 1 (d1 < 0
 // when absent); units go from the highest diagonals down.
-__device__ __forceinline__ void oz_unit(int slices, int u, int& d0, int& d1) {
+__host__ __device__ __forceinline__ void oz_unit(int slices, int u, int& d0, int& d1) {
     const int units = (slices + 1) / 2;
     d0 = 2 * (units - 1 - u);
     d1 = (d0 + 1 < slices) ? d0 + 1 : -1;
+}
+
+// Work item -> tile t and units [u_lo, u_hi). Items below the fused count are
+// whole tiles (tt = -1). The others are single units of the tail tiles (tt:
+// index among them), ranked by cost -- pair 0 of a chunk, the highest
+// diagonals, has the most products -- and dealt to the CTAs in a snake, so
+// a CTA that took an expensive unit in one pass takes a cheap one in the
+// next. G is the grid size; any G gives a bijection, the balance assumes the
+// fused count is a multiple of G.
+__host__ __device__ __forceinline__ void oz_item(int num_tiles, int tail_tiles, int kchunks, int upc, int G,
+                                                 int item, int& t, int& u_lo, int& u_hi, int& tt) {
+    const int fused = num_tiles - tail_tiles;
+    if (item < fused) {
+        t = item;
+        u_lo = 0;
+        u_hi = kchunks * upc;
+        tt = -1;
+        return;
+    }
+    const int j = item - fused;
+    const int total = tail_tiles * kchunks * upc;
+    const int pass = j / G, q = j - pass * G;
+    const int len = (total - pass * G < G) ? total - pass * G : G;
+    const int rank = (pass & 1) ? pass * G + (len - 1 - q) : j;
+    const int per_pair = tail_tiles * kchunks;
+    const int pair = rank / per_pair, rest = rank - pair * per_pair;
+    const int chunk = rest / tail_tiles;
+    tt = rest - chunk * tail_tiles;
+    t = fused + tt;
+    u_lo = chunk * upc + pair;
+    u_hi = u_lo + 1;
 }
 
 __global__ void __launch_bounds__(kOzThreads, 1)
@@ -365,7 +402,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const uint32_t tmem_base = bar->tmem_base;
     const int upc = (p.slices + 1) / 2;  // units per chunk
     const int units = p.kchunks * upc;
-    const int items = p.unit_parallel ? p.num_tiles * units : p.num_tiles;
+    const int items = p.num_tiles + p.tail_tiles * (units - 1);
     bool ok = true;
 
     if (warp == 0 && lane == 0) {
@@ -374,11 +411,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         prefetch_tmap(&tmB);
         uint32_t it = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            const int t = p.unit_parallel ? item / units : item;
+            int t, u_lo, u_hi, tt;
+            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
             int tm, tn;
             raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
-            const int u_lo = p.unit_parallel ? item % units : 0, u_hi = p.unit_parallel ? u_lo + 1 : units;
             for (int u = u_lo; ok && u < u_hi; ++u) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
@@ -413,7 +450,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ------------------------------ MMA issuer ------------------------------
         uint32_t it = 0, uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            const int u_lo = p.unit_parallel ? item % units : 0, u_hi = p.unit_parallel ? u_lo + 1 : units;
+            int t, u_lo, u_hi, tt;
+            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
             for (int u = u_lo; ok && u < u_hi; ++u, ++uc) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
@@ -465,14 +503,15 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         const int row_in_tile = quarter * 32 + lane;
         uint32_t uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            const int t = p.unit_parallel ? item / units : item;
+            int t, u_lo, u_hi, tt;
+            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
+            const bool split = tt >= 0;
             int tm, tn;
             raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
             const int er = row_ok ? p.row_exp[r] : kExpSentinel;
-            const int u_lo = p.unit_parallel ? item % units : 0, u_hi = p.unit_parallel ? u_lo + 1 : units;
             for (int u = u_lo; ok && u < u_hi; ++u, ++uc) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
@@ -486,10 +525,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 // digits of both operands are scaled by 2^-(e+1): weight 2^-(14+8d) per diagonal
                 const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0) - 2;
                 // C is read (beta*C0 on the first unit, the running sum after)
-                // (unit-parallel: the unit's terms go to its workspace plane, C is untouched)
-                const bool read_c = !p.unit_parallel && (!first_unit || p.beta_mode != 0);
-                const bool live = row_ok && (p.unit_parallel || !(er == kExpSentinel && !first_unit));
-                double* wplane = p.unit_parallel ? p.ws + static_cast<size_t>(u) * p.ws_plane : nullptr;
+                // (a split item: the unit's terms go to its workspace plane, C is untouched)
+                const bool read_c = !split && (!first_unit || p.beta_mode != 0);
+                const bool live = row_ok && (split || !(er == kExpSentinel && !first_unit));
+                double* wplane =
+                    split ? p.ws + (static_cast<size_t>(tt) * units + u) * kOzTileElems + row_in_tile : nullptr;
 #pragma unroll 1
                 for (int ch = 0; ch < 8; ++ch) {
                     // 16 columns at a time; the chunk's C values are requested
@@ -518,7 +558,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                                 term = scale_pow2(sv, er + fc - wexp);
                             }
                             if (wplane) {
-                                wplane[r + static_cast<size_t>(col) * p.ldw] = term;
+                                wplane[static_cast<size_t>(col0 + jj) * kUM] = term;
                             } else {
                                 double acc = cv[jj];
                                 if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
@@ -542,22 +582,29 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
 }
 
-// Unit-parallel mode: C = the fused epilogue's sequence over the unit planes,
-// element by element -- acc = beta-pass(C0) for the first unit, then
-// acc = fma(alpha, term_u, acc) in unit order; rows with a zero exponent
-// take only the first unit's step, as in the fused epilogue.
+// Split tail: C of the tail tiles = the fused epilogue's sequence over the
+// unit planes, element by element -- acc = beta-pass(C0) for the first unit,
+// then acc = fma(alpha, term_u, acc) in unit order; rows with a zero exponent
+// take only the first unit's step, as in the fused epilogue. Consecutive
+// threads take consecutive rows of a tile column (coalesced C and planes).
 __global__ void ozaki_reduce_kernel(const OzParams p, int units) {
-    const size_t total = static_cast<size_t>(p.m) * p.n;
+    const int fused = p.num_tiles - p.tail_tiles;
+    const size_t total = static_cast<size_t>(p.tail_tiles) * kOzTileElems;
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int col = static_cast<int>(idx / p.m), r = static_cast<int>(idx - static_cast<size_t>(col) * p.m);
+        const int tt = static_cast<int>(idx / kOzTileElems);
+        const int local = static_cast<int>(idx - static_cast<size_t>(tt) * kOzTileElems);
+        int tm, tn;
+        raster_tile(fused + tt, p.tiles_m, p.tiles_n, tm, tn);
+        const int r = tm * kUM + local % kUM, col = tn * 256 + local / kUM;
+        if (r >= p.m || col >= p.n) continue;
         double* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
         double acc = 0.0;
         if (p.beta_mode == 1) acc = *cp;
         else if (p.beta_mode == 2) acc = p.beta * *cp;
-        const double* w = p.ws + r + static_cast<size_t>(col) * p.ldw;
+        const double* w = p.ws + static_cast<size_t>(tt) * units * kOzTileElems + local;
         const int last = (p.row_exp[r] == kExpSentinel) ? 1 : units;
-        for (int u = 0; u < last; ++u) acc = fma(p.alpha, w[static_cast<size_t>(u) * p.ws_plane], acc);
+        for (int u = 0; u < last; ++u) acc = fma(p.alpha, w[static_cast<size_t>(u) * kOzTileElems], acc);
         *cp = acc;
     }
 }
@@ -657,8 +704,7 @@ __device__ __forceinline__ void load_tile(const T* __restrict__ x, size_t rs, si
 // result: signed 8-bit digits with y = sum_t d_t 2^-(7+8t) + rem,
 // 0 <= rem < 2^-N, and tail digits symmetric about zero, so the dropped cross
 // products do not accumulate a bias along K. No floating-point rounding
-// occurs anywhere in the extraction.
-constexpr int kMaxSlices = 12;
+// occurs anywhere in the extraction (slices: 2 to 12).
 
 // floor(x * 2^n) for |x * 2^n| < 2^94 (Int = __int128) or < 2^62 (long long)
 template <typename Int>
@@ -719,7 +765,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
         *reinterpret_cast<uint4*>(out + t * plane + off) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
 }
 
-// Host dispatch on the slice count (2 .. kMaxSlices).
+// Host dispatch on the slice count (2 .. 12).
 void launch_ozaki_slices(dim3 grid, cudaStream_t st, const double* x, size_t rs, size_t ps, int R, int K,
                          const int* e, int slices, int8_t* out, size_t kp, size_t plane) {
     switch (slices) {
@@ -919,6 +965,35 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     return e;
 }
 
+// Tail tiles to run unit by unit (OzParams::tail_tiles): the tiles of the
+// partial last wave (all tiles when there are fewer than SMs), when dealing
+// their units as oz_item does finishes clearly before one more whole tile
+// would, counting the reduce pass over their planes and C; else 0. Times are
+// modelled from the products per unit (a diagonal d has d + 1) at the B200's
+// INT8 rate per SM and its copy rate; only their ratio matters.
+int ozaki_tail_tiles(int num_tiles, int slices, int kchunks, int k, int sms) {
+    const int upc = (slices + 1) / 2;
+    if (kchunks != 1 || upc < 2 || sms < 1) return 0;
+    const int full = num_tiles / sms;
+    const int tail = num_tiles - full * sms;
+    if (tail == 0) return 0;
+    const int total = tail * upc;
+    const int G = full > 0 ? sms : std::min(total, sms);
+    std::vector<int> load(G, 0);
+    for (int j = 0; j < total; ++j) {
+        int t, lo, hi, tt, d0, d1;
+        oz_item(num_tiles, tail, 1, upc, G, num_tiles - tail + j, t, lo, hi, tt);
+        oz_unit(slices, lo % upc, d0, d1);
+        load[(num_tiles - tail + j) % G] += (d0 + 1) + (d1 >= 0 ? d1 + 1 : 0);
+    }
+    const int max_load = *std::max_element(load.begin(), load.end());
+    const double product_s = 2.0 * kUM * 256 * static_cast<double>(k) / (4.4e15 / 148);
+    const double whole_tile_s = product_s * slices * (slices + 1) / 2;
+    const double reduce_s = 4e-6 + tail * (upc + 2.0) * kOzTileElems * sizeof(double) / 6.5e12;
+    const bool fits = static_cast<size_t>(tail) * upc * kOzTileElems * sizeof(double) <= (size_t(512) << 20);
+    return (fits && product_s * max_load + reduce_s < 0.9 * whole_tile_s) ? tail : 0;
+}
+
 cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A,
                               size_t lda, const double* B, size_t ldb, double beta, double* C,
                               size_t ldc, int slices, cudaStream_t st, CUresult* cu_err) {
@@ -927,22 +1002,18 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     void* buf = nullptr;
     const size_t exps = round_up((static_cast<size_t>(m) + n) * sizeof(int), 256);
     const size_t a_bytes = round_up(slices * pa, 256);
-    // unit-parallel when the tiles alone leave SMs idle (see OzParams)
+    // the partial last wave runs unit by unit when that pays (see OzParams)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int num_tiles = ((m + kUM - 1) / kUM) * ((n + 255) / 256);
     const int upc = (slices + 1) / 2;
     const long long kt_chunk = 2147483647LL / (static_cast<long long>(slices) * 128 * 128) / 128;
-    const bool one_chunk = (k + 127) / 128 <= kt_chunk;
-    const size_t plane = static_cast<size_t>(m) * n;
-    // only while the tiles leave at least half the SMs idle: near a full wave
-    // (2048^3: 128 tiles) the fused epilogue wins (measured 44.7 vs 32.3
-    // TFLOP/s), well below one it loses (1024^3: 9.5 vs 15.7)
-    const bool unit_parallel = one_chunk && 2 * num_tiles <= sms && upc > 1 &&
-                               upc * plane * sizeof(double) <= (size_t(512) << 20);
+    const long long ktc = std::max(kt_chunk, 1LL);
+    const int kchunks = static_cast<int>(((k + 127) / 128 + ktc - 1) / ktc);
+    const int tail_tiles = ozaki_tail_tiles(num_tiles, slices, kchunks, k, sms);
     const size_t b_bytes = round_up(slices * pb, 256);
-    const size_t w_bytes = unit_parallel ? upc * plane * sizeof(double) : 0;
+    const size_t w_bytes = static_cast<size_t>(tail_tiles) * upc * kOzTileElems * sizeof(double);
     cudaError_t e = scratch_alloc(&buf, exps + a_bytes + b_bytes + w_bytes, st);
     if (e != cudaSuccess) return e;
     int* ea = static_cast<int*>(buf);
@@ -987,11 +1058,9 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     p.c = C; p.ldc = ldc;
     p.row_exp = ea; p.col_exp = eb;
     p.err = device_error_word();
-    if (unit_parallel) {
-        p.unit_parallel = 1;
+    if (tail_tiles > 0) {
+        p.tail_tiles = tail_tiles;
         p.ws = reinterpret_cast<double*>(static_cast<uint8_t*>(buf) + exps + a_bytes + b_bytes);
-        p.ldw = static_cast<size_t>(m);
-        p.ws_plane = plane;
     }
 
     constexpr int smem = kOzST * kOzStage + 256 + 1024;
@@ -1001,16 +1070,17 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
         if (e != cudaSuccess) { cudaFreeAsync(buf, st); return e; }
         attr = true;
     }
-    const int items = unit_parallel ? p.num_tiles * upc : p.num_tiles;
+    const int items = p.num_tiles + p.tail_tiles * (p.kchunks * upc - 1);
     const int grid = items < sms ? items : sms;
     KernelTimer tmr;
     kernel_timing_begin("umma_ozaki_i8", 2.0 * m * n * static_cast<double>(k) * slices * (slices + 1) / 2, st, &tmr);
     ozaki_gemm_kernel<<<grid, kOzThreads, smem, st>>>(tma, tmb, p);
     kernel_timing_end(&tmr, st);
     count_launch();
-    if (unit_parallel) {
-        const size_t blocks = std::min<size_t>((plane + 255) / 256, static_cast<size_t>(sms) * 16);
-        ozaki_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(p, upc);
+    if (p.tail_tiles > 0) {
+        const size_t elems = static_cast<size_t>(p.tail_tiles) * kOzTileElems;
+        const size_t blocks = std::min<size_t>((elems + 255) / 256, static_cast<size_t>(sms) * 16);
+        ozaki_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(p, p.kchunks * upc);
         count_launch();
     }
     e = cudaGetLastError();

@@ -190,10 +190,15 @@ def test_config_sizes_error_report():
 
 @pytest.mark.parametrize("layout,ta,tb,m,n,k", [(Layout.ColMajor, 0, 0, 300, 257, 513),
                                                  (Layout.RowMajor, 1, 1, 1000, 900, 700),
-                                                 (Layout.ColMajor, 1, 0, 64, 64, 4096)])
+                                                 (Layout.ColMajor, 1, 0, 64, 64, 4096),
+                                                 (Layout.ColMajor, 0, 0, 2560, 2048, 512),
+                                                 (Layout.RowMajor, 1, 0, 3200, 2048, 1024)])
 def test_ozaki_unit_parallel_matches_fused_epilogue_exactly(layout, ta, tb, m, n, k):
-    """Problems with fewer tiles than SMs run one diagonal-pair unit per CTA
-    and fold the units' exact terms in unit order afterwards; that is the
+    """Tiles that would leave SMs idle -- all of them when there are fewer
+    tiles than SMs (the first three shapes), the partial last wave otherwise
+    (2560 x 2048: one full wave of 148 tiles and 12 split; 3200 x 2048: 52
+    split, dealt over two snake passes) -- run one diagonal-pair unit per work
+    item and fold the units' exact terms in unit order afterwards; that is the
     fused epilogue's arithmetic, so the result equals the fused path's (run
     here through the allocation-free entry point, which always fuses) bit
     for bit -- including a zero row, a zero column and beta = 0 with NaN C."""
