@@ -280,20 +280,24 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 //
 // Slice products of equal weight (t + u = d: digit t has weight 2^-(7+8t))
 // form diagonal d; S_d = sum_{t+u=d} A_t B_u^T is exact in INT32 over a K
-// chunk. Diagonals are processed two at a time ("units" {d0, d0+1}) with
-// both accumulators in TMEM (2 x 256 columns): for each B slice j the stage
-// holds B_j and the two A slices it pairs with, A_{d0-j} -> S_d0 and
-// A_{d0+1-j} -> S_{d0+1}, so every B tile feeds two MMAs. The epilogue
-// folds the unit exactly, S_d0 * 2^8 + S_{d0+1} (< 2^40), scales by
-// alpha * 2^(e_i + f_j + 2 - 14 - 8(d0+1)) and accumulates into C in FP64;
-// units run from the smallest weight up, the first one adding beta*C0.
+// chunk. Diagonals are processed two at a time ("units" {d0, d1 = d0+1})
+// with both accumulators in TMEM (2 x 256 columns). For each K tile the
+// stages walk the A slices i = d1 .. 0, stage i holding A_i and B_{d1-i}:
+// S_d1 takes A_i x B_{d1-i} from the stage, S_d0 takes A_i x B_{d0-i}, which
+// is the B tile of the previous stage. So every stage brings one new A and
+// one new B tile (48 KiB) for two MMAs, and a stage is released once the
+// next one's MMAs have been issued. (The order of the INT32 additions does
+// not change the exact sums.) The epilogue folds the unit exactly,
+// S_d0 * 2^8 + S_d1 (< 2^40), scales by alpha * 2^(e_i + f_j + 2 - 14 -
+// 8 d1) and accumulates into C in FP64; units run from the smallest weight
+// up, the first one adding beta*C0.
 // Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 epilogue (two
 // warps per TMEM lane quarter, 128 columns each).
 // ------------------------------------------------------------------------------
 
 __host__ __device__ constexpr uint32_t kBTileOz() { return 256u * kRowBytes; }
-constexpr int kOzST = 3;                         // stages of (B_j, A, A)
-constexpr int kOzStage = 2 * kATile + 256 * kRowBytes;  // 64 KiB
+constexpr int kOzST = 4;                            // stages of (B_{d1-i}, A_i)
+constexpr int kOzStage = kATile + 256 * kRowBytes;  // 48 KiB
 constexpr int kOzThreads = 320;
 
 struct OzParams {
@@ -420,24 +424,20 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                const int jmax = d1 >= 0 ? d1 : d0;
-                for (int j = 0; ok && j <= jmax; ++j) {
-                    const bool a0 = j <= d0, a1 = d1 >= 0;  // A_{d0-j} valid; A_{d1-j} valid (j <= d1)
-                    const uint32_t bytes = kBTileOz() + (a0 ? kATile : 0) + (a1 ? kATile : 0);
-                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                const int top = d1 >= 0 ? d1 : d0;
+                for (int kt = kt0; ok && kt < kt1; ++kt) {
+                    const int k0 = kt * 128;
+                    for (int i = top; ok && i >= 0; --i, ++it) {  // stage: A_i and B_{top-i}
                         const int s = it % ST;
                         if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x301)) {
                             ok = false;
                             break;
                         }
                         uint8_t* sb = smem + s * kOzStage;
-                        uint8_t* sa0 = sb + kBTileOz();
-                        uint8_t* sa1 = sa0 + kATile;
-                        mbar_arrive_expect_tx(&bar->full[s], bytes);
-                        const int k0 = kt * 128;
-                        tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, j);
-                        if (a0) tma_load_3d(sa0, &tmA, &bar->full[s], k0, m0, d0 - j);
-                        if (a1) tma_load_3d(sa1, &tmA, &bar->full[s], k0, m0, d1 - j);
+                        uint8_t* sa = sb + kBTileOz();
+                        mbar_arrive_expect_tx(&bar->full[s], kBTileOz() + kATile);
+                        tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, top - i);
+                        tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, i);
                     }
                 }
             }
@@ -456,18 +456,21 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                const int jmax = d1 >= 0 ? d1 : d0;
                 if (uc >= 1 && !mbar_wait(&bar->acc_empty[0], (uc - 1) & 1, p.err, 0x302)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                uint32_t acc0 = 0, acc1 = 0;
-                for (int j = 0; ok && j <= jmax; ++j) {
-                    const bool a0 = j <= d0, a1 = d1 >= 0;
-                    constexpr uint32_t id0 = umma_idesc(2, 1, kUM, UN);  // s32 <- s8 x s8
-                    constexpr uint32_t id1 = id0;
-                    for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                // S_top (d1, or d0 alone) at tmem_base + UN for a pair, tmem_base
+                // otherwise; S_d0 of a pair at tmem_base (the epilogue's layout)
+                const bool pair = d1 >= 0;
+                const int top = pair ? d1 : d0;
+                const uint32_t acc_top = pair ? tmem_base + UN : tmem_base;
+                constexpr uint32_t idesc = umma_idesc(2, 1, kUM, UN);  // s32 <- s8 x s8
+                uint32_t f_top = 0, f_low = 0;
+                for (int kt = kt0; ok && kt < kt1; ++kt) {
+                    int prev_s = -1;
+                    for (int i = top; ok && i >= 0; --i, ++it) {
                         const int s = it % ST;
                         if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x303)) {
                             ok = false;
@@ -475,21 +478,29 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         }
                         tc_fence_after();
                         const uint32_t sb = smem_u32(smem + s * kOzStage);
-                        const uint32_t sa0 = sb + kBTileOz(), sa1 = sa0 + kATile;
+                        const uint32_t sa = sb + kBTileOz();
+                        const bool low = pair && prev_s >= 0;  // A_i x B_{d0-i}: the previous stage's B
+                        const uint32_t pb = low ? smem_u32(smem + prev_s * kOzStage) : 0u;
 #pragma unroll
                         for (int kk = 0; kk < KSTEPS; ++kk) {
-                            const uint64_t bd = sw128_kmajor_desc(sb) + 2 * kk;
-                            if (a0) {
-                                umma_i8(tmem_base, sw128_kmajor_desc(sa0) + 2 * kk, bd, id0, acc0);
-                                acc0 = 1;
-                            }
-                            if (a1) {
-                                umma_i8(tmem_base + UN, sw128_kmajor_desc(sa1) + 2 * kk, bd, id1, acc1);
-                                acc1 = 1;
+                            const uint64_t ad = sw128_kmajor_desc(sa) + 2 * kk;
+                            umma_i8(acc_top, ad, sw128_kmajor_desc(sb) + 2 * kk, idesc, f_top);
+                            f_top = 1;
+                            if (low) {
+                                umma_i8(tmem_base, ad, sw128_kmajor_desc(pb) + 2 * kk, idesc, f_low);
+                                f_low = 1;
                             }
                         }
-                        tc_commit(&bar->empty[s]);
+                        // the previous stage is consumed once these MMAs complete;
+                        // without a pair the stage itself is
+                        if (pair) {
+                            if (prev_s >= 0) tc_commit(&bar->empty[prev_s]);
+                            prev_s = s;
+                        } else {
+                            tc_commit(&bar->empty[s]);
+                        }
                     }
+                    if (pair && prev_s >= 0) tc_commit(&bar->empty[prev_s]);
                 }
                 if (ok) tc_commit(&bar->acc_full[0]);
             }
