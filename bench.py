@@ -396,9 +396,9 @@ def run_ours(args):
         psrc = "FP64 DFMA throughput measured in-run by rb_probe_fma_peak_tflops; not in MEASURED_PEAKS.json"
     # DRAM bytes per launch of the dominant kernel, measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
-    # the step's shapes: 2.562 GB at 4096^3 (x4 per step), 1.268 GB at
+    # the step's shapes: 2.516 GB at 4096^3 (x4 per step), 1.297 GB at
     # 3000x5000x2048 (x1)
-    traffic = (4 * 2.562e9 + 1.268e9) / 5 if kname == "umma_ozaki_i8" else None
+    traffic = (4 * 2.516e9 + 1.297e9) / 5 if kname == "umma_ozaki_i8" else None
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                 "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over "
