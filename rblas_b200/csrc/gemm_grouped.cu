@@ -208,6 +208,7 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         } else {
             if (!mbar_wait(&item_full[slot], (q >> 1) & 1, err, 0x112)) return;
             item = item_slot[slot];
+            __threadfence_block();  // each lane's read of the slot precedes the release
             __syncwarp();
             if (lane == 0) mbar_arrive(&item_empty[slot]);
         }

@@ -1,12 +1,16 @@
-// simt_tile.cuh -- the plain (SIMT FFMA / DFMA) GEMM tile pipeline, shared by
-// the single-problem kernel (gemm_simt.cu) and the grouped persistent kernel
-// (gemm_grouped.cu).
+// simt_tile.cuh -- the plain GEMM tile pipeline, shared by the single-problem
+// kernel (gemm_simt.cu) and the grouped persistent kernel (gemm_grouped.cu):
+// true-FP32 SGEMM on FFMA, FP64 DGEMM on the FP64 tensor cores (mma.sync
+// m16n8k8 f64, DMMA).
 //
-// One C tile = BM x BN. 8 compute warps (2 along M x 4 along N, each lane an
-// 8 x TN register tile) consume a STAGES-deep ring of shared-memory stages
-// that one producer lane fills with TMA. A K-major operand tile lands as
-// [mn][k] 128-byte rows with the hardware 128-byte swizzle; an MN-major tile
-// as [k][mn] rows, unswizzled. Both read patterns are bank-conflict free.
+// One C tile = BM x BN. 8 compute warps (2 along M x 4 along N) consume a
+// STAGES-deep ring of shared-memory stages that one producer lane fills with
+// TMA. f32: each lane an 8 x TN register tile of FFMA. f64: each warp a
+// 64 x 16 tile of 4 x 2 DMMA blocks (16 x 8 each, 4 accumulators per lane;
+// the same 32 values per lane as an 8 x 4 register tile). A K-major operand
+// tile lands as [mn][k] 128-byte rows with the hardware 128-byte swizzle; an
+// MN-major tile as [k][mn] rows, unswizzled. All read patterns are
+// bank-conflict free.
 // The ring's mbarrier phases run on a counter `it` that continues across
 // tiles, so a persistent CTA streams tile after tile through one ring.
 #pragma once
@@ -99,12 +103,114 @@ struct SimtOut {
     int tri;        // 0 full C; 1 upper triangle only (row <= col); 2 lower (row >= col)
 };
 
+// ---- f64 on the tensor cores (DMMA) -------------------------------------------
+// mma.sync m16n8k8 f64, lane = 4g + t:
+//   a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]}   (16 x 8, row-major)
+//   b = {B[t][g], B[t+4][g]}                             (8 x 8, col-major)
+//   c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]} (16 x 8)
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+__device__ __forceinline__ double lds64(const uint8_t* p) { return *reinterpret_cast<const double*>(p); }
+__device__ __forceinline__ double2 lds128d(const uint8_t* p) { return *reinterpret_cast<const double2*>(p); }
+// byte offset of element k of row `row` in a 128-byte-swizzled [row][16 doubles] tile
+__device__ __forceinline__ int swz64(int row, int k) { return row * 128 + ((((k >> 1) ^ (row & 7))) << 4) + ((k & 1) << 3); }
+
+// Which C element DMMA accumulator q of block (mb, nb) holds, in the warp's
+// 64 x 16 tile. K-major operands keep the fragment's natural rows / columns.
+// An MN-major operand is read 16 bytes at a time: fragment rows g and g+8 of
+// an A block are the adjacent rows 2g, 2g+1, and fragment column j of B
+// block nb is column 2j + nb, so each lane's load brings both values and a
+// quarter-warp reads one 128-byte row segment.
+template <bool A_K>
+__device__ __forceinline__ int dmma_row(int mb, int q, int g) {
+    const int hi = q >> 1;  // q = 2, 3: fragment row g + 8
+    return mb * 16 + (A_K ? g + 8 * hi : 2 * g + hi);
+}
+template <bool B_K>
+__device__ __forceinline__ int dmma_col(int nb, int q, int t) {
+    const int j = 2 * t + (q & 1);
+    return B_K ? nb * 8 + j : 2 * j + nb;
+}
+
+template <bool A_K, bool B_K>
+__device__ __forceinline__ bool dmma_mainloop(double (&acc)[8][4], int num_kt, const uint8_t* smem, int stage_stride,
+                                              uint64_t* full, uint64_t* empty, uint32_t& it, uint32_t* err,
+                                              int warp, int lane) {
+    using Cfg = SimtCfg<double>;
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, ST = Cfg::STAGES;
+    constexpr int A_BYTES = simt_a_bytes<double>();
+    static_assert(BK == 16 && BM == 128 && BN == 64, "the DMMA tile assumes 128 x 64 x 16");
+    const int wm0 = (warp & 1) * 64, wn0 = (warp >> 1) * 16;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = 0.0;
+
+    for (int kt = 0; kt < num_kt; ++kt, ++it) {
+        const int s = it % ST;
+        if (!mbar_wait(&full[s], (it / ST) & 1, err, 0x102)) return false;
+        const uint8_t* sa = smem + s * stage_stride;
+        const uint8_t* sb = sa + A_BYTES;
+#pragma unroll
+        for (int ks = 0; ks < BK; ks += 8) {
+            double a[4][4], b[2][2];
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb) {
+                if constexpr (A_K) {
+                    const int row = wm0 + mb * 16 + g;  // row & 7 == g: the 8 rows' chunks differ
+                    a[mb][0] = lds64(sa + swz64(row, ks + t));
+                    a[mb][1] = lds64(sa + swz64(row + 8, ks + t));
+                    a[mb][2] = lds64(sa + swz64(row, ks + t + 4));
+                    a[mb][3] = lds64(sa + swz64(row + 8, ks + t + 4));
+                } else {
+                    const int m = wm0 + mb * 16 + 2 * g;
+                    const double2 v0 = lds128d(sa + ((ks + t) * BM + m) * 8);
+                    const double2 v1 = lds128d(sa + ((ks + t + 4) * BM + m) * 8);
+                    a[mb][0] = v0.x; a[mb][1] = v0.y; a[mb][2] = v1.x; a[mb][3] = v1.y;
+                }
+            }
+            if constexpr (B_K) {
+#pragma unroll
+                for (int nb = 0; nb < 2; ++nb) {
+                    const int row = wn0 + nb * 8 + g;
+                    b[nb][0] = lds64(sb + swz64(row, ks + t));
+                    b[nb][1] = lds64(sb + swz64(row, ks + t + 4));
+                }
+            } else {
+                const int n = wn0 + 2 * g;
+                const double2 v0 = lds128d(sb + ((ks + t) * BN + n) * 8);
+                const double2 v1 = lds128d(sb + ((ks + t + 4) * BN + n) * 8);
+                b[0][0] = v0.x; b[1][0] = v0.y; b[0][1] = v1.x; b[1][1] = v1.y;
+            }
+#pragma unroll
+            for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+                for (int nb = 0; nb < 2; ++nb) dmma_16x8x8(acc[mb * 2 + nb], a[mb], b[nb]);
+        }
+        // every lane's shared-memory reads of the stage are ordered before
+        // the warp's release (lane 0's arrive orders only its own accesses,
+        // and __syncwarp alone did not keep in-flight reads ahead of the
+        // producer's next TMA write into the stage)
+        __threadfence_block();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    return true;
+}
+
 // Compute warps: consume num_kt stages from ring iteration it into the
 // thread's 8 x TN accumulator. Returns false if a wait gave up.
 template <typename T, bool A_K, bool B_K>
 __device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T>::TN], int num_kt, const uint8_t* smem,
                                               int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
                                               uint32_t* err, int warp, int lane) {
+    if constexpr (sizeof(T) == 8) {
+        return dmma_mainloop<A_K, B_K>(acc, num_kt, smem, stage_stride, full, empty, it, err, warp, lane);
+    }
     using Cfg = SimtCfg<T>;
     constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, TN = Cfg::TN, ST = Cfg::STAGES;
     constexpr int VEC = Vec16<T>::N;  // elements per 16-byte load
@@ -183,6 +289,11 @@ __device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T>::TN], int n
 #pragma unroll
                     for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[q][i], b[q][j], acc[i][j]);
         }
+        // every lane's shared-memory reads of the stage are ordered before
+        // the warp's release (lane 0's arrive orders only its own accesses,
+        // and __syncwarp alone did not keep in-flight reads ahead of the
+        // producer's next TMA write into the stage)
+        __threadfence_block();
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
@@ -196,6 +307,28 @@ __device__ __forceinline__ void simt_epilogue(const SimtOut<T>& o, const T (&acc
     constexpr int TN = SimtCfg<T>::TN;
     constexpr int VEC = Vec16<T>::N;
     const int wm = warp & 1, wn = warp >> 1;
+    if constexpr (sizeof(T) == 8) {
+        // DMMA accumulators: acc[mb * 2 + nb][q], placed by dmma_row / dmma_col
+        const int g = lane >> 2, tq = lane & 3;
+        const int wm0 = wm * 64, wn0 = wn * 16;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = m0 + wm0 + dmma_row<A_K>(i >> 1, q, g);
+                const int cidx = n0 + wn0 + dmma_col<B_K>(i & 1, q, tq);
+                if (r >= o.m || cidx >= o.n) continue;
+                if ((o.tri == 1 && r > cidx) || (o.tri == 2 && r < cidx)) continue;
+                T* cp = o.c + r + static_cast<size_t>(cidx) * o.ldc;
+                T tv = T(0);
+                if (o.beta_mode != 0) {
+                    const T cv = o.cin[r + static_cast<size_t>(cidx) * o.ldcin];
+                    tv = (o.beta_mode == 1) ? cv : o.beta * cv;
+                }
+                *cp = fma(o.alpha, acc[i][q], tv);
+            }
+        return;
+    }
     const int lane_m = lane & 7, lane_n = lane >> 3;
     const int wm0 = wm * 64, wn0 = wn * (4 * TN);
 #pragma unroll
