@@ -393,7 +393,8 @@ def run_ours(args):
         psrc = "INT8 tcgen05 throughput measured in-run by rb_probe_tensor_peak_tflops (back-to-back M128 N256 K32 UMMAs, smem operands); not in MEASURED_PEAKS.json"
     else:
         peak, unit, bound = peaks["fp64_fma_tflops"], "TFLOP/s", "fp64"
-        psrc = "FP64 DFMA throughput measured in-run by rb_probe_fma_peak_tflops; not in MEASURED_PEAKS.json"
+        psrc = ("FP64 throughput measured in-run by rb_probe_fma_peak_tflops (DFMA; the plain DGEMM runs on DMMA, "
+                "whose peak on this GPU measured the same, 36.8-37.0 TFLOP/s); not in MEASURED_PEAKS.json")
     # DRAM bytes per launch of the dominant kernel, measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
     # the step's shapes: 2.516 GB at 4096^3 (x4 per step), 1.297 GB at

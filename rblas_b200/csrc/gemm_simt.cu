@@ -1,10 +1,11 @@
-// gemm_simt.cu -- the plain GEMM forms: true-FP32 SGEMM and FP64 DGEMM on the
-// CUDA cores (FFMA / DFMA), fed by TMA.
+// gemm_simt.cu -- the plain GEMM forms, fed by TMA: true-FP32 SGEMM on the
+// CUDA cores (FFMA) and FP64 DGEMM on the FP64 tensor cores (mma.sync f64;
+// the tile code is in simt_tile.cuh).
 //
 // Replaces rblas's CPU blocking driver, packing and microkernels
 // (src/kernel/gemm.rs:185-429, src/kernel/gemm_avx2.rs:26-155). sm_100's
-// tensor cores have no FP32xFP32 product and tcgen05 has no f64 kind, so the
-// plain (drop-in) forms run here; the tensor-core forms live elsewhere.
+// tcgen05 has no FP32xFP32 product and no f64 kind, so the plain (drop-in)
+// forms run here; the tcgen05 precision forms live elsewhere.
 //
 // Structure (one CTA per C tile, 8 compute warps + 1 TMA producer warp):
 //   producer lane 0: for each K tile, wait `empty[s]`, arm `full[s]` with the
