@@ -498,7 +498,8 @@ public:
             CUresult r = CUDA_SUCCESS;
             if (pl.num_kt > 0) {
                 r = a_k ? make_tmap_2d(&g.tmA, a, dt, el, pl.k, pl.m, lda, BK, BM, true)
-                        : make_tmap_2d(&g.tmA, a, dt, el, pl.m, pl.k, lda, BM, BK, false);
+                        : make_tmap_2d(&g.tmA, a, dt, el, pl.m, pl.k, lda, simt_mn_a_box(el), BK,
+                                       simt_mn_a_swizzled(el));
                 if (r == CUDA_SUCCESS)
                     r = b_k ? make_tmap_2d(&g.tmB, b, dt, el, pl.k, pl.n, ldb, BK, BN, true)
                             : make_tmap_2d(&g.tmB, b, dt, el, pl.n, pl.k, ldb, BN, BK, false);

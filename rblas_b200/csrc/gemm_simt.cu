@@ -146,7 +146,8 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
     if (a_kmajor)
         r = make_tmap_2d(&ta, A, tmap_dtype<T>(), sizeof(T), k, m, lda, Cfg::BK, Cfg::BM, true);
     else
-        r = make_tmap_2d(&ta, A, tmap_dtype<T>(), sizeof(T), m, k, lda, Cfg::BM, Cfg::BK, false);
+        r = make_tmap_2d(&ta, A, tmap_dtype<T>(), sizeof(T), m, k, lda, simt_mn_a_box(sizeof(T)), Cfg::BK,
+                         simt_mn_a_swizzled(sizeof(T)));
     if (r != CUDA_SUCCESS) { if (cu_err) *cu_err = r; return cudaErrorInvalidValue; }
     // op(B) is k x n: K-major when stored k x n (NoTrans), else stored n x k.
     if (b_kmajor)

@@ -51,6 +51,13 @@ constexpr int simt_smem_bytes() {
     return Cfg::STAGES * (Cfg::BM + Cfg::BN) * Cfg::BK * (int)sizeof(T) + 2 * Cfg::STAGES * 8 + 1024;
 }
 
+// An MN-major f64 A tile lands as BM/16 boxes of 16 m x BK k, each [k][16 m]
+// with the 128-byte swizzle (2 KiB apiece), so that the DMMA fragment reads
+// below are bank-conflict free; every other MN-major tile is one unswizzled
+// [k][mn] box. Box rows (mn) of the A tensor map and its swizzle, by element size.
+__host__ __device__ constexpr uint32_t simt_mn_a_box(size_t elem) { return elem == 8 ? 16u : 128u; }
+__host__ __device__ constexpr bool simt_mn_a_swizzled(size_t elem) { return elem == 8; }
+
 // Byte offsets of the A and B tiles inside a stage.
 template <typename T>
 __host__ __device__ constexpr int simt_a_bytes() { return SimtCfg<T>::BM * SimtCfg<T>::BK * (int)sizeof(T); }
@@ -81,8 +88,14 @@ __device__ __forceinline__ bool simt_produce(const CUtensorMap* tmA, const CUten
         uint8_t* sb = sa + A_BYTES;
         mbar_arrive_expect_tx(&full[s], TX);
         const int k0 = (kt0 + kt) * BK;
-        if (A_K) tma_load_2d(sa, tmA, &full[s], k0, m0);
-        else     tma_load_2d(sa, tmA, &full[s], m0, k0);
+        if constexpr (A_K) {
+            tma_load_2d(sa, tmA, &full[s], k0, m0);
+        } else if constexpr (simt_mn_a_swizzled(sizeof(T))) {
+#pragma unroll
+            for (int c = 0; c < Cfg::BM / 16; ++c) tma_load_2d(sa + c * 2048, tmA, &full[s], m0 + 16 * c, k0);
+        } else {
+            tma_load_2d(sa, tmA, &full[s], m0, k0);
+        }
         if (B_K) tma_load_2d(sb, tmB, &full[s], k0, n0);
         else     tma_load_2d(sb, tmB, &full[s], n0, k0);
     }
@@ -122,8 +135,11 @@ __device__ __forceinline__ int swz64(int row, int k) { return row * 128 + ((((k 
 // 64 x 16 tile. K-major operands keep the fragment's natural rows / columns.
 // An MN-major operand is read 16 bytes at a time: fragment rows g and g+8 of
 // an A block are the adjacent rows 2g, 2g+1, and fragment column j of B
-// block nb is column 2j + nb, so each lane's load brings both values and a
-// quarter-warp reads one 128-byte row segment.
+// block nb is column 2j + nb, so each lane's load brings both values.
+// With an MN-major A the fragment's k slots t and t+4 also take the physical
+// k rows 2t and 2t+1 (for A and B alike; the k order of a sum of exact
+// products changes nothing): a quarter-warp's A reads then fall on 8
+// distinct swizzle chunks of the [k][16 m] boxes, one wavefront.
 template <bool A_K>
 __device__ __forceinline__ int dmma_row(int mb, int q, int g) {
     const int hi = q >> 1;  // q = 2, 3: fragment row g + 8
@@ -167,23 +183,33 @@ __device__ __forceinline__ bool dmma_mainloop(double (&acc)[8][4], int num_kt, c
                     a[mb][2] = lds64(sa + swz64(row, ks + t + 4));
                     a[mb][3] = lds64(sa + swz64(row + 8, ks + t + 4));
                 } else {
-                    const int m = wm0 + mb * 16 + 2 * g;
-                    const double2 v0 = lds128d(sa + ((ks + t) * BM + m) * 8);
-                    const double2 v1 = lds128d(sa + ((ks + t + 4) * BM + m) * 8);
+                    // box (wm0 + 16 mb) / 16, rows k = ks + 2t, ks + 2t + 1, chunk g (m = 2g, 2g + 1)
+                    const uint8_t* box = sa + ((wm0 >> 4) + mb) * 2048;
+                    const int k0r = ks + 2 * t, k1r = k0r + 1;
+                    const double2 v0 = lds128d(box + k0r * 128 + ((g ^ (k0r & 7)) << 4));
+                    const double2 v1 = lds128d(box + k1r * 128 + ((g ^ (k1r & 7)) << 4));
                     a[mb][0] = v0.x; a[mb][1] = v0.y; a[mb][2] = v1.x; a[mb][3] = v1.y;
                 }
             }
+            // B follows A's k slots: t, t+4 (K-major A) or 2t, 2t+1 (MN-major A)
             if constexpr (B_K) {
 #pragma unroll
                 for (int nb = 0; nb < 2; ++nb) {
                     const int row = wn0 + nb * 8 + g;
-                    b[nb][0] = lds64(sb + swz64(row, ks + t));
-                    b[nb][1] = lds64(sb + swz64(row, ks + t + 4));
+                    if constexpr (A_K) {
+                        b[nb][0] = lds64(sb + swz64(row, ks + t));
+                        b[nb][1] = lds64(sb + swz64(row, ks + t + 4));
+                    } else {
+                        const double2 v = lds128d(sb + swz64(row, ks + 2 * t));  // k = ks+2t, ks+2t+1
+                        b[nb][0] = v.x;
+                        b[nb][1] = v.y;
+                    }
                 }
             } else {
                 const int n = wn0 + 2 * g;
-                const double2 v0 = lds128d(sb + ((ks + t) * BN + n) * 8);
-                const double2 v1 = lds128d(sb + ((ks + t + 4) * BN + n) * 8);
+                const int k0r = A_K ? ks + t : ks + 2 * t, k1r = A_K ? ks + t + 4 : ks + 2 * t + 1;
+                const double2 v0 = lds128d(sb + (k0r * BN + n) * 8);
+                const double2 v1 = lds128d(sb + (k1r * BN + n) * 8);
                 b[0][0] = v0.x; b[1][0] = v0.y; b[0][1] = v1.x; b[1][1] = v1.y;
             }
 #pragma unroll
