@@ -171,3 +171,39 @@ def test_pipelined_host_call_matches_device_call_exactly(dtype, prec, layout, ta
                     dtype, prec=Precision(prec))
     torch.cuda.synchronize()
     assert np.array_equal(host, Cd.cpu().numpy())
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_long_k_results_repeat_bit_for_bit(dtype, ta, tb):
+    """Each compute warp fences its shared-memory reads before releasing a
+    pipeline stage. Without that fence the producer's next TMA write could
+    land under reads still in flight, which showed up as whole 16-row
+    fragment blocks wrong, differently from call to call, once K spanned
+    many stages. Three calls on 512^3 must agree bit for bit and with the
+    restatement."""
+    torch = pytest.importorskip("torch")
+    m = n = k = 512
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    g = torch.Generator(device="cuda")
+    g.manual_seed(31 + 2 * ta + tb)
+    A = torch.randn(m * k, dtype=tdt, device="cuda", generator=g)
+    B = torch.randn(k * n, dtype=tdt, device="cuda", generator=g)
+    lda, ldb = (k if ta else m), (n if tb else k)
+    outs = []
+    for _ in range(3):
+        C = torch.zeros(m * n, dtype=tdt, device="cuda")
+        level3.gemm_dev(Layout.ColMajor, ta, tb, m, n, k, 1.0, A.data_ptr(), lda, B.data_ptr(), ldb, 0.0,
+                        C.data_ptr(), m, dtype)
+        torch.cuda.synchronize()
+        outs.append(C.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    a = A.cpu().numpy().astype(np.float64).reshape((k, m) if not ta else (m, k)).T  # column-major views
+    b = B.cpu().numpy().astype(np.float64).reshape((n, k) if not tb else (k, n)).T
+    opa = a.T if ta else a
+    opb = b.T if tb else b
+    ref = opa @ opb
+    got = outs[0].astype(np.float64).reshape(n, m).T
+    u = 2.0 ** -24 if dtype == np.float32 else 2.0 ** -53
+    err = np.linalg.norm(got - ref) / (np.linalg.norm(opa) * np.linalg.norm(opb))
+    assert err <= 4 * k * u, err
