@@ -291,14 +291,20 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // S_d0 * 2^8 + S_d1 (< 2^40), scales by alpha * 2^(e_i + f_j + 2 - 14 -
 // 8 d1) and accumulates into C in FP64; units run from the smallest weight
 // up, the first one adding beta*C0.
-// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 epilogue (two
-// warps per TMEM lane quarter, 128 columns each).
+// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..17 epilogue (four
+// warps per TMEM lane quarter, 64 columns each). The epilogue runs while the
+// tensor cores wait for the accumulators, so it is written for latency: 16
+// warps, a per-warp table of the tile's column scales in shared memory, and
+// the first chunk's C values requested before the accumulator wait.
 // ------------------------------------------------------------------------------
 
 __host__ __device__ constexpr uint32_t kBTileOz() { return 256u * kRowBytes; }
 constexpr int kOzST = 4;                            // stages of (B_{d1-i}, A_i)
 constexpr int kOzStage = kATile + 256 * kRowBytes;  // 48 KiB
-constexpr int kOzThreads = 320;
+constexpr int kOzEpiWarps = 16;
+constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;
+constexpr int kOzColTab = 64 * (8 + 4);             // per epilogue warp: 2^fc (double) and fc (int), 64 columns
+constexpr int kOzSmem = kOzST * kOzStage + 256 + kOzEpiWarps * kOzColTab + 1024;
 
 struct OzParams {
     int m, n, k;
@@ -327,6 +333,11 @@ struct OzParams {
 };
 
 constexpr int kOzTileElems = kUM * 256;
+
+// 2^x for x in [-1022, 1023]
+__device__ __forceinline__ double pow2_normal(int x) {
+    return __longlong_as_double(static_cast<long long>(x + 1023) << 52);
+}
 
 // v * 2^x: one multiply by an exactly representable power of two (the same
 // single rounding as scalbn), scalbn only where 2^x is not a double.
@@ -392,7 +403,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             mbar_init(&bar->empty[s], 1);
         }
         mbar_init(&bar->acc_full[0], 1);
-        mbar_init(&bar->acc_empty[0], 8);
+        mbar_init(&bar->acc_empty[0], kOzEpiWarps);
         mbar_init(&bar->drain, 1);
         fence_barrier_init();
     }
@@ -509,9 +520,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         mbar_wait_drain(&bar->drain, 0);
     } else if (warp >= 2) {
         // ------------------------------ epilogue ------------------------------
-        const int quarter = warp & 3;
-        const int half = (warp - 2) >> 2;  // which 128 columns
+        const int quarter = warp & 3;      // TMEM lanes 32*quarter.. (the warp's rank in its warpgroup)
+        const int cq = (warp - 2) >> 2;    // columns 64*cq .. 64*cq+63 of the tile
         const int row_in_tile = quarter * 32 + lane;
+        // this warp's column table: 2^fc where fc is in [-1022, 1023], else 0
+        // (a zero or absent column, or an exponent outside the normal range),
+        // and fc itself
+        uint8_t* tab = smem + ST * kOzStage + 256 + (warp - 2) * kOzColTab;
+        double* col_scale = reinterpret_cast<double*>(tab);
+        int* col_e = reinterpret_cast<int*>(tab + 64 * sizeof(double));
+        const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
         uint32_t uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
             int t, u_lo, u_hi, tt;
@@ -523,61 +541,123 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
             const int er = row_ok ? p.row_exp[r] : kExpSentinel;
+            __syncwarp();  // the previous item's reads of the table are done
+            // bit j of colmask: column j of the warp's 64 has a nonzero table
+            // scale (so it also lies inside C)
+            uint64_t colmask = 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = lane + 32 * h;
+                const int col = n0 + cq * 64 + j;
+                const int fc = col < p.n ? __ldg(p.col_exp + col) : kExpSentinel;
+                const bool normal = fc != kExpSentinel && fc >= -1022 && fc <= 1023;
+                col_e[j] = fc;
+                col_scale[j] = normal ? pow2_normal(fc) : 0.0;
+                colmask |= static_cast<uint64_t>(__ballot_sync(0xffffffffu, normal)) << (32 * h);
+            }
+            __syncwarp();
+            double* const crow = p.c + (row_ok ? r : 0);
+            const size_t ldc = p.ldc;
             for (int u = u_lo; ok && u < u_hi; ++u, ++uc) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
-                if (!mbar_wait(&bar->acc_full[0], uc & 1, p.err, 0x304)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
                 const bool first_unit = (u == 0);
                 // digits of both operands are scaled by 2^-(e+1): weight 2^-(14+8d) per diagonal
                 const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0) - 2;
+                // the row's part of the scale first: sv * 2^(er - wexp) is exact
+                // (a nonzero integer below 2^40 times a power of two, landing in
+                // [2^-1022, 2^1000)), so the second multiply, by 2^fc, is the only
+                // rounding -- the same single rounding as scale_pow2(sv, er+fc-wexp)
+                const int ra = er - wexp;
+                const bool row_fast = er != kExpSentinel && ra >= -1022 && ra <= 960;
+                const double rs = row_fast ? pow2_normal(ra) : 0.0;
                 // C is read (beta*C0 on the first unit, the running sum after)
                 // (a split item: the unit's terms go to its workspace plane, C is untouched)
                 const bool read_c = !split && (!first_unit || p.beta_mode != 0);
                 const bool live = row_ok && (split || !(er == kExpSentinel && !first_unit));
+                // every live row of the warp takes the two-multiply scaling
+                const bool warp_fast = __all_sync(0xffffffffu, row_fast || !live);
                 double* wplane =
                     split ? p.ws + (static_cast<size_t>(tt) * units + u) * kOzTileElems + row_in_tile : nullptr;
+                // chunk ch's C values are requested one chunk ahead (the first
+                // chunk's before the accumulator wait), so a chunk's L2 round
+                // trip overlaps the previous chunk's arithmetic
+                double cv[8];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    const int cbase = n0 + cq * 64;
+                    cv[jj] = (live && read_c && cbase + jj < p.n) ? crow[static_cast<size_t>(cbase + jj) * ldc] : 0.0;
+                }
+                {
+                    const bool got = mbar_wait(&bar->acc_full[0], uc & 1, p.err, 0x304);
+                    if (!__all_sync(0xffffffffu, got)) {  // the whole warp goes on, or the whole warp stops
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                }
 #pragma unroll 1
                 for (int ch = 0; ch < 8; ++ch) {
-                    // 16 columns at a time; the chunk's C values are requested
-                    // before the TMEM wait, so their latencies overlap
-                    const int col0 = half * 128 + ch * 16;
+                    // 8 columns at a time
+                    const int j0 = ch * 8;
+                    const int col0 = cq * 64 + j0;
                     const int cbase = n0 + col0;
-                    double cv[16];
+                    double* const cp = crow + static_cast<size_t>(cbase) * ldc;
+                    double cn[8];
 #pragma unroll
-                    for (int jj = 0; jj < 16; ++jj)
-                        cv[jj] = (live && read_c && cbase + jj < p.n)
-                                     ? p.c[r + static_cast<size_t>(cbase + jj) * p.ldc] : 0.0;
-                    uint32_t v0[16], v1[16];
-                    tmem_ld16(lanebase + col0, v0);
-                    if (d1 >= 0) tmem_ld16(lanebase + UN + col0, v1);
+                    for (int jj = 0; jj < 8; ++jj)
+                        cn[jj] = (live && read_c && ch < 7 && cbase + 8 + jj < p.n) ? cp[(8 + jj) * ldc] : 0.0;
+                    uint32_t v0[8], v1[8];
+                    tmem_ld8(lanebase + col0, v0);
+                    if (d1 >= 0) tmem_ld8(lanebase + UN + col0, v1);
                     tmem_ld_wait();
-                    if (!live) continue;
+                    if (live) {
+                        if (warp_fast && ((colmask >> j0) & 0xffu) == 0xffu) {
+                            // branch-free: eight independent chains the compiler can interleave
 #pragma unroll
-                    for (int jj = 0; jj < 16; ++jj) {
-                        const int col = cbase + jj;
-                        if (col < p.n) {
-                            const int fc = __ldg(p.col_exp + col);
-                            double term = 0.0;
-                            if (er != kExpSentinel && fc != kExpSentinel) {
+                            for (int jj = 0; jj < 8; ++jj) {
                                 double sv = static_cast<double>(static_cast<int32_t>(v0[jj]));
                                 if (d1 >= 0) sv = fma(sv, 256.0, static_cast<double>(static_cast<int32_t>(v1[jj])));
-                                term = scale_pow2(sv, er + fc - wexp);
+                                const double term = (sv * rs) * col_scale[j0 + jj];
+                                if (wplane) {
+                                    wplane[static_cast<size_t>(col0 + jj) * kUM] = term;
+                                } else {
+                                    double acc = cv[jj];
+                                    if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
+                                    cp[jj * ldc] = fma(p.alpha, term, acc);
+                                }
                             }
-                            if (wplane) {
-                                wplane[static_cast<size_t>(col0 + jj) * kUM] = term;
-                            } else {
-                                double acc = cv[jj];
-                                if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
-                                p.c[r + static_cast<size_t>(col) * p.ldc] = fma(p.alpha, term, acc);
+                        } else {
+#pragma unroll
+                            for (int jj = 0; jj < 8; ++jj) {
+                                if (cbase + jj < p.n) {
+                                    double sv = static_cast<double>(static_cast<int32_t>(v0[jj]));
+                                    if (d1 >= 0)
+                                        sv = fma(sv, 256.0, static_cast<double>(static_cast<int32_t>(v1[jj])));
+                                    const double cs = col_scale[j0 + jj];
+                                    double term;
+                                    if (row_fast && cs != 0.0) {
+                                        term = (sv * rs) * cs;
+                                    } else {
+                                        const int fc = col_e[j0 + jj];
+                                        term = (er != kExpSentinel && fc != kExpSentinel)
+                                                   ? scale_pow2(sv, er + fc - wexp) : 0.0;
+                                    }
+                                    if (wplane) {
+                                        wplane[static_cast<size_t>(col0 + jj) * kUM] = term;
+                                    } else {
+                                        double acc = cv[jj];
+                                        if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
+                                        cp[jj * ldc] = fma(p.alpha, term, acc);
+                                    }
+                                }
                             }
                         }
                     }
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj) cv[jj] = cn[jj];
                 }
+                if (!ok) break;
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bar->acc_empty[0]);
@@ -1074,7 +1154,7 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
         p.ws = reinterpret_cast<double*>(static_cast<uint8_t*>(buf) + exps + a_bytes + b_bytes);
     }
 
-    constexpr int smem = kOzST * kOzStage + 256 + 1024;
+    constexpr int smem = kOzSmem;
     static bool attr = false;
     if (!attr) {
         e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1240,7 +1320,7 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         p.c = c; p.ldc = ldc;
         p.row_exp = ea; p.col_exp = eb;
         p.err = status;
-        constexpr int smem = kOzST * kOzStage + 256 + 1024;
+        constexpr int smem = kOzSmem;
         e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
         int sms = 148;
