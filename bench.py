@@ -956,7 +956,7 @@ def main():
                     help="time the batched f64 trsm (512 x 512, 64 RHS) on BATCH members only")
     ap.add_argument("--serve", action="store_true", help="serving sweep (request stream replay)")
     ap.add_argument("--requests", type=int, default=20000)
-    ap.add_argument("--rates", default="1000,2000,5000,8000,10000,12500,15000,17500,20000,25000,30000,50000")
+    ap.add_argument("--rates", default="1000,2000,5000,8000,10000,12500,15000,17500,20000,25000,30000,35000,40000,50000")
     ap.add_argument("--no-autotune", action="store_true", help="serving: keep the built-in split-K rule")
     ap.add_argument("--serve-thresholds", default="", metavar="F32,F64",
                     help="serving: flop thresholds for the precision forms (default 2e8,1e9)")
