@@ -829,6 +829,36 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     const int er = e[r0 + r];
     const int n = 7 + 8 * (slices - 1) - er - 1;  // Y = floor(x * 2^n)
     uint32_t w[S][4];
+    if constexpr (S <= 8) {
+        // Balancing by bytes: adding 0x80 to each of the S-1 low bytes of Y
+        // makes the carries of the loop below (a byte >= 128 becomes byte-256
+        // and carries 1 upward); flipping those bytes back (xor 0x80) leaves
+        // each balanced digit as a two's-complement byte, and byte S-1 (the
+        // top digit, carry included) is already one. So digit t is byte
+        // S-1-t of Z = (Y + B) ^ B, and four elements' digit t pack into one
+        // word with byte permutes.
+        constexpr unsigned long long B = 0x0080808080808080ull >> (8 * (8 - S));
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint32_t lo[4], hi[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const long long Y = (er == kExpSentinel) ? 0LL : floor_scaled<long long>(tile[r][c * 16 + g * 4 + q], n);
+                const unsigned long long Z = (static_cast<unsigned long long>(Y) + B) ^ B;
+                lo[q] = static_cast<uint32_t>(Z);
+                hi[q] = static_cast<uint32_t>(Z >> 32);
+            }
+#pragma unroll
+            for (int t = 0; t < S; ++t) {
+                const int b = S - 1 - t;  // byte of Z holding digit t
+                const uint32_t* src = b < 4 ? lo : hi;
+                const uint32_t sel = static_cast<uint32_t>((b & 3) | (((b & 3) + 4) << 4));
+                const uint32_t x01 = __byte_perm(src[0], src[1], sel);
+                const uint32_t x23 = __byte_perm(src[2], src[3], sel);
+                w[t][g] = __byte_perm(x01, x23, 0x5410);
+            }
+        }
+    } else {
 #pragma unroll
     for (int t = 0; t < S; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
 #pragma unroll
@@ -849,6 +879,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
         }
 #pragma unroll
         for (int t = 0; t < S; ++t) w[t][i >> 2] |= (static_cast<uint32_t>(d[t]) & 0xFFu) << (8 * (i & 3));
+    }
     }
     const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 16;
 #pragma unroll
