@@ -720,21 +720,24 @@ __global__ void fill_int_kernel(int* p, int n, int v) {
 }
 
 // e[r] = max over p of frexp_exp(x(r,p)) (kExpSentinel if the row is zero);
-// atomicMax merges the K slabs.
+// atomicMax merges the K slabs. frexp_exp is non-decreasing in |x|, and the
+// bit patterns of non-negative doubles (subnormals, inf and NaN included)
+// order as their values, so the row's exponent is frexp_exp of the largest
+// |x| bit pattern: one mask and one 64-bit max per element (0 for a zero row).
+__device__ __forceinline__ long long abs_bits(double v) {
+    return __double_as_longlong(v) & 0x7FFFFFFFFFFFFFFFLL;
+}
 // K-contiguous view: one warp per row, a 1024-wide K slab per blockIdx.y.
 __global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, int R, int K,
                                        int* __restrict__ e) {
     const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (r >= R) return;
     const int p0 = blockIdx.y * 1024, p1 = min(K, p0 + 1024);
-    int best = kExpSentinel;
+    long long best = 0;
 #pragma unroll 8
-    for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) {
-        const double v = x[static_cast<size_t>(r) * rs + q];
-        if (v != 0.0) best = max(best, frexp_exp(v));
-    }
+    for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) best = max(best, abs_bits(x[static_cast<size_t>(r) * rs + q]));
     for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if ((threadIdx.x & 31) == 0 && best != kExpSentinel) atomicMax(e + r, best);
+    if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(e + r, frexp_exp(__longlong_as_double(best)));
 }
 // R-contiguous view: one thread per row (coalesced across the warp), a
 // 32-wide K slab per blockIdx.y so the grid covers the whole matrix.
@@ -743,13 +746,10 @@ __global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, 
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     const int p0 = blockIdx.y * 32, p1 = min(K, p0 + 32);
-    int best = kExpSentinel;
+    long long best = 0;
 #pragma unroll 8
-    for (int q = p0; q < p1; ++q) {
-        const double v = x[r + static_cast<size_t>(q) * ps];
-        if (v != 0.0) best = max(best, frexp_exp(v));
-    }
-    if (best != kExpSentinel) atomicMax(e + r, best);
+    for (int q = p0; q < p1; ++q) best = max(best, abs_bits(x[r + static_cast<size_t>(q) * ps]));
+    if (best != 0) atomicMax(e + r, frexp_exp(__longlong_as_double(best)));
 }
 
 constexpr int kTile = 64;
