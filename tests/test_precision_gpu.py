@@ -148,17 +148,16 @@ def test_unsupported_pairings_are_rejected():
 
 
 def _report_path():
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    d = os.path.join(root, "gpurun_out")
-    return os.path.join(d, "precision_report.json") if os.path.isdir(d) else None
+    """Where to write the error report: the file named by RB_PRECISION_REPORT, if set."""
+    return os.environ.get("RB_PRECISION_REPORT") or None
 
 
 def test_config_sizes_error_report():
     """Errors at the configuration sizes (row-sampled double-double oracle):
     DGEMM 4096^3 row-major all four transposes (normal and 2^e sets), and
     SGEMM 8192^3 / 65536x128x8192 col-major beta=1 (uniform and log-uniform).
-    Asserts the targets; writes the numbers for the record when run with an
-    output folder present."""
+    Asserts the targets; writes the numbers to the file named by
+    RB_PRECISION_REPORT when that is set."""
     rng = np.random.default_rng(99)
     report = {}
     for dist in ("normal", "pow2"):
