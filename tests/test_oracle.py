@@ -1,6 +1,6 @@
 """CPU tests of the oracle itself: it must satisfy every assertion of the
-reference's own test suite (the golden cases) before it is trusted as the
-checker for the GPU library."""
+reference's own test suite (the golden cases) before the GPU library's
+parity tests compare against it."""
 from __future__ import annotations
 
 import numpy as np
