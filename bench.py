@@ -399,7 +399,7 @@ def run_ours(args):
     # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
     # the step's shapes: 2.516 GB at 4096^3 (x4 per step), 1.297 GB at
     # 3000x5000x2048 (x1)
-    traffic = (4 * 2.516e9 + 1.297e9) / 5 if kname == "umma_ozaki_i8" else None
+    traffic = (4 * 2.484e9 + 1.289e9) / 5 if kname == "umma_ozaki_i8" else None
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                 "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over "
