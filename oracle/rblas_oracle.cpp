@@ -94,9 +94,13 @@ void micro_16x6_f32(size_t mr, size_t nr, size_t kc, float alpha, const float* a
             hi[s] = _mm256_fmadd_ps(a_hi, bs, hi[s]);
         }
     }
+    // Every access to lo[] / hi[] uses a compile-time index, so the twelve
+    // accumulators stay in registers through the k loop (a runtime index in
+    // the edge path made the compiler store them to the stack every step).
     __m256 va = _mm256_set1_ps(alpha);
     if (mr == 16 && nr == 6) {
-        for (size_t s = 0; s < 6; ++s) {
+#pragma GCC unroll 6
+        for (int s = 0; s < 6; ++s) {
             float* cptr = c + ci + (cj + s) * ldc;
             __m256 c_lo = _mm256_loadu_ps(cptr);
             __m256 c_hi = _mm256_loadu_ps(cptr + 8);
@@ -104,13 +108,16 @@ void micro_16x6_f32(size_t mr, size_t nr, size_t kc, float alpha, const float* a
             _mm256_storeu_ps(cptr + 8, _mm256_fmadd_ps(va, hi[s], c_hi));
         }
     } else {
-        float buf[16];
+        alignas(32) float buf[6][16];
+#pragma GCC unroll 6
+        for (int s = 0; s < 6; ++s) {
+            _mm256_store_ps(buf[s], lo[s]);
+            _mm256_store_ps(buf[s] + 8, hi[s]);
+        }
         for (size_t s = 0; s < nr; ++s) {
-            _mm256_storeu_ps(buf, lo[s]);
-            _mm256_storeu_ps(buf + 8, hi[s]);
             float* col = c + ci + (cj + s) * ldc;
             for (size_t r = 0; r < mr; ++r) {
-                float t = alpha * buf[r];
+                float t = alpha * buf[s][r];
                 col[r] = col[r] + t;
             }
         }
@@ -134,9 +141,11 @@ void micro_8x6_f64(size_t mr, size_t nr, size_t kc, double alpha, const double* 
             hi[s] = _mm256_fmadd_pd(a_hi, bs, hi[s]);
         }
     }
+    // compile-time indices only, as in micro_16x6_f32
     __m256d va = _mm256_set1_pd(alpha);
     if (mr == 8 && nr == 6) {
-        for (size_t s = 0; s < 6; ++s) {
+#pragma GCC unroll 6
+        for (int s = 0; s < 6; ++s) {
             double* cptr = c + ci + (cj + s) * ldc;
             __m256d c_lo = _mm256_loadu_pd(cptr);
             __m256d c_hi = _mm256_loadu_pd(cptr + 4);
@@ -144,13 +153,16 @@ void micro_8x6_f64(size_t mr, size_t nr, size_t kc, double alpha, const double* 
             _mm256_storeu_pd(cptr + 4, _mm256_fmadd_pd(va, hi[s], c_hi));
         }
     } else {
-        double buf[8];
+        alignas(32) double buf[6][8];
+#pragma GCC unroll 6
+        for (int s = 0; s < 6; ++s) {
+            _mm256_store_pd(buf[s], lo[s]);
+            _mm256_store_pd(buf[s] + 4, hi[s]);
+        }
         for (size_t s = 0; s < nr; ++s) {
-            _mm256_storeu_pd(buf, lo[s]);
-            _mm256_storeu_pd(buf + 4, hi[s]);
             double* col = c + ci + (cj + s) * ldc;
             for (size_t r = 0; r < mr; ++r) {
-                double t = alpha * buf[r];
+                double t = alpha * buf[s][r];
                 col[r] = col[r] + t;
             }
         }
