@@ -217,15 +217,42 @@ __global__ void __launch_bounds__(kL2Threads)
     ger_real_kernel(T* A, size_t ld, int R, int C, const T* __restrict__ x, long long incx, const T* __restrict__ y,
                     long long incy, T alpha, int x_on_rows) {
     const int rbase = blockIdx.x * kSweepRows + threadIdx.x;
-    for (int c = blockIdx.y; c < C; c += gridDim.y) {
+    // the row-indexed factor (alpha*x_i, or y_j) does not depend on the
+    // column: computed once per thread and row, with the same operations
+    T rowv[kRowsPerThread];
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        const int r = rbase + q * kL2Threads;
+        rowv[q] = r < R ? (x_on_rows ? mul_rn(alpha, __ldg(x + static_cast<long long>(r) * incx))  // src/level2.rs:83
+                                     : __ldg(y + static_cast<long long>(r) * incy))
+                        : T(0);
+    }
+    // two columns per pass: 2 * kRowsPerThread loads of A in flight
+    const int step = gridDim.y;
+    for (int c = blockIdx.y; c < C; c += 2 * step) {
+        const int c2 = c + step;
+        const bool two = c2 < C;
         T* col = A + static_cast<size_t>(c) * ld;
+        T* col2 = A + static_cast<size_t>(two ? c2 : c) * ld;
+        const T colv = x_on_rows ? __ldg(y + static_cast<long long>(c) * incy)
+                                 : mul_rn(alpha, __ldg(x + static_cast<long long>(c) * incx));
+        const T colv2 = !two ? T(0)
+                        : (x_on_rows ? __ldg(y + static_cast<long long>(c2) * incy)
+                                     : mul_rn(alpha, __ldg(x + static_cast<long long>(c2) * incx)));
+        T a1[kRowsPerThread], a2[kRowsPerThread];
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) {
+            const int r = rbase + q * kL2Threads;
+            a1[q] = r < R ? col[r] : T(0);
+            a2[q] = (two && r < R) ? col2[r] : T(0);
+        }
 #pragma unroll
         for (int q = 0; q < kRowsPerThread; ++q) {
             const int r = rbase + q * kL2Threads;
             if (r < R) {
-                const int xi = x_on_rows ? r : c, yj = x_on_rows ? c : r;
-                const T axi = mul_rn(alpha, __ldg(x + static_cast<long long>(xi) * incx));  // src/level2.rs:83
-                col[r] = fma(axi, __ldg(y + static_cast<long long>(yj) * incy), col[r]);     // src/level2.rs:86
+                // axi * y_j + a with axi = alpha*x_i (src/level2.rs:86)
+                col[r] = x_on_rows ? fma(rowv[q], colv, a1[q]) : fma(colv, rowv[q], a1[q]);
+                if (two) col2[r] = x_on_rows ? fma(rowv[q], colv2, a2[q]) : fma(colv2, rowv[q], a2[q]);
             }
         }
     }
