@@ -598,6 +598,15 @@ uint64_t rb_launch_count(void);
  * Synchronises the device. Returns RB_OK when no error was recorded. */
 rb_status rb_device_error(int clear, uint32_t* detail);
 
+/* Self-test of the bounded device waits (no rblas counterpart). Launches one
+ * kernel on the current device whose mbarrier wait cannot complete (one
+ * arrival expected, none made). The wait gives up after its time limit (2 s)
+ * and records the timeout in the device error word. The call clears the
+ * word before the launch, reads and clears it afterwards, and returns
+ * RB_ERR_TIMEOUT with *detail = the recorded code; any other status means
+ * the bound did not work as designed. The device stays usable. */
+rb_status rb_probe_wait_timeout(uint32_t* detail);
+
 /* Per-kernel timing of the main GEMM kernels: while enabled, CUDA events are
  * recorded on the launching stream around each main kernel launch.
  * rb_kernel_timing_report synchronises those events, writes one line per

@@ -20,6 +20,7 @@
 
 #include "../../include/rblas_b200.h"
 #include "rb_internal.h"
+#include "rb_device.cuh"
 
 namespace rb {
 
@@ -619,6 +620,21 @@ uint32_t* device_error_word() {
     return c ? c->err_word : nullptr;
 }
 
+namespace {
+// One thread waits on an mbarrier that expects one arrival and never gets
+// it (the flag nothing sets): the bounded wait gives up after
+// RB_WAIT_LIMIT_NS and records RB_DEVERR_TIMEOUT | kProbeWaitSite.
+constexpr uint32_t kProbeWaitSite = 0x7F0;
+__global__ void wait_timeout_probe_kernel(uint32_t* err, uint32_t* completed) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+        *completed = mbar_wait(&bar, 0, err, kProbeWaitSite) ? 1u : 0u;
+    }
+}
+}  // namespace
+
 }  // namespace rb
 
 using namespace rb;
@@ -714,6 +730,24 @@ rb_status rb_device_error(int clear, uint32_t* detail) {
     if (clear && w) cudaMemset(c->err_word, 0, sizeof(uint32_t));
     if (w == 0) return RB_OK;
     return ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
+}
+
+rb_status rb_probe_wait_timeout(uint32_t* detail) {
+    if (detail) *detail = 0;
+    uint32_t* err = device_error_word();
+    if (!err) return RB_ERR_CUDA;
+    if (rb_device_error(1, nullptr) == RB_ERR_CUDA) return RB_ERR_CUDA;  // start from a clear word
+    uint32_t* done = nullptr;
+    if (cudaMalloc(&done, sizeof(uint32_t)) != cudaSuccess) return RB_ERR_ALLOC;
+    wait_timeout_probe_kernel<<<1, 32>>>(err, done);
+    count_launch();
+    uint32_t completed = 1;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(&completed, done, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(done);
+    if (e != cudaSuccess) return RB_ERR_CUDA;
+    const rb_status st = rb_device_error(1, detail);  // reads and clears the word
+    return completed ? RB_ERR_DEVICE : st;  // a wait that completed means the probe itself is broken
 }
 
 void rb_kernel_timing_enable(int on) { g_timing_on.store(on != 0); }
