@@ -598,6 +598,12 @@ uint64_t rb_launch_count(void);
  * Synchronises the device. Returns RB_OK when no error was recorded. */
 rb_status rb_device_error(int clear, uint32_t* detail);
 
+/* Parallel width of the GEMM path: the current device's multiprocessor
+ * count (each persistent GEMM kernel runs one CTA per SM); 0 when no device
+ * is usable. Replaces level3::num_threads (src/level3.rs:11-17), which
+ * reports the size of rblas's rayon pool. */
+size_t rb_num_threads(void);
+
 /* Self-test of the bounded device waits (no rblas counterpart). Launches one
  * kernel on the current device whose mbarrier wait cannot complete (one
  * arrival expected, none made). The wait gives up after its time limit (2 s)

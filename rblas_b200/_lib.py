@@ -123,6 +123,7 @@ SIGNATURES = {
     "rb_launch_count": (C.c_uint64, []),
     "rb_device_error": (_i, [_i, C.POINTER(C.c_uint32)]),
     "rb_probe_wait_timeout": (_i, [C.POINTER(C.c_uint32)]),
+    "rb_num_threads": (C.c_size_t, []),
     "rb_release_cached_memory": (None, []),
     "rb_set_scratch_cache_bytes": (None, [_sz]),
     "rb_probe_fma_peak_tflops": (C.c_double, [_i, _i]),

@@ -732,6 +732,16 @@ rb_status rb_device_error(int clear, uint32_t* detail) {
     return ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
 }
 
+size_t rb_num_threads(void) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();  // no usable device: report no workers, leave no sticky error
+        return 0;
+    }
+    return sms > 0 ? static_cast<size_t>(sms) : 0;
+}
+
 rb_status rb_probe_wait_timeout(uint32_t* detail) {
     if (detail) *detail = 0;
     uint32_t* err = device_error_word();

@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from .types import Layout, Precision, Transpose
 
-__all__ = ["gemm", "try_gemm", "gemm_dev", "syrk", "symm", "trsm"]
+__all__ = ["num_threads", "gemm", "try_gemm", "gemm_dev", "syrk", "symm", "trsm"]
 
 
 def _as_slice(x, dtype, name, writable=False):
@@ -52,6 +52,13 @@ def try_gemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ld
             _ptr(a), lda, a.size, _ptr(b), ldb, b.size, beta, _ptr(c), ldc, c.size,
             int(Precision(prec)), C.byref(err))
     return _lib.raise_for(st, err)
+
+
+def num_threads():
+    """level3::num_threads (src/level3.rs:11-17): the parallel width of the
+    GEMM path -- the current device's SM count (one CTA per SM in every
+    persistent GEMM kernel); 0 when no device is usable."""
+    return int(_lib.load().rb_num_threads())
 
 
 def gemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,

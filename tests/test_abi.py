@@ -107,3 +107,15 @@ def test_invalid_enum_rejected_by_the_c_layer():
     assert st == 4 and err.code == 4
     with pytest.raises(ValueError):
         level3.try_gemm(7, 0, 0, 2, 2, 2, 1.0, buf, 2, buf, 2, 0.0, buf, 2)
+
+
+def test_num_threads_mirrors_level3():
+    """level3::num_threads: the SM count on a GPU, 0 where no device is usable."""
+    from rblas_b200 import level3
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count if torch.cuda.is_available() else 0
+    except ImportError:
+        sms = None
+    got = level3.num_threads()
+    assert got == sms if sms is not None else got >= 0
