@@ -397,11 +397,18 @@ def run_ours(args):
                 "whose peak on this GPU measured the same, 36.8-37.0 TFLOP/s); not in MEASURED_PEAKS.json")
     # DRAM bytes per launch of the dominant kernel, measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
-    # the step's shapes: 2.516 GB at 4096^3 (x4 per step), 1.297 GB at
+    # the step's shapes: 2.484 GB at 4096^3 (x4 per step), 1.289 GB at
     # 3000x5000x2048 (x1)
     traffic = (4 * 2.484e9 + 1.289e9) / 5 if kname == "umma_ozaki_i8" else None
+    # second denominator for the INT8 pipe: twice the driver-measured dense
+    # BF16 cuBLAS burst (the INT8 tensor rate is twice the BF16 rate)
+    mp = measured_peaks() or {}
+    alt = 2.0 * mp["bf16_tflops"] if (kname.startswith("umma_ozaki") and mp.get("bf16_tflops")) else None
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                "frac": achieved / peak if peak > 0 else None,
+                "peak_alt": alt, "frac_alt": achieved / alt if alt else None,
+                "peak_alt_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst)" if alt else None,
+                "traffic": traffic,
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, averaged over "
                                    "the step's launch shapes") if traffic else None,
                 "kernel": kname, "launches": cnt, "avg_launch_ms": kms / cnt,
@@ -428,6 +435,29 @@ def run_ours(args):
                                            "pipe_tflops": v[2] / (v[1] * 1e-3) / 1e12}
                                        for k, v in kr2.items()}}
         del SA, SB, SC
+        torch.cuda.empty_cache()
+
+    # ---- DGEMM 8192^3 row-major N/N alpha=1.5 beta=-0.5: plain (DMMA) vs Ozaki
+    dgemm8 = {}
+    if not args.no_sgemm:
+        n8 = 8192
+        gd = torch.Generator(device=dev)
+        gd.manual_seed(78)
+        DA = torch.randn(n8 * n8, dtype=torch.float64, device=dev, generator=gd)
+        DB = torch.randn(n8 * n8, dtype=torch.float64, device=dev, generator=gd)
+        DC = torch.randn(n8 * n8, dtype=torch.float64, device=dev, generator=gd)
+        for name, prec, reps in (("plain", Precision.Plain, 3), ("ozaki", Precision.Ozaki, 5)):
+            def one():
+                level3.gemm_dev(Layout.RowMajor, 0, 0, n8, n8, n8, ALPHA, DA.data_ptr(), n8, DB.data_ptr(),
+                                n8, BETA, DC.data_ptr(), n8, np.float64, prec=prec, stream=sh)
+            ms, launches, kr2 = timed(one, reps, 2)
+            dgemm8[name] = {"tflops": 2.0 * n8 ** 3 / (ms * 1e-3) / 1e12, "ms": ms,
+                            "kernels": {k: {"launches": v[0], "ms": v[1],
+                                            "pipe_tflops": v[2] / (v[1] * 1e-3) / 1e12}
+                                        for k, v in kr2.items()}}
+        if "plain" in dgemm8 and "ozaki" in dgemm8:
+            dgemm8["ozaki_over_plain"] = dgemm8["ozaki"]["tflops"] / dgemm8["plain"]["tflops"]
+        del DA, DB, DC
         torch.cuda.empty_cache()
 
     # ---- the other configurations: SGEMM 1024^3 (C1), tall-skinny SGEMM
@@ -606,7 +636,7 @@ def run_ours(args):
             "form": headline_name, "config": config_block(args), "forms": forms,
             "clocks": clocks, "e2e": e2e, "gpu_launches": hl["gpu_launches"],
             "roofline": roofline, "cpu_baseline": cpu, "peaks_measured": peaks,
-            "sgemm_8192": sgemm, "configs": others, "serving": serving,
+            "sgemm_8192": sgemm, "dgemm_8192": dgemm8, "configs": others, "serving": serving,
             "device_error": {"after_headline": err_status[0], "end_of_run": rb.device_error()[0]},
         }
         print(json.dumps(line))

@@ -533,9 +533,20 @@ rb_status rb_server_set_forms(void* server, int f32_form, int f64_form, double f
  * layout. Returns at once; RB_ERR_BUSY if D could never fit the budget. */
 rb_status rb_server_submit(void* server, const rb_gemm_problem* p, uint64_t* id);
 /* Wait for a request (timeout_us < 0: forever; 0: poll). On RB_OK, *d_out /
- * *ldd give the result in HBM (valid until rb_server_release). */
+ * *ldd give the result in HBM (valid until rb_server_release). A request
+ * whose batch saw the device error word set (a kernel's bounded wait gave up,
+ * or a bounds check failed) finishes with RB_ERR_TIMEOUT / RB_ERR_DEVICE and
+ * its result must not be used; the server clears the word and goes on. A
+ * cancelled request finishes with RB_ERR_CANCELLED. RB_ERR_TIMEOUT is also
+ * the answer when timeout_us runs out first (the request is then still
+ * pending). */
 rb_status rb_server_wait(void* server, uint64_t id, int64_t timeout_us, void** d_out, size_t* ldd,
                          rb_request_times* times);
+/* Cancel a request that is still queued (not yet admitted): it never runs,
+ * and rb_server_wait reports RB_ERR_CANCELLED for it (release it as usual).
+ * RB_ERR_BUSY once it has been admitted (running or finished);
+ * RB_ERR_INVALID_ARG for an unknown id. */
+rb_status rb_server_cancel(void* server, uint64_t id);
 /* Return a finished request's result memory to the budget. */
 rb_status rb_server_release(void* server, uint64_t id);
 rb_status rb_server_destroy(void* server);
@@ -566,8 +577,11 @@ rb_status rb_server_run_trace(void* server, const rb_gemm_problem* problems,
  *     slices; larger problems get RB_ERR_SCRATCH_LIMIT (err->got = bytes
  *     needed, err->min_or_need = bytes available) and touch nothing.
  *   - The first call on a device, with that device current, looks up the
- *     array's device address (cudaGetSymbolAddress); make that first call
- *     before any stream capture.
+ *     array's device address (cudaGetSymbolAddress), and so does the first
+ *     call after that device's context was replaced (cudaDeviceReset); make
+ *     that first call before any stream capture.
+ *   - Null a or b (with k > 0) or null c: RB_ERR_INVALID_ARG, as for
+ *     rb_dgemm_dev.
  *   - Every call shares the array and leaves its contents behind: calls whose
  *     work overlaps on the GPU (different streams, or different host threads)
  *     race on it. The call clears the status word it needs, and returns after
@@ -599,10 +613,32 @@ uint64_t rb_launch_count(void);
 rb_status rb_device_error(int clear, uint32_t* detail);
 
 /* Parallel width of the GEMM path: the current device's multiprocessor
- * count (each persistent GEMM kernel runs one CTA per SM); 0 when no device
- * is usable. Replaces level3::num_threads (src/level3.rs:11-17), which
- * reports the size of rblas's rayon pool. */
+ * count (each persistent GEMM kernel runs one CTA per SM); 1 when no device
+ * is usable, so that like rayon's pool size it is never 0. Replaces
+ * level3::num_threads (src/level3.rs:11-17), which reports the size of
+ * rblas's rayon pool. */
 size_t rb_num_threads(void);
+
+/* Device allocations the library has requested since load, on all devices:
+ * scratch-pool blocks, staging buffers, plan tables, serving pools, the
+ * per-device error word (no rblas counterpart; rblas's only allocations are
+ * its thread-local pack buffers, src/kernel/gemm.rs:58-84). */
+uint64_t rb_device_alloc_count(void);
+
+/* Host-side fault injection for tests of the error paths (no rblas
+ * counterpart). Nothing here faults, traps or hangs a GPU.
+ *   RB_INJECT_ALLOC: the next `count` device allocations the library
+ *     requests fail as if the device were out of memory; the call that made
+ *     them returns RB_ERR_ALLOC and leaves its outputs untouched. count 0
+ *     clears any pending failures; `value` is ignored.
+ *   RB_INJECT_DEVICE_WORD: waits for the current device to go idle, then
+ *     writes `value` (nonzero, kind << 24 | site as the kernels write it)
+ *     into its error word, as a kernel does when a bounded wait gives up.
+ *     The next call or serving batch that reads the word reports it
+ *     (RB_ERR_TIMEOUT for kind 1, else RB_ERR_DEVICE). `count` is ignored.
+ * RB_ERR_INVALID_ARG for an unknown kind, a negative count or a zero word. */
+typedef enum { RB_INJECT_ALLOC = 1, RB_INJECT_DEVICE_WORD = 2 } rb_inject_kind;
+rb_status rb_debug_inject(int kind, uint32_t value, int count);
 
 /* Self-test of the bounded device waits (no rblas counterpart). Launches one
  * kernel on the current device whose mbarrier wait cannot complete (one

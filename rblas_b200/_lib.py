@@ -115,6 +115,7 @@ SIGNATURES = {
     "rb_server_wait": (_i, [_vp, C.c_uint64, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                             C.POINTER(RbRequestTimes)]),
     "rb_server_release": (_i, [_vp, C.c_uint64]),
+    "rb_server_cancel": (_i, [_vp, C.c_uint64]),
     "rb_server_destroy": (_i, [_vp]),
     "rb_server_run_trace": (_i, [_vp, C.POINTER(RbGemmProblem), C.POINTER(C.c_uint64), _sz,
                                  C.POINTER(RbRequestTimes)]),
@@ -124,6 +125,8 @@ SIGNATURES = {
     "rb_device_error": (_i, [_i, C.POINTER(C.c_uint32)]),
     "rb_probe_wait_timeout": (_i, [C.POINTER(C.c_uint32)]),
     "rb_num_threads": (C.c_size_t, []),
+    "rb_device_alloc_count": (C.c_uint64, []),
+    "rb_debug_inject": (_i, [_i, C.c_uint32, _i]),
     "rb_release_cached_memory": (None, []),
     "rb_set_scratch_cache_bytes": (None, [_sz]),
     "rb_probe_fma_peak_tflops": (C.c_double, [_i, _i]),

@@ -653,7 +653,7 @@ int grouped_plan_create(const rb_gemm_problem* probs, size_t count, void** out, 
     const size_t ws_bytes = gb.slots * kSlotBytes;
     const size_t total = rup(gb.all_bytes, 256) + ws_bytes + gb.scratch;
     cudaError_t e = cudaSuccess;
-    if (total) e = cudaMalloc(&pl->mem, total);
+    if (total) e = dev_alloc(reinterpret_cast<void**>(&pl->mem), total);
     if (e != cudaSuccess) {
         if (ce) *ce = e;
         delete pl;

@@ -1225,7 +1225,9 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
 // that loads this library holds its 64 MiB + 64 KiB until the process exits.
 // In host code `g_noalloc_scratch` is only a host-side stand-in for the
 // symbol, so its device address is looked up with cudaGetSymbolAddress, once
-// per device, on the first call made with that device current.
+// per device, on the first call made with that device current (and again
+// if that device's context has been replaced since, e.g. after a
+// cudaDeviceReset, since the old address then belongs to a dead context).
 // ==============================================================================
 
 namespace rb {
@@ -1235,10 +1237,23 @@ constexpr size_t kNoAllocScratchBytes = (64u << 20) + (64u << 10);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {};
+struct NoAllocAddr {
+    void* ptr;
+    unsigned long long ctx;  // the context the address was looked up in (0: unknown)
+};
+NoAllocAddr g_noalloc_addr[64] = {};
 
-size_t noalloc_bytes_needed(size_t m, size_t n, size_t kp, int slices) {
-    return 256 + round_up((m + n) * sizeof(int), 256) + round_up(slices * m * kp, 256) + slices * n * kp;
+// Bytes of the array one problem uses: the status word, the exponents and
+// both digit planes. Returns false (nothing computed) when that exceeds
+// `cap`; each step is checked before it can wrap, since m, n and k may each
+// be up to 2^31 - 1.
+bool noalloc_bytes_needed(size_t m, size_t n, size_t kp, int slices, size_t cap, size_t* need) {
+    *need = cap + 1;
+    if (m > cap || n > cap || kp > cap) return false;
+    const size_t per_k = static_cast<size_t>(slices) * (m + n);  // < 12 * 2^33
+    if (kp != 0 && per_k > cap / kp) return false;
+    *need = 256 + round_up((m + n) * sizeof(int), 256) + round_up(slices * m * kp, 256) + slices * n * kp;
+    return *need <= cap;
 }
 
 }  // namespace
@@ -1284,25 +1299,34 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         ca = b; cb = a;
         clda = ldb; cldb = lda;
     }
+    if ((k > 0 && (!a || !b)) || !c) return fail(RB_ERR_INVALID_ARG);
     if (cm > 0x7fffffff || cn > 0x7fffffff || k > 0x7fffffff) return fail(RB_ERR_INVALID_ARG);
     const int slices = rb_get_ozaki_slices();
     const size_t kp = round_up(k, 16);
-    const size_t need = noalloc_bytes_needed(cm, cn, kp, slices);
-    if (need > kNoAllocScratchBytes) return fail(RB_ERR_SCRATCH_LIMIT, need, kNoAllocScratchBytes);
+    size_t need = 0;
+    if (!noalloc_bytes_needed(cm, cn, kp, slices, kNoAllocScratchBytes, &need))
+        return fail(RB_ERR_SCRATCH_LIMIT, need, kNoAllocScratchBytes);
 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) return fail(RB_ERR_CUDA, 0, 0, e);
     uint8_t* base;
     {
+        // set-up, once per device (and context): the array's device address
+        unsigned long long ctx = 0;
+        const bool have_ctx = current_context_id(&ctx);
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        NoAllocAddr& s = g_noalloc_addr[dev];
+        if (!s.ptr || !have_ctx || s.ctx != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) return fail(RB_ERR_CUDA, 0, 0, e);
-            g_noalloc_ptr[dev] = p;
+            s.ptr = p;
+            // without a context id the lookup is simply repeated on every call
+            if (!have_ctx) current_context_id(&ctx);
+            s.ctx = ctx;
         }
-        base = static_cast<uint8_t*>(g_noalloc_ptr[dev]);
+        base = static_cast<uint8_t*>(s.ptr);
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     uint32_t* status = reinterpret_cast<uint32_t*>(base);

@@ -32,7 +32,7 @@ static double probe(int iters) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int blocks = sms * 8;
     T* out = nullptr;
-    if (cudaMalloc(&out, blocks * sizeof(T)) != cudaSuccess) return -1.0;
+    if (dev_alloc(reinterpret_cast<void**>(&out), blocks * sizeof(T)) != cudaSuccess) return -1.0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

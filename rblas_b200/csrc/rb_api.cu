@@ -53,7 +53,35 @@ cudaMemPool_t pool_for_current(cudaError_t* err) {
 }
 }  // namespace
 
+namespace {
+std::atomic<uint64_t> g_device_allocs{0};
+std::atomic<int64_t> g_inject_alloc{0};  // pending injected allocation failures
+}  // namespace
+
+void count_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+
+bool take_injected_alloc_failure() {
+    int64_t n = g_inject_alloc.load();
+    while (n > 0)
+        if (g_inject_alloc.compare_exchange_weak(n, n - 1)) return true;
+    return false;
+}
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    count_device_alloc();
+    if (take_injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 cudaError_t scratch_alloc_raw(void** p, size_t bytes, cudaStream_t st) {
+    count_device_alloc();
+    if (take_injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
     cudaError_t e;
     cudaMemPool_t pool = pool_for_current(&e);
     if (!pool) return e == cudaSuccess ? cudaErrorMemoryAllocation : e;
@@ -164,6 +192,7 @@ DeviceCtx* ctx_for_current(cudaError_t* e) {
     if (!c.init) {
         *e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
         if (*e != cudaSuccess) return nullptr;
+        count_device_alloc();
         *e = cudaMalloc(&c.err_word, 64);
         if (*e != cudaSuccess) return nullptr;
         *e = cudaMemset(c.err_word, 0, 64);
@@ -186,10 +215,11 @@ cudaError_t ensure_buf(DeviceCtx* c, int slot, size_t bytes) {
     c->buf[slot] = nullptr;
     c->cap[slot] = 0;
     size_t want = std::max(bytes, c->cap[slot] * 2);
-    cudaError_t e = cudaMalloc(&c->buf[slot], want);
+    cudaError_t e = dev_alloc(&c->buf[slot], want);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        e = cudaMalloc(&c->buf[slot], bytes);
+        if (want == bytes) return e;
+        e = dev_alloc(&c->buf[slot], bytes);
         if (e != cudaSuccess) return e;
         want = bytes;
     }
@@ -208,9 +238,13 @@ void set_err(rb_error* err, int32_t code, char which = 0, uint64_t got = 0, uint
     }
 }
 
+// A failed CUDA call; an out-of-memory one is RB_ERR_ALLOC (cuda_error keeps
+// the CUDA code either way).
 rb_status cuda_fail(rb_error* err, cudaError_t e) {
-    set_err(err, RB_ERR_CUDA, 0, 0, 0, static_cast<int32_t>(e));
-    return RB_ERR_CUDA;
+    const rb_status s = (e == cudaErrorMemoryAllocation) ? RB_ERR_ALLOC : RB_ERR_CUDA;
+    if (s == RB_ERR_ALLOC) cudaGetLastError();  // not sticky: clear it for the next call
+    set_err(err, s, 0, 0, 0, static_cast<int32_t>(e));
+    return s;
 }
 
 // src/level3.rs:107-140. Zero dims are valid; InvalidLeadingDim before
@@ -528,6 +562,10 @@ rb_status dev_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, s
     if ((s = check_matrix(layout, 'b', tb ? n : k, tb ? k : n, ldb, 0, false, err)) != RB_OK) return s;
     if ((s = check_matrix(layout, 'c', m, n, ldc, 0, false, err)) != RB_OK) return s;
     if (m == 0 || n == 0) return RB_OK;
+    if ((k > 0 && (!a || !b)) || !c) {
+        set_err(err, RB_ERR_INVALID_ARG);
+        return RB_ERR_INVALID_ARG;
+    }
     cudaError_t e;
     if (!ctx_for_current(&e)) return cuda_fail(err, e);
     ColProblem<T> p = normalise<T>(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
@@ -736,10 +774,35 @@ size_t rb_num_threads(void) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-        cudaGetLastError();  // no usable device: report no workers, leave no sticky error
-        return 0;
+        cudaGetLastError();  // no usable device: leave no sticky error
+        return 1;            // like rayon's pool size, never 0 (callers divide by it)
     }
-    return sms > 0 ? static_cast<size_t>(sms) : 0;
+    return sms > 0 ? static_cast<size_t>(sms) : 1;
+}
+
+uint64_t rb_device_alloc_count(void) { return g_device_allocs.load(); }
+
+rb_status rb_debug_inject(int kind, uint32_t value, int count) {
+    switch (kind) {
+        case RB_INJECT_ALLOC:
+            if (count < 0) return RB_ERR_INVALID_ARG;
+            g_inject_alloc.store(count);
+            return RB_OK;
+        case RB_INJECT_DEVICE_WORD: {
+            if (value == 0) return RB_ERR_INVALID_ARG;
+            cudaError_t e;
+            DeviceCtx* c = ctx_for_current(&e);
+            if (!c) return RB_ERR_CUDA;
+            // ordered after the work already queued on the device's streams
+            // that use the word, like a kernel setting it
+            if (cudaDeviceSynchronize() != cudaSuccess) return RB_ERR_CUDA;
+            if (cudaMemcpy(c->err_word, &value, sizeof(value), cudaMemcpyHostToDevice) != cudaSuccess)
+                return RB_ERR_CUDA;
+            return RB_OK;
+        }
+        default:
+            return RB_ERR_INVALID_ARG;
+    }
 }
 
 rb_status rb_probe_wait_timeout(uint32_t* detail) {
@@ -748,7 +811,7 @@ rb_status rb_probe_wait_timeout(uint32_t* detail) {
     if (!err) return RB_ERR_CUDA;
     if (rb_device_error(1, nullptr) == RB_ERR_CUDA) return RB_ERR_CUDA;  // start from a clear word
     uint32_t* done = nullptr;
-    if (cudaMalloc(&done, sizeof(uint32_t)) != cudaSuccess) return RB_ERR_ALLOC;
+    if (dev_alloc(reinterpret_cast<void**>(&done), sizeof(uint32_t)) != cudaSuccess) return RB_ERR_ALLOC;
     wait_timeout_probe_kernel<<<1, 32>>>(err, done);
     count_launch();
     uint32_t completed = 1;

@@ -65,9 +65,9 @@ rb_status rb_autotune_grouped(const char* cache_path, int* buckets_tuned) {
     const size_t maxdim = size_t(1) << (kHiBucket + 1);  // representative shapes stay below 2^13
     const size_t maxel = maxdim * maxdim;
     void *A = nullptr, *B = nullptr, *Cm = nullptr;
-    cudaError_t e = cudaMalloc(&A, maxel * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&B, maxel * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&Cm, maxel * 8);
+    cudaError_t e = dev_alloc(&A, maxel * 8);
+    if (e == cudaSuccess) e = dev_alloc(&B, maxel * 8);
+    if (e == cudaSuccess) e = dev_alloc(&Cm, maxel * 8);
     if (e == cudaSuccess) e = cudaMemset(A, 0, maxel * 8);
     if (e == cudaSuccess) e = cudaMemset(B, 0, maxel * 8);
     if (e == cudaSuccess) e = cudaMemset(Cm, 0, maxel * 8);

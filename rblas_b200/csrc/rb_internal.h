@@ -70,6 +70,22 @@ void set_scratch_cache_bytes(size_t bytes);
 // Per-device error word (device memory, zero when healthy).
 uint32_t* device_error_word();
 
+// ---- device allocations ---------------------------------------------------------
+// Every device allocation the library makes outside the pool (staging
+// buffers, plan tables, serving pools) goes through dev_alloc; it and
+// scratch_alloc_raw count into rb_device_alloc_count and fail with
+// cudaErrorMemoryAllocation while an injected failure is pending
+// (rb_debug_inject(RB_INJECT_ALLOC, ...)).
+cudaError_t dev_alloc(void** p, size_t bytes);
+// True (and one pending failure consumed) when an injected allocation
+// failure is due; callers that allocate by other means use it directly.
+bool take_injected_alloc_failure();
+void count_device_alloc();
+
+// The driver's unique id of the calling thread's current context (0 and
+// false when there is none or the driver lacks cuCtxGetId).
+bool current_context_id(unsigned long long* id);
+
 // ---- launchers (all operands column-major after row-major normalisation) ------
 
 // Plain SIMT GEMM, C = alpha*op(A)op(B) + beta*C. a_kmajor: op(A) is stored

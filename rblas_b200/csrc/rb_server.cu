@@ -47,7 +47,7 @@ size_t rup(size_t x, size_t m) { return (x + m - 1) / m * m; }
 class Pool {
 public:
     bool init(size_t bytes, cudaError_t* e) {
-        *e = cudaMalloc(&base_, bytes);
+        *e = dev_alloc(&base_, bytes);
         if (*e != cudaSuccess) return false;
         size_ = bytes;
         free_[0] = bytes;
@@ -118,6 +118,7 @@ struct Batch {
     std::vector<Request*> reqs;
     cudaEvent_t done;
     int stream;
+    int word;            // slot in the pinned status words: the device error word after the batch
     int form[2];         // forms and thresholds in force when the batch formed
     double min_flop[2];
 };
@@ -148,6 +149,18 @@ public:
     GroupStaging staging[2] = {{nullptr, nullptr, 0, nullptr, 0}, {nullptr, nullptr, 0, nullptr, 0}};
     size_t ws_slot_cap = 0;
     std::vector<cudaEvent_t> free_events;
+    // Per batch, a pinned copy of the device error word taken on the batch's
+    // stream after its kernels (before its completion event), so a kernel
+    // that gave up a bounded wait fails the requests of its batch.
+    static constexpr int kWordSlots = 4096 + 64;
+    uint32_t* words = nullptr;     // pinned host, kWordSlots
+    uint32_t* dev_word = nullptr;  // the device's error word
+    std::vector<int> free_words;
+    // A batch saw the word set. Kernels that find it set give up their waits,
+    // so every batch in flight alongside may hold a partial result: they all
+    // fail (the word stays set until they have retired), no new batch starts,
+    // and the word is cleared once nothing is in flight.
+    bool poisoned = false;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request*> queue;
@@ -164,6 +177,17 @@ public:
         *e = cudaGetDevice(&device);
         if (*e != cudaSuccess) return RB_ERR_CUDA;
         if (!pool.init(budget, e)) return RB_ERR_ALLOC;
+        dev_word = device_error_word();
+        if (!dev_word) {
+            *e = cudaErrorInitializationError;
+            return RB_ERR_CUDA;
+        }
+        *e = cudaMallocHost(&words, kWordSlots * sizeof(uint32_t));
+        if (*e != cudaSuccess) return RB_ERR_ALLOC;
+        for (int i = kWordSlots - 1; i >= 0; --i) {
+            words[i] = 0;
+            free_words.push_back(i);
+        }
         for (auto& s : streams) {
             *e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
             if (*e != cudaSuccess) return RB_ERR_CUDA;
@@ -179,7 +203,7 @@ public:
             for (auto& g : staging) {
                 *e = cudaMallocHost(&g.host, tb);
                 if (*e != cudaSuccess) return RB_ERR_ALLOC;
-                *e = cudaMalloc(&g.dev, tb + kWsBytes);
+                *e = dev_alloc(&g.dev, tb + kWsBytes);
                 if (*e != cudaSuccess) return RB_ERR_ALLOC;
                 g.bytes = tb;
                 g.ws = static_cast<uint8_t*>(g.dev) + tb;
@@ -216,6 +240,8 @@ public:
             g = GroupStaging{nullptr, nullptr, 0, nullptr, 0};
         }
         for (auto& kv : reqs) delete kv.second;
+        if (words) cudaFreeHost(words);
+        words = nullptr;
         pool.release_all();
     }
 
@@ -232,6 +258,12 @@ public:
 
     size_t inflight_count() const { return inflight[0].size() + inflight[1].size(); }
 
+    int take_word() {
+        const int w = free_words.back();
+        free_words.pop_back();
+        return w;
+    }
+
     // retire finished batches, in order per stream (caller holds mu)
     bool retire() {
         bool any = false;
@@ -239,11 +271,20 @@ public:
             while (!q.empty() && cudaEventQuery(q.front().done) == cudaSuccess) {
                 Batch& b = q.front();
                 const uint64_t t = now_ns();
+                // the device error word as the batch's stream saw it after its kernels
+                const uint32_t w = words[b.word];
+                int st = RB_OK;
+                if (w != 0) {
+                    st = ((w >> 24) == (RB_DEVERR_TIMEOUT >> 24)) ? RB_ERR_TIMEOUT : RB_ERR_DEVICE;
+                    words[b.word] = 0;
+                    poisoned = true;
+                }
                 for (Request* r : b.reqs) {
-                    if (r->status < 0) r->status = RB_OK;
+                    if (r->status < 0) r->status = st;
                     r->t.finish_ns = t;
                     if (track_completed) completed.push_back(r->id);
                 }
+                free_words.push_back(b.word);
                 free_events.push_back(b.done);
                 q.pop_front();
                 any = true;
@@ -306,6 +347,7 @@ public:
                 cudaStreamWaitEvent(st, form_events[f], 0);
             }
         }
+        cudaMemcpyAsync(&words[b.word], dev_word, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         cudaEventRecord(b.done, st);
         return rc;
     }
@@ -344,6 +386,18 @@ public:
         std::unique_lock<std::mutex> lk(mu);
         while (!stop) {
             if (retire()) cv_done.notify_all();
+            if (poisoned) {
+                if (inflight_count()) {
+                    lk.unlock();
+                    std::this_thread::sleep_for(std::chrono::microseconds(10));
+                    lk.lock();
+                    continue;
+                }
+                // nothing in flight can still read the word: clear it, then go on
+                cudaMemsetAsync(dev_word, 0, sizeof(uint32_t), streams[0]);
+                cudaStreamSynchronize(streams[0]);
+                poisoned = false;
+            }
             if (grouped) {
                 // continuous batching: one batch running, one queued behind it;
                 // everything that arrived meanwhile forms the next batch
@@ -367,7 +421,7 @@ public:
                     }
                 }
                 if (!batch.empty()) {
-                    inflight[s].push_back(Batch{std::move(batch), get_event(), s, {form[0], form[1]},
+                    inflight[s].push_back(Batch{std::move(batch), get_event(), s, take_word(), {form[0], form[1]},
                                                 {min_flop[0], min_flop[1]}});
                     next_stream = s ^ 1;
                     const Batch& b = inflight[s].back();
@@ -391,8 +445,8 @@ public:
                     queue.pop_front();
                     const int s = next_stream;
                     next_stream ^= 1;
-                    inflight[s].push_back(Batch{std::vector<Request*>{r}, get_event(), s, {form[0], form[1]},
-                                                {min_flop[0], min_flop[1]}});
+                    inflight[s].push_back(Batch{std::vector<Request*>{r}, get_event(), s, take_word(),
+                                                {form[0], form[1]}, {min_flop[0], min_flop[1]}});
                     fresh.push_back(&inflight[s].back());
                 }
                 if (!fresh.empty()) {
@@ -416,6 +470,8 @@ public:
         }
     }
     static constexpr size_t kMaxInflightRequests = 4096;
+    // per-request mode keeps at most kMaxInflightRequests batches in flight, grouped mode two
+    static_assert(kWordSlots >= kMaxInflightRequests + 2, "a status word per batch in flight");
 };
 
 }  // namespace
@@ -567,6 +623,25 @@ rb_status rb_server_wait(void* server, uint64_t id, int64_t timeout_us, void** d
     if (ldd) *ldd = r->ldd;
     if (times) *times = r->t;
     return static_cast<rb_status>(r->status);
+}
+
+rb_status rb_server_cancel(void* server, uint64_t id) {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return RB_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        if (it == s->reqs.end()) return RB_ERR_INVALID_ARG;
+        Request* r = it->second;
+        if (r->status != -1) return RB_ERR_BUSY;  // admitted: running or finished
+        auto q = std::find(s->queue.begin(), s->queue.end(), r);
+        if (q != s->queue.end()) s->queue.erase(q);
+        r->status = RB_ERR_CANCELLED;
+        r->t.finish_ns = now_ns();
+        if (s->track_completed) s->completed.push_back(r->id);
+    }
+    s->cv_done.notify_all();
+    return RB_OK;
 }
 
 rb_status rb_server_release(void* server, uint64_t id) {

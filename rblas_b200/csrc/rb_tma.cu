@@ -52,4 +52,31 @@ CUresult make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dt
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
+namespace {
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_id = nullptr;
+std::once_flag g_ctx_once;
+
+void load_ctx_fns() {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 4000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(fn);
+}
+}  // namespace
+
+bool current_context_id(unsigned long long* id) {
+    *id = 0;
+    std::call_once(g_ctx_once, load_ctx_fns);
+    if (!g_ctx_current || !g_ctx_id) return false;
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return g_ctx_id(ctx, id) == CUDA_SUCCESS;
+}
+
 }  // namespace rb

@@ -57,7 +57,8 @@ def try_gemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ld
 def num_threads():
     """level3::num_threads (src/level3.rs:11-17): the parallel width of the
     GEMM path -- the current device's SM count (one CTA per SM in every
-    persistent GEMM kernel); 0 when no device is usable."""
+    persistent GEMM kernel); 1 when no device is usable (like rayon's pool
+    size, never 0)."""
     return int(_lib.load().rb_num_threads())
 
 

@@ -159,6 +159,11 @@ class Server:
     def release(self, rid: int) -> int:
         return self._lib.rb_server_release(self._h, rid)
 
+    def cancel(self, rid: int) -> int:
+        """Cancel a still-queued request (rb_server_cancel): 0 when cancelled
+        (its wait then reports RB_ERR_CANCELLED), RB_ERR_BUSY once admitted."""
+        return self._lib.rb_server_cancel(self._h, rid)
+
     def run_trace(self, problems, arrival_ns):
         """Replay a trace natively; returns an (n, 3) uint64 array of
         (enqueue, admit, finish) ns and the status."""

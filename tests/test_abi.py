@@ -4,6 +4,7 @@ rblas's try_gemm error contract (src/level3.rs:68-140) -- none of these
 calls reach the GPU."""
 from __future__ import annotations
 
+import ctypes as C
 import os
 import re
 
@@ -110,12 +111,59 @@ def test_invalid_enum_rejected_by_the_c_layer():
 
 
 def test_num_threads_mirrors_level3():
-    """level3::num_threads: the SM count on a GPU, 0 where no device is usable."""
+    """level3::num_threads: the SM count on a GPU, 1 where no device is usable
+    (rblas's rayon pool size is never 0, and callers divide by it)."""
     from rblas_b200 import level3
     try:
         import torch
-        sms = torch.cuda.get_device_properties(0).multi_processor_count if torch.cuda.is_available() else 0
+        sms = torch.cuda.get_device_properties(0).multi_processor_count if torch.cuda.is_available() else 1
     except ImportError:
         sms = None
     got = level3.num_threads()
-    assert got == sms if sms is not None else got >= 0
+    assert got == sms if sms is not None else got >= 1
+
+
+def test_debug_inject_argument_checks():
+    """rb_debug_inject rejects unknown kinds, negative counts and a zero
+    device word before touching any device."""
+    lib = _lib.load()
+    assert lib.rb_debug_inject(0, 0, 0) == 4
+    assert lib.rb_debug_inject(3, 1, 1) == 4
+    assert lib.rb_debug_inject(1, 0, -1) == 4
+    assert lib.rb_debug_inject(2, 0, 0) == 4
+    assert lib.rb_debug_inject(1, 0, 2) == 0  # arm two failures ...
+    assert lib.rb_debug_inject(1, 0, 0) == 0  # ... and clear them again
+    assert lib.rb_device_alloc_count() >= 0
+
+
+def test_noalloc_rejects_null_pointers_before_any_device_work():
+    """rb_dgemm_ozaki_noalloc, like rb_dgemm_dev, rejects a null a or b (k > 0)
+    or a null c with RB_ERR_INVALID_ARG; it checks before touching a device,
+    so this runs without one."""
+    lib = _lib.load()
+    buf = np.zeros(64, dtype=np.float64)
+    p = C.c_void_p(buf.ctypes.data)
+    for a, b, c in ((None, p, p), (p, None, p), (p, p, None)):
+        err = _lib.RbError()
+        st = lib.rb_dgemm_ozaki_noalloc(1, 0, 0, 4, 4, 4, 1.0, a, 4, b, 4, 0.0, c, 4, None, C.byref(err))
+        assert st == 4 and err.code == 4
+    # k == 0 never reads a or b: only c must be given
+    err = _lib.RbError()
+    st = lib.rb_dgemm_ozaki_noalloc(1, 0, 0, 4, 4, 0, 1.0, None, 4, None, 1, 0.0, None, 4, None, C.byref(err))
+    assert st == 4
+    # leading dimensions are still checked first, as in check_matrix
+    err = _lib.RbError()
+    st = lib.rb_dgemm_ozaki_noalloc(1, 0, 0, 4, 4, 4, 1.0, None, 3, p, 4, 0.0, p, 4, None, C.byref(err))
+    assert st == 1 and err.which == b"a"
+
+
+def test_noalloc_scratch_limit_is_overflow_safe():
+    """Sizes whose scratch bytes would wrap a 64-bit product are rejected with
+    RB_ERR_SCRATCH_LIMIT before any device work (no device needed)."""
+    lib = _lib.load()
+    buf = np.zeros(8, dtype=np.float64)
+    p = C.c_void_p(buf.ctypes.data)
+    big = 2 ** 31 - 1
+    err = _lib.RbError()
+    st = lib.rb_dgemm_ozaki_noalloc(1, 0, 0, big, big, big, 1.0, p, big, p, big, 0.0, p, big, None, C.byref(err))
+    assert st == 12 and err.got > err.min_or_need == (64 << 20) + (64 << 10)

@@ -3,12 +3,15 @@
 Callers that cannot let a library allocate device memory -- a process that
 reserved the whole GPU for its own pool, or a latency-critical path where a
 cudaMalloc could block or fail mid-run -- use this entry point instead of
-rb_dgemm_dev(..., RB_PREC_OZAKI, ...). It must give the same result on the
-same inputs. The test calls it twice in a row through the C ABI (with a
-smaller second problem, so stale scratch from the first call would show) and
-compares each result with the allocating entry point's within the normwise
-tolerance the GPU tests use (4*k*u_f64). This file is named to be collected
-last; it also passes when run on its own.
+rb_dgemm_dev(..., RB_PREC_OZAKI, ...). It runs the same Ozaki arithmetic, so
+it must give the same result on the same inputs, bit for bit. The test calls
+it twice in a row through the C ABI (with a smaller second problem, so stale
+scratch from the first call would show) and compares each result with the
+allocating entry point's: equal, and so also within the normwise tolerance
+the GPU tests use (4*k*u_f64). Around a further call it checks that nothing
+was allocated: the library's count of device allocations and the device's
+free memory do not move. This file is named to be collected last; it also
+passes when run on its own.
 """
 from __future__ import annotations
 
@@ -65,6 +68,22 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(first):
         d = (got - ref).double()
         den = abs(alpha) * A.norm().item() * B.norm().item() + abs(beta) * C0.norm().item()
         assert (d.norm().item() / den) <= 4 * k * 2.0 ** -53, f"call {i}: {d.abs().max().item():.3e}"
+        assert torch.equal(got, ref), f"call {i}: max diff {d.abs().max().item():.3e}"
+    # a third call, after the warm-up above: no device allocation of any kind
+    lib = _lib.load()
+    layout, ta, tb, m, n, k = first
+    A, B, C0, lda, ldb, ldc = _case(torch, layout, ta, tb, m, n, k, seed=97)
+    got = C0.clone()
+    torch.cuda.synchronize()
+    allocs0 = lib.rb_device_alloc_count()
+    free0, _ = torch.cuda.mem_get_info()
+    st, err = _noalloc(layout, ta, tb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta,
+                       got.data_ptr(), ldc, stream)
+    assert st == 0, (st, err.code)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert lib.rb_device_alloc_count() == allocs0
+    assert free1 == free0, (free0, free1)
 
 
 def test_noalloc_rejects_problems_beyond_its_scratch():
