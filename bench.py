@@ -705,12 +705,14 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
         row = {"rate_req_s": rate}
         modes = [("grouped", True, False), ("per_request", False, False)]
         if with_forms:
-            modes.append(("grouped_forms", True, True))
+            modes += [("grouped_forms", True, True), ("per_request_forms", False, True)]
         for mode, grouped, forms in modes:
             # all modes admit the same sets; per-request mode launches the
             # single-problem plain kernel once per request, grouped mode one
             # grouped plain launch per set, grouped_forms runs the large
-            # requests of each set in the precision forms
+            # requests of each set in the precision forms (the f64 ones in one
+            # grouped Ozaki launch), per_request_forms the same arithmetic
+            # with one launch per request
             with Server(budget_bytes=budget, max_batch=max_batch, grouped=grouped) as srv:
                 if forms:
                     srv.set_forms(**SERVE_FORMS)
@@ -725,14 +727,16 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
     slo = []
     for bound in (2.0, 5.0, 10.0, 20.0, 50.0, 100.0):
         best = {}
-        for mode in ("grouped", "per_request", "grouped_forms"):
+        for mode in ("grouped", "per_request", "grouped_forms", "per_request_forms"):
             ok = [r[mode]["tflops"] for r in out["rates"] if mode in r and r[mode]["p99_ms"] <= bound]
             best[mode] = max(ok) if ok else None
-        pr = best["per_request"]
+        pr, prf = best["per_request"], best["per_request_forms"]
         slo.append({"p99_bound_ms": bound, "grouped_tflops": best["grouped"], "per_request_tflops": pr,
-                    "grouped_forms_tflops": best["grouped_forms"],
+                    "grouped_forms_tflops": best["grouped_forms"], "per_request_forms_tflops": prf,
                     "ratio": (best["grouped"] / pr) if best["grouped"] and pr else None,
-                    "ratio_forms": (best["grouped_forms"] / pr) if best["grouped_forms"] and pr else None})
+                    "ratio_forms": (best["grouped_forms"] / pr) if best["grouped_forms"] and pr else None,
+                    "ratio_forms_same_arith": (best["grouped_forms"] / prf) if best["grouped_forms"] and prf
+                    else None})
     out["at_equal_p99"] = slo
     if with_forms:
         out["forms"] = dict(SERVE_FORMS, note="grouped_forms: requests at or above the flop thresholds run alone "
@@ -743,7 +747,10 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
                         "ratio": sat["grouped"]["tflops"] / sat["per_request"]["tflops"]}
     if with_forms:
         out["saturated"]["grouped_forms_tflops"] = sat["grouped_forms"]["tflops"]
+        out["saturated"]["per_request_forms_tflops"] = sat["per_request_forms"]["tflops"]
         out["saturated"]["ratio_forms"] = sat["grouped_forms"]["tflops"] / sat["per_request"]["tflops"]
+        out["saturated"]["ratio_forms_same_arith"] = (sat["grouped_forms"]["tflops"] /
+                                                      sat["per_request_forms"]["tflops"])
     del pools
     torch.cuda.empty_cache()
     return out

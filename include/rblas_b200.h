@@ -479,6 +479,16 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
  * partials are summed in a fixed order, so a problem's result is the same
  * whatever else shares the launch. 0 for an invalid problem. */
 int rb_gemm_grouped_splits(const rb_gemm_problem* p);
+/* Many f64 GEMMs in the Ozaki form (RB_PREC_OZAKI) in one grouped launch on
+ * `stream` (no rblas counterpart; each entry stands for one
+ * level3::gemm::<f64>, src/level3.rs:32-62): one exponent pass and one slice
+ * pass over every operand, then one persistent tensor-core kernel over the
+ * tiles of all problems, longest tiles first. Each result equals that
+ * problem's own rb_dgemm_dev(..., RB_PREC_OZAKI, ...) bit for bit. Every
+ * entry must be f64 (RB_ERR_UNSUPPORTED, err->got = its index, otherwise);
+ * checks as rb_gemm_grouped_dev. Returns once the work is enqueued. */
+rb_status rb_gemm_grouped_ozaki_dev(const rb_gemm_problem* problems, size_t count, void* stream,
+                                    rb_error* err);
 
 /* A grouped launch frozen into a CUDA graph: the problem table (with its
  * TMA descriptors), the split-K workspace and any repack scratch are built

@@ -601,7 +601,11 @@ int grouped_gemm_dev(const rb_gemm_problem* probs, size_t count, const void* con
     uint8_t* mem = nullptr;
     if (own) {
         e = scratch_alloc(reinterpret_cast<void**>(&mem), own, st);
-        if (e != cudaSuccess) { if (ce) *ce = e; return RB_ERR_CUDA; }
+        if (e != cudaSuccess) {
+            if (ce) *ce = e;
+            if (e == cudaErrorMemoryAllocation) cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? RB_ERR_ALLOC : RB_ERR_CUDA;
+        }
     }
     if (staged) {
         host = static_cast<uint8_t*>(staging->host);

@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <vector>
 #include <type_traits>
@@ -305,6 +306,12 @@ constexpr int kOzEpiWarps = 16;
 constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;
 constexpr int kOzColTab = 64 * (8 + 4);             // per epilogue warp: 2^fc (double) and fc (int), 64 columns
 constexpr int kOzSmem = kOzST * kOzStage + 256 + kOzEpiWarps * kOzColTab + 1024;
+// Tile rows per rasterisation group. A wave of 148 tiles walks R row panels
+// of A and C column panels of B, each once per diagonal-pair unit; B panels
+// (256 columns) are twice the A panels (128 rows), so R ~ 2C (16 x ~9)
+// moves fewer digit-plane bytes through L2 than the 8 x ~18 of the plain
+// kernels.
+constexpr int kOzRaster = 16;
 
 struct OzParams {
     int m, n, k;
@@ -317,6 +324,7 @@ struct OzParams {
     double alpha, beta;
     double* c;
     size_t ldc;
+    const double* cin;  // C0, read for beta != 0: c itself, or a separate input with c's leading dimension
     const int* row_exp;
     const int* col_exp;
     uint32_t* err;
@@ -386,9 +394,67 @@ __host__ __device__ __forceinline__ void oz_item(int num_tiles, int tail_tiles, 
     u_hi = u_lo + 1;
 }
 
-__global__ void __launch_bounds__(kOzThreads, 1)
-    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                      const OzParams p) {
+// One problem of a grouped Ozaki launch: its digit-plane tensor maps (TMA
+// reads them from global memory: 64-byte aligned) and its parameters.
+struct alignas(64) OzGroupEntry {
+    CUtensorMap tmA, tmB;
+    OzParams p;
+};
+
+// One work item as a CTA sees it: its problem, tile and units (oz_item).
+struct OzWork {
+    const OzParams* p;
+    const CUtensorMap* ta;
+    const CUtensorMap* tb;
+    int t, u_lo, u_hi, tt;
+};
+
+// Work of the single-problem kernel: whole tiles, then the split tail's
+// units (oz_item).
+struct OzSingleSrc {
+    const OzParams* p;
+    const CUtensorMap* ta;
+    const CUtensorMap* tb;
+    __device__ __forceinline__ uint32_t* err() const { return p->err; }
+    __device__ __forceinline__ int items() const {
+        const int units = p->kchunks * ((p->slices + 1) / 2);
+        return p->num_tiles + p->tail_tiles * (units - 1);
+    }
+    __device__ __forceinline__ OzWork get(int item) const {
+        OzWork w{p, ta, tb, 0, 0, 0, -1};
+        oz_item(p->num_tiles, p->tail_tiles, p->kchunks, (p->slices + 1) / 2, gridDim.x, item, w.t, w.u_lo, w.u_hi,
+                w.tt);
+        return w;
+    }
+};
+
+// Work of the grouped kernel: item i is one whole tile (fused epilogue, every
+// unit) of problem j, where starts[j] <= i < starts[j+1]. The host orders the
+// problems by the cost of one tile, largest first, so the CTAs' strided walk
+// over the items deals the long tiles out first.
+struct OzGroupSrc {
+    const OzGroupEntry* tab;
+    const int* starts;
+    int nprob;
+    uint32_t* error;
+    __device__ __forceinline__ uint32_t* err() const { return error; }
+    __device__ __forceinline__ int items() const { return __ldg(starts + nprob); }
+    __device__ __forceinline__ OzWork get(int item) const {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(starts + mid) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const OzGroupEntry* g = tab + lo;
+        OzWork w{&g->p, &g->tmA, &g->tmB, item - __ldg(starts + lo), 0, 0, -1};
+        w.u_hi = g->p.kchunks * ((g->p.slices + 1) / 2);
+        return w;
+    }
+};
+
+template <class Src>
+__device__ __forceinline__ void ozaki_body(const Src& src) {
     constexpr int ST = kOzST;
     constexpr int UN = 256;
     constexpr int KSTEPS = 4;
@@ -415,23 +481,27 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = bar->tmem_base;
-    const int upc = (p.slices + 1) / 2;  // units per chunk
-    const int units = p.kchunks * upc;
-    const int items = p.num_tiles + p.tail_tiles * (units - 1);
+    const int items = src.items();
+    uint32_t* const err = src.err();
     bool ok = true;
 
     if (warp == 0 && lane == 0) {
         // ------------------------------ TMA producer ------------------------------
-        prefetch_tmap(&tmA);
-        prefetch_tmap(&tmB);
         uint32_t it = 0;
+        const CUtensorMap* fetched = nullptr;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            int t, u_lo, u_hi, tt;
-            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
+            const OzWork w = src.get(item);
+            const OzParams& p = *w.p;
+            if (w.ta != fetched) {
+                prefetch_tmap(w.ta);
+                prefetch_tmap(w.tb);
+                fetched = w.ta;
+            }
+            const int upc = (p.slices + 1) / 2;
             int tm, tn;
-            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            raster_tile<kOzRaster>(w.t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
-            for (int u = u_lo; ok && u < u_hi; ++u) {
+            for (int u = w.u_lo; ok && u < w.u_hi; ++u) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
@@ -440,15 +510,15 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     const int k0 = kt * 128;
                     for (int i = top; ok && i >= 0; --i, ++it) {  // stage: A_i and B_{top-i}
                         const int s = it % ST;
-                        if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x301)) {
+                        if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, err, 0x301)) {
                             ok = false;
                             break;
                         }
                         uint8_t* sb = smem + s * kOzStage;
                         uint8_t* sa = sb + kBTileOz();
                         mbar_arrive_expect_tx(&bar->full[s], kBTileOz() + kATile);
-                        tma_load_3d(sb, &tmB, &bar->full[s], k0, n0, top - i);
-                        tma_load_3d(sa, &tmA, &bar->full[s], k0, m0, i);
+                        tma_load_3d(sb, w.tb, &bar->full[s], k0, n0, top - i);
+                        tma_load_3d(sa, w.ta, &bar->full[s], k0, m0, i);
                     }
                 }
             }
@@ -461,13 +531,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ------------------------------ MMA issuer ------------------------------
         uint32_t it = 0, uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            int t, u_lo, u_hi, tt;
-            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
-            for (int u = u_lo; ok && u < u_hi; ++u, ++uc) {
+            const OzWork w = src.get(item);
+            const OzParams& p = *w.p;
+            const int upc = (p.slices + 1) / 2;
+            for (int u = w.u_lo; ok && u < w.u_hi; ++u, ++uc) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                if (uc >= 1 && !mbar_wait(&bar->acc_empty[0], (uc - 1) & 1, p.err, 0x302)) {
+                if (uc >= 1 && !mbar_wait(&bar->acc_empty[0], (uc - 1) & 1, err, 0x302)) {
                     ok = false;
                     break;
                 }
@@ -483,7 +554,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     int prev_s = -1;
                     for (int i = top; ok && i >= 0; --i, ++it) {
                         const int s = it % ST;
-                        if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x303)) {
+                        if (!mbar_wait(&bar->full[s], (it / ST) & 1, err, 0x303)) {
                             ok = false;
                             break;
                         }
@@ -530,13 +601,18 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         double* col_scale = reinterpret_cast<double*>(tab);
         int* col_e = reinterpret_cast<int*>(tab + 64 * sizeof(double));
         const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
+        // C between the units of a tile stays in L2 (the tiles in flight hold
+        // ~38 MB of it) while the digit planes stream past; C0's read and the
+        // last unit's write are the tile's final touches
         uint32_t uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
-            int t, u_lo, u_hi, tt;
-            oz_item(p.num_tiles, p.tail_tiles, p.kchunks, upc, gridDim.x, item, t, u_lo, u_hi, tt);
-            const bool split = tt >= 0;
+            const OzWork w = src.get(item);
+            const OzParams& p = *w.p;
+            const int upc = (p.slices + 1) / 2;
+            const int units = p.kchunks * upc;
+            const bool split = w.tt >= 0;
             int tm, tn;
-            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            raster_tile<kOzRaster>(w.t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
@@ -557,11 +633,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             }
             __syncwarp();
             double* const crow = p.c + (row_ok ? r : 0);
+            const double* const c0row = p.cin + (row_ok ? r : 0);
             const size_t ldc = p.ldc;
-            for (int u = u_lo; ok && u < u_hi; ++u, ++uc) {
+            for (int u = w.u_lo; ok && u < w.u_hi; ++u, ++uc) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const bool first_unit = (u == 0);
+                const uint64_t pol_ld = first_unit ? l2_evict_first_policy() : l2_evict_last_policy();
+                const uint64_t pol_st = (u == units - 1) ? l2_evict_first_policy() : l2_evict_last_policy();
+                // the first unit reads C0 (beta * C0), the later ones the running sum in C
+                const double* const srow = first_unit ? c0row : crow;
                 // digits of both operands are scaled by 2^-(e+1): weight 2^-(14+8d) per diagonal
                 const int wexp = 14 + 8 * (d1 >= 0 ? d1 : d0) - 2;
                 // the row's part of the scale first: sv * 2^(er - wexp) is exact
@@ -578,7 +659,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 // every live row of the warp takes the two-multiply scaling
                 const bool warp_fast = __all_sync(0xffffffffu, row_fast || !live);
                 double* wplane =
-                    split ? p.ws + (static_cast<size_t>(tt) * units + u) * kOzTileElems + row_in_tile : nullptr;
+                    split ? p.ws + (static_cast<size_t>(w.tt) * units + u) * kOzTileElems + row_in_tile : nullptr;
                 // chunk ch's C values are requested one chunk ahead (the first
                 // chunk's before the accumulator wait), so a chunk's L2 round
                 // trip overlaps the previous chunk's arithmetic
@@ -586,10 +667,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
                     const int cbase = n0 + cq * 64;
-                    cv[jj] = (live && read_c && cbase + jj < p.n) ? crow[static_cast<size_t>(cbase + jj) * ldc] : 0.0;
+                    cv[jj] = (live && read_c && cbase + jj < p.n)
+                                 ? ld_l2hint(srow + static_cast<size_t>(cbase + jj) * ldc, pol_ld) : 0.0;
                 }
                 {
-                    const bool got = mbar_wait(&bar->acc_full[0], uc & 1, p.err, 0x304);
+                    const bool got = mbar_wait(&bar->acc_full[0], uc & 1, err, 0x304);
                     if (!__all_sync(0xffffffffu, got)) {  // the whole warp goes on, or the whole warp stops
                         ok = false;
                         break;
@@ -603,10 +685,12 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     const int col0 = cq * 64 + j0;
                     const int cbase = n0 + col0;
                     double* const cp = crow + static_cast<size_t>(cbase) * ldc;
+                    const double* const sp = srow + static_cast<size_t>(cbase) * ldc;
                     double cn[8];
 #pragma unroll
                     for (int jj = 0; jj < 8; ++jj)
-                        cn[jj] = (live && read_c && ch < 7 && cbase + 8 + jj < p.n) ? cp[(8 + jj) * ldc] : 0.0;
+                        cn[jj] = (live && read_c && ch < 7 && cbase + 8 + jj < p.n)
+                                     ? ld_l2hint(sp + static_cast<size_t>(8 + jj) * ldc, pol_ld) : 0.0;
                     uint32_t v0[8], v1[8];
                     tmem_ld8(lanebase + col0, v0);
                     if (d1 >= 0) tmem_ld8(lanebase + UN + col0, v1);
@@ -624,7 +708,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                                 } else {
                                     double acc = cv[jj];
                                     if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
-                                    cp[jj * ldc] = fma(p.alpha, term, acc);
+                                    st_l2hint(cp + static_cast<size_t>(jj) * ldc, fma(p.alpha, term, acc), pol_st);
                                 }
                             }
                         } else {
@@ -648,7 +732,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                                     } else {
                                         double acc = cv[jj];
                                         if (first_unit && p.beta_mode == 2) acc = p.beta * acc;
-                                        cp[jj * ldc] = fma(p.alpha, term, acc);
+                                        st_l2hint(cp + static_cast<size_t>(jj) * ldc, fma(p.alpha, term, acc),
+                                                  pol_st);
                                     }
                                 }
                             }
@@ -673,6 +758,20 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
 }
 
+__global__ void __launch_bounds__(kOzThreads, 1)
+    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const __grid_constant__ OzParams p) {
+    ozaki_body(OzSingleSrc{&p, &tmA, &tmB});
+}
+
+// Many f64 problems in one persistent launch (the serving loop's Ozaki
+// batches): the same tiles and epilogue as ozaki_gemm_kernel, whole tiles only.
+__global__ void __launch_bounds__(kOzThreads, 1)
+    ozaki_grouped_kernel(const OzGroupEntry* __restrict__ tab, const int* __restrict__ starts, int nprob,
+                         uint32_t* err) {
+    ozaki_body(OzGroupSrc{tab, starts, nprob, err});
+}
+
 // Split tail: C of the tail tiles = the fused epilogue's sequence over the
 // unit planes, element by element -- acc = beta-pass(C0) for the first unit,
 // then acc = fma(alpha, term_u, acc) in unit order; rows with a zero exponent
@@ -686,13 +785,14 @@ __global__ void ozaki_reduce_kernel(const OzParams p, int units) {
         const int tt = static_cast<int>(idx / kOzTileElems);
         const int local = static_cast<int>(idx - static_cast<size_t>(tt) * kOzTileElems);
         int tm, tn;
-        raster_tile(fused + tt, p.tiles_m, p.tiles_n, tm, tn);
+        raster_tile<kOzRaster>(fused + tt, p.tiles_m, p.tiles_n, tm, tn);
         const int r = tm * kUM + local % kUM, col = tn * 256 + local / kUM;
         if (r >= p.m || col >= p.n) continue;
         double* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
+        const double c0 = p.beta_mode ? p.cin[r + static_cast<size_t>(col) * p.ldc] : 0.0;
         double acc = 0.0;
-        if (p.beta_mode == 1) acc = *cp;
-        else if (p.beta_mode == 2) acc = p.beta * *cp;
+        if (p.beta_mode == 1) acc = c0;
+        else if (p.beta_mode == 2) acc = p.beta * c0;
         const double* w = p.ws + static_cast<size_t>(tt) * units * kOzTileElems + local;
         const int last = (p.row_exp[r] == kExpSentinel) ? 1 : units;
         for (int u = 0; u < last; ++u) acc = fma(p.alpha, w[static_cast<size_t>(u) * kOzTileElems], acc);
@@ -727,12 +827,13 @@ __global__ void fill_int_kernel(int* p, int n, int v) {
 __device__ __forceinline__ long long abs_bits(double v) {
     return __double_as_longlong(v) & 0x7FFFFFFFFFFFFFFFLL;
 }
-// K-contiguous view: one warp per row, a 1024-wide K slab per blockIdx.y.
-__global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, int R, int K,
-                                       int* __restrict__ e) {
-    const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+// K-contiguous view: one warp per row (8 rows per 256-thread block), a
+// 1024-wide K slab per block row by.
+__device__ __forceinline__ void row_exp_kcontig(const double* __restrict__ x, size_t rs, int R, int K,
+                                                int* __restrict__ e, int bx, int by) {
+    const int r = bx * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (r >= R) return;
-    const int p0 = blockIdx.y * 1024, p1 = min(K, p0 + 1024);
+    const int p0 = by * 1024, p1 = min(K, p0 + 1024);
     long long best = 0;
 #pragma unroll 8
     for (int q = p0 + (threadIdx.x & 31); q < p1; q += 32) best = max(best, abs_bits(x[static_cast<size_t>(r) * rs + q]));
@@ -740,16 +841,24 @@ __global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, 
     if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(e + r, frexp_exp(__longlong_as_double(best)));
 }
 // R-contiguous view: one thread per row (coalesced across the warp), a
-// 32-wide K slab per blockIdx.y so the grid covers the whole matrix.
-__global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, int R, int K,
-                                       int* __restrict__ e) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+// 32-wide K slab per block row by so the grid covers the whole matrix.
+__device__ __forceinline__ void row_exp_rcontig(const double* __restrict__ x, size_t ps, int R, int K,
+                                                int* __restrict__ e, int bx, int by) {
+    const int r = bx * blockDim.x + threadIdx.x;
     if (r >= R) return;
-    const int p0 = blockIdx.y * 32, p1 = min(K, p0 + 32);
+    const int p0 = by * 32, p1 = min(K, p0 + 32);
     long long best = 0;
 #pragma unroll 8
     for (int q = p0; q < p1; ++q) best = max(best, abs_bits(x[r + static_cast<size_t>(q) * ps]));
     if (best != 0) atomicMax(e + r, frexp_exp(__longlong_as_double(best)));
+}
+__global__ void row_exp_kcontig_kernel(const double* __restrict__ x, size_t rs, int R, int K,
+                                       int* __restrict__ e) {
+    row_exp_kcontig(x, rs, R, K, e, blockIdx.x, blockIdx.y);
+}
+__global__ void row_exp_rcontig_kernel(const double* __restrict__ x, size_t ps, int R, int K,
+                                       int* __restrict__ e) {
+    row_exp_rcontig(x, ps, R, K, e, blockIdx.x, blockIdx.y);
 }
 
 constexpr int kTile = 64;
@@ -813,14 +922,16 @@ __device__ __forceinline__ Int floor_scaled(double x, int n) {
 }
 
 // S slices known at compile time: up to 8 digits the integer fits 64 bits.
+// One 64 x 64 tile of the R x K view per 256-thread block: K tile bx, row
+// tile by.
 template <int S>
-__global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
-                                                          int R, int K, const int* __restrict__ e,
-                                                          int8_t* __restrict__ out, size_t kp, size_t plane) {
+__device__ __forceinline__ void ozaki_slice_tile(const double* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                                                 const int* __restrict__ e, int8_t* __restrict__ out, size_t kp,
+                                                 size_t plane, int bx, int by) {
     using Int = typename std::conditional<(S <= 8), long long, __int128>::type;
     constexpr int slices = S;
     __shared__ double tile[kTile][kTile + 1];
-    const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
+    const int r0 = by * kTile, p0 = bx * kTile;
     load_tile<double>(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;  // 64 rows x 4 chunks of 16
@@ -885,6 +996,58 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
 #pragma unroll
     for (int t = 0; t < S; ++t)
         *reinterpret_cast<uint4*>(out + t * plane + off) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ x, size_t rs, size_t ps,
+                                                          int R, int K, const int* __restrict__ e,
+                                                          int8_t* __restrict__ out, size_t kp, size_t plane) {
+    ozaki_slice_tile<S>(x, rs, ps, R, K, e, out, kp, plane, blockIdx.x, blockIdx.y);
+}
+
+// ---- grouped pre-pass: one launch per pass over every operand of a batch ------
+
+// One operand of a grouped Ozaki launch, viewed as R x K (element (r, p) at
+// x[r*rs + p*ps]): its exponents e[R] and digit planes out[slices][R][kp].
+// exp_blocks / slice_blocks: the blocks it takes in each pass (the grid's
+// blocks are dealt to operands by the prefix sums exp_start / slice_start).
+struct OzOperand {
+    const double* x;
+    size_t rs, ps;
+    int R, K;
+    int* e;
+    int8_t* out;
+    size_t kp, plane;
+    int exp_gx, slice_gx;  // blocks along R (exponent pass) / along K (slice pass)
+    int exp_start, slice_start;
+};
+
+__device__ __forceinline__ int oz_find_operand(const OzOperand* ops, int nops, int b, bool slice) {
+    int lo = 0, hi = nops - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((slice ? ops[mid].slice_start : ops[mid].exp_start) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The exponent pass of every operand (grid = total exponent blocks; e
+// pre-filled with the zero-row sentinel).
+__global__ void __launch_bounds__(256) ozaki_exp_grouped_kernel(const OzOperand* __restrict__ ops, int nops) {
+    const OzOperand& o = ops[oz_find_operand(ops, nops, blockIdx.x, false)];
+    const int b = blockIdx.x - o.exp_start;
+    const int bx = b % o.exp_gx, by = b / o.exp_gx;
+    if (o.ps == 1) row_exp_kcontig(o.x, o.rs, o.R, o.K, o.e, bx, by);
+    else           row_exp_rcontig(o.x, o.ps, o.R, o.K, o.e, bx, by);
+}
+
+// The slice pass of every operand (grid = total slice tiles).
+template <int S>
+__global__ void __launch_bounds__(256) ozaki_slice_grouped_kernel(const OzOperand* __restrict__ ops, int nops) {
+    const OzOperand& o = ops[oz_find_operand(ops, nops, blockIdx.x, true)];
+    const int b = blockIdx.x - o.slice_start;
+    ozaki_slice_tile<S>(o.x, o.rs, o.ps, o.R, o.K, o.e, o.out, o.kp, o.plane, b % o.slice_gx, b / o.slice_gx);
 }
 
 // Host dispatch on the slice count (2 .. 12).
@@ -1178,6 +1341,7 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     p.beta_mode = (beta == 0.0) ? 0 : (beta == 1.0 ? 1 : 2);
     p.alpha = alpha; p.beta = beta;
     p.c = C; p.ldc = ldc;
+    p.cin = C;
     p.row_exp = ea; p.col_exp = eb;
     p.err = device_error_word();
     if (tail_tiles > 0) {
@@ -1208,6 +1372,212 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     e = cudaGetLastError();
     cudaFreeAsync(buf, st);
     return e;
+}
+
+// Many f64 GEMMs in the Ozaki form with three launches for the whole batch:
+// one exponent pass and one slice pass over every operand, then one
+// persistent ozaki_grouped_kernel over every problem's tiles. probs[i] is
+// column-major or row-major like rb_gemm_problem; its C0 is read from
+// cin[i] (leading dimension ldcin[i]; probs[i].c itself when cin is null) and
+// the result goes to probs[i].c. Every tile runs the fused epilogue of
+// ozaki_gemm_kernel, so each result equals that problem's own
+// rb_dgemm_dev(..., RB_PREC_OZAKI, ...) bit for bit.
+int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
+                      cudaStream_t st, int32_t* ce) {
+    const int slices = rb_get_ozaki_slices();
+    const long long kt_chunk = std::max(2147483647LL / (static_cast<long long>(slices) * 128 * 128) / 128, 1LL);
+    struct Job {
+        bool ta, tb;
+        int m, n, k;
+        const double *a, *b;
+        size_t lda, ldb;
+        double* c;
+        const double* c0;
+        size_t ldc;
+        double alpha, beta;
+        size_t kp, off_exp, off_a, off_b;
+        int num_kt;
+    };
+    std::vector<Job> jobs;
+    jobs.reserve(count);
+    size_t exps = 0, planes = 0;
+    cudaError_t e = cudaSuccess;
+    for (size_t i = 0; i < count; ++i) {
+        const rb_gemm_problem& q = probs[i];
+        if (q.dtype != 1) return RB_ERR_UNSUPPORTED;
+        const int v = validate_problem(q);
+        if (v != RB_OK) return v;
+        const bool col = q.layout == RB_COL_MAJOR;
+        const size_t m = col ? q.m : q.n, n = col ? q.n : q.m;
+        if (m == 0 || n == 0) continue;
+        if (m > 0x7fffffff || n > 0x7fffffff || q.k > 0x7fffffff) return RB_ERR_INVALID_ARG;
+        double* c = static_cast<double*>(q.c);
+        const double* c0 = cin ? static_cast<const double*>(cin[i]) : c;
+        const size_t ldc0 = cin ? ldcin[i] : q.ldc;
+        if (q.beta != 0.0 && c0 != c && ldc0 != q.ldc) {
+            // the kernels read C0 with C's leading dimension: bring it into C first
+            e = cudaMemcpy2DAsync(c, q.ldc * 8, c0, ldc0 * 8, m * 8, n, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) break;
+            c0 = c;
+        }
+        if (q.k == 0 || q.alpha == 0.0) {  // C = beta * C0 only (gemm_contig's early out)
+            if (q.beta != 0.0 && c0 != c) {
+                e = cudaMemcpy2DAsync(c, q.ldc * 8, c0, q.ldc * 8, m * 8, n, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) break;
+            }
+            e = launch_scale_c<double>(static_cast<int>(m), static_cast<int>(n), q.beta, c, q.ldc, st);
+            if (e != cudaSuccess) break;
+            continue;
+        }
+        Job j{};
+        const bool ta = q.transa != RB_NO_TRANS, tb = q.transb != RB_NO_TRANS;
+        j.ta = col ? ta : tb;
+        j.tb = col ? tb : ta;
+        j.m = static_cast<int>(m);
+        j.n = static_cast<int>(n);
+        j.k = static_cast<int>(q.k);
+        j.a = static_cast<const double*>(col ? q.a : q.b);
+        j.b = static_cast<const double*>(col ? q.b : q.a);
+        j.lda = col ? q.lda : q.ldb;
+        j.ldb = col ? q.ldb : q.lda;
+        j.c = c;
+        j.c0 = c0;
+        j.ldc = q.ldc;
+        j.alpha = q.alpha;
+        j.beta = q.beta;
+        j.kp = round_up(q.k, 16);
+        j.num_kt = static_cast<int>((q.k + 127) / 128);
+        j.off_exp = exps;
+        exps += m + n;
+        j.off_a = planes;
+        planes += round_up(slices * m * j.kp, 256);
+        j.off_b = planes;
+        planes += round_up(slices * n * j.kp, 256);
+        jobs.push_back(j);
+    }
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        return RB_ERR_CUDA;
+    }
+    if (jobs.empty()) return RB_OK;
+    // longest tiles first: the CTAs walk the items with a stride of the grid
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& x, const Job& y) { return x.num_kt > y.num_kt; });
+    const int np = static_cast<int>(jobs.size());
+    // device image: [entries][starts][operands] then exponents, then planes
+    const size_t ent_bytes = round_up(np * sizeof(OzGroupEntry), 256);
+    const size_t starts_bytes = round_up((np + 1) * sizeof(int), 256);
+    const size_t ops_bytes = round_up(2 * np * sizeof(OzOperand), 256);
+    const size_t img_bytes = ent_bytes + starts_bytes + ops_bytes;
+    const size_t exp_bytes = round_up(exps * sizeof(int), 256);
+    uint8_t* mem = nullptr;
+    e = scratch_alloc(reinterpret_cast<void**>(&mem), img_bytes + exp_bytes + planes, st);
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        if (e == cudaErrorMemoryAllocation) cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? RB_ERR_ALLOC : RB_ERR_CUDA;
+    }
+    std::vector<uint8_t> img(img_bytes, 0);
+    int* starts = reinterpret_cast<int*>(img.data() + ent_bytes);
+    OzOperand* ops = reinterpret_cast<OzOperand*>(img.data() + ent_bytes + starts_bytes);
+    int* dexp = reinterpret_cast<int*>(mem + img_bytes);
+    int8_t* dplanes = reinterpret_cast<int8_t*>(mem + img_bytes + exp_bytes);
+    uint32_t* err_word = device_error_word();
+    int tiles = 0, exp_blocks = 0, slice_blocks = 0;
+    double work = 0;
+    CUresult r = CUDA_SUCCESS;
+    for (int i = 0; i < np && r == CUDA_SUCCESS; ++i) {
+        const Job& j = jobs[i];
+        int* ea = dexp + j.off_exp;
+        int* eb = ea + j.m;
+        int8_t* sla = dplanes + j.off_a;
+        int8_t* slb = dplanes + j.off_b;
+        size_t ars, aps, brs, bps;
+        operand_views(j.ta, j.tb, j.lda, j.ldb, ars, aps, brs, bps);
+        const int kb = (j.k + 1023) / 1024, k32 = (j.k + 31) / 32;
+        const int skb = static_cast<int>((j.kp + kTile - 1) / kTile);
+        const struct { const double* x; size_t rs, ps; int R; int* e; int8_t* out; } od[2] = {
+            {j.a, ars, aps, j.m, ea, sla}, {j.b, brs, bps, j.n, eb, slb}};
+        for (int h = 0; h < 2; ++h) {
+            OzOperand& o = ops[2 * i + h];
+            o.x = od[h].x; o.rs = od[h].rs; o.ps = od[h].ps;
+            o.R = od[h].R; o.K = j.k;
+            o.e = od[h].e; o.out = od[h].out;
+            o.kp = j.kp; o.plane = static_cast<size_t>(od[h].R) * j.kp;
+            o.exp_gx = (o.ps == 1) ? (o.R + 7) / 8 : (o.R + 255) / 256;
+            o.slice_gx = skb;
+            o.exp_start = exp_blocks;
+            o.slice_start = slice_blocks;
+            exp_blocks += o.exp_gx * ((o.ps == 1) ? kb : k32);
+            slice_blocks += skb * ((o.R + kTile - 1) / kTile);
+        }
+        OzGroupEntry g{};  // 64-byte aligned here; copied into the image below
+        r = make_tmap_planes(&g.tmA, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, j.k, j.m, slices, j.kp, kUM);
+        if (r == CUDA_SUCCESS)
+            r = make_tmap_planes(&g.tmB, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, j.k, j.n, slices, j.kp, 256);
+        OzParams& p = g.p;
+        p.m = j.m; p.n = j.n; p.k = j.k;
+        p.tiles_m = (j.m + kUM - 1) / kUM;
+        p.tiles_n = (j.n + 255) / 256;
+        p.num_tiles = p.tiles_m * p.tiles_n;
+        p.num_kt = j.num_kt;
+        p.slices = slices;
+        p.kt_per_chunk = static_cast<int>(kt_chunk);
+        p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
+        p.beta_mode = (j.beta == 0.0) ? 0 : (j.beta == 1.0 ? 1 : 2);
+        p.alpha = j.alpha; p.beta = j.beta;
+        p.c = j.c; p.ldc = j.ldc;
+        p.cin = j.c0;
+        p.row_exp = ea; p.col_exp = eb;
+        p.err = err_word;
+        std::memcpy(img.data() + i * sizeof(OzGroupEntry), &g, sizeof(OzGroupEntry));
+        starts[i] = tiles;
+        tiles += p.num_tiles;
+        work += 2.0 * j.m * j.n * static_cast<double>(j.k) * slices * (slices + 1) / 2;
+    }
+    starts[np] = tiles;
+    if (r != CUDA_SUCCESS) {
+        if (ce) *ce = static_cast<int32_t>(r);
+        cudaFreeAsync(mem, st);
+        return RB_ERR_CUDA;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    constexpr int smem = kOzSmem;
+    static bool attr = false;
+    if (!attr) {
+        e = cudaFuncSetAttribute(ozaki_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess) attr = true;
+    }
+    // a pageable source: the driver has staged the image when the call returns
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mem, img.data(), img_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const OzOperand* dops = reinterpret_cast<const OzOperand*>(mem + ent_bytes + starts_bytes);
+        fill_int_kernel<<<static_cast<unsigned>(std::min<size_t>((exps + 255) / 256, 1024)), 256, 0, st>>>(
+            dexp, static_cast<int>(exps), kExpSentinel);
+        ozaki_exp_grouped_kernel<<<exp_blocks, 256, 0, st>>>(dops, 2 * np);
+        switch (slices) {
+#define RB_SLICES(S) \
+    case S: ozaki_slice_grouped_kernel<S><<<slice_blocks, 256, 0, st>>>(dops, 2 * np); break;
+            RB_SLICES(2) RB_SLICES(3) RB_SLICES(4) RB_SLICES(5) RB_SLICES(6) RB_SLICES(7) RB_SLICES(8)
+            RB_SLICES(9) RB_SLICES(10) RB_SLICES(11) RB_SLICES(12)
+#undef RB_SLICES
+            default: break;
+        }
+        KernelTimer tmr;
+        kernel_timing_begin("umma_ozaki_grouped_i8", work, st, &tmr);
+        ozaki_grouped_kernel<<<tiles < sms ? tiles : sms, kOzThreads, smem, st>>>(
+            reinterpret_cast<const OzGroupEntry*>(mem), reinterpret_cast<const int*>(mem + ent_bytes), np, err_word);
+        kernel_timing_end(&tmr, st);
+        count_launch(4);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(mem, st);
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        return RB_ERR_CUDA;
+    }
+    return RB_OK;
 }
 
 }  // namespace rb
@@ -1373,6 +1743,7 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         p.beta_mode = (beta == 0.0) ? 0 : (beta == 1.0 ? 1 : 2);
         p.alpha = alpha; p.beta = beta;
         p.c = c; p.ldc = ldc;
+        p.cin = c;
         p.row_exp = ea; p.col_exp = eb;
         p.err = status;
         constexpr int smem = kOzSmem;

@@ -280,7 +280,26 @@ struct ColProblem {
     const T* b; size_t ldb;
     T* c; size_t ldc;
     int tri = 0;  // syrk: restrict C to one triangle
+    bool split_ok = true;  // the plain form may take the grouped kernel's split-K
 };
+
+// The plain problem as one grouped-kernel entry; true when the grouped
+// kernel's shape rule splits its K (fewer C tiles than SMs and a long K).
+template <typename T>
+bool plain_split(const ColProblem<T>& p, rb_gemm_problem* q) {
+    *q = rb_gemm_problem{};
+    q->dtype = sizeof(T) == 8 ? 1 : 0;
+    q->layout = RB_COL_MAJOR;
+    q->transa = p.ta ? RB_TRANS : RB_NO_TRANS;
+    q->transb = p.tb ? RB_TRANS : RB_NO_TRANS;
+    q->m = p.m; q->n = p.n; q->k = p.k;
+    q->alpha = static_cast<double>(p.alpha);
+    q->beta = static_cast<double>(p.beta);
+    q->a = p.a; q->lda = p.lda;
+    q->b = p.b; q->ldb = p.ldb;
+    q->c = p.c; q->ldc = p.ldc;
+    return !p.tri && grouped_splits(*q) > 1;
+}
 
 template <typename T>
 ColProblem<T> normalise(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
@@ -352,6 +371,16 @@ rb_status run_dev(const ColProblem<T>& p, rb_precision prec, cudaStream_t st, rb
             return RB_ERR_UNSUPPORTED;
         }
         return run_precision_form(p, prec, st, err);
+    }
+    // Fewer C tiles than SMs and a long K (the 1024^3 SGEMM: 64 tiles): the
+    // grouped kernel's deterministic split-K fills the GPU. The factor
+    // depends on the shape alone, so a call's bits repeat from call to call.
+    rb_gemm_problem gq;
+    if (p.split_ok && plain_split(p, &gq)) {
+        int32_t ce = 0;
+        const int rc = grouped_gemm_dev(&gq, 1, nullptr, nullptr, st, &ce, nullptr);
+        if (rc != RB_OK) set_err(err, rc, 0, 0, 0, ce);
+        return static_cast<rb_status>(rc);
     }
     const T* A = p.a;
     const T* B = p.b;
@@ -472,7 +501,11 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
     const size_t el = sizeof(T);
     const size_t total_bytes = (need_ab ? (a_rows * a_cols + b_rows * b_cols) * el : 0) +
                                p.m * p.n * el * (read_c ? 2 : 1);
-    if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256) {
+    // a plain call whose whole shape takes split-K runs whole (a panel's
+    // split could differ, and with it the summation order)
+    rb_gemm_problem whole;
+    const bool whole_split = prec == RB_PREC_PLAIN && plain_split(p, &whole);
+    if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256 && !whole_split) {
         const size_t width = std::max<size_t>(256, (p.n + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
         if (need_ab) {
             e = cudaMemcpy2DAsync(dA, lda_d * el, p.a, p.lda * el, a_rows * el, a_cols, cudaMemcpyHostToDevice, st);
@@ -502,6 +535,7 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
             }
             ColProblem<T> q = p;
             q.n = jn;
+            q.split_ok = false;  // as in the whole call
             q.a = dA; q.lda = lda_d;
             q.b = p.tb ? dB + j0 : dB + j0 * ldb_d; q.ldb = ldb_d;
             q.c = dC + j0 * ldc_d; q.ldc = ldc_d;

@@ -243,12 +243,38 @@ __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// ---- L2 eviction priority -------------------------------------------------------
+
+// Cache policies for ld/st.global.L2::cache_hint: evict_last keeps a line in
+// L2 ahead of normal traffic (data the same CTA comes back to), evict_first
+// lets it go first (data read or written for the last time).
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// volatile: kept in program order with the hinted stores to the same lines
+// (every access of the Ozaki epilogue to C goes through these two)
+__device__ __forceinline__ double ld_l2hint(const double* p, uint64_t pol) {
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_l2hint(double* p, double v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+
 // ---- grid rasterisation --------------------------------------------------------
 
 // Linear block id -> (tile_m, tile_n), walking tile columns in groups of G
 // tile rows so concurrently resident CTAs share A rows and B columns in L2.
+template <int G = 8>
 __device__ __forceinline__ void raster_tile(int bid, int tiles_m, int tiles_n, int& tm, int& tn) {
-    constexpr int G = 8;
     const int per_group = G * tiles_n;
     const int group = bid / per_group;
     const int first_m = group * G;

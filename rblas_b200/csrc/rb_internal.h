@@ -128,6 +128,13 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
                               size_t lda, const double* B, size_t ldb, double beta, double* C,
                               size_t ldc, int slices, cudaStream_t st, CUresult* cu_err);
 
+// Many f64 problems in the Ozaki form in one grouped launch (plus one
+// exponent and one slice pass over all operands). cin / ldcin (optional)
+// name each problem's C0 when it is not probs[i].c. Results equal each
+// problem's own Ozaki call bit for bit. Returns an rb_status value.
+int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
+                      cudaStream_t st, int32_t* ce);
+
 // ---- Level-3 routines on device pointers (all column-major; complex
 // operands interleaved {re, im}; return rb_status values) -------------------
 template <typename T>

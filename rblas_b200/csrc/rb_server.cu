@@ -335,7 +335,32 @@ public:
             for (size_t i = 0; i < plain.size() && rc == RB_OK; ++i)
                 rc = single_gemm_dev(&plain[i], plain_cin[i], plain_ldcin[i], st, &ce);
         }
+        // the batch's f64 requests in the Ozaki form: one grouped launch when
+        // there are several (a lone one takes the single-problem kernel,
+        // whose unit-split tail keeps every SM busy on a few tiles)
+        std::vector<rb_gemm_problem> oz;
+        std::vector<const void*> oz_cin;
+        std::vector<size_t> oz_ldcin;
+        size_t n_oz = 0;
+        for (size_t i : alone) n_oz += (probs[i].dtype == 1 && b.form[1] == RB_PREC_OZAKI);
+        const bool group_oz = n_oz >= 2;
+        for (size_t i : alone)
+            if (group_oz && probs[i].dtype == 1) {
+                oz.push_back(probs[i]);
+                oz_cin.push_back(cin[i]);
+                oz_ldcin.push_back(ldcin[i]);
+            }
+        if (!oz.empty() && rc == RB_OK) {
+            const int f = next_form_stream;
+            next_form_stream = (next_form_stream + 1) % kFormStreams;
+            rc = ozaki_grouped_dev(oz.data(), oz.size(), oz_cin.data(), oz_ldcin.data(), form_streams[f], &ce);
+            if (rc == RB_OK) {
+                cudaEventRecord(form_events[f], form_streams[f]);
+                cudaStreamWaitEvent(st, form_events[f], 0);
+            }
+        }
         for (size_t i = 0; i < alone.size() && rc == RB_OK; ++i) {
+            if (group_oz && probs[alone[i]].dtype == 1) continue;  // in the grouped launch
             // on a form stream; the batch's stream then waits for it, so the
             // batch's completion event covers the request
             const int f = next_form_stream;
@@ -500,6 +525,33 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
 }
 
 int rb_gemm_grouped_splits(const rb_gemm_problem* p) { return p ? grouped_splits(*p) : 0; }
+
+rb_status rb_gemm_grouped_ozaki_dev(const rb_gemm_problem* problems, size_t count, void* stream, rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if (count && !problems) {
+        if (err) err->code = RB_ERR_INVALID_ARG;
+        return RB_ERR_INVALID_ARG;
+    }
+    for (size_t i = 0; i < count; ++i) {
+        const rb_gemm_problem& q = problems[i];
+        const int v = q.dtype != 1 ? RB_ERR_UNSUPPORTED : validate_problem(q);
+        const bool null_ptr = q.m && q.n && (!q.c || (q.k && q.alpha != 0.0 && (!q.a || !q.b)));
+        if (v != RB_OK || null_ptr) {
+            if (err) {
+                err->code = v != RB_OK ? v : RB_ERR_INVALID_ARG;
+                err->got = i;
+            }
+            return static_cast<rb_status>(v != RB_OK ? v : RB_ERR_INVALID_ARG);
+        }
+    }
+    int32_t ce = 0;
+    const int rc = ozaki_grouped_dev(problems, count, nullptr, nullptr, static_cast<cudaStream_t>(stream), &ce);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
 
 rb_status rb_gemm_grouped_plan_create(const rb_gemm_problem* problems, size_t count, void** plan, rb_error* err) {
     if (err) *err = rb_error{0, 0, 0, 0, 0};

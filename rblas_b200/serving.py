@@ -11,7 +11,7 @@ import numpy as np
 from . import _lib
 from .types import Layout, Transpose
 
-__all__ = ["Problem", "grouped_gemm", "grouped_splits", "GroupedPlan", "Server", "autotune", "autotune_load",
+__all__ = ["Problem", "grouped_gemm", "grouped_gemm_ozaki", "grouped_splits", "GroupedPlan", "Server", "autotune", "autotune_load",
            "autotune_reset"]
 
 
@@ -55,6 +55,16 @@ def grouped_gemm(problems, stream=0):
     err = _lib.RbError()
     st = _lib.load().rb_gemm_grouped_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
                                          C.byref(err))
+    _lib.check(st, err)
+
+
+def grouped_gemm_ozaki(problems, stream=0):
+    """Run f64 problems in the Ozaki form in one grouped launch on `stream`
+    (rb_gemm_grouped_ozaki_dev); each result equals its own Ozaki call."""
+    arr = _array(problems)
+    err = _lib.RbError()
+    st = _lib.load().rb_gemm_grouped_ozaki_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
+                                               C.byref(err))
     _lib.check(st, err)
 
 

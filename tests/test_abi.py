@@ -167,3 +167,23 @@ def test_noalloc_scratch_limit_is_overflow_safe():
     err = _lib.RbError()
     st = lib.rb_dgemm_ozaki_noalloc(1, 0, 0, big, big, big, 1.0, p, big, p, big, 0.0, p, big, None, C.byref(err))
     assert st == 12 and err.got > err.min_or_need == (64 << 20) + (64 << 10)
+
+
+def test_grouped_ozaki_rejects_non_f64_entries_before_any_device_work():
+    """rb_gemm_grouped_ozaki_dev takes f64 problems only: an f32 entry is
+    RB_ERR_UNSUPPORTED with its index, a null C is RB_ERR_INVALID_ARG; both
+    are found before anything is enqueued (no device needed)."""
+    lib = _lib.load()
+    buf = np.zeros(64, dtype=np.float64)
+    p = buf.ctypes.data
+    arr = (_lib.RbGemmProblem * 2)()
+    for i in range(2):
+        arr[i] = _lib.RbGemmProblem(1, 1, 0, 0, 4, 4, 4, 1.0, 0.0, C.c_void_p(p), 4, C.c_void_p(p), 4,
+                                    C.c_void_p(p), 4)
+    arr[1].dtype = 0
+    err = _lib.RbError()
+    assert lib.rb_gemm_grouped_ozaki_dev(arr, 2, None, C.byref(err)) == 5 and err.got == 1
+    arr[1].dtype = 1
+    arr[0].c = None
+    err = _lib.RbError()
+    assert lib.rb_gemm_grouped_ozaki_dev(arr, 2, None, C.byref(err)) == 4 and err.got == 0
