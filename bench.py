@@ -941,6 +941,138 @@ def run_grouped_only(args):
                       "tflops": flops / (ms * 1e-3) / 1e12}))
 
 
+def run_grouped_ozaki_only(args):
+    """The f64 requests among the first `--grouped-ozaki N` requests of the
+    serving stream in the Ozaki form: one grouped launch
+    (rb_gemm_grouped_ozaki_dev) against one single-problem Ozaki call per
+    request and one grouped plain launch, warmup + steps times each."""
+    import torch
+
+    from rblas_b200 import level3
+    from rblas_b200.serving import Problem, grouped_gemm, grouped_gemm_ozaki
+    from rblas_b200.types import Precision
+
+    tr = serving_trace(args.grouped_ozaki)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(6)
+    pool = torch.randn(4096 * 4096 + (1 << 22), dtype=torch.float64, device="cuda", generator=g)
+    probs, flops = [], 0.0
+    keep = []
+    min_flop = args.min_flop
+    for i in range(args.grouped_ozaki):
+        m, n, k = (int(x) for x in tr["mnk"][i])
+        if int(tr["dtype"][i]) != 1 or 2.0 * m * n * k < min_flop:
+            continue
+        layout, ta, tb = int(tr["layout"][i]), int(tr["ta"][i]), int(tr["tb"][i])
+        ar, ac = (k, m) if ta else (m, k)
+        br, bc = (n, k) if tb else (k, n)
+        lda = ar if layout == 1 else ac
+        ldb = br if layout == 1 else bc
+        ldc = m if layout == 1 else n
+        offs = [int(o) // 16 * 16 for o in tr["offs"][i]]
+        c = torch.empty(m * n, dtype=torch.float64, device="cuda").normal_()
+        keep.append(c)
+        probs.append(Problem(np.float64, layout, ta, tb, m, n, k, float(tr["alpha"][i]),
+                             pool.data_ptr() + offs[0] * 8, lda, pool.data_ptr() + offs[1] * 8, ldb,
+                             float(tr["beta"][i]), c.data_ptr(), ldc))
+        flops += 2.0 * m * n * k
+    sh = torch.cuda.current_stream().cuda_stream
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for i in range(args.warmup + args.steps):
+            if i == args.warmup:
+                e0.record()
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(args.steps, 1)
+
+    def singles():
+        for p in probs:
+            level3.gemm_dev(p.layout, p.transa, p.transb, p.m, p.n, p.k, p.alpha, p.a, p.lda, p.b, p.ldb, p.beta,
+                            p.c, p.ldc, np.float64, prec=Precision.Ozaki, stream=sh)
+
+    out = {"grouped_ozaki": len(probs), "flop": flops}
+    for name, fn in (("grouped_ozaki", lambda: grouped_gemm_ozaki(probs, sh)), ("single_ozaki", singles),
+                     ("grouped_plain", lambda: grouped_gemm(probs, sh))):
+        ms = timed(fn)
+        out[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+    print(json.dumps(out))
+
+
+def run_level3_only(args):
+    """One complex GEMM (ConjTrans x NoTrans, `--cplx`) or one Level-3
+    routine (`--level3 syrk|symm|trsm|trmm`, f64, n = k = the shape's N and K)
+    on the `--kernel-only` shape, warmup + steps times (bounded ncu captures
+    of the complex and Level-3 kernels)."""
+    import torch
+
+    from rblas_b200 import _lib, complex3
+    from rblas_b200.types import Precision
+
+    m, n, k = args.shape
+    sh = torch.cuda.current_stream().cuda_stream
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    prec = {"plain": Precision.Plain, "ozaki": Precision.Ozaki, "bf16x3": Precision.Bf16x3,
+            "bf16x6": Precision.Bf16x6}[args.form if args.form != "auto" else "plain"]
+    if args.cplx:
+        dt = torch.float64 if args.dtype == "f64" else torch.float32
+        A, B, C = (torch.randn(2 * x, dtype=dt, device="cuda", generator=g) for x in (k * m, k * n, m * n))
+        cdt = np.complex128 if args.dtype == "f64" else np.complex64
+
+        def one():
+            complex3.gemm_dev(2, 0, m, n, k, 1.0 + 0.5j, A.data_ptr(), k, B.data_ptr(), k, 0.0, C.data_ptr(), m, cdt,
+                              prec=prec, stream=sh)
+        work = 8.0 * m * n * k
+    else:
+        import ctypes as Cc
+        lib = _lib.load()
+        A = torch.randn(max(m, k) * max(m, k), dtype=torch.float64, device="cuda", generator=g) * 0.01
+        A.view(max(m, k), max(m, k)).diagonal().uniform_(1.0, 2.0)
+        B = torch.randn(max(m, k) * max(n, k), dtype=torch.float64, device="cuda", generator=g)
+        C = torch.randn(m * max(n, m), dtype=torch.float64, device="cuda", generator=g)
+        name = args.level3
+        hA, hB, hC = (np.ascontiguousarray(t.cpu().numpy()) for t in (A, B, C))
+        vp = lambda x: Cc.c_void_p(x.ctypes.data)  # noqa: E731
+        err = _lib.RbError()
+        if name == "syrk":
+            def one():
+                lib.rb_dsyrk(1, 0, m, k, 1.0, vp(hA), m, hA.size, 0.5, vp(hC), m, hC.size, Cc.byref(err))
+            work = 1.0 * m * m * k
+        elif name == "symm":
+            def one():
+                lib.rb_dsymm(0, 1, m, n, 1.0, vp(hA), m, hA.size, vp(hB), m, hB.size, 0.5, vp(hC), m, hC.size,
+                             Cc.byref(err))
+            work = 2.0 * m * m * n
+        elif name == "trmm":
+            def one():
+                lib.rb_dtrmm(0, 1, 0, 0, m, n, 1.0, vp(hA), m, hA.size, vp(hB), m, hB.size, Cc.byref(err))
+            work = 1.0 * m * m * n
+        else:
+            def one():
+                lib.rb_dtrsm(0, 1, 0, 0, m, n, 1.0, vp(hA), m, hA.size, vp(hB), m, hB.size, Cc.byref(err))
+            work = 1.0 * m * m * n
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    import time as _t
+    t0 = 0.0
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            torch.cuda.synchronize()
+            e0.record()
+            t0 = _t.perf_counter()
+        one()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"level3_only": args.level3 or "complex", "shape": [m, n, k], "ms": ms,
+                      "wall_ms": (_t.perf_counter() - t0) * 1e3 / max(args.steps, 1),
+                      "tflops": work / (ms * 1e-3) / 1e12}))
+
+
 def run_trsm_batched_only(args):
     """The batched f64 trsm of the C4 configuration (512 x 512 lower, 64
     right-hand sides) on `--trsm-batched BATCH` members, launched warmup +
@@ -989,6 +1121,12 @@ def main():
                     help="Level-1 calls on N-scalar f64 vectors only (bounded ncu captures)")
     ap.add_argument("--grouped-batch", type=int, default=0, metavar="N",
                     help="time one grouped launch of the first N serving requests only")
+    ap.add_argument("--grouped-ozaki", type=int, default=0, metavar="N",
+                    help="the f64 requests among the first N serving requests: grouped Ozaki vs single calls")
+    ap.add_argument("--min-flop", type=float, default=1e9, help="--grouped-ozaki: smallest request kept")
+    ap.add_argument("--cplx", action="store_true", help="--kernel-only shape as a complex C/N GEMM")
+    ap.add_argument("--level3", choices=["", "syrk", "symm", "trsm", "trmm"], default="",
+                    help="--kernel-only shape through one f64 Level-3 host call")
     ap.add_argument("--trsm-batched", type=int, default=0, metavar="BATCH",
                     help="time the batched f64 trsm (512 x 512, 64 RHS) on BATCH members only")
     ap.add_argument("--serve", action="store_true", help="serving sweep (request stream replay)")
@@ -1005,6 +1143,10 @@ def main():
     args = ap.parse_args()
     if args.trsm_batched:
         run_trsm_batched_only(args)
+    elif args.grouped_ozaki:
+        run_grouped_ozaki_only(args)
+    elif args.shape and (args.cplx or args.level3):
+        run_level3_only(args)
     elif args.grouped_batch:
         run_grouped_only(args)
     elif args.level2:

@@ -26,6 +26,7 @@
 #include "../../include/rblas_b200.h"
 #include "rb_device.cuh"
 #include "rb_internal.h"
+#include "simt_tile.cuh"
 
 namespace rb {
 
@@ -254,6 +255,242 @@ cudaError_t tb_launch(const T* A, T* B, T alpha, const TbParams& p, size_t batch
 
 constexpr size_t kTbSmemMax = 227 * 1024;
 
+// ---- f64 on the FP64 tensor cores ------------------------------------------------
+//
+// The substitution above runs 64 dependent steps (shuffle, divide, fold) per
+// diagonal block on one CTA per SM; at the C4 shape it kept the FP64 pipe 17 %
+// busy. The f64 path instead turns every step into a GEMM on DMMA
+// (mma.sync m16n8k8 f64), blocked like the substitution:
+//   1. trsm_inv_diag_kernel inverts every 64 x 64 diagonal block of every
+//      member once, W_b = inv(L_bb) (forward substitution of the unit
+//      vectors; Unit takes the diagonal as 1), into a workspace;
+//   2. trsm_dmma_kernel keeps the member's q x RB slice Y = alpha*B in shared
+//      memory and for each block b computes X_b = W_b * Y_b, then
+//      Y_trailing -= L[trailing, b] * X_b. Both products read A and W as
+//      DMMA fragments straight from global memory (L2: each member's A is
+//      shared by its nrhs/RB CTAs) and Y from shared memory.
+// Rounding differs from rblas's substitution (src/level3.rs:440-512: the
+// blocks' inverses replace the divisions inside each block); the result
+// stays within the normwise backward-error bound the tests state.
+constexpr int kInvNB = 64;
+
+constexpr int kInvSmem = 2 * kInvNB * (kInvNB + 1) * static_cast<int>(sizeof(double));
+
+__global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __restrict__ A0, TbParams p,
+                                                                double* __restrict__ W, int nblocks) {
+    extern __shared__ __align__(16) unsigned char inv_smem[];
+    // L[r][c] of the diagonal block, zero outside it; Wt[c][r] = inv(L)[r][c]
+    // (column c, written by thread c)
+    auto L = reinterpret_cast<double (*)[kInvNB + 1]>(inv_smem);
+    auto Wt = reinterpret_cast<double (*)[kInvNB + 1]>(inv_smem + kInvNB * (kInvNB + 1) * sizeof(double));
+    const int b = blockIdx.x, member = blockIdx.y;
+    const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
+    const int o = b * kInvNB, nb = min(kInvNB, p.q - o);
+    for (int idx = threadIdx.x; idx < kInvNB * kInvNB; idx += kInvNB) {
+        const int r = idx % kInvNB, c = idx / kInvNB;
+        L[r][c] = (r < nb && c < r) ? *a_ptr(A, p, o + r, o + c)
+                                   : ((r < nb && c == r && !p.unit) ? *a_ptr(A, p, o + r, o + c) : 0.0);
+    }
+    __syncthreads();
+    // column j of the inverse, rows in order: w_r = (delta_rj - sum_{s<r} L[r][s] w_s) / L[r][r];
+    // every thread runs the same trip counts (w_s = 0 above row j), so the
+    // warp never diverges and L[r][s] is one broadcast read
+    const int j = threadIdx.x;
+    for (int r = 0; r < kInvNB; ++r) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int s = 0;
+        for (; s + 4 <= r; s += 4) {
+            s0 = fma(L[r][s], Wt[j][s], s0);
+            s1 = fma(L[r][s + 1], Wt[j][s + 1], s1);
+            s2 = fma(L[r][s + 2], Wt[j][s + 2], s2);
+            s3 = fma(L[r][s + 3], Wt[j][s + 3], s3);
+        }
+        for (; s < r; ++s) s0 = fma(L[r][s], Wt[j][s], s0);
+        double w = ((r == j) ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3));
+        if (r >= nb || j >= nb || r < j) w = 0.0;
+        else if (!p.unit) w = w / L[r][r];
+        Wt[j][r] = w;
+    }
+    __syncthreads();
+    double* Wb = W + (static_cast<size_t>(member) * nblocks + b) * (kInvNB * kInvNB);
+    for (int idx = threadIdx.x; idx < kInvNB * kInvNB; idx += kInvNB) {
+        const int r = idx % kInvNB, c = idx / kInvNB;  // column-major: coalesced stores
+        Wb[idx] = Wt[c][r];
+    }
+}
+
+// Y rows padded so that a DMMA B-fragment read (lanes 4g + t reading rows t
+// and t+4, columns g) hits distinct banks: (2 * YS) % 32 must be 8 or 24.
+template <int RB> struct TdCfg;
+template <> struct TdCfg<16> { static constexpr int YS = 20; };
+template <> struct TdCfg<8> { static constexpr int YS = 12; };
+
+template <int RB>
+__global__ void __launch_bounds__(kTbThreads, 2)
+    trsm_dmma_kernel(const double* __restrict__ A0, double* __restrict__ B0, double alpha, TbParams p,
+                     const double* __restrict__ W, int nblocks) {
+    constexpr int YS = TdCfg<RB>::YS;
+    constexpr int NBLK = RB / 8;  // DMMA n-blocks across the slice
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* Y = reinterpret_cast<double*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int member = blockIdx.y;
+    const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
+    double* B = B0 + static_cast<size_t>(member) * p.stride_b;
+    const double* Wm = W + static_cast<size_t>(member) * nblocks * (kInvNB * kInvNB);
+    const int c0 = blockIdx.x * RB;
+    const int ncols = min(RB, p.nrhs - c0);
+    const int q = p.q;
+
+    // Y = alpha * B slice (rows reversed when rev), one rounding per element
+    // as rblas's B := alpha*B (src/level3.rs:403-409)
+    const bool rows_fast = p.ldb_rs == 1;
+    for (int idx = tid; idx < q * RB; idx += kTbThreads) {
+        const int i = rows_fast ? idx % q : idx / RB;
+        const int j = rows_fast ? idx / q : idx % RB;
+        double v = 0.0;
+        if (j < ncols) {
+            v = B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs];
+            if (alpha != 1.0) v = alpha * v;
+        }
+        Y[(p.rev ? q - 1 - i : i) * YS + j] = v;
+    }
+    __syncthreads();
+
+    for (int b = 0; b < nblocks; ++b) {
+        const int o = b * kInvNB, nb = min(kInvNB, q - o);
+        // ---- X_b = W_b * Y_b: 4 m-blocks x NBLK n-blocks, one (m, n) pair per warp
+        const double* Wb = Wm + static_cast<size_t>(b) * (kInvNB * kInvNB);
+        double xacc[4] = {0.0, 0.0, 0.0, 0.0};
+        const bool xw = warp < 4 * NBLK;
+        const int xm = warp % 4, xn = warp / 4;
+        if (xw) {
+            double a[8][4];
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {  // W is column-major 64 x 64, zero outside the block
+                const int r = 16 * xm + g, k = 8 * kk + t;
+                a[kk][0] = __ldg(Wb + r + 64 * k);
+                a[kk][1] = __ldg(Wb + r + 8 + 64 * k);
+                a[kk][2] = __ldg(Wb + r + 64 * (k + 4));
+                a[kk][3] = __ldg(Wb + r + 8 + 64 * (k + 4));
+            }
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                const int k = 8 * kk + t;
+                double bf[2];
+                bf[0] = (k < nb) ? Y[(o + k) * YS + 8 * xn + g] : 0.0;
+                bf[1] = (k + 4 < nb) ? Y[(o + k + 4) * YS + 8 * xn + g] : 0.0;
+                dmma_16x8x8(xacc, a[kk], bf);
+            }
+        }
+        __syncthreads();  // every read of Y_b is done
+        if (xw) {
+            const int r = 16 * xm + g, c = 8 * xn + 2 * t;
+            if (r < nb) {
+                Y[(o + r) * YS + c] = xacc[0];
+                Y[(o + r) * YS + c + 1] = xacc[1];
+            }
+            if (r + 8 < nb) {
+                Y[(o + r + 8) * YS + c] = xacc[2];
+                Y[(o + r + 8) * YS + c + 1] = xacc[3];
+            }
+        }
+        __syncthreads();
+        // ---- trailing rows -= L[trailing, block] * X_b, 16-row m-blocks dealt to the warps
+        const int r_first = o + nb;
+        for (int r0 = r_first + 16 * warp; r0 < q; r0 += 16 * 8) {
+            double a[8][4];
+            const int ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {  // nb == 64 here: only the last block has no trailing rows
+                const int k = o + 8 * kk + t;
+                a[kk][0] = (ra < q) ? __ldg(a_ptr(A, p, ra, k)) : 0.0;
+                a[kk][1] = (rb < q) ? __ldg(a_ptr(A, p, rb, k)) : 0.0;
+                a[kk][2] = (ra < q) ? __ldg(a_ptr(A, p, ra, k + 4)) : 0.0;
+                a[kk][3] = (rb < q) ? __ldg(a_ptr(A, p, rb, k + 4)) : 0.0;
+            }
+            double acc[NBLK][4];
+#pragma unroll
+            for (int n = 0; n < NBLK; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                const int k = o + 8 * kk + t;
+#pragma unroll
+                for (int n = 0; n < NBLK; ++n) {
+                    double bf[2] = {Y[k * YS + 8 * n + g], Y[(k + 4) * YS + 8 * n + g]};
+                    dmma_16x8x8(acc[n], a[kk], bf);
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < NBLK; ++n) {
+                const int c = 8 * n + 2 * t;
+                if (ra < q) {
+                    Y[ra * YS + c] -= acc[n][0];
+                    Y[ra * YS + c + 1] -= acc[n][1];
+                }
+                if (rb < q) {
+                    Y[rb * YS + c] -= acc[n][2];
+                    Y[rb * YS + c + 1] -= acc[n][3];
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    for (int idx = tid; idx < q * RB; idx += kTbThreads) {
+        const int i = rows_fast ? idx % q : idx / RB;
+        const int j = rows_fast ? idx / q : idx % RB;
+        if (j < ncols)
+            B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs] =
+                Y[(p.rev ? q - 1 - i : i) * YS + j];
+    }
+}
+
+template <int RB>
+size_t td_smem(int q) {
+    return static_cast<size_t>(q) * TdCfg<RB>::YS * sizeof(double);
+}
+
+// Workspace of the diagonal-block inverses is bounded: members go in chunks.
+constexpr size_t kTdWorkspace = size_t(256) << 20;
+
+template <int RB>
+cudaError_t td_launch(const double* A, double* B, double alpha, const TbParams& p, size_t batch, cudaStream_t st,
+                      bool* alloc_failed) {
+    const size_t smem = td_smem<RB>(p.q);
+    cudaError_t e = cudaFuncSetAttribute(trsm_dmma_kernel<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(trsm_inv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInvSmem);
+    if (e != cudaSuccess) return e;
+    const int nblocks = (p.q + kInvNB - 1) / kInvNB;
+    const size_t per_member = static_cast<size_t>(nblocks) * kInvNB * kInvNB * sizeof(double);
+    const size_t chunk = std::max<size_t>(1, std::min(batch, kTdWorkspace / per_member));
+    double* W = nullptr;
+    e = scratch_alloc(&W, chunk * per_member, st);
+    if (e != cudaSuccess) {
+        *alloc_failed = e == cudaErrorMemoryAllocation;
+        return e;
+    }
+    KernelTimer tmr;
+    kernel_timing_begin("trsm_batched_d", static_cast<double>(p.q) * p.q * p.nrhs * static_cast<double>(batch), st,
+                        &tmr);
+    for (size_t b0 = 0; b0 < batch && e == cudaSuccess; b0 += chunk) {
+        const size_t nm = std::min(chunk, batch - b0);
+        const double* Ac = A + b0 * p.stride_a;
+        double* Bc = B + b0 * p.stride_b;
+        trsm_inv_diag_kernel<<<dim3(nblocks, static_cast<unsigned>(nm)), kInvNB, kInvSmem, st>>>(Ac, p, W, nblocks);
+        trsm_dmma_kernel<RB><<<dim3((p.nrhs + RB - 1) / RB, static_cast<unsigned>(nm)), kTbThreads, smem, st>>>(
+            Ac, Bc, alpha, p, W, nblocks);
+        count_launch(2);
+        e = cudaGetLastError();
+    }
+    kernel_timing_end(&tmr, st);
+    cudaFreeAsync(W, st);
+    return e;
+}
+
 }  // namespace
 
 template <typename T>
@@ -303,8 +540,23 @@ int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n
     p.ldb_rs = (side == RB_LEFT) ? 1 : ldb;
     p.ldb_cs = (side == RB_LEFT) ? ldb : 1;
     p.stride_b = stride_b;
-    cudaError_t e;
-    if (tb_smem<T, 32>(p.q) <= kTbSmemMax) e = tb_launch<T, 32>(A, B, alpha, p, batch, st);
+    cudaError_t e = cudaSuccess;
+    bool alloc_failed = false;
+    int td_rb = 0;  // f64: slice width of the tensor-core path (0: not used)
+    if constexpr (sizeof(T) == 8) {
+        // 16-wide slices while two CTAs fit an SM, then 8-wide, then one CTA per SM
+        if (td_smem<16>(p.q) <= kTbSmemMax / 2) td_rb = 16;
+        else if (td_smem<8>(p.q) <= kTbSmemMax / 2) td_rb = 8;
+        else if (td_smem<16>(p.q) <= kTbSmemMax) td_rb = 16;
+        else if (td_smem<8>(p.q) <= kTbSmemMax) td_rb = 8;
+        if (td_rb == 16) e = td_launch<16>(reinterpret_cast<const double*>(A), reinterpret_cast<double*>(B), alpha, p,
+                                           batch, st, &alloc_failed);
+        else if (td_rb == 8) e = td_launch<8>(reinterpret_cast<const double*>(A), reinterpret_cast<double*>(B), alpha,
+                                              p, batch, st, &alloc_failed);
+    }
+    if (td_rb) {
+        // launched above
+    } else if (tb_smem<T, 32>(p.q) <= kTbSmemMax) e = tb_launch<T, 32>(A, B, alpha, p, batch, st);
     else if (tb_smem<T, 16>(p.q) <= kTbSmemMax) e = tb_launch<T, 16>(A, B, alpha, p, batch, st);
     else if (tb_smem<T, 8>(p.q) <= kTbSmemMax) e = tb_launch<T, 8>(A, B, alpha, p, batch, st);
     else {
@@ -318,7 +570,8 @@ int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n
     }
     if (e != cudaSuccess) {
         if (ce) *ce = static_cast<int32_t>(e);
-        return RB_ERR_CUDA;
+        if (alloc_failed) cudaGetLastError();
+        return alloc_failed ? RB_ERR_ALLOC : RB_ERR_CUDA;
     }
     return RB_OK;
 }

@@ -2,9 +2,13 @@
 restatement of rblas's trsm (src/level3.rs:390-520) run per batch member.
 
 Well-conditioned triangular A (unit-range diagonal, small off-diagonal
-entries, junk in the unreferenced triangle); the same relative bound as the
-single-problem trsm tests (1e3 * u of the dtype, max-norm relative to the
-oracle's solution). Covers every side/uplo/trans/diag, ragged sizes,
+entries, junk in the unreferenced triangle). Two bounds, u of the dtype:
+the forward error against the oracle's solution, max-norm relative, within
+1e3 * u (as the single-problem trsm tests), and the normwise backward error
+of every member, ||op(A) X - alpha B||_F / (||A_tri||_F ||X||_F +
+|alpha| ||B||_F) <= 4 * q * u (q the order of A) -- the bound of a blocked
+substitution, which the f64 path's inverted diagonal blocks must also meet.
+Covers every side/uplo/trans/diag, ragged sizes,
 several right-hand-side slices per problem, the 16- and 8-wide slices of
 large orders, padded leading dimensions and gaps between members (which must
 stay untouched), and the leading-dimension errors.
@@ -53,7 +57,20 @@ def run_batch(rng, dtype, side, uplo, trans, diag, m, n, batch, alpha, pad=3):
     torch.cuda.synchronize()
     got = B_d.cpu().numpy()
     worst = 0.0
+    q_ord = m if side == 0 else n
     for i in range(batch):
+        # backward error: op(A) X = alpha B (Left) or X op(A) = alpha B (Right)
+        Am = a_host[i * sa:i * sa + lda * q_ord].reshape(q_ord, lda).T[:q_ord, :].astype(np.float64)
+        T = np.tril(Am) if uplo == 1 else np.triu(Am)
+        if diag == 1:
+            np.fill_diagonal(T, 1.0)
+        opA = T.T if trans else T
+        X = got[i * sb:i * sb + ldb * n].reshape(n, ldb).T[:m, :].astype(np.float64)
+        B0 = b_host[i * sb:i * sb + ldb * n].reshape(n, ldb).T[:m, :].astype(np.float64)
+        R = (opA @ X if side == 0 else X @ opA) - alpha * B0
+        den = np.linalg.norm(T) * np.linalg.norm(X) + abs(alpha) * np.linalg.norm(B0)
+        back = np.linalg.norm(R) / den if den > 0 else np.linalg.norm(R)
+        assert back <= 4 * q_ord * _u(dtype), (i, back, 4 * q_ord * _u(dtype))
         ref = b_host[i * sb:(i + 1) * sb].copy()
         oracle.trsm(side, uplo, trans, diag, m, n, alpha, np.ascontiguousarray(a_host[i * sa:(i + 1) * sa]), lda,
                     ref, ldb)
@@ -83,15 +100,16 @@ def test_batched_trsm_parity(dtype, side, uplo, trans):
 
 
 def test_batched_trsm_config_shape_f64():
-    """512 x 512 lower, 64 right-hand sides, f64 (two 32-wide slices)."""
+    """512 x 512 lower, 64 right-hand sides, f64 (four 16-wide slices on the
+    FP64 tensor cores, two CTAs per SM)."""
     rng = np.random.default_rng(90)
     rel = run_batch(rng, np.float64, 0, 1, 0, 0, 512, 64, 6, 1.0)
     assert rel <= 1e3 * _u(np.float64)
 
 
 def test_batched_trsm_wide_orders_use_narrow_slices():
-    """Orders beyond the 32-wide slice's shared memory (f64 q = 700 uses
-    16-wide slices, q = 1400 8-wide)."""
+    """Large orders: f64 q = 700 still fits two 16-wide slices per SM; q = 1400
+    runs one 16-wide slice per SM (its q x 20 doubles of shared memory)."""
     rng = np.random.default_rng(91)
     for q, n in ((700, 20), (1400, 9)):
         rel = run_batch(rng, np.float64, 0, 0, 1, 0, q, n, 2, -1.5)
