@@ -489,6 +489,14 @@ int rb_gemm_grouped_splits(const rb_gemm_problem* p);
  * checks as rb_gemm_grouped_dev. Returns once the work is enqueued. */
 rb_status rb_gemm_grouped_ozaki_dev(const rb_gemm_problem* problems, size_t count, void* stream,
                                     rb_error* err);
+/* The same for f32 problems in a BF16-split form (form RB_PREC_BF16X3 or
+ * RB_PREC_BF16X6; each entry one level3::gemm::<f32>): one split pass over
+ * every operand, then one persistent tensor-core kernel over the tiles of all
+ * problems. Each result equals that problem's own rb_sgemm_dev(..., form,
+ * ...) bit for bit. Every entry must be f32 (RB_ERR_UNSUPPORTED, err->got =
+ * its index, otherwise); another form is RB_ERR_INVALID_ARG. */
+rb_status rb_gemm_grouped_bf16_dev(const rb_gemm_problem* problems, size_t count, rb_precision form,
+                                   void* stream, rb_error* err);
 
 /* A grouped launch frozen into a CUDA graph: the problem table (with its
  * TMA descriptors), the split-K workspace and any repack scratch are built

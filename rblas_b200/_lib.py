@@ -104,6 +104,7 @@ SIGNATURES = {
     "rb_gemm_grouped_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _vp, _perr]),
     "rb_gemm_grouped_splits": (_i, [C.POINTER(RbGemmProblem)]),
     "rb_gemm_grouped_ozaki_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _vp, _perr]),
+    "rb_gemm_grouped_bf16_dev": (_i, [C.POINTER(RbGemmProblem), _sz, _i, _vp, _perr]),
     "rb_gemm_grouped_plan_create": (_i, [C.POINTER(RbGemmProblem), _sz, C.POINTER(C.c_void_p), _perr]),
     "rb_gemm_grouped_plan_launch": (_i, [_vp, _vp, _perr]),
     "rb_gemm_grouped_plan_destroy": (_i, [_vp]),

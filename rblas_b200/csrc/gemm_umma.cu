@@ -88,6 +88,7 @@ struct UParams {
     float alpha_f, beta_f;
     float* c;
     size_t ldc;
+    const float* cin;  // C0, read for beta != 0: c itself, or a separate input with c's leading dimension
     uint32_t* err;
 };
 
@@ -96,14 +97,57 @@ struct Bar {
     uint32_t tmem_base;
 };
 
+// One problem of a grouped BF16-split launch: its plane tensor maps (64-byte
+// aligned for TMA) and parameters.
+struct alignas(64) UGroupEntry {
+    CUtensorMap tmA, tmB;
+    UParams p;
+};
+
+struct UWork {
+    const UParams* p;
+    const CUtensorMap* ta;
+    const CUtensorMap* tb;
+    int t;  // tile of the problem
+};
+
+// The single-problem kernel's tiles, one problem.
+struct USingleSrc {
+    const UParams* p;
+    const CUtensorMap* ta;
+    const CUtensorMap* tb;
+    __device__ __forceinline__ uint32_t* err() const { return p->err; }
+    __device__ __forceinline__ int items() const { return p->num_tiles; }
+    __device__ __forceinline__ UWork get(int item) const { return UWork{p, ta, tb, item}; }
+};
+
+// Grouped: item i is tile i - starts[j] of problem j (starts[j] <= i <
+// starts[j+1]); problems ordered by K, longest first.
+struct UGroupSrc {
+    const UGroupEntry* tab;
+    const int* starts;
+    int nprob;
+    uint32_t* error;
+    __device__ __forceinline__ uint32_t* err() const { return error; }
+    __device__ __forceinline__ int items() const { return __ldg(starts + nprob); }
+    __device__ __forceinline__ UWork get(int item) const {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(starts + mid) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const UGroupEntry* g = tab + lo;
+        return UWork{&g->p, &g->tmA, &g->tmB, item - __ldg(starts + lo)};
+    }
+};
+
 // Work of one tile is a sequence of accumulation units: unit c covers K
 // tiles [c*G, (c+1)*G) with all plane products, and the epilogue promotes
 // each unit's FP32 partial into FP32 registers (tcgen05's accumulation
 // truncates; short units keep that error small).
-template <int MODE>
-__global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
-    umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     const UParams p) {
+template <int MODE, class Src>
+__device__ __forceinline__ void umma_body(const Src& src) {
     using Cfg = UCfg<MODE>;
     constexpr int UN = Cfg::UN, NA = Cfg::NA, NB = Cfg::NB, ST = Cfg::STAGES;
     constexpr int BTILE = UN * kRowBytes;
@@ -137,21 +181,28 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = bar->tmem_base;
-    const int units = p.kchunks;
+    const int items = src.items();
+    uint32_t* const err = src.err();
     bool ok = true;
 
     if (warp == 0 && lane == 0) {
         // ------------------------------ TMA producer ------------------------------
-        prefetch_tmap(&tmA);
-        prefetch_tmap(&tmB);
         uint32_t it = 0;
-        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+        const CUtensorMap* fetched = nullptr;
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            const UWork w = src.get(item);
+            const UParams& p = *w.p;
+            if (w.ta != fetched) {
+                prefetch_tmap(w.ta);
+                prefetch_tmap(w.tb);
+                fetched = w.ta;
+            }
             int tm, tn;
-            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            raster_tile(w.t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
             for (int kt = 0; kt < p.num_kt; ++kt, ++it) {
                 const int s = it % ST;
-                if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, p.err, 0x201)) {
+                if (it >= ST && !mbar_wait(&bar->empty[s], ((it / ST) - 1) & 1, err, 0x201)) {
                     ok = false;
                     break;
                 }
@@ -160,9 +211,9 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
                 mbar_arrive_expect_tx(&bar->full[s], STAGE_BYTES);
                 const int k0 = kt * 64;  // bf16 elements per 128-byte row
 #pragma unroll
-                for (int q = 0; q < NA; ++q) tma_load_3d(sa + q * kATile, &tmA, &bar->full[s], k0, m0, q);
+                for (int q = 0; q < NA; ++q) tma_load_3d(sa + q * kATile, w.ta, &bar->full[s], k0, m0, q);
 #pragma unroll
-                for (int q = 0; q < NB; ++q) tma_load_3d(sb + q * BTILE, &tmB, &bar->full[s], k0, n0, q);
+                for (int q = 0; q < NB; ++q) tma_load_3d(sb + q * BTILE, w.tb, &bar->full[s], k0, n0, q);
             }
         }
         if (!ok) {
@@ -172,11 +223,14 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
     } else if (warp == 1 && lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
         uint32_t it = 0, uc = 0;
-        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            const UWork w = src.get(item);
+            const UParams& p = *w.p;
+            const int units = p.kchunks;
             for (int u = 0; ok && u < units; ++u, ++uc) {
                 const int kt0 = u * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
                 const uint32_t b = uc & 1;
-                if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, p.err, 0x202)) {
+                if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, err, 0x202)) {
                     ok = false;
                     break;
                 }
@@ -185,7 +239,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
                 uint32_t accumulate = 0;
                 for (int kt = kt0; kt < kt1; ++kt, ++it) {
                     const int s = it % ST;
-                    if (!mbar_wait(&bar->full[s], (it / ST) & 1, p.err, 0x203)) {
+                    if (!mbar_wait(&bar->full[s], (it / ST) & 1, err, 0x203)) {
                         ok = false;
                         break;
                     }
@@ -215,9 +269,12 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
         const int quarter = warp & 3;
         const int row_in_tile = quarter * 32 + lane;
         uint32_t uc = 0;
-        for (int t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            const UWork w = src.get(item);
+            const UParams& p = *w.p;
+            const int units = p.kchunks;
             int tm, tn;
-            raster_tile(t, p.tiles_m, p.tiles_n, tm, tn);
+            raster_tile(w.t, p.tiles_m, p.tiles_n, tm, tn);
             const int m0 = tm * kUM, n0 = tn * UN;
             const int r = m0 + row_in_tile;
             const bool row_ok = r < p.m;
@@ -226,7 +283,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
             for (int j = 0; j < UN; ++j) sum[j] = 0.f;
             for (int u = 0; ok && u < units; ++u, ++uc) {
                 const uint32_t b = uc & 1;
-                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, p.err, 0x204)) {
+                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, err, 0x204)) {
                     ok = false;
                     break;
                 }
@@ -245,7 +302,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
                 if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
             }
             if (ok && row_ok) {
-                // C read 16 values at a time, all requested before use, so
+                // C0 read 16 values at a time, all requested before use, so
                 // the loads' latencies overlap instead of adding up
 #pragma unroll
                 for (int g = 0; g < UN / 16; ++g) {
@@ -253,7 +310,7 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 #pragma unroll
                     for (int jj = 0; jj < 16; ++jj) {
                         const int col = n0 + g * 16 + jj;
-                        cv[jj] = (p.beta_mode != 0 && col < p.n) ? p.c[r + static_cast<size_t>(col) * p.ldc] : 0.f;
+                        cv[jj] = (p.beta_mode != 0 && col < p.n) ? p.cin[r + static_cast<size_t>(col) * p.ldc] : 0.f;
                     }
 #pragma unroll
                     for (int jj = 0; jj < 16; ++jj) {
@@ -274,6 +331,22 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
         tc_fence_after();
         tmem_dealloc(tmem_base, TMEM_COLS);
     }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const __grid_constant__ UParams p) {
+    umma_body<MODE>(USingleSrc{&p, &tmA, &tmB});
+}
+
+// Many f32 problems in one persistent launch (the serving loop's BF16-split
+// batches): the same tiles and epilogue as umma_gemm_kernel.
+template <int MODE>
+__global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
+    umma_grouped_kernel(const UGroupEntry* __restrict__ tab, const int* __restrict__ starts, int nprob,
+                        uint32_t* err) {
+    umma_body<MODE>(UGroupSrc{tab, starts, nprob, err});
 }
 
 // ------------------------------------------------------------------------------
@@ -1066,12 +1139,12 @@ void launch_ozaki_slices(dim3 grid, cudaStream_t st, const double* x, size_t rs,
 // BF16 split into `planes` (2 or 3) planes: out[0] = bf16(x),
 // out[1] = bf16(x - out[0]), out[2] = bf16(x - out[0] - out[1]); every
 // difference is exact in FP32.
-__global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict__ x, size_t rs, size_t ps,
-                                                         int R, int K, int planes,
-                                                         __nv_bfloat16* __restrict__ out, size_t kp,
-                                                         size_t plane) {
+// One 64 x 64 tile of the R x K view per 256-thread block (K tile bx, row tile by).
+__device__ __forceinline__ void bf16_split_tile(const float* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                                                int planes, __nv_bfloat16* __restrict__ out, size_t kp, size_t plane,
+                                                int bx, int by) {
     __shared__ float tile[kTile][kTile + 1];
-    const int r0 = blockIdx.y * kTile, p0 = blockIdx.x * kTile;
+    const int r0 = by * kTile, p0 = bx * kTile;
     load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     for (int job = threadIdx.x; job < kTile * 8; job += blockDim.x) {
@@ -1091,6 +1164,37 @@ __global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict
         for (int q = 0; q < planes; ++q)
             *reinterpret_cast<uint4*>(out + q * plane + off) = *reinterpret_cast<const uint4*>(h[q]);
     }
+}
+
+__global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict__ x, size_t rs, size_t ps,
+                                                         int R, int K, int planes,
+                                                         __nv_bfloat16* __restrict__ out, size_t kp,
+                                                         size_t plane) {
+    bf16_split_tile(x, rs, ps, R, K, planes, out, kp, plane, blockIdx.x, blockIdx.y);
+}
+
+// One operand of a grouped BF16-split launch, viewed as R x K, and its
+// planes out[planes][R][kp]; gx K tiles per row tile, `start` its first block.
+struct BsOperand {
+    const float* x;
+    size_t rs, ps;
+    int R, K, planes;
+    __nv_bfloat16* out;
+    size_t kp, plane;
+    int gx, start;
+};
+
+// The split pass over every operand of a batch (grid = all their tiles).
+__global__ void __launch_bounds__(256) bf16_split_grouped_kernel(const BsOperand* __restrict__ ops, int nops) {
+    int lo = 0, hi = nops - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ops[mid].start <= static_cast<int>(blockIdx.x)) lo = mid;
+        else hi = mid - 1;
+    }
+    const BsOperand& o = ops[lo];
+    const int b = blockIdx.x - o.start;
+    bf16_split_tile(o.x, o.rs, o.ps, o.R, o.K, o.planes, o.out, o.kp, o.plane, b % o.gx, b / o.gx);
 }
 
 CUresult make_tmap_planes(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
@@ -1244,10 +1348,211 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     p.beta_mode = (beta == 0.f) ? 0 : (beta == 1.f ? 1 : 2);
     p.alpha_f = alpha; p.beta_f = beta;
     p.c = C; p.ldc = ldc;
+    p.cin = C;
     p.err = device_error_word();
     e = (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
     cudaFreeAsync(buf, st);
     return e;
+}
+
+// Many f32 GEMMs in a BF16-split form (planes 2: 3xBF16, 3: BF16X6) with two
+// launches for the whole batch: one split pass over every operand, then one
+// persistent umma_grouped_kernel over every problem's tiles. C0 of problem i
+// comes from cin[i] (leading dimension ldcin[i]) or probs[i].c. Each result
+// equals that problem's own rb_sgemm_dev(..., form, ...) bit for bit.
+int bf16_grouped_dev(int planes, const rb_gemm_problem* probs, size_t count, const void* const* cin,
+                     const size_t* ldcin, cudaStream_t st, int32_t* ce) {
+    constexpr int UN = 128;
+    struct Job {
+        bool ta, tb;
+        int m, n, k;
+        const float *a, *b;
+        size_t lda, ldb;
+        float* c;
+        const float* c0;
+        size_t ldc;
+        float alpha, beta;
+        size_t kp, off_a, off_b;
+        int num_kt;
+    };
+    std::vector<Job> jobs;
+    jobs.reserve(count);
+    size_t elems = 0;  // bf16 plane elements, every operand 256-byte aligned
+    cudaError_t e = cudaSuccess;
+    for (size_t i = 0; i < count; ++i) {
+        const rb_gemm_problem& q = probs[i];
+        if (q.dtype != 0) return RB_ERR_UNSUPPORTED;
+        const int v = validate_problem(q);
+        if (v != RB_OK) return v;
+        const bool col = q.layout == RB_COL_MAJOR;
+        const size_t m = col ? q.m : q.n, n = col ? q.n : q.m;
+        if (m == 0 || n == 0) continue;
+        if (m > 0x7fffffff || n > 0x7fffffff || q.k > 0x7fffffff) return RB_ERR_INVALID_ARG;
+        float* c = static_cast<float*>(q.c);
+        const float* c0 = cin ? static_cast<const float*>(cin[i]) : c;
+        const size_t ldc0 = cin ? ldcin[i] : q.ldc;
+        const float beta = static_cast<float>(q.beta), alpha = static_cast<float>(q.alpha);
+        if (beta != 0.f && c0 != c && ldc0 != q.ldc) {
+            // the kernels read C0 with C's leading dimension: bring it into C first
+            e = cudaMemcpy2DAsync(c, q.ldc * 4, c0, ldc0 * 4, m * 4, n, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) break;
+            c0 = c;
+        }
+        if (q.k == 0 || alpha == 0.f) {  // C = beta * C0 only (gemm_contig's early out)
+            if (beta != 0.f && c0 != c) {
+                e = cudaMemcpy2DAsync(c, q.ldc * 4, c0, q.ldc * 4, m * 4, n, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) break;
+            }
+            e = launch_scale_c<float>(static_cast<int>(m), static_cast<int>(n), beta, c, q.ldc, st);
+            if (e != cudaSuccess) break;
+            continue;
+        }
+        Job j{};
+        const bool ta = q.transa != RB_NO_TRANS, tb = q.transb != RB_NO_TRANS;
+        j.ta = col ? ta : tb;
+        j.tb = col ? tb : ta;
+        j.m = static_cast<int>(m);
+        j.n = static_cast<int>(n);
+        j.k = static_cast<int>(q.k);
+        j.a = static_cast<const float*>(col ? q.a : q.b);
+        j.b = static_cast<const float*>(col ? q.b : q.a);
+        j.lda = col ? q.lda : q.ldb;
+        j.ldb = col ? q.ldb : q.lda;
+        j.c = c;
+        j.c0 = c0;
+        j.ldc = q.ldc;
+        j.alpha = alpha;
+        j.beta = beta;
+        j.kp = round_up(q.k, 8);  // 16-byte rows of bf16
+        j.num_kt = static_cast<int>((q.k + 63) / 64);
+        j.off_a = elems;
+        elems += round_up(planes * m * j.kp, 128);
+        j.off_b = elems;
+        elems += round_up(planes * n * j.kp, 128);
+        jobs.push_back(j);
+    }
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        return RB_ERR_CUDA;
+    }
+    if (jobs.empty()) return RB_OK;
+    // longest tiles first: the CTAs walk the items with a stride of the grid
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& x, const Job& y) { return x.num_kt > y.num_kt; });
+    const int np = static_cast<int>(jobs.size());
+    // device image: [entries][starts][operands], then the planes
+    const size_t ent_bytes = round_up(np * sizeof(UGroupEntry), 256);
+    const size_t starts_bytes = round_up((np + 1) * sizeof(int), 256);
+    const size_t ops_bytes = round_up(2 * np * sizeof(BsOperand), 256);
+    const size_t img_bytes = ent_bytes + starts_bytes + ops_bytes;
+    uint8_t* mem = nullptr;
+    e = scratch_alloc(reinterpret_cast<void**>(&mem), img_bytes + elems * sizeof(__nv_bfloat16), st);
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        if (e == cudaErrorMemoryAllocation) cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? RB_ERR_ALLOC : RB_ERR_CUDA;
+    }
+    std::vector<uint8_t> img(img_bytes, 0);
+    int* starts = reinterpret_cast<int*>(img.data() + ent_bytes);
+    BsOperand* ops = reinterpret_cast<BsOperand*>(img.data() + ent_bytes + starts_bytes);
+    __nv_bfloat16* dplanes = reinterpret_cast<__nv_bfloat16*>(mem + img_bytes);
+    uint32_t* err_word = device_error_word();
+    int tiles = 0, split_blocks = 0;
+    double work = 0;
+    CUresult r = CUDA_SUCCESS;
+    for (int i = 0; i < np && r == CUDA_SUCCESS; ++i) {
+        const Job& j = jobs[i];
+        __nv_bfloat16* sa = dplanes + j.off_a;
+        __nv_bfloat16* sb = dplanes + j.off_b;
+        size_t ars, aps, brs, bps;
+        operand_views(j.ta, j.tb, j.lda, j.ldb, ars, aps, brs, bps);
+        const int gx = (j.k + kTile - 1) / kTile;
+        const struct { const float* x; size_t rs, ps; int R; __nv_bfloat16* out; } od[2] = {
+            {j.a, ars, aps, j.m, sa}, {j.b, brs, bps, j.n, sb}};
+        for (int h = 0; h < 2; ++h) {
+            BsOperand& o = ops[2 * i + h];
+            o.x = od[h].x; o.rs = od[h].rs; o.ps = od[h].ps;
+            o.R = od[h].R; o.K = j.k; o.planes = planes;
+            o.out = od[h].out;
+            o.kp = j.kp; o.plane = static_cast<size_t>(od[h].R) * j.kp;
+            o.gx = gx;
+            o.start = split_blocks;
+            split_blocks += gx * ((o.R + kTile - 1) / kTile);
+        }
+        UGroupEntry g{};  // 64-byte aligned here; copied into the image below
+        r = make_tmap_planes(&g.tmA, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, j.k, j.m, planes, j.kp, kUM);
+        if (r == CUDA_SUCCESS)
+            r = make_tmap_planes(&g.tmB, sb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, j.k, j.n, planes, j.kp, UN);
+        UParams& p = g.p;
+        p.m = j.m; p.n = j.n; p.k = j.k;
+        p.tiles_m = (j.m + kUM - 1) / kUM;
+        p.tiles_n = (j.n + UN - 1) / UN;
+        p.num_tiles = p.tiles_m * p.tiles_n;
+        p.num_kt = j.num_kt;
+        p.kt_per_chunk = 2;  // FP32 promotion every 128 elements of K
+        p.kchunks = (p.num_kt + p.kt_per_chunk - 1) / p.kt_per_chunk;
+        p.beta_mode = (j.beta == 0.f) ? 0 : (j.beta == 1.f ? 1 : 2);
+        p.alpha_f = j.alpha; p.beta_f = j.beta;
+        p.c = j.c; p.ldc = j.ldc;
+        p.cin = j.c0;
+        p.err = err_word;
+        std::memcpy(img.data() + i * sizeof(UGroupEntry), &g, sizeof(UGroupEntry));
+        starts[i] = tiles;
+        tiles += p.num_tiles;
+        work += 2.0 * j.m * j.n * static_cast<double>(j.k) * (planes == 2 ? 3 : 6);
+    }
+    starts[np] = tiles;
+    if (r != CUDA_SUCCESS) {
+        if (ce) *ce = static_cast<int32_t>(r);
+        cudaFreeAsync(mem, st);
+        return RB_ERR_CUDA;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = tiles < sms ? tiles : sms;
+    // a pageable source: the driver has staged the image when the call returns
+    e = cudaMemcpyAsync(mem, img.data(), img_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        bf16_split_grouped_kernel<<<split_blocks, 256, 0, st>>>(
+            reinterpret_cast<const BsOperand*>(mem + ent_bytes + starts_bytes), 2 * np);
+        const UGroupEntry* dtab = reinterpret_cast<const UGroupEntry*>(mem);
+        const int* dstarts = reinterpret_cast<const int*>(mem + ent_bytes);
+        KernelTimer tmr;
+        if (planes == 2) {
+            constexpr int smem = umma_smem_bytes<kModeBf16x3>();
+            static bool attr3 = false;
+            if (!attr3) {
+                e = cudaFuncSetAttribute(umma_grouped_kernel<kModeBf16x3>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                attr3 = e == cudaSuccess;
+            }
+            kernel_timing_begin("umma_bf16x3_grouped", work, st, &tmr);
+            if (e == cudaSuccess)
+                umma_grouped_kernel<kModeBf16x3><<<grid, UCfg<kModeBf16x3>::THREADS, smem, st>>>(dtab, dstarts, np,
+                                                                                                 err_word);
+        } else {
+            constexpr int smem = umma_smem_bytes<kModeBf16x6>();
+            static bool attr6 = false;
+            if (!attr6) {
+                e = cudaFuncSetAttribute(umma_grouped_kernel<kModeBf16x6>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                attr6 = e == cudaSuccess;
+            }
+            kernel_timing_begin("umma_bf16x6_grouped", work, st, &tmr);
+            if (e == cudaSuccess)
+                umma_grouped_kernel<kModeBf16x6><<<grid, UCfg<kModeBf16x6>::THREADS, smem, st>>>(dtab, dstarts, np,
+                                                                                                 err_word);
+        }
+        kernel_timing_end(&tmr, st);
+        count_launch(2);
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
+    cudaFreeAsync(mem, st);
+    if (e != cudaSuccess) {
+        if (ce) *ce = e;
+        return RB_ERR_CUDA;
+    }
+    return RB_OK;
 }
 
 // Tail tiles to run unit by unit (OzParams::tail_tiles): the tiles of the

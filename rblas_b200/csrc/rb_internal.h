@@ -134,6 +134,11 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
 // problem's own Ozaki call bit for bit. Returns an rb_status value.
 int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* const* cin, const size_t* ldcin,
                       cudaStream_t st, int32_t* ce);
+// Many f32 problems in a BF16-split form (planes 2: 3xBF16, 3: BF16X6) in
+// one grouped launch plus one split pass; results equal each problem's own
+// call in that form bit for bit. Returns an rb_status value.
+int bf16_grouped_dev(int planes, const rb_gemm_problem* probs, size_t count, const void* const* cin,
+                     const size_t* ldcin, cudaStream_t st, int32_t* ce);
 
 // ---- Level-3 routines on device pointers (all column-major; complex
 // operands interleaved {re, im}; return rb_status values) -------------------

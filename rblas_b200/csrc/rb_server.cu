@@ -341,9 +341,12 @@ public:
         std::vector<rb_gemm_problem> oz;
         std::vector<const void*> oz_cin;
         std::vector<size_t> oz_ldcin;
-        size_t n_oz = 0;
-        for (size_t i : alone) n_oz += (probs[i].dtype == 1 && b.form[1] == RB_PREC_OZAKI);
-        const bool group_oz = n_oz >= 2;
+        size_t n_oz = 0, n_bf = 0;
+        for (size_t i : alone) {
+            n_oz += (probs[i].dtype == 1);
+            n_bf += (probs[i].dtype == 0);
+        }
+        const bool group_oz = n_oz >= 2, group_bf = n_bf >= 2;
         for (size_t i : alone)
             if (group_oz && probs[i].dtype == 1) {
                 oz.push_back(probs[i]);
@@ -359,8 +362,29 @@ public:
                 cudaStreamWaitEvent(st, form_events[f], 0);
             }
         }
+        // the f32 ones in the batch's BF16-split form: one grouped launch too
+        std::vector<rb_gemm_problem> bf;
+        std::vector<const void*> bf_cin;
+        std::vector<size_t> bf_ldcin;
+        for (size_t i : alone)
+            if (group_bf && probs[i].dtype == 0) {
+                bf.push_back(probs[i]);
+                bf_cin.push_back(cin[i]);
+                bf_ldcin.push_back(ldcin[i]);
+            }
+        if (!bf.empty() && rc == RB_OK) {
+            const int f = next_form_stream;
+            next_form_stream = (next_form_stream + 1) % kFormStreams;
+            rc = bf16_grouped_dev(b.form[0] == RB_PREC_BF16X3 ? 2 : 3, bf.data(), bf.size(), bf_cin.data(),
+                                  bf_ldcin.data(), form_streams[f], &ce);
+            if (rc == RB_OK) {
+                cudaEventRecord(form_events[f], form_streams[f]);
+                cudaStreamWaitEvent(st, form_events[f], 0);
+            }
+        }
         for (size_t i = 0; i < alone.size() && rc == RB_OK; ++i) {
             if (group_oz && probs[alone[i]].dtype == 1) continue;  // in the grouped launch
+            if (group_bf && probs[alone[i]].dtype == 0) continue;
             // on a form stream; the batch's stream then waits for it, so the
             // batch's completion event covers the request
             const int f = next_form_stream;
@@ -525,6 +549,35 @@ rb_status rb_gemm_grouped_dev(const rb_gemm_problem* problems, size_t count, voi
 }
 
 int rb_gemm_grouped_splits(const rb_gemm_problem* p) { return p ? grouped_splits(*p) : 0; }
+
+rb_status rb_gemm_grouped_bf16_dev(const rb_gemm_problem* problems, size_t count, rb_precision form, void* stream,
+                                   rb_error* err) {
+    if (err) *err = rb_error{0, 0, 0, 0, 0};
+    if ((form != RB_PREC_BF16X3 && form != RB_PREC_BF16X6) || (count && !problems)) {
+        if (err) err->code = RB_ERR_INVALID_ARG;
+        return RB_ERR_INVALID_ARG;
+    }
+    for (size_t i = 0; i < count; ++i) {
+        const rb_gemm_problem& q = problems[i];
+        const int v = q.dtype != 0 ? RB_ERR_UNSUPPORTED : validate_problem(q);
+        const bool null_ptr = q.m && q.n && (!q.c || (q.k && q.alpha != 0.0 && (!q.a || !q.b)));
+        if (v != RB_OK || null_ptr) {
+            if (err) {
+                err->code = v != RB_OK ? v : RB_ERR_INVALID_ARG;
+                err->got = i;
+            }
+            return static_cast<rb_status>(v != RB_OK ? v : RB_ERR_INVALID_ARG);
+        }
+    }
+    int32_t ce = 0;
+    const int rc = bf16_grouped_dev(form == RB_PREC_BF16X3 ? 2 : 3, problems, count, nullptr, nullptr,
+                                    static_cast<cudaStream_t>(stream), &ce);
+    if (rc != RB_OK && err) {
+        err->code = rc;
+        err->cuda_error = ce;
+    }
+    return static_cast<rb_status>(rc);
+}
 
 rb_status rb_gemm_grouped_ozaki_dev(const rb_gemm_problem* problems, size_t count, void* stream, rb_error* err) {
     if (err) *err = rb_error{0, 0, 0, 0, 0};

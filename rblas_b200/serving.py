@@ -11,7 +11,7 @@ import numpy as np
 from . import _lib
 from .types import Layout, Transpose
 
-__all__ = ["Problem", "grouped_gemm", "grouped_gemm_ozaki", "grouped_splits", "GroupedPlan", "Server", "autotune", "autotune_load",
+__all__ = ["Problem", "grouped_gemm", "grouped_gemm_bf16", "grouped_gemm_ozaki", "grouped_splits", "GroupedPlan", "Server", "autotune", "autotune_load",
            "autotune_reset"]
 
 
@@ -55,6 +55,17 @@ def grouped_gemm(problems, stream=0):
     err = _lib.RbError()
     st = _lib.load().rb_gemm_grouped_dev(arr, len(problems), C.c_void_p(stream) if stream else None,
                                          C.byref(err))
+    _lib.check(st, err)
+
+
+def grouped_gemm_bf16(problems, form, stream=0):
+    """Run f32 problems in a BF16-split form (Precision.Bf16x3 / Bf16x6) in
+    one grouped launch on `stream` (rb_gemm_grouped_bf16_dev); each result
+    equals its own call in that form."""
+    arr = _array(problems)
+    err = _lib.RbError()
+    st = _lib.load().rb_gemm_grouped_bf16_dev(arr, len(problems), int(form), C.c_void_p(stream) if stream else None,
+                                              C.byref(err))
     _lib.check(st, err)
 
 

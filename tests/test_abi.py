@@ -187,3 +187,20 @@ def test_grouped_ozaki_rejects_non_f64_entries_before_any_device_work():
     arr[0].c = None
     err = _lib.RbError()
     assert lib.rb_gemm_grouped_ozaki_dev(arr, 2, None, C.byref(err)) == 4 and err.got == 0
+
+
+def test_grouped_bf16_rejects_bad_tables_before_any_device_work():
+    """rb_gemm_grouped_bf16_dev: a form other than BF16X3/BF16X6 is
+    RB_ERR_INVALID_ARG, an f64 entry RB_ERR_UNSUPPORTED with its index."""
+    lib = _lib.load()
+    buf = np.zeros(64, dtype=np.float32)
+    p = buf.ctypes.data
+    arr = (_lib.RbGemmProblem * 2)()
+    for i in range(2):
+        arr[i] = _lib.RbGemmProblem(0, 1, 0, 0, 4, 4, 4, 1.0, 0.0, C.c_void_p(p), 4, C.c_void_p(p), 4,
+                                    C.c_void_p(p), 4)
+    err = _lib.RbError()
+    assert lib.rb_gemm_grouped_bf16_dev(arr, 2, 2, None, C.byref(err)) == 4  # Ozaki is not a BF16 form
+    arr[1].dtype = 1
+    err = _lib.RbError()
+    assert lib.rb_gemm_grouped_bf16_dev(arr, 2, 3, None, C.byref(err)) == 5 and err.got == 1
