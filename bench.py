@@ -943,25 +943,30 @@ def run_grouped_only(args):
 
 def run_grouped_ozaki_only(args):
     """The f64 requests among the first `--grouped-ozaki N` requests of the
-    serving stream in the Ozaki form: one grouped launch
-    (rb_gemm_grouped_ozaki_dev) against one single-problem Ozaki call per
-    request and one grouped plain launch, warmup + steps times each."""
+    serving stream in the Ozaki form (or, with `--grouped-bf16 N`, the f32
+    ones in BF16X6): one grouped launch (rb_gemm_grouped_ozaki_dev /
+    rb_gemm_grouped_bf16_dev) against one single-problem call per request in
+    the same form and one grouped plain launch, warmup + steps times each."""
     import torch
 
     from rblas_b200 import level3
-    from rblas_b200.serving import Problem, grouped_gemm, grouped_gemm_ozaki
+    from rblas_b200.serving import Problem, grouped_gemm, grouped_gemm_bf16, grouped_gemm_ozaki
     from rblas_b200.types import Precision
 
-    tr = serving_trace(args.grouped_ozaki)
+    f32 = args.grouped_bf16 > 0
+    count = args.grouped_bf16 if f32 else args.grouped_ozaki
+    npdt, tdt, es = (np.float32, torch.float32, 4) if f32 else (np.float64, torch.float64, 8)
+    prec = Precision.Bf16x6 if f32 else Precision.Ozaki
+    tr = serving_trace(count)
     g = torch.Generator(device="cuda")
     g.manual_seed(6)
-    pool = torch.randn(4096 * 4096 + (1 << 22), dtype=torch.float64, device="cuda", generator=g)
+    pool = torch.randn(4096 * 4096 + (1 << 22), dtype=tdt, device="cuda", generator=g)
     probs, flops = [], 0.0
     keep = []
     min_flop = args.min_flop
-    for i in range(args.grouped_ozaki):
+    for i in range(count):
         m, n, k = (int(x) for x in tr["mnk"][i])
-        if int(tr["dtype"][i]) != 1 or 2.0 * m * n * k < min_flop:
+        if int(tr["dtype"][i]) != (0 if f32 else 1) or 2.0 * m * n * k < min_flop:
             continue
         layout, ta, tb = int(tr["layout"][i]), int(tr["ta"][i]), int(tr["tb"][i])
         ar, ac = (k, m) if ta else (m, k)
@@ -970,10 +975,10 @@ def run_grouped_ozaki_only(args):
         ldb = br if layout == 1 else bc
         ldc = m if layout == 1 else n
         offs = [int(o) // 16 * 16 for o in tr["offs"][i]]
-        c = torch.empty(m * n, dtype=torch.float64, device="cuda").normal_()
+        c = torch.empty(m * n, dtype=tdt, device="cuda").normal_()
         keep.append(c)
-        probs.append(Problem(np.float64, layout, ta, tb, m, n, k, float(tr["alpha"][i]),
-                             pool.data_ptr() + offs[0] * 8, lda, pool.data_ptr() + offs[1] * 8, ldb,
+        probs.append(Problem(npdt, layout, ta, tb, m, n, k, float(tr["alpha"][i]),
+                             pool.data_ptr() + offs[0] * es, lda, pool.data_ptr() + offs[1] * es, ldb,
                              float(tr["beta"][i]), c.data_ptr(), ldc))
         flops += 2.0 * m * n * k
     sh = torch.cuda.current_stream().cuda_stream
@@ -992,10 +997,12 @@ def run_grouped_ozaki_only(args):
     def singles():
         for p in probs:
             level3.gemm_dev(p.layout, p.transa, p.transb, p.m, p.n, p.k, p.alpha, p.a, p.lda, p.b, p.ldb, p.beta,
-                            p.c, p.ldc, np.float64, prec=Precision.Ozaki, stream=sh)
+                            p.c, p.ldc, npdt, prec=prec, stream=sh)
 
-    out = {"grouped_ozaki": len(probs), "flop": flops}
-    for name, fn in (("grouped_ozaki", lambda: grouped_gemm_ozaki(probs, sh)), ("single_ozaki", singles),
+    form = "bf16x6" if f32 else "ozaki"
+    grouped_form = (lambda: grouped_gemm_bf16(probs, prec, sh)) if f32 else (lambda: grouped_gemm_ozaki(probs, sh))
+    out = {"requests": len(probs), "form": form, "min_flop": min_flop, "flop": flops}
+    for name, fn in (("grouped_" + form, grouped_form), ("single_" + form, singles),
                      ("grouped_plain", lambda: grouped_gemm(probs, sh))):
         ms = timed(fn)
         out[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
@@ -1123,7 +1130,9 @@ def main():
                     help="time one grouped launch of the first N serving requests only")
     ap.add_argument("--grouped-ozaki", type=int, default=0, metavar="N",
                     help="the f64 requests among the first N serving requests: grouped Ozaki vs single calls")
-    ap.add_argument("--min-flop", type=float, default=1e9, help="--grouped-ozaki: smallest request kept")
+    ap.add_argument("--grouped-bf16", type=int, default=0, metavar="N",
+                    help="the f32 requests among the first N serving requests: grouped BF16X6 vs single calls")
+    ap.add_argument("--min-flop", type=float, default=1e9, help="--grouped-ozaki/-bf16: smallest request kept")
     ap.add_argument("--cplx", action="store_true", help="--kernel-only shape as a complex C/N GEMM")
     ap.add_argument("--level3", choices=["", "syrk", "symm", "trsm", "trmm"], default="",
                     help="--kernel-only shape through one f64 Level-3 host call")
@@ -1143,7 +1152,7 @@ def main():
     args = ap.parse_args()
     if args.trsm_batched:
         run_trsm_batched_only(args)
-    elif args.grouped_ozaki:
+    elif args.grouped_ozaki or args.grouped_bf16:
         run_grouped_ozaki_only(args)
     elif args.shape and (args.cplx or args.level3):
         run_level3_only(args)
