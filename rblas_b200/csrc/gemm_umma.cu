@@ -154,7 +154,16 @@ __device__ __forceinline__ void umma_body(const Src& src) {
     constexpr int STAGE_BYTES = NA * kATile + NB * BTILE;
     constexpr int KSTEPS = 4;  // UMMA K steps of 32 bytes per 128-byte tile row
     constexpr uint32_t IDESC = umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
-    constexpr uint32_t TMEM_COLS = 2 * UN;
+    // BF16X6 keeps hi*hi apart from the five smaller products: tcgen05's FP32
+    // accumulation truncates, so each of its roundings costs up to one ulp of
+    // the accumulator it adds into. In an accumulator of their own the small
+    // products' roundings are ~2^-8 of hi*hi's, and hi*hi's own are one per
+    // instruction instead of one per product. (At K ~ 400 the shared
+    // accumulator left BF16X6 at up to 4x plain SGEMM's error.)
+    constexpr bool SPLIT_ACC = (MODE == kModeBf16x6);
+    constexpr uint32_t ACC_COLS = SPLIT_ACC ? 2 * UN : UN;  // per accumulator buffer
+    constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;
+    static_assert(TMEM_COLS <= 512, "two buffers must fit the SM's TMEM");
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -235,7 +244,8 @@ __device__ __forceinline__ void umma_body(const Src& src) {
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d_tmem = tmem_base + b * UN;
+                const uint32_t d_tmem = tmem_base + b * ACC_COLS;        // the products (all, or all but hi*hi)
+                const uint32_t d_big = SPLIT_ACC ? d_tmem + UN : d_tmem;  // hi*hi
                 uint32_t accumulate = 0;
                 for (int kt = kt0; kt < kt1; ++kt, ++it) {
                     const int s = it % ST;
@@ -250,9 +260,10 @@ __device__ __forceinline__ void umma_body(const Src& src) {
                     for (int kk = 0; kk < KSTEPS; ++kk) {
 #pragma unroll
                         for (int q = 0; q < Cfg::NPROD; ++q) {
-                            umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
+                            const bool big = SPLIT_ACC && q == Cfg::NPROD - 1;
+                            umma_f16(big ? d_big : d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
                                      sw128_kmajor_desc(sb + Cfg::pb(q) * BTILE) + 2 * kk, IDESC,
-                                     (q == 0) ? accumulate : 1u);
+                                     (q == 0 || big) ? accumulate : 1u);
                         }
                         accumulate = 1;
                     }
@@ -288,14 +299,18 @@ __device__ __forceinline__ void umma_body(const Src& src) {
                     break;
                 }
                 tc_fence_after();
-                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * ACC_COLS;
+                // the smaller products first, then hi*hi (SPLIT_ACC)
 #pragma unroll
-                for (int ch = 0; ch < UN / 32; ++ch) {
-                    uint32_t v[32];
-                    tmem_ld32(taddr + ch * 32, v);
-                    tmem_ld_wait();
+                for (int part = 0; part < (SPLIT_ACC ? 2 : 1); ++part) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                    for (int ch = 0; ch < UN / 32; ++ch) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + part * UN + ch * 32, v);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
