@@ -318,6 +318,34 @@ void set_tuned_splits(std::shared_ptr<const std::map<uint32_t, int>> table) {
 
 void force_grouped_splits(int s) { t_forced_splits = s; }
 
+// Tuned Ozaki tile widths per shape bucket (the f64 buckets of tune_key),
+// installed alongside the split factors.
+namespace {
+std::shared_ptr<const std::map<uint32_t, int>> g_tuned_oz;
+thread_local int t_forced_oz_width = 0;
+}  // namespace
+
+void set_tuned_ozaki_widths(std::shared_ptr<const std::map<uint32_t, int>> table) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned_oz = std::move(table);
+}
+
+void force_ozaki_width(int w) { t_forced_oz_width = w; }
+
+int ozaki_tile_n(size_t m, size_t n, size_t k) {
+    if (t_forced_oz_width) return t_forced_oz_width;
+    std::shared_ptr<const std::map<uint32_t, int>> t;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        t = g_tuned_oz;
+    }
+    if (t) {
+        auto it = t->find(tune_key(1, m, n, k));
+        if (it != t->end()) return it->second;
+    }
+    return n <= 128 ? 128 : 256;  // one narrow tile column: no padding to 256
+}
+
 namespace {
 
 std::shared_ptr<const std::map<uint32_t, int>> tuned_snapshot() {

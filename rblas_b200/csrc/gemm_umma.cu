@@ -387,13 +387,21 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // the first chunk's C values requested before the accumulator wait.
 // ------------------------------------------------------------------------------
 
-__host__ __device__ constexpr uint32_t kBTileOz() { return 256u * kRowBytes; }
-constexpr int kOzST = 4;                            // stages of (B_{d1-i}, A_i)
-constexpr int kOzStage = kATile + 256 * kRowBytes;  // 48 KiB
 constexpr int kOzEpiWarps = 16;
 constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;
 constexpr int kOzColTab = 64 * (8 + 4);             // per epilogue warp: 2^fc (double) and fc (int), 64 columns
-constexpr int kOzSmem = kOzST * kOzStage + 256 + kOzEpiWarps * kOzColTab + 1024;
+// Per tile width UN (256, or 128 for narrow problems): stages of
+// (B_{d1-i}, A_i), their bytes, the columns each epilogue warp drains, and
+// the dynamic shared memory.
+template <int UN>
+struct OzCfg {
+    static_assert(UN == 256 || UN == 128, "Ozaki tiles are 128 x 256 or 128 x 128");
+    static constexpr int ST = UN == 256 ? 4 : 6;
+    static constexpr int BTILE = UN * kRowBytes;
+    static constexpr int STAGE = kATile + BTILE;  // 48 KiB / 32 KiB
+    static constexpr int CW = UN / 4;             // four epilogue warps per TMEM lane quarter
+    static constexpr int SMEM = ST * STAGE + 256 + kOzEpiWarps * kOzColTab + 1024;
+};
 // Tile rows per rasterisation group. A wave of 148 tiles walks R row panels
 // of A and C column panels of B, each once per diagonal-pair unit; B panels
 // (256 columns) are twice the A panels (128 rows), so R ~ 2C (16 x ~9)
@@ -418,17 +426,16 @@ struct OzParams {
     uint32_t* err;
     // Split tail: the last tail_tiles tiles (in raster order) run as one work
     // item per (tile, unit). Such an item's epilogue writes the unit's exact
-    // FP64 terms to its own plane of ws (kOzTileElems doubles per tile and
-    // unit, element (row, col) of the tile at row + col * kUM), and
+    // FP64 terms to its own plane of ws (kUM * un doubles per tile and unit,
+    // element (row, col) of the tile at row + col * kUM), and
     // ozaki_reduce_kernel folds the planes into C in unit order afterwards:
     // the same operations as the fused epilogue, so the same bits. Used where
     // whole tiles would leave SMs idle (a partial last wave, or fewer tiles
     // than SMs). 0: every tile fused.
     double* ws;
     int tail_tiles;
+    int un;  // tile width (256 or 128): the split tail's plane size and the reduce kernel's tiling
 };
-
-constexpr int kOzTileElems = kUM * 256;
 
 // 2^x for x in [-1022, 1023]
 __device__ __forceinline__ double pow2_normal(int x) {
@@ -541,14 +548,15 @@ struct OzGroupSrc {
     }
 };
 
-template <class Src>
+template <int UN, class Src>
 __device__ __forceinline__ void ozaki_body(const Src& src) {
-    constexpr int ST = kOzST;
-    constexpr int UN = 256;
+    using Cfg = OzCfg<UN>;
+    constexpr int ST = Cfg::ST, CW = Cfg::CW, NCH = CW / 8;
+    constexpr int TILE_ELEMS = kUM * UN;
     constexpr int KSTEPS = 4;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    Bar* bar = reinterpret_cast<Bar*>(smem + ST * kOzStage);
+    Bar* bar = reinterpret_cast<Bar*>(smem + ST * Cfg::STAGE);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -602,9 +610,9 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                             ok = false;
                             break;
                         }
-                        uint8_t* sb = smem + s * kOzStage;
-                        uint8_t* sa = sb + kBTileOz();
-                        mbar_arrive_expect_tx(&bar->full[s], kBTileOz() + kATile);
+                        uint8_t* sb = smem + s * Cfg::STAGE;
+                        uint8_t* sa = sb + Cfg::BTILE;
+                        mbar_arrive_expect_tx(&bar->full[s], Cfg::BTILE + kATile);
                         tma_load_3d(sb, w.tb, &bar->full[s], k0, n0, top - i);
                         tma_load_3d(sa, w.ta, &bar->full[s], k0, m0, i);
                     }
@@ -647,10 +655,10 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                             break;
                         }
                         tc_fence_after();
-                        const uint32_t sb = smem_u32(smem + s * kOzStage);
-                        const uint32_t sa = sb + kBTileOz();
+                        const uint32_t sb = smem_u32(smem + s * Cfg::STAGE);
+                        const uint32_t sa = sb + Cfg::BTILE;
                         const bool low = pair && prev_s >= 0;  // A_i x B_{d0-i}: the previous stage's B
-                        const uint32_t pb = low ? smem_u32(smem + prev_s * kOzStage) : 0u;
+                        const uint32_t pb = low ? smem_u32(smem + prev_s * Cfg::STAGE) : 0u;
 #pragma unroll
                         for (int kk = 0; kk < KSTEPS; ++kk) {
                             const uint64_t ad = sw128_kmajor_desc(sa) + 2 * kk;
@@ -680,12 +688,12 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
     } else if (warp >= 2) {
         // ------------------------------ epilogue ------------------------------
         const int quarter = warp & 3;      // TMEM lanes 32*quarter.. (the warp's rank in its warpgroup)
-        const int cq = (warp - 2) >> 2;    // columns 64*cq .. 64*cq+63 of the tile
+        const int cq = (warp - 2) >> 2;    // columns CW*cq .. CW*cq+CW-1 of the tile
         const int row_in_tile = quarter * 32 + lane;
         // this warp's column table: 2^fc where fc is in [-1022, 1023], else 0
         // (a zero or absent column, or an exponent outside the normal range),
         // and fc itself
-        uint8_t* tab = smem + ST * kOzStage + 256 + (warp - 2) * kOzColTab;
+        uint8_t* tab = smem + ST * Cfg::STAGE + 256 + (warp - 2) * kOzColTab;
         double* col_scale = reinterpret_cast<double*>(tab);
         int* col_e = reinterpret_cast<int*>(tab + 64 * sizeof(double));
         const uint32_t lanebase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
@@ -706,13 +714,13 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
             const bool row_ok = r < p.m;
             const int er = row_ok ? p.row_exp[r] : kExpSentinel;
             __syncwarp();  // the previous item's reads of the table are done
-            // bit j of colmask: column j of the warp's 64 has a nonzero table
+            // bit j of colmask: column j of the warp's CW has a nonzero table
             // scale (so it also lies inside C)
             uint64_t colmask = 0;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < CW / 32; ++h) {
                 const int j = lane + 32 * h;
-                const int col = n0 + cq * 64 + j;
+                const int col = n0 + cq * CW + j;
                 const int fc = col < p.n ? __ldg(p.col_exp + col) : kExpSentinel;
                 const bool normal = fc != kExpSentinel && fc >= -1022 && fc <= 1023;
                 col_e[j] = fc;
@@ -747,14 +755,14 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                 // every live row of the warp takes the two-multiply scaling
                 const bool warp_fast = __all_sync(0xffffffffu, row_fast || !live);
                 double* wplane =
-                    split ? p.ws + (static_cast<size_t>(w.tt) * units + u) * kOzTileElems + row_in_tile : nullptr;
+                    split ? p.ws + (static_cast<size_t>(w.tt) * units + u) * TILE_ELEMS + row_in_tile : nullptr;
                 // chunk ch's C values are requested one chunk ahead (the first
                 // chunk's before the accumulator wait), so a chunk's L2 round
                 // trip overlaps the previous chunk's arithmetic
                 double cv[8];
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
-                    const int cbase = n0 + cq * 64;
+                    const int cbase = n0 + cq * CW;
                     cv[jj] = (live && read_c && cbase + jj < p.n)
                                  ? ld_l2hint(srow + static_cast<size_t>(cbase + jj) * ldc, pol_ld) : 0.0;
                 }
@@ -767,17 +775,17 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                     tc_fence_after();
                 }
 #pragma unroll 1
-                for (int ch = 0; ch < 8; ++ch) {
+                for (int ch = 0; ch < NCH; ++ch) {
                     // 8 columns at a time
                     const int j0 = ch * 8;
-                    const int col0 = cq * 64 + j0;
+                    const int col0 = cq * CW + j0;
                     const int cbase = n0 + col0;
                     double* const cp = crow + static_cast<size_t>(cbase) * ldc;
                     const double* const sp = srow + static_cast<size_t>(cbase) * ldc;
                     double cn[8];
 #pragma unroll
                     for (int jj = 0; jj < 8; ++jj)
-                        cn[jj] = (live && read_c && ch < 7 && cbase + 8 + jj < p.n)
+                        cn[jj] = (live && read_c && ch < NCH - 1 && cbase + 8 + jj < p.n)
                                      ? ld_l2hint(sp + static_cast<size_t>(8 + jj) * ldc, pol_ld) : 0.0;
                     uint32_t v0[8], v1[8];
                     tmem_ld8(lanebase + col0, v0);
@@ -846,18 +854,20 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
     }
 }
 
+template <int UN>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ OzParams p) {
-    ozaki_body(OzSingleSrc{&p, &tmA, &tmB});
+    ozaki_body<UN>(OzSingleSrc{&p, &tmA, &tmB});
 }
 
 // Many f64 problems in one persistent launch (the serving loop's Ozaki
 // batches): the same tiles and epilogue as ozaki_gemm_kernel, whole tiles only.
+template <int UN>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_grouped_kernel(const OzGroupEntry* __restrict__ tab, const int* __restrict__ starts, int nprob,
                          uint32_t* err) {
-    ozaki_body(OzGroupSrc{tab, starts, nprob, err});
+    ozaki_body<UN>(OzGroupSrc{tab, starts, nprob, err});
 }
 
 // Split tail: C of the tail tiles = the fused epilogue's sequence over the
@@ -867,23 +877,24 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 // threads take consecutive rows of a tile column (coalesced C and planes).
 __global__ void ozaki_reduce_kernel(const OzParams p, int units) {
     const int fused = p.num_tiles - p.tail_tiles;
-    const size_t total = static_cast<size_t>(p.tail_tiles) * kOzTileElems;
+    const int tile_elems = kUM * p.un;
+    const size_t total = static_cast<size_t>(p.tail_tiles) * tile_elems;
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int tt = static_cast<int>(idx / kOzTileElems);
-        const int local = static_cast<int>(idx - static_cast<size_t>(tt) * kOzTileElems);
+        const int tt = static_cast<int>(idx / tile_elems);
+        const int local = static_cast<int>(idx - static_cast<size_t>(tt) * tile_elems);
         int tm, tn;
         raster_tile<kOzRaster>(fused + tt, p.tiles_m, p.tiles_n, tm, tn);
-        const int r = tm * kUM + local % kUM, col = tn * 256 + local / kUM;
+        const int r = tm * kUM + local % kUM, col = tn * p.un + local / kUM;
         if (r >= p.m || col >= p.n) continue;
         double* cp = p.c + r + static_cast<size_t>(col) * p.ldc;
         const double c0 = p.beta_mode ? p.cin[r + static_cast<size_t>(col) * p.ldc] : 0.0;
         double acc = 0.0;
         if (p.beta_mode == 1) acc = c0;
         else if (p.beta_mode == 2) acc = p.beta * c0;
-        const double* w = p.ws + static_cast<size_t>(tt) * units * kOzTileElems + local;
+        const double* w = p.ws + static_cast<size_t>(tt) * units * tile_elems + local;
         const int last = (p.row_exp[r] == kExpSentinel) ? 1 : units;
-        for (int u = 0; u < last; ++u) acc = fma(p.alpha, w[static_cast<size_t>(u) * kOzTileElems], acc);
+        for (int u = 0; u < last; ++u) acc = fma(p.alpha, w[static_cast<size_t>(u) * tile_elems], acc);
         *cp = acc;
     }
 }
@@ -1576,7 +1587,27 @@ int bf16_grouped_dev(int planes, const rb_gemm_problem* probs, size_t count, con
 // would, counting the reduce pass over their planes and C; else 0. Times are
 // modelled from the products per unit (a diagonal d has d + 1) at the B200's
 // INT8 rate per SM and its copy rate; only their ratio matters.
-int ozaki_tail_tiles(int num_tiles, int slices, int kchunks, int k, int sms) {
+// Dynamic shared memory of both Ozaki tile widths, set once per process.
+cudaError_t ozaki_kernel_attributes() {
+    static std::once_flag once;
+    static cudaError_t result = cudaSuccess;
+    std::call_once(once, [] {
+        result = cudaFuncSetAttribute(ozaki_gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      OzCfg<256>::SMEM);
+        if (result == cudaSuccess)
+            result = cudaFuncSetAttribute(ozaki_gemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          OzCfg<128>::SMEM);
+        if (result == cudaSuccess)
+            result = cudaFuncSetAttribute(ozaki_grouped_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          OzCfg<256>::SMEM);
+        if (result == cudaSuccess)
+            result = cudaFuncSetAttribute(ozaki_grouped_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          OzCfg<128>::SMEM);
+    });
+    return result;
+}
+
+int ozaki_tail_tiles(int num_tiles, int slices, int kchunks, int k, int sms, int un) {
     const int upc = (slices + 1) / 2;
     if (kchunks != 1 || upc < 2 || sms < 1) return 0;
     const int full = num_tiles / sms;
@@ -1592,10 +1623,11 @@ int ozaki_tail_tiles(int num_tiles, int slices, int kchunks, int k, int sms) {
         load[(num_tiles - tail + j) % G] += (d0 + 1) + (d1 >= 0 ? d1 + 1 : 0);
     }
     const int max_load = *std::max_element(load.begin(), load.end());
-    const double product_s = 2.0 * kUM * 256 * static_cast<double>(k) / (4.4e15 / 148);
+    const double tile_elems = static_cast<double>(kUM) * un;
+    const double product_s = 2.0 * tile_elems * static_cast<double>(k) / (4.4e15 / 148);
     const double whole_tile_s = product_s * slices * (slices + 1) / 2;
-    const double reduce_s = 4e-6 + tail * (upc + 2.0) * kOzTileElems * sizeof(double) / 6.5e12;
-    const bool fits = static_cast<size_t>(tail) * upc * kOzTileElems * sizeof(double) <= (size_t(512) << 20);
+    const double reduce_s = 4e-6 + tail * (upc + 2.0) * tile_elems * sizeof(double) / 6.5e12;
+    const bool fits = tail * upc * tile_elems * sizeof(double) <= static_cast<double>(size_t(512) << 20);
     return (fits && product_s * max_load + reduce_s < 0.9 * whole_tile_s) ? tail : 0;
 }
 
@@ -1611,14 +1643,15 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int num_tiles = ((m + kUM - 1) / kUM) * ((n + 255) / 256);
+    const int un = ozaki_tile_n(m, n, k);
+    const int num_tiles = ((m + kUM - 1) / kUM) * ((n + un - 1) / un);
     const int upc = (slices + 1) / 2;
     const long long kt_chunk = 2147483647LL / (static_cast<long long>(slices) * 128 * 128) / 128;
     const long long ktc = std::max(kt_chunk, 1LL);
     const int kchunks = static_cast<int>(((k + 127) / 128 + ktc - 1) / ktc);
-    const int tail_tiles = ozaki_tail_tiles(num_tiles, slices, kchunks, k, sms);
+    const int tail_tiles = ozaki_tail_tiles(num_tiles, slices, kchunks, k, sms, un);
     const size_t b_bytes = round_up(slices * pb, 256);
-    const size_t w_bytes = static_cast<size_t>(tail_tiles) * upc * kOzTileElems * sizeof(double);
+    const size_t w_bytes = static_cast<size_t>(tail_tiles) * upc * kUM * un * sizeof(double);
     cudaError_t e = scratch_alloc(&buf, exps + a_bytes + b_bytes + w_bytes, st);
     if (e != cudaSuccess) return e;
     int* ea = static_cast<int*>(buf);
@@ -1640,7 +1673,7 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     count_launch(5);
     CUtensorMap tma, tmb;
     CUresult r = make_tmap_planes(&tma, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, m, slices, kp, kUM);
-    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, 256);
+    if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, k, n, slices, kp, un);
     if (r != CUDA_SUCCESS) {
         if (cu_err) *cu_err = r;
         cudaFreeAsync(buf, st);
@@ -1648,8 +1681,9 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
     }
     OzParams p{};
     p.m = m; p.n = n; p.k = k;
+    p.un = un;
     p.tiles_m = (m + kUM - 1) / kUM;
-    p.tiles_n = (n + 255) / 256;
+    p.tiles_n = (n + un - 1) / un;
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.num_kt = static_cast<int>((k + 127) / 128);
     p.slices = slices;
@@ -1669,22 +1703,18 @@ cudaError_t launch_ozaki_gemm(bool ta, bool tb, int m, int n, int k, double alph
         p.ws = reinterpret_cast<double*>(static_cast<uint8_t*>(buf) + exps + a_bytes + b_bytes);
     }
 
-    constexpr int smem = kOzSmem;
-    static bool attr = false;
-    if (!attr) {
-        e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) { cudaFreeAsync(buf, st); return e; }
-        attr = true;
-    }
+    e = ozaki_kernel_attributes();
+    if (e != cudaSuccess) { cudaFreeAsync(buf, st); return e; }
     const int items = p.num_tiles + p.tail_tiles * (p.kchunks * upc - 1);
     const int grid = items < sms ? items : sms;
     KernelTimer tmr;
     kernel_timing_begin("umma_ozaki_i8", 2.0 * m * n * static_cast<double>(k) * slices * (slices + 1) / 2, st, &tmr);
-    ozaki_gemm_kernel<<<grid, kOzThreads, smem, st>>>(tma, tmb, p);
+    if (un == 256) ozaki_gemm_kernel<256><<<grid, kOzThreads, OzCfg<256>::SMEM, st>>>(tma, tmb, p);
+    else           ozaki_gemm_kernel<128><<<grid, kOzThreads, OzCfg<128>::SMEM, st>>>(tma, tmb, p);
     kernel_timing_end(&tmr, st);
     count_launch();
     if (p.tail_tiles > 0) {
-        const size_t elems = static_cast<size_t>(p.tail_tiles) * kOzTileElems;
+        const size_t elems = static_cast<size_t>(p.tail_tiles) * kUM * un;
         const size_t blocks = std::min<size_t>((elems + 255) / 256, static_cast<size_t>(sms) * 16);
         ozaki_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(p, p.kchunks * upc);
         count_launch();
@@ -1717,6 +1747,7 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         double alpha, beta;
         size_t kp, off_exp, off_a, off_b;
         int num_kt;
+        int un;  // tile width
     };
     std::vector<Job> jobs;
     jobs.reserve(count);
@@ -1767,6 +1798,7 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         j.beta = q.beta;
         j.kp = round_up(q.k, 16);
         j.num_kt = static_cast<int>((q.k + 127) / 128);
+        j.un = ozaki_tile_n(j.m, j.n, j.k);
         j.off_exp = exps;
         exps += m + n;
         j.off_a = planes;
@@ -1780,12 +1812,15 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         return RB_ERR_CUDA;
     }
     if (jobs.empty()) return RB_OK;
-    // longest tiles first: the CTAs walk the items with a stride of the grid
-    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& x, const Job& y) { return x.num_kt > y.num_kt; });
+    // one launch per tile width, wide tiles first; inside each, longest tiles
+    // first: the CTAs walk the items with a stride of the grid
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& x, const Job& y) {
+        return x.un != y.un ? x.un > y.un : x.num_kt > y.num_kt;
+    });
     const int np = static_cast<int>(jobs.size());
     // device image: [entries][starts][operands] then exponents, then planes
     const size_t ent_bytes = round_up(np * sizeof(OzGroupEntry), 256);
-    const size_t starts_bytes = round_up((np + 1) * sizeof(int), 256);
+    const size_t starts_bytes = round_up((np + 2) * sizeof(int), 256);  // starts of each width's table
     const size_t ops_bytes = round_up(2 * np * sizeof(OzOperand), 256);
     const size_t img_bytes = ent_bytes + starts_bytes + ops_bytes;
     const size_t exp_bytes = round_up(exps * sizeof(int), 256);
@@ -1803,6 +1838,7 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
     int8_t* dplanes = reinterpret_cast<int8_t*>(mem + img_bytes + exp_bytes);
     uint32_t* err_word = device_error_word();
     int tiles = 0, exp_blocks = 0, slice_blocks = 0;
+    int n_wide = 0, tiles_wide = 0;  // the problems (and their tiles) of the 256-wide launch
     double work = 0;
     CUresult r = CUDA_SUCCESS;
     for (int i = 0; i < np && r == CUDA_SUCCESS; ++i) {
@@ -1833,11 +1869,12 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         OzGroupEntry g{};  // 64-byte aligned here; copied into the image below
         r = make_tmap_planes(&g.tmA, sla, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, j.k, j.m, slices, j.kp, kUM);
         if (r == CUDA_SUCCESS)
-            r = make_tmap_planes(&g.tmB, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, j.k, j.n, slices, j.kp, 256);
+            r = make_tmap_planes(&g.tmB, slb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, j.k, j.n, slices, j.kp, j.un);
         OzParams& p = g.p;
         p.m = j.m; p.n = j.n; p.k = j.k;
+        p.un = j.un;
         p.tiles_m = (j.m + kUM - 1) / kUM;
-        p.tiles_n = (j.n + 255) / 256;
+        p.tiles_n = (j.n + j.un - 1) / j.un;
         p.num_tiles = p.tiles_m * p.tiles_n;
         p.num_kt = j.num_kt;
         p.slices = slices;
@@ -1850,11 +1887,20 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         p.row_exp = ea; p.col_exp = eb;
         p.err = err_word;
         std::memcpy(img.data() + i * sizeof(OzGroupEntry), &g, sizeof(OzGroupEntry));
-        starts[i] = tiles;
+        // the wide launch's starts at [0, n_wide], the narrow launch's at
+        // [n_wide + 1, np + 1], each counting from its own first tile
+        if (j.un == 256) {
+            starts[i] = tiles;
+            n_wide = i + 1;
+            tiles_wide = tiles + p.num_tiles;
+        } else {
+            starts[i + 1] = tiles - tiles_wide;
+        }
         tiles += p.num_tiles;
         work += 2.0 * j.m * j.n * static_cast<double>(j.k) * slices * (slices + 1) / 2;
     }
-    starts[np] = tiles;
+    starts[n_wide] = tiles_wide;        // end of the wide table
+    starts[np + 1] = tiles - tiles_wide;  // end of the narrow table (at n_wide + 1 .. np + 1)
     if (r != CUDA_SUCCESS) {
         if (ce) *ce = static_cast<int32_t>(r);
         cudaFreeAsync(mem, st);
@@ -1863,12 +1909,7 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    constexpr int smem = kOzSmem;
-    static bool attr = false;
-    if (!attr) {
-        e = cudaFuncSetAttribute(ozaki_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess) attr = true;
-    }
+    e = ozaki_kernel_attributes();
     // a pageable source: the driver has staged the image when the call returns
     if (e == cudaSuccess) e = cudaMemcpyAsync(mem, img.data(), img_bytes, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
@@ -1886,10 +1927,17 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         }
         KernelTimer tmr;
         kernel_timing_begin("umma_ozaki_grouped_i8", work, st, &tmr);
-        ozaki_grouped_kernel<<<tiles < sms ? tiles : sms, kOzThreads, smem, st>>>(
-            reinterpret_cast<const OzGroupEntry*>(mem), reinterpret_cast<const int*>(mem + ent_bytes), np, err_word);
+        const OzGroupEntry* dtab = reinterpret_cast<const OzGroupEntry*>(mem);
+        const int* dstarts = reinterpret_cast<const int*>(mem + ent_bytes);
+        const int tiles_narrow = tiles - tiles_wide;
+        if (n_wide > 0)
+            ozaki_grouped_kernel<256><<<std::min(tiles_wide, sms), kOzThreads, OzCfg<256>::SMEM, st>>>(
+                dtab, dstarts, n_wide, err_word);
+        if (np > n_wide)
+            ozaki_grouped_kernel<128><<<std::min(tiles_narrow, sms), kOzThreads, OzCfg<128>::SMEM, st>>>(
+                dtab + n_wide, dstarts + n_wide + 1, np - n_wide, err_word);
         kernel_timing_end(&tmr, st);
-        count_launch(4);
+        count_launch(3 + (n_wide > 0) + (np > n_wide));
         e = cudaGetLastError();
     }
     cudaFreeAsync(mem, st);
@@ -2052,6 +2100,7 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         if (r != CUDA_SUCCESS) return fail(RB_ERR_CUDA, 0, 0, static_cast<int32_t>(r));
         OzParams p{};
         p.m = M; p.n = N; p.k = K;
+        p.un = 256;  // always the wide tile, and never the split tail: its scratch is sized for that
         p.tiles_m = (M + kUM - 1) / kUM;
         p.tiles_n = (N + 255) / 256;
         p.num_tiles = p.tiles_m * p.tiles_n;
@@ -2066,12 +2115,12 @@ extern "C" rb_status rb_dgemm_ozaki_noalloc(rb_layout layout, rb_transpose trans
         p.cin = c;
         p.row_exp = ea; p.col_exp = eb;
         p.err = status;
-        constexpr int smem = kOzSmem;
-        e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = ozaki_kernel_attributes();
         if (e != cudaSuccess) return fail(RB_ERR_CUDA, 0, 0, e);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        ozaki_gemm_kernel<<<p.num_tiles < sms ? p.num_tiles : sms, kOzThreads, smem, st>>>(tma, tmb, p);
+        ozaki_gemm_kernel<256><<<p.num_tiles < sms ? p.num_tiles : sms, kOzThreads, OzCfg<256>::SMEM, st>>>(
+            tma, tmb, p);
         count_launch();
         e = cudaGetLastError();
     }

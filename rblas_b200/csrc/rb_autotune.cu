@@ -1,23 +1,32 @@
-// rb_autotune.cu -- split-K autotuner for the grouped kernel, with a cache
-// file.
+// rb_autotune.cu -- autotuner of the GEMM kernels' per-shape parameters,
+// with a cache file.
 //
-// The grouped kernel's tile shape is fixed per dtype (128 x 128 f32,
-// 128 x 64 f64: the register budget of the 8-warp SIMT tile) and it runs
-// without clusters, so its free parameter per problem is the split-K factor.
-// The tuner walks shape buckets (floor(log2) of the column-major m, n and of
-// k, for 32 <= m, n, k <= 4096, per dtype), times every candidate factor on
-// the bucket's representative shape (each dimension 1.41x its bucket floor)
-// launched alone through the grouped path, and keeps the fastest; a larger
-// factor must win by 3% to be kept. Buckets with a full wave of C tiles, or
-// too short a K for two ranges of four K-tiles, are left to the built-in
-// rule. The table is written as text:
+// Two parameters are tuned per shape bucket (floor(log2) of the
+// column-major m, n and of k, for 32 <= m, n, k <= 4096):
+//   - the split-K factor of the grouped plain kernel, per dtype. Its tile is
+//     fixed per dtype (128 x 128 f32, 128 x 64 f64: the register budget of
+//     the 8-warp SIMT tile) and it runs without clusters. Every candidate
+//     factor is timed on the bucket's representative shape (each dimension
+//     1.41x its bucket floor) launched alone through the grouped path; a
+//     larger factor must win by 3% to be kept. Buckets with a full wave of C
+//     tiles, or too short a K for two ranges of four K-tiles, are left to
+//     the built-in rule.
+//   - the tile width of the Ozaki tensor-core kernels, 128 x 256 or
+//     128 x 128 (f64 buckets with n below 2048): the narrow tile pads less
+//     and deals more tiles to the SMs, the wide one lands fewer operand bytes
+//     per MAC. The narrow one must win by 3%. The width changes no result
+//     bit.
+// The table is written as text:
 //
-//   rblas_b200 grouped split-k v1
+//   rblas_b200 grouped autotune v2
 //   device <name with spaces replaced by _> <sm count>
-//   <dtype 0|1> <log2 m> <log2 n> <log2 k> <splits>
+//   <kind> <log2 m> <log2 n> <log2 k> <value>
 //   ...
 //
-// and installed process-wide; loading checks the device line.
+// kind 0 / 1: split factor of an f32 / f64 bucket; kind 2: Ozaki tile width
+// of an f64 bucket. Files written by the first version ("... split-k v1",
+// split lines only) still load. The tables are installed process-wide;
+// loading checks the device line.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -149,20 +158,55 @@ rb_status rb_autotune_grouped(const char* cache_path, int* buckets_tuned) {
                     ++tuned;
                 }
     }
+    // Ozaki tile width per f64 bucket (n below 2048)
+    auto oz_table = std::make_shared<std::map<uint32_t, int>>();
+    for (int lm = kLoBucket; lm <= kHiBucket && status == RB_OK; ++lm)
+        for (int ln = kLoBucket; ln <= 10 && status == RB_OK; ++ln)
+            for (int lk = kLoBucket; lk <= kHiBucket && status == RB_OK; ++lk) {
+                const int m = static_cast<int>(std::ldexp(1.41, lm));
+                const int n = static_cast<int>(std::ldexp(1.41, ln));
+                const int k = static_cast<int>(std::ldexp(1.41, lk));
+                float ms[2] = {0, 0};
+                for (int w = 0; w < 2 && status == RB_OK; ++w) {
+                    force_ozaki_width(w == 0 ? 256 : 128);
+                    CUresult cu = CUDA_SUCCESS;
+                    cudaError_t ce = launch_ozaki_gemm(false, false, m, n, k, 1.0, static_cast<const double*>(A), m,
+                                                       static_cast<const double*>(B), k, 0.0,
+                                                       static_cast<double*>(Cm), m, rb_get_ozaki_slices(), st, &cu);
+                    if (ce == cudaSuccess) cudaEventRecord(ev0, st);
+                    for (int r = 0; r < 3 && ce == cudaSuccess; ++r)
+                        ce = launch_ozaki_gemm(false, false, m, n, k, 1.0, static_cast<const double*>(A), m,
+                                               static_cast<const double*>(B), k, 0.0, static_cast<double*>(Cm), m,
+                                               rb_get_ozaki_slices(), st, &cu);
+                    if (ce == cudaSuccess) ce = cudaEventRecord(ev1, st);
+                    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+                    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms[w], ev0, ev1);
+                    if (ce != cudaSuccess || cu != CUDA_SUCCESS) status = RB_ERR_CUDA;
+                }
+                force_ozaki_width(0);
+                if (status != RB_OK) break;
+                (*oz_table)[tune_key(1, m, n, k)] = (ms[1] < 0.97f * ms[0]) ? 128 : 256;
+                ++tuned;
+            }
+    force_ozaki_width(0);
     if (status == RB_OK) {
         if (cache_path && *cache_path) {
             std::ofstream out(cache_path);
             if (!out) {
                 status = RB_ERR_INVALID_ARG;
             } else {
-                out << "rblas_b200 grouped split-k v1\n";
+                out << "rblas_b200 grouped autotune v2\n";
                 out << "device " << device_tag() << "\n";
                 for (const auto& kv : *table)
                     out << ((kv.first >> 24) & 1) << ' ' << ((kv.first >> 16) & 255) << ' ' << ((kv.first >> 8) & 255)
                         << ' ' << (kv.first & 255) << ' ' << kv.second << "\n";
+                for (const auto& kv : *oz_table)
+                    out << 2 << ' ' << ((kv.first >> 16) & 255) << ' ' << ((kv.first >> 8) & 255) << ' '
+                        << (kv.first & 255) << ' ' << kv.second << "\n";
             }
         }
         set_tuned_splits(table);
+        set_tuned_ozaki_widths(oz_table);
         if (buckets_tuned) *buckets_tuned = tuned;
     }
     cleanup();
@@ -174,25 +218,36 @@ rb_status rb_autotune_load(const char* cache_path) {
     std::ifstream in(cache_path);
     if (!in) return RB_ERR_INVALID_ARG;
     std::string line;
-    if (!std::getline(in, line) || line != "rblas_b200 grouped split-k v1") return RB_ERR_INVALID_ARG;
+    if (!std::getline(in, line)) return RB_ERR_INVALID_ARG;
+    const bool v2 = line == "rblas_b200 grouped autotune v2";
+    if (!v2 && line != "rblas_b200 grouped split-k v1") return RB_ERR_INVALID_ARG;
     if (!std::getline(in, line) || line != "device " + device_tag()) return RB_ERR_INVALID_ARG;
     auto table = std::make_shared<std::map<uint32_t, int>>();
+    auto oz_table = std::make_shared<std::map<uint32_t, int>>();
     while (std::getline(in, line)) {
         if (line.empty()) continue;
         std::istringstream ls(line);
-        int dt, lm, ln, lk, s;
-        if (!(ls >> dt >> lm >> ln >> lk >> s) || dt < 0 || dt > 1 || lm < 0 || lm > 31 || ln < 0 || ln > 31 ||
-            lk < 0 || lk > 31 || s < 1 || s > kGroupedMaxSplit)
+        int kind, lm, ln, lk, v;
+        if (!(ls >> kind >> lm >> ln >> lk >> v) || kind < 0 || kind > (v2 ? 2 : 1) || lm < 0 || lm > 31 || ln < 0 ||
+            ln > 31 || lk < 0 || lk > 31)
             return RB_ERR_INVALID_ARG;
         const size_t m = size_t(1) << lm, n = size_t(1) << ln, k = size_t(1) << lk;
-        (*table)[tune_key(dt, m, n, k)] = s;
+        if (kind == 2) {
+            if (v != 128 && v != 256) return RB_ERR_INVALID_ARG;
+            (*oz_table)[tune_key(1, m, n, k)] = v;
+        } else {
+            if (v < 1 || v > kGroupedMaxSplit) return RB_ERR_INVALID_ARG;
+            (*table)[tune_key(kind, m, n, k)] = v;
+        }
     }
     set_tuned_splits(table);
+    set_tuned_ozaki_widths(oz_table);
     return RB_OK;
 }
 
 rb_status rb_autotune_reset(void) {
     set_tuned_splits(nullptr);
+    set_tuned_ozaki_widths(nullptr);
     return RB_OK;
 }
 

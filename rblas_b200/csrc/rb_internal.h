@@ -185,6 +185,13 @@ uint32_t tune_key(int dtype, size_t m, size_t n, size_t k);
 void set_tuned_splits(std::shared_ptr<const std::map<uint32_t, int>> table);
 void force_grouped_splits(int s);
 constexpr int kGroupedMaxSplit = 16;
+// Tile width (256 or 128 columns) of the Ozaki kernels for a column-major
+// m x n x k problem: the installed autotuner table's choice for its bucket,
+// else 128 when n <= 128 and 256 otherwise. The width changes no result
+// bit, only the speed. force_ozaki_width(w) fixes it on this thread (0: off).
+int ozaki_tile_n(size_t m, size_t n, size_t k);
+void set_tuned_ozaki_widths(std::shared_ptr<const std::map<uint32_t, int>> table);
+void force_ozaki_width(int w);
 
 // rblas's argument checks for one table entry (dtype, layout, transposes,
 // leading dimensions) plus the 32-bit tile-index limit; an rb_status value.
