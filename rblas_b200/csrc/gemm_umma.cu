@@ -92,10 +92,13 @@ struct UParams {
     uint32_t* err;
 };
 
+constexpr int kMaxStages = 8;  // mbarrier pairs in Bar: every kernel's ring must fit
+
 struct Bar {
-    uint64_t full[4], empty[4], acc_full[2], acc_empty[2], drain;
+    uint64_t full[kMaxStages], empty[kMaxStages], acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
 };
+static_assert(sizeof(Bar) <= 256, "the kernels reserve 256 bytes of shared memory for Bar");
 
 // One problem of a grouped BF16-split launch: its plane tensor maps (64-byte
 // aligned for TMA) and parameters.
@@ -150,6 +153,7 @@ template <int MODE, class Src>
 __device__ __forceinline__ void umma_body(const Src& src) {
     using Cfg = UCfg<MODE>;
     constexpr int UN = Cfg::UN, NA = Cfg::NA, NB = Cfg::NB, ST = Cfg::STAGES;
+    static_assert(ST <= kMaxStages, "Bar holds kMaxStages stages");
     constexpr int BTILE = UN * kRowBytes;
     constexpr int STAGE_BYTES = NA * kATile + NB * BTILE;
     constexpr int KSTEPS = 4;  // UMMA K steps of 32 bytes per 128-byte tile row
@@ -397,6 +401,7 @@ template <int UN>
 struct OzCfg {
     static_assert(UN == 256 || UN == 128, "Ozaki tiles are 128 x 256 or 128 x 128");
     static constexpr int ST = UN == 256 ? 4 : 6;
+    static_assert(ST <= kMaxStages, "Bar holds kMaxStages stages");
     static constexpr int BTILE = UN * kRowBytes;
     static constexpr int STAGE = kATile + BTILE;  // 48 KiB / 32 KiB
     static constexpr int CW = UN / 4;             // four epilogue warps per TMEM lane quarter
