@@ -43,6 +43,10 @@ struct TbParams {
     // op'(A)[r][c] (reversed when rev) at A_i + a_off + r*a_dr + c*a_dc
     long long a_off, a_dr, a_dc;
     size_t stride_a, ldb_rs, ldb_cs, stride_b;  // B element (i, j) of the solve at i*rs + j*cs
+    // f64 tensor-core path: rows of op'(A) are unit stride and every even row
+    // starts on 16 bytes (a_dr == 1, no offset, even lda and stride_a,
+    // aligned base), so two adjacent rows load as one double2
+    int vec_a;
 };
 
 template <typename T>
@@ -263,7 +267,8 @@ constexpr size_t kTbSmemMax = 227 * 1024;
 // (mma.sync m16n8k8 f64), blocked like the substitution:
 //   1. trsm_inv_diag_kernel inverts every 64 x 64 diagonal block of every
 //      member once, W_b = inv(L_bb) (forward substitution of the unit
-//      vectors; Unit takes the diagonal as 1), into a workspace;
+//      vectors, one column per thread held in registers; Unit takes the
+//      diagonal as 1), into a workspace;
 //   2. trsm_dmma_kernel keeps the member's q x RB slice Y = alpha*B in shared
 //      memory and for each block b computes X_b = W_b * Y_b, then
 //      Y_trailing -= L[trailing, b] * X_b. Both products read A and W as
@@ -274,15 +279,14 @@ constexpr size_t kTbSmemMax = 227 * 1024;
 // stays within the normwise backward-error bound the tests state.
 constexpr int kInvNB = 64;
 
-constexpr int kInvSmem = 2 * kInvNB * (kInvNB + 1) * static_cast<int>(sizeof(double));
+constexpr int kInvSmem = kInvNB * (kInvNB + 1) * static_cast<int>(sizeof(double));
 
 __global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __restrict__ A0, TbParams p,
                                                                 double* __restrict__ W, int nblocks) {
     extern __shared__ __align__(16) unsigned char inv_smem[];
-    // L[r][c] of the diagonal block, zero outside it; Wt[c][r] = inv(L)[r][c]
-    // (column c, written by thread c)
+    // L[r][c] of the diagonal block, zero outside it (and zero on the
+    // diagonal for Unit); afterwards the same buffer holds the inverse
     auto L = reinterpret_cast<double (*)[kInvNB + 1]>(inv_smem);
-    auto Wt = reinterpret_cast<double (*)[kInvNB + 1]>(inv_smem + kInvNB * (kInvNB + 1) * sizeof(double));
     const int b = blockIdx.x, member = blockIdx.y;
     const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
     const int o = b * kInvNB, nb = min(kInvNB, p.q - o);
@@ -292,30 +296,31 @@ __global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __r
                                    : ((r < nb && c == r && !p.unit) ? *a_ptr(A, p, o + r, o + c) : 0.0);
     }
     __syncthreads();
-    // column j of the inverse, rows in order: w_r = (delta_rj - sum_{s<r} L[r][s] w_s) / L[r][r];
-    // every thread runs the same trip counts (w_s = 0 above row j), so the
-    // warp never diverges and L[r][s] is one broadcast read
+    // Thread j solves column j of the inverse, rows in order:
+    //   w_r = (delta_rj - sum_{s<r} L[r][s] w_s) / L[r][r]  (w_s = 0 above row j).
+    // Both loops are unrolled, so the column stays in registers; every thread
+    // runs the same sequence (no divergence) and L[r][s] is one broadcast
+    // read. Four partial sums (s mod 4) keep the dependent chain short.
     const int j = threadIdx.x;
+    double w[kInvNB];
+#pragma unroll
     for (int r = 0; r < kInvNB; ++r) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int s = 0;
-        for (; s + 4 <= r; s += 4) {
-            s0 = fma(L[r][s], Wt[j][s], s0);
-            s1 = fma(L[r][s + 1], Wt[j][s + 1], s1);
-            s2 = fma(L[r][s + 2], Wt[j][s + 2], s2);
-            s3 = fma(L[r][s + 3], Wt[j][s + 3], s3);
-        }
-        for (; s < r; ++s) s0 = fma(L[r][s], Wt[j][s], s0);
-        double w = ((r == j) ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3));
-        if (r >= nb || j >= nb || r < j) w = 0.0;
-        else if (!p.unit) w = w / L[r][r];
-        Wt[j][r] = w;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int s = 0; s < r; ++s) acc[s & 3] = fma(L[r][s], w[s], acc[s & 3]);
+        double v = ((r == j) ? 1.0 : 0.0) - ((acc[0] + acc[1]) + (acc[2] + acc[3]));
+        if (r >= nb || j >= nb || r < j) v = 0.0;
+        else if (!p.unit) v = v / L[r][r];
+        w[r] = v;
     }
+    __syncthreads();  // every thread is done reading L
+#pragma unroll
+    for (int r = 0; r < kInvNB; ++r) L[r][j] = w[r];
     __syncthreads();
     double* Wb = W + (static_cast<size_t>(member) * nblocks + b) * (kInvNB * kInvNB);
     for (int idx = threadIdx.x; idx < kInvNB * kInvNB; idx += kInvNB) {
         const int r = idx % kInvNB, c = idx / kInvNB;  // column-major: coalesced stores
-        Wb[idx] = Wt[c][r];
+        Wb[idx] = L[r][c];
     }
 }
 
@@ -365,15 +370,20 @@ __global__ void __launch_bounds__(kTbThreads, 2)
         double xacc[4] = {0.0, 0.0, 0.0, 0.0};
         const bool xw = warp < 4 * NBLK;
         const int xm = warp % 4, xn = warp / 4;
+        // DMMA fragment rows g and g+8 take the adjacent rows 2g and 2g+1 of
+        // the 16-row block (the output rows follow), so each pair is one
+        // 16-byte load; the fragment layout is in simt_tile.cuh (dmma_16x8x8)
         if (xw) {
             double a[8][4];
 #pragma unroll
             for (int kk = 0; kk < 8; ++kk) {  // W is column-major 64 x 64, zero outside the block
-                const int r = 16 * xm + g, k = 8 * kk + t;
-                a[kk][0] = __ldg(Wb + r + 64 * k);
-                a[kk][1] = __ldg(Wb + r + 8 + 64 * k);
-                a[kk][2] = __ldg(Wb + r + 64 * (k + 4));
-                a[kk][3] = __ldg(Wb + r + 8 + 64 * (k + 4));
+                const int r = 16 * xm + 2 * g, k = 8 * kk + t;
+                const double2 lo = __ldg(reinterpret_cast<const double2*>(Wb + r + 64 * k));
+                const double2 hi = __ldg(reinterpret_cast<const double2*>(Wb + r + 64 * (k + 4)));
+                a[kk][0] = lo.x;
+                a[kk][1] = lo.y;
+                a[kk][2] = hi.x;
+                a[kk][3] = hi.y;
             }
 #pragma unroll
             for (int kk = 0; kk < 8; ++kk) {
@@ -386,14 +396,14 @@ __global__ void __launch_bounds__(kTbThreads, 2)
         }
         __syncthreads();  // every read of Y_b is done
         if (xw) {
-            const int r = 16 * xm + g, c = 8 * xn + 2 * t;
+            const int r = 16 * xm + 2 * g, c = 8 * xn + 2 * t;
             if (r < nb) {
                 Y[(o + r) * YS + c] = xacc[0];
                 Y[(o + r) * YS + c + 1] = xacc[1];
             }
-            if (r + 8 < nb) {
-                Y[(o + r + 8) * YS + c] = xacc[2];
-                Y[(o + r + 8) * YS + c + 1] = xacc[3];
+            if (r + 1 < nb) {
+                Y[(o + r + 1) * YS + c] = xacc[2];
+                Y[(o + r + 1) * YS + c + 1] = xacc[3];
             }
         }
         __syncthreads();
@@ -401,14 +411,28 @@ __global__ void __launch_bounds__(kTbThreads, 2)
         const int r_first = o + nb;
         for (int r0 = r_first + 16 * warp; r0 < q; r0 += 16 * 8) {
             double a[8][4];
-            const int ra = r0 + g, rb = r0 + g + 8;
+            const int ra = r0 + 2 * g, rb = ra + 1;  // fragment rows g and g+8 (see the X step)
+            if (p.vec_a && r0 + 16 <= q) {
+                // r0 is even (o + 64 + 16 * i), so every pair starts on 16 bytes
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {  // nb == 64 here: only the last block has no trailing rows
-                const int k = o + 8 * kk + t;
-                a[kk][0] = (ra < q) ? __ldg(a_ptr(A, p, ra, k)) : 0.0;
-                a[kk][1] = (rb < q) ? __ldg(a_ptr(A, p, rb, k)) : 0.0;
-                a[kk][2] = (ra < q) ? __ldg(a_ptr(A, p, ra, k + 4)) : 0.0;
-                a[kk][3] = (rb < q) ? __ldg(a_ptr(A, p, rb, k + 4)) : 0.0;
+                for (int kk = 0; kk < 8; ++kk) {  // nb == 64 here: only the last block has no trailing rows
+                    const int k = o + 8 * kk + t;
+                    const double2 lo = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k)));
+                    const double2 hi = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k + 4)));
+                    a[kk][0] = lo.x;
+                    a[kk][1] = lo.y;
+                    a[kk][2] = hi.x;
+                    a[kk][3] = hi.y;
+                }
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    const int k = o + 8 * kk + t;
+                    a[kk][0] = (ra < q) ? __ldg(a_ptr(A, p, ra, k)) : 0.0;
+                    a[kk][1] = (rb < q) ? __ldg(a_ptr(A, p, rb, k)) : 0.0;
+                    a[kk][2] = (ra < q) ? __ldg(a_ptr(A, p, ra, k + 4)) : 0.0;
+                    a[kk][3] = (rb < q) ? __ldg(a_ptr(A, p, rb, k + 4)) : 0.0;
+                }
             }
             double acc[NBLK][4];
 #pragma unroll
@@ -540,6 +564,8 @@ int trsm_batched_dev(int side, int uplo, int trans, int diag, size_t m, size_t n
     p.ldb_rs = (side == RB_LEFT) ? 1 : ldb;
     p.ldb_cs = (side == RB_LEFT) ? ldb : 1;
     p.stride_b = stride_b;
+    p.vec_a = (p.a_dr == 1 && p.a_off == 0 && lda % 2 == 0 && stride_a % 2 == 0 &&
+               reinterpret_cast<uintptr_t>(A) % 16 == 0) ? 1 : 0;
     cudaError_t e = cudaSuccess;
     bool alloc_failed = false;
     int td_rb = 0;  // f64: slice width of the tensor-core path (0: not used)
