@@ -397,9 +397,9 @@ def run_ours(args):
                 "whose peak on this GPU measured the same, 36.8-37.0 TFLOP/s); not in MEASURED_PEAKS.json")
     # DRAM bytes per launch of the dominant kernel, measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of each of
-    # the step's shapes: 2.484 GB at 4096^3 (x4 per step), 1.289 GB at
+    # the step's shapes: 2.186 GB at 4096^3 (x4 per step), 1.067 GB at
     # 3000x5000x2048 (x1)
-    traffic = (4 * 2.484e9 + 1.289e9) / 5 if kname == "umma_ozaki_i8" else None
+    traffic = (4 * 2.186e9 + 1.067e9) / 5 if kname == "umma_ozaki_i8" else None
     # second denominator for the INT8 pipe: twice the driver-measured dense
     # BF16 cuBLAS burst (the INT8 tensor rate is twice the BF16 rate)
     mp = measured_peaks() or {}
