@@ -290,10 +290,20 @@ __global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __r
     const int b = blockIdx.x, member = blockIdx.y;
     const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
     const int o = b * kInvNB, nb = min(kInvNB, p.q - o);
-    for (int idx = threadIdx.x; idx < kInvNB * kInvNB; idx += kInvNB) {
-        const int r = idx % kInvNB, c = idx / kInvNB;
-        L[r][c] = (r < nb && c < r) ? *a_ptr(A, p, o + r, o + c)
-                                   : ((r < nb && c == r && !p.unit) ? *a_ptr(A, p, o + r, o + c) : 0.0);
+    const int j = threadIdx.x;
+    double w[kInvNB];
+    {
+        // thread r loads row r of the block; the loop is unrolled so that
+        // all of the row's loads are in flight at once (threads r = 0..63 of
+        // one column c read consecutive addresses when A's rows are fast)
+        const int r = j;
+#pragma unroll
+        for (int c = 0; c < kInvNB; ++c) {
+            const bool in = r < nb && (c < r || (c == r && !p.unit));
+            w[c] = in ? __ldg(a_ptr(A, p, o + r, o + c)) : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < kInvNB; ++c) L[r][c] = w[c];
     }
     __syncthreads();
     // Thread j solves column j of the inverse, rows in order:
@@ -301,8 +311,6 @@ __global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __r
     // Both loops are unrolled, so the column stays in registers; every thread
     // runs the same sequence (no divergence) and L[r][s] is one broadcast
     // read. Four partial sums (s mod 4) keep the dependent chain short.
-    const int j = threadIdx.x;
-    double w[kInvNB];
 #pragma unroll
     for (int r = 0; r < kInvNB; ++r) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -350,16 +358,29 @@ __global__ void __launch_bounds__(kTbThreads, 2)
 
     // Y = alpha * B slice (rows reversed when rev), one rounding per element
     // as rblas's B := alpha*B (src/level3.rs:403-409)
+    // (eight loads in flight per thread before their stores)
     const bool rows_fast = p.ldb_rs == 1;
-    for (int idx = tid; idx < q * RB; idx += kTbThreads) {
-        const int i = rows_fast ? idx % q : idx / RB;
-        const int j = rows_fast ? idx / q : idx % RB;
-        double v = 0.0;
-        if (j < ncols) {
-            v = B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs];
-            if (alpha != 1.0) v = alpha * v;
+    constexpr int kYU = 8;
+    for (int base = tid; base < q * RB; base += kTbThreads * kYU) {
+        double v[kYU];
+#pragma unroll
+        for (int u = 0; u < kYU; ++u) {
+            const int idx = base + u * kTbThreads;
+            const int i = rows_fast ? idx % q : idx / RB;
+            const int j = rows_fast ? idx / q : idx % RB;
+            v[u] = (idx < q * RB && j < ncols)
+                       ? B[static_cast<size_t>(i) * p.ldb_rs + static_cast<size_t>(c0 + j) * p.ldb_cs]
+                       : 0.0;
         }
-        Y[(p.rev ? q - 1 - i : i) * YS + j] = v;
+#pragma unroll
+        for (int u = 0; u < kYU; ++u) {
+            const int idx = base + u * kTbThreads;
+            if (idx < q * RB) {
+                const int i = rows_fast ? idx % q : idx / RB;
+                const int j = rows_fast ? idx / q : idx % RB;
+                Y[(p.rev ? q - 1 - i : i) * YS + j] = (j < ncols && alpha != 1.0) ? alpha * v[u] : v[u];
+            }
+        }
     }
     __syncthreads();
 
