@@ -711,8 +711,9 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
             # single-problem plain kernel once per request, grouped mode one
             # grouped plain launch per set, grouped_forms runs the large
             # requests of each set in the precision forms (the f64 ones in one
-            # grouped Ozaki launch), per_request_forms the same arithmetic
-            # with one launch per request
+            # grouped Ozaki launch, the f32 ones in one grouped BF16X6
+            # launch), per_request_forms the same arithmetic with one launch
+            # per request
             with Server(budget_bytes=budget, max_batch=max_batch, grouped=grouped) as srv:
                 if forms:
                     srv.set_forms(**SERVE_FORMS)
@@ -739,8 +740,10 @@ def run_serving(torch, rates, n_req, budget, max_batch=256, seed=5, with_forms=T
                     else None})
     out["at_equal_p99"] = slo
     if with_forms:
-        out["forms"] = dict(SERVE_FORMS, note="grouped_forms: requests at or above the flop thresholds run alone "
-                                              "in BF16X6 (f32) / Ozaki (f64), the rest grouped plain")
+        out["forms"] = dict(SERVE_FORMS, note="grouped_forms: the requests of a set at or above the flop "
+                                              "thresholds run in one grouped BF16X6 launch (f32) and one grouped "
+                                              "Ozaki launch (f64), the rest in one grouped plain launch; "
+                                              "per_request_forms: the same forms, one launch per request")
     sat = max(out["rates"], key=lambda r: r["rate_req_s"])
     out["saturated"] = {"rate_req_s": sat["rate_req_s"], "grouped_tflops": sat["grouped"]["tflops"],
                         "per_request_tflops": sat["per_request"]["tflops"],

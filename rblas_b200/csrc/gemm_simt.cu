@@ -40,13 +40,13 @@ struct SimtParams {
     uint32_t* err;
 };
 
-template <typename T, bool A_K, bool B_K>
-__global__ void __launch_bounds__(kSimtThreads, 1)
+template <typename T, bool A_K, bool B_K, int V>
+__global__ void __launch_bounds__(kSimtThreads, V == 1 ? 2 : 1)
     simt_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const SimtParams<T> p) {
-    using Cfg = SimtCfg<T>;
+    using Cfg = SimtCfg<T, V>;
     constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, ST = Cfg::STAGES;
-    constexpr int STAGE_BYTES = simt_stage_bytes<T>();
+    constexpr int STAGE_BYTES = simt_stage_bytes<T, V>();
 
     extern __shared__ uint8_t smem_raw[];
     // Align by offsetting the __shared__ array itself (not through an integer
@@ -78,12 +78,13 @@ __global__ void __launch_bounds__(kSimtThreads, 1)
         if (lane == 0) {
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            simt_produce<T, A_K, B_K>(&tmA, &tmB, m0, n0, 0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err);
+            simt_produce<T, A_K, B_K, V>(&tmA, &tmB, m0, n0, 0, num_kt, smem, STAGE_BYTES, full, empty, it,
+                                         p.err);
         }
         return;
     }
     const SimtOut<T> o{p.c, p.ldc, p.cin, p.ldcin, p.m, p.n, p.alpha, p.beta, p.beta_mode, p.tri};
-    simt_consume<T, A_K, B_K>(o, m0, n0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err, warp, lane);
+    simt_consume<T, A_K, B_K, V>(o, m0, n0, num_kt, smem, STAGE_BYTES, full, empty, it, p.err, warp, lane);
 }
 
 template <typename T>
@@ -114,11 +115,11 @@ static CUtensorMapDataType tmap_dtype();
 template <> CUtensorMapDataType tmap_dtype<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
 template <> CUtensorMapDataType tmap_dtype<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
 
-template <typename T, bool A_K, bool B_K>
+template <typename T, bool A_K, bool B_K, int V>
 static cudaError_t launch_variant(const CUtensorMap& ta, const CUtensorMap& tb, const SimtParams<T>& p,
                                   cudaStream_t st) {
-    auto kern = simt_gemm_kernel<T, A_K, B_K>;
-    constexpr int smem = simt_smem_bytes<T>();
+    auto kern = simt_gemm_kernel<T, A_K, B_K, V>;
+    constexpr int smem = simt_smem_bytes<T, V>();
     static bool attr_set = false;  // per instantiation; benign race (idempotent)
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -134,12 +135,12 @@ static cudaError_t launch_variant(const CUtensorMap& ta, const CUtensorMap& tb, 
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
-                             const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
-                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri, const T* Cin,
-                             size_t ldcin) {
-    using Cfg = SimtCfg<T>;
+template <typename T, int V>
+static cudaError_t launch_simt_tiles(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
+                                     const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
+                                     size_t ldc, cudaStream_t st, CUresult* cu_err, int tri, const T* Cin,
+                                     size_t ldcin) {
+    using Cfg = SimtCfg<T, V>;
     CUtensorMap ta, tb;
     CUresult r;
     // op(A) is m x k: K-major when stored k x m (Trans), else stored m x k.
@@ -169,11 +170,40 @@ cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, 
     p.err = device_error_word();
     if (!p.err) return cudaErrorMemoryAllocation;
     if (a_kmajor) {
-        if (b_kmajor) return launch_variant<T, true, true>(ta, tb, p, st);
-        return launch_variant<T, true, false>(ta, tb, p, st);
+        if (b_kmajor) return launch_variant<T, true, true, V>(ta, tb, p, st);
+        return launch_variant<T, true, false, V>(ta, tb, p, st);
     }
-    if (b_kmajor) return launch_variant<T, false, true>(ta, tb, p, st);
-    return launch_variant<T, false, false>(ta, tb, p, st);
+    if (b_kmajor) return launch_variant<T, false, true, V>(ta, tb, p, st);
+    return launch_variant<T, false, false, V>(ta, tb, p, st);
+}
+
+bool simt_narrow_f32(size_t m, size_t n) {
+    static int sms = 0;  // benign race: every thread stores the same value
+    if (!sms) {
+        int dev = 0, v = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            sms = v;
+        else
+            return false;
+    }
+    const size_t tm = (m + 127) / 128;
+    const size_t wide = tm * ((n + 127) / 128), narrow = tm * ((n + 63) / 64);
+    return wide < static_cast<size_t>(sms) && 4 * narrow >= 3 * static_cast<size_t>(sms);
+}
+
+template <typename T>
+cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
+                             const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
+                             size_t ldc, cudaStream_t st, CUresult* cu_err, int tri, const T* Cin,
+                             size_t ldcin) {
+    if constexpr (sizeof(T) == 4) {
+        if (simt_narrow_f32(m, n))
+            return launch_simt_tiles<T, 1>(a_kmajor, b_kmajor, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st,
+                                           cu_err, tri, Cin, ldcin);
+    }
+    return launch_simt_tiles<T, 0>(a_kmajor, b_kmajor, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, cu_err,
+                                   tri, Cin, ldcin);
 }
 
 template cudaError_t launch_simt_gemm<float>(bool, bool, int, int, int, float, const float*, size_t,

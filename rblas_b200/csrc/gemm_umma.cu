@@ -385,10 +385,13 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // 8 d1) and accumulates into C in FP64; units run from the smallest weight
 // up, the first one adding beta*C0.
 // Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..17 epilogue (four
-// warps per TMEM lane quarter, 64 columns each). The epilogue runs while the
-// tensor cores wait for the accumulators, so it is written for latency: 16
-// warps, a per-warp table of the tile's column scales in shared memory, and
-// the first chunk's C values requested before the accumulator wait.
+// warps per TMEM lane quarter, UN/4 columns each). With the 128 x 256 tile a
+// unit's two accumulators fill TMEM, so the tensor cores wait while the
+// epilogue drains them; the epilogue is written for that latency: 16 warps,
+// a per-warp table of the tile's column scales in shared memory, and the
+// first chunk's C values requested before the accumulator wait. The
+// 128 x 128 tile keeps two sets of accumulators and alternates them, so its
+// drain overlaps the next unit's MMAs.
 // ------------------------------------------------------------------------------
 
 constexpr int kOzEpiWarps = 16;
@@ -406,6 +409,9 @@ struct OzCfg {
     static constexpr int STAGE = kATile + BTILE;  // 48 KiB / 32 KiB
     static constexpr int CW = UN / 4;             // four epilogue warps per TMEM lane quarter
     static constexpr int SMEM = ST * STAGE + 256 + kOzEpiWarps * kOzColTab + 1024;
+    // accumulator sets of 2 x UN columns in TMEM's 512: the 128-wide tile
+    // keeps two, so the MMAs of the next unit run while this one drains
+    static constexpr int NBUF = 512 / (2 * UN);
 };
 // Tile rows per rasterisation group. A wave of 148 tiles walks R row panels
 // of A and C column panels of B, each once per diagonal-pair unit; B panels
@@ -569,13 +575,15 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
             mbar_init(&bar->full[s], 1);
             mbar_init(&bar->empty[s], 1);
         }
-        mbar_init(&bar->acc_full[0], 1);
-        mbar_init(&bar->acc_empty[0], kOzEpiWarps);
+        for (int b = 0; b < Cfg::NBUF; ++b) {
+            mbar_init(&bar->acc_full[b], 1);
+            mbar_init(&bar->acc_empty[b], kOzEpiWarps);
+        }
         mbar_init(&bar->drain, 1);
         fence_barrier_init();
     }
     if (warp == 1) {
-        tmem_alloc(&bar->tmem_base, 2 * UN);
+        tmem_alloc(&bar->tmem_base, 512);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -639,16 +647,19 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                 int d0, d1;
                 oz_unit(p.slices, u % upc, d0, d1);
                 const int kt0 = (u / upc) * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
-                if (uc >= 1 && !mbar_wait(&bar->acc_empty[0], (uc - 1) & 1, err, 0x302)) {
+                const int bsel = static_cast<int>(uc % Cfg::NBUF);
+                if (uc >= static_cast<uint32_t>(Cfg::NBUF) &&
+                    !mbar_wait(&bar->acc_empty[bsel], ((uc / Cfg::NBUF) - 1) & 1, err, 0x302)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                // S_top (d1, or d0 alone) at tmem_base + UN for a pair, tmem_base
-                // otherwise; S_d0 of a pair at tmem_base (the epilogue's layout)
+                // S_top (d1, or d0 alone) at acc + UN for a pair, acc otherwise;
+                // S_d0 of a pair at acc (the epilogue's layout)
+                const uint32_t acc = tmem_base + bsel * (2 * UN);
                 const bool pair = d1 >= 0;
                 const int top = pair ? d1 : d0;
-                const uint32_t acc_top = pair ? tmem_base + UN : tmem_base;
+                const uint32_t acc_top = pair ? acc + UN : acc;
                 constexpr uint32_t idesc = umma_idesc(2, 1, kUM, UN);  // s32 <- s8 x s8
                 uint32_t f_top = 0, f_low = 0;
                 for (int kt = kt0; ok && kt < kt1; ++kt) {
@@ -670,7 +681,7 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                             umma_i8(acc_top, ad, sw128_kmajor_desc(sb) + 2 * kk, idesc, f_top);
                             f_top = 1;
                             if (low) {
-                                umma_i8(tmem_base, ad, sw128_kmajor_desc(pb) + 2 * kk, idesc, f_low);
+                                umma_i8(acc, ad, sw128_kmajor_desc(pb) + 2 * kk, idesc, f_low);
                                 f_low = 1;
                             }
                         }
@@ -685,7 +696,7 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                     }
                     if (pair && prev_s >= 0) tc_commit(&bar->empty[prev_s]);
                 }
-                if (ok) tc_commit(&bar->acc_full[0]);
+                if (ok) tc_commit(&bar->acc_full[bsel]);
             }
         }
         tc_commit(&bar->drain);
@@ -771,8 +782,10 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                     cv[jj] = (live && read_c && cbase + jj < p.n)
                                  ? ld_l2hint(srow + static_cast<size_t>(cbase + jj) * ldc, pol_ld) : 0.0;
                 }
+                const int bsel = static_cast<int>(uc % Cfg::NBUF);
+                const uint32_t accbase = lanebase + bsel * (2 * UN);
                 {
-                    const bool got = mbar_wait(&bar->acc_full[0], uc & 1, err, 0x304);
+                    const bool got = mbar_wait(&bar->acc_full[bsel], (uc / Cfg::NBUF) & 1, err, 0x304);
                     if (!__all_sync(0xffffffffu, got)) {  // the whole warp goes on, or the whole warp stops
                         ok = false;
                         break;
@@ -793,8 +806,8 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                         cn[jj] = (live && read_c && ch < NCH - 1 && cbase + 8 + jj < p.n)
                                      ? ld_l2hint(sp + static_cast<size_t>(8 + jj) * ldc, pol_ld) : 0.0;
                     uint32_t v0[8], v1[8];
-                    tmem_ld8(lanebase + col0, v0);
-                    if (d1 >= 0) tmem_ld8(lanebase + UN + col0, v1);
+                    tmem_ld8(accbase + col0, v0);
+                    if (d1 >= 0) tmem_ld8(accbase + UN + col0, v1);
                     tmem_ld_wait();
                     if (live) {
                         if (warp_fast && ((colmask >> j0) & 0xffu) == 0xffu) {
@@ -846,7 +859,7 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
                 if (!ok) break;
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&bar->acc_empty[0]);
+                if (lane == 0) mbar_arrive(&bar->acc_empty[bsel]);
             }
         }
     }
@@ -855,7 +868,7 @@ __device__ __forceinline__ void ozaki_body(const Src& src) {
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, 2 * UN);
+        tmem_dealloc(tmem_base, 512);
     }
 }
 
@@ -1935,15 +1948,27 @@ int ozaki_grouped_dev(const rb_gemm_problem* probs, size_t count, const void* co
         const OzGroupEntry* dtab = reinterpret_cast<const OzGroupEntry*>(mem);
         const int* dstarts = reinterpret_cast<const int*>(mem + ent_bytes);
         const int tiles_narrow = tiles - tiles_wide;
+        // with both widths, the narrow launch goes on a forked stream: its
+        // CTAs take the SMs that the wide launch's CTAs leave as they finish
+        // (each persistent CTA holds a whole SM), instead of waiting for the
+        // wide launch's last tile
+        ForkedStream fk;
+        const bool fork = n_wide > 0 && np > n_wide && fork_stream(st, &fk) == cudaSuccess;
         if (n_wide > 0)
             ozaki_grouped_kernel<256><<<std::min(tiles_wide, sms), kOzThreads, OzCfg<256>::SMEM, st>>>(
                 dtab, dstarts, n_wide, err_word);
         if (np > n_wide)
-            ozaki_grouped_kernel<128><<<std::min(tiles_narrow, sms), kOzThreads, OzCfg<128>::SMEM, st>>>(
-                dtab + n_wide, dstarts + n_wide + 1, np - n_wide, err_word);
+            ozaki_grouped_kernel<128><<<std::min(tiles_narrow, sms), kOzThreads, OzCfg<128>::SMEM,
+                                        fork ? fk.s : st>>>(dtab + n_wide, dstarts + n_wide + 1, np - n_wide,
+                                                            err_word);
+        e = cudaGetLastError();
+        if (fork) {
+            const cudaError_t je = join_stream(st, &fk);
+            if (e == cudaSuccess) e = je;
+        }
         kernel_timing_end(&tmr, st);
         count_launch(3 + (n_wide > 0) + (np > n_wide));
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
     cudaFreeAsync(mem, st);
     if (e != cudaSuccess) {

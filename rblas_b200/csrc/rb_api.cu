@@ -298,6 +298,8 @@ bool plain_split(const ColProblem<T>& p, rb_gemm_problem* q) {
     q->a = p.a; q->lda = p.lda;
     q->b = p.b; q->ldb = p.ldb;
     q->c = p.c; q->ldc = p.ldc;
+    // an f32 problem the narrow tile fills the GPU with runs unsplit
+    if (sizeof(T) == 4 && simt_narrow_f32(p.m, p.n)) return false;
     return !p.tri && grouped_splits(*q) > 1;
 }
 
@@ -502,10 +504,12 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
     const size_t total_bytes = (need_ab ? (a_rows * a_cols + b_rows * b_cols) * el : 0) +
                                p.m * p.n * el * (read_c ? 2 : 1);
     // a plain call whose whole shape takes split-K runs whole (a panel's
-    // split could differ, and with it the summation order)
+    // split could differ, and with it the summation order), and so does one
+    // whose C the narrow f32 tile spreads over the SMs (its panels would not)
     rb_gemm_problem whole;
-    const bool whole_split = prec == RB_PREC_PLAIN && plain_split(p, &whole);
-    if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256 && !whole_split) {
+    const bool whole_call = prec == RB_PREC_PLAIN &&
+                            (plain_split(p, &whole) || (sizeof(T) == 4 && simt_narrow_f32(p.m, p.n)));
+    if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256 && !whole_call) {
         const size_t width = std::max<size_t>(256, (p.n + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
         if (need_ab) {
             e = cudaMemcpy2DAsync(dA, lda_d * el, p.a, p.lda * el, a_rows * el, a_cols, cudaMemcpyHostToDevice, st);
@@ -690,6 +694,52 @@ uint32_t* device_error_word() {
     cudaError_t e;
     DeviceCtx* c = ctx_for_current(&e);
     return c ? c->err_word : nullptr;
+}
+
+namespace {
+constexpr int kAuxStreams = 4;
+struct AuxSlot {
+    std::mutex mu;
+    bool init = false;
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+AuxSlot g_aux[kMaxDevices][kAuxStreams];
+}  // namespace
+
+cudaError_t fork_stream(cudaStream_t st, ForkedStream* f) {
+    const int d = current_device();
+    if (d < 0 || d >= kMaxDevices) return cudaErrorInvalidDevice;
+    const int slot = static_cast<int>((reinterpret_cast<uintptr_t>(st) >> 4) % kAuxStreams);
+    AuxSlot& a = g_aux[d][slot];
+    a.mu.lock();
+    cudaError_t e = cudaSuccess;
+    if (!a.init) {
+        e = cudaStreamCreateWithFlags(&a.s, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming);
+        a.init = e == cudaSuccess;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(a.fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(a.s, a.fork, 0);
+    if (e != cudaSuccess) {
+        a.mu.unlock();
+        return e;
+    }
+    f->s = a.s;
+    f->slot = d * kAuxStreams + slot;
+    return cudaSuccess;
+}
+
+cudaError_t join_stream(cudaStream_t st, ForkedStream* f) {
+    if (f->slot < 0) return cudaSuccess;
+    AuxSlot& a = g_aux[f->slot / kAuxStreams][f->slot % kAuxStreams];
+    cudaError_t e = cudaEventRecord(a.join, a.s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, a.join, 0);
+    f->slot = -1;
+    f->s = nullptr;
+    a.mu.unlock();
+    return e;
 }
 
 namespace {

@@ -70,6 +70,19 @@ void set_scratch_cache_bytes(size_t bytes);
 // Per-device error word (device memory, zero when healthy).
 uint32_t* device_error_word();
 
+// A second stream for work that may overlap the caller's stream st: after
+// fork_stream, f->s starts behind everything queued on st so far; after
+// join_stream, st waits for everything queued on f->s. The pair holds one
+// of a few per-device auxiliary streams (picked by st) locked in between,
+// so concurrent callers never interleave their fork and join records.
+// Both also work while st is being captured into a CUDA graph.
+struct ForkedStream {
+    cudaStream_t s = nullptr;
+    int slot = -1;
+};
+cudaError_t fork_stream(cudaStream_t st, ForkedStream* f);
+cudaError_t join_stream(cudaStream_t st, ForkedStream* f);
+
 // ---- device allocations ---------------------------------------------------------
 // Every device allocation the library makes outside the pool (staging
 // buffers, plan tables, serving pools) goes through dev_alloc; it and
@@ -94,11 +107,14 @@ bool current_context_id(unsigned long long* id);
 // Requirements: A/B 16-byte aligned with lda/ldb*sizeof(T) % 16 == 0.
 // tri: 0 whole C; 1 only the upper triangle (row <= col); 2 only the lower.
 // Cin (optional): a separate C0 read for beta != 0, the result going to C.
+// f32 problems whose 128 x 128 tiles leave SMs idle while 128 x 64 tiles
+// fill at least three quarters of them run the narrow tile.
 template <typename T>
 cudaError_t launch_simt_gemm(bool a_kmajor, bool b_kmajor, int m, int n, int k, T alpha,
                              const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
                              size_t ldc, cudaStream_t st, CUresult* cu_err, int tri = 0,
                              const T* Cin = nullptr, size_t ldcin = 0);
+bool simt_narrow_f32(size_t m, size_t n);
 
 // C := beta*C over an m x n column-major block (beta == 0 writes zeros
 // without reading; beta == 1 is a no-op and launches nothing); tri as above.

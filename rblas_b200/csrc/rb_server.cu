@@ -129,15 +129,16 @@ public:
     int max_batch;
     int grouped;
     // arithmetic forms for large requests (rb_server_set_forms): requests of
-    // at least min_flop[dtype] flop run alone in form[dtype]; the rest take
+    // at least min_flop[dtype] flop run in form[dtype] (a batch's requests of
+    // one form in one grouped launch when there are several); the rest take
     // the plain path (grouped or single)
     int form[2] = {RB_PREC_PLAIN, RB_PREC_PLAIN};
     double min_flop[2] = {0.0, 0.0};
     int device = 0;
     Pool pool;
     cudaStream_t streams[2] = {nullptr, nullptr};
-    // requests that run alone in a precision form go round-robin over these,
-    // so medium-sized ones share the GPU instead of running one after another
+    // the precision-form launches go round-robin over these, so they share
+    // the GPU with the batch's plain launch instead of running after it
     static constexpr int kFormStreams = 4;
     cudaStream_t form_streams[kFormStreams] = {};
     cudaEvent_t form_events[kFormStreams] = {};  // re-recorded per use; a wait takes the latest record
@@ -310,7 +311,7 @@ public:
             probs.push_back(q);
         }
         int rc = RB_OK;
-        // large requests in a precision form run on their own; the rest stay plain
+        // large requests take a precision form; the rest stay plain
         std::vector<size_t> alone;
         std::vector<rb_gemm_problem> plain;
         std::vector<const void*> plain_cin;

@@ -22,11 +22,15 @@
 
 namespace rb {
 
-template <typename T> struct SimtCfg;
+// Tile shape per element type; V = 1 is the narrow f32 tile.
+template <typename T, int V = 0> struct SimtCfg;
 // f32: 128x128 C tile, 8x8 per thread, BK = 32 (one 128-byte swizzle row).
-template <> struct SimtCfg<float> { static constexpr int BM = 128, BN = 128, BK = 32, TN = 8, STAGES = 4; };
+template <> struct SimtCfg<float, 0> { static constexpr int BM = 128, BN = 128, BK = 32, TN = 8, STAGES = 4; };
+// f32 narrow: 128x64 C tile, 8x4 per thread, for problems whose 128 x 128
+// tiles leave SMs idle (twice the tiles; 96 KiB of stages, two CTAs per SM).
+template <> struct SimtCfg<float, 1> { static constexpr int BM = 128, BN = 64, BK = 32, TN = 4, STAGES = 4; };
 // f64: 128x64 C tile, 8x4 per thread, BK = 16 (one 128-byte swizzle row).
-template <> struct SimtCfg<double> { static constexpr int BM = 128, BN = 64, BK = 16, TN = 4, STAGES = 4; };
+template <> struct SimtCfg<double, 0> { static constexpr int BM = 128, BN = 64, BK = 16, TN = 4, STAGES = 4; };
 
 constexpr int kSimtComputeWarps = 8;
 constexpr int kSimtThreads = (kSimtComputeWarps + 1) * 32;
@@ -45,9 +49,9 @@ __device__ __forceinline__ void lds16(const uint8_t* p, T (&v)[Vec16<T>::N]) {
     }
 }
 
-template <typename T>
+template <typename T, int V = 0>
 constexpr int simt_smem_bytes() {
-    using Cfg = SimtCfg<T>;
+    using Cfg = SimtCfg<T, V>;
     return Cfg::STAGES * (Cfg::BM + Cfg::BN) * Cfg::BK * (int)sizeof(T) + 2 * Cfg::STAGES * 8 + 1024;
 }
 
@@ -59,24 +63,24 @@ __host__ __device__ constexpr uint32_t simt_mn_a_box(size_t elem) { return elem 
 __host__ __device__ constexpr bool simt_mn_a_swizzled(size_t elem) { return elem == 8; }
 
 // Byte offsets of the A and B tiles inside a stage.
-template <typename T>
-__host__ __device__ constexpr int simt_a_bytes() { return SimtCfg<T>::BM * SimtCfg<T>::BK * (int)sizeof(T); }
-template <typename T>
+template <typename T, int V = 0>
+__host__ __device__ constexpr int simt_a_bytes() { return SimtCfg<T, V>::BM * SimtCfg<T, V>::BK * (int)sizeof(T); }
+template <typename T, int V = 0>
 __host__ __device__ constexpr int simt_stage_bytes() {
-    return (SimtCfg<T>::BM + SimtCfg<T>::BN) * SimtCfg<T>::BK * (int)sizeof(T);
+    return (SimtCfg<T, V>::BM + SimtCfg<T, V>::BN) * SimtCfg<T, V>::BK * (int)sizeof(T);
 }
 
 // Producer lane: issue the num_kt K-tile loads (starting at K-tile kt0) of
 // the tile at (m0, n0) on ring iterations it, it+1, ... Returns false (after
 // letting its own copies land) if a wait gave up.
-template <typename T, bool A_K, bool B_K>
+template <typename T, bool A_K, bool B_K, int V = 0>
 __device__ __forceinline__ bool simt_produce(const CUtensorMap* tmA, const CUtensorMap* tmB, int m0, int n0,
                                              int kt0, int num_kt, uint8_t* smem, int stage_stride, uint64_t* full,
                                              uint64_t* empty, uint32_t& it, uint32_t* err) {
-    using Cfg = SimtCfg<T>;
+    using Cfg = SimtCfg<T, V>;
     constexpr int ST = Cfg::STAGES, BK = Cfg::BK;
-    constexpr int A_BYTES = simt_a_bytes<T>();
-    constexpr uint32_t TX = simt_stage_bytes<T>();
+    constexpr int A_BYTES = simt_a_bytes<T, V>();
+    constexpr uint32_t TX = simt_stage_bytes<T, V>();
     for (int kt = 0; kt < num_kt; ++kt, ++it) {
         const int s = it % ST;
         if (it >= ST && !mbar_wait(&empty[s], ((it / ST) - 1) & 1, err, 0x101)) {
@@ -230,17 +234,17 @@ __device__ __forceinline__ bool dmma_mainloop(double (&acc)[8][4], int num_kt, c
 
 // Compute warps: consume num_kt stages from ring iteration it into the
 // thread's 8 x TN accumulator. Returns false if a wait gave up.
-template <typename T, bool A_K, bool B_K>
-__device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T>::TN], int num_kt, const uint8_t* smem,
+template <typename T, bool A_K, bool B_K, int V = 0>
+__device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T, V>::TN], int num_kt, const uint8_t* smem,
                                               int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
                                               uint32_t* err, int warp, int lane) {
     if constexpr (sizeof(T) == 8) {
         return dmma_mainloop<A_K, B_K>(acc, num_kt, smem, stage_stride, full, empty, it, err, warp, lane);
     }
-    using Cfg = SimtCfg<T>;
+    using Cfg = SimtCfg<T, V>;
     constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, TN = Cfg::TN, ST = Cfg::STAGES;
     constexpr int VEC = Vec16<T>::N;  // elements per 16-byte load
-    constexpr int A_BYTES = simt_a_bytes<T>();
+    constexpr int A_BYTES = simt_a_bytes<T, V>();
     static_assert(BK * sizeof(T) == 128, "a K-major tile row must be one 128-byte swizzle row");
     static_assert(A_BYTES % 1024 == 0, "swizzled tiles need 1 KiB alignment");
     const int wm = warp & 1, wn = warp >> 1;          // 2 x 4 warps
@@ -327,10 +331,10 @@ __device__ __forceinline__ bool simt_mainloop(T (&acc)[8][SimtCfg<T>::TN], int n
 }
 
 // Compute warps: C = alpha*acc + beta*Cin for the tile at (m0, n0).
-template <typename T, bool A_K, bool B_K>
-__device__ __forceinline__ void simt_epilogue(const SimtOut<T>& o, const T (&acc)[8][SimtCfg<T>::TN], int m0,
+template <typename T, bool A_K, bool B_K, int V = 0>
+__device__ __forceinline__ void simt_epilogue(const SimtOut<T>& o, const T (&acc)[8][SimtCfg<T, V>::TN], int m0,
                                               int n0, int warp, int lane) {
-    constexpr int TN = SimtCfg<T>::TN;
+    constexpr int TN = SimtCfg<T, V>::TN;
     constexpr int VEC = Vec16<T>::N;
     const int wm = warp & 1, wn = warp >> 1;
     if constexpr (sizeof(T) == 8) {
@@ -380,13 +384,14 @@ __device__ __forceinline__ void simt_epilogue(const SimtOut<T>& o, const T (&acc
 }
 
 // Mainloop then epilogue: one whole tile.
-template <typename T, bool A_K, bool B_K>
+template <typename T, bool A_K, bool B_K, int V = 0>
 __device__ __forceinline__ bool simt_consume(const SimtOut<T>& o, int m0, int n0, int num_kt, uint8_t* smem,
                                              int stage_stride, uint64_t* full, uint64_t* empty, uint32_t& it,
                                              uint32_t* err, int warp, int lane) {
-    T acc[8][SimtCfg<T>::TN];
-    if (!simt_mainloop<T, A_K, B_K>(acc, num_kt, smem, stage_stride, full, empty, it, err, warp, lane)) return false;
-    simt_epilogue<T, A_K, B_K>(o, acc, m0, n0, warp, lane);
+    T acc[8][SimtCfg<T, V>::TN];
+    if (!simt_mainloop<T, A_K, B_K, V>(acc, num_kt, smem, stage_stride, full, empty, it, err, warp, lane))
+        return false;
+    simt_epilogue<T, A_K, B_K, V>(o, acc, m0, n0, warp, lane);
     return true;
 }
 

@@ -92,6 +92,22 @@ def test_alpha_zero_and_k_zero_scale_c_only(dtype):
     assert np.array_equal(p.result(c), p.result(p.reference_restatement()))
 
 
+@pytest.mark.parametrize("layout", [Layout.ColMajor, Layout.RowMajor])
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("tb", [0, 1])
+def test_narrow_f32_tile_parity(layout, ta, tb):
+    """f32 shapes whose 128 x 128 tiles leave SMs idle while 128 x 64 tiles
+    fill them (the narrow tile, no split-K), ragged edges included."""
+    for i, (m, n, k) in enumerate([(1000, 1000, 777), (900, 1100, 300), (1024, 960, 64)]):
+        p = Problem(layout, ta, tb, m, n, k, np.float32, alpha=1.5, beta=-0.5, seed=300 + i)
+        c = _gpu_gemm(p)
+        ref = p.reference_restatement()
+        err = p.normwise(c, ref)
+        assert err <= p.tol(), f"{(m, n, k)} normwise vs restatement {err:.3e} > {p.tol():.3e}"
+        rows = np.sort(np.random.default_rng(7 + i).choice(p.m, 32, replace=False))
+        assert p.normwise_vs_dd(c, rows=rows) <= p.tol()
+
+
 def test_sgemm_1024_colmajor_nn_matches_rblas():
     """Plain SGEMM, f32, col-major NN, 1024^3, alpha=1, beta=0, A/B from the
     reference tests' LCG (seed 0x12345678): within 4*k*u_f32 normwise of the

@@ -11,7 +11,8 @@ substitution, which the f64 path's inverted diagonal blocks must also meet.
 Covers every side/uplo/trans/diag, ragged sizes,
 several right-hand-side slices per problem, the 16- and 8-wide slices of
 large orders, padded leading dimensions and gaps between members (which must
-stay untouched), and the leading-dimension errors.
+stay untouched), unpadded even leading dimensions (the 16-byte operand
+loads), and the leading-dimension errors.
 """
 from __future__ import annotations
 
@@ -39,10 +40,10 @@ def _u(dtype):
     return 2.0 ** -24 if np.dtype(dtype) == np.float32 else 2.0 ** -53
 
 
-def run_batch(rng, dtype, side, uplo, trans, diag, m, n, batch, alpha, pad=3):
+def run_batch(rng, dtype, side, uplo, trans, diag, m, n, batch, alpha, pad=3, gap=(5, 7)):
     q = m if side == 0 else n
     lda, ldb = q + pad, m + pad
-    sa, sb = lda * q + 5, ldb * n + 7
+    sa, sb = lda * q + gap[0], ldb * n + gap[1]
     a_host = np.zeros(sa * batch, dtype=dtype)
     b_host = rng.uniform(-1, 1, sb * batch).astype(dtype)
     for i in range(batch):
@@ -114,6 +115,24 @@ def test_batched_trsm_wide_orders_use_narrow_slices():
     for q, n in ((700, 20), (1400, 9)):
         rel = run_batch(rng, np.float64, 0, 0, 1, 0, q, n, 2, -1.5)
         assert rel <= 1e3 * _u(np.float64), (q, rel)
+
+
+@pytest.mark.parametrize("side,q,nrhs,uplo,trans,diag,alpha", [
+    (0, 512, 64, 1, 0, 0, 1.0),     # the config shape, Left Lower NoTrans: paired 16-byte A loads
+    (0, 200, 40, 1, 0, 1, -0.75),   # ragged last diagonal block, Unit, three 16-wide slices
+    (1, 256, 48, 1, 1, 0, 1.5),     # Right Lower Trans: the same loads, B read along its rows
+    (0, 96, 17, 0, 1, 0, 2.0),      # Left Upper Trans: op(A)'s rows strided (element loads)
+    (0, 700, 33, 1, 0, 0, 0.5),     # a large order: 16-wide slices, paired loads
+])
+def test_batched_trsm_aligned_operands_f64(side, q, nrhs, uplo, trans, diag, alpha):
+    """Even leading dimensions and member strides on 16-byte-aligned
+    operands: where op(A)'s rows are unit stride, adjacent A rows of a DMMA
+    fragment load as one 16-byte pair. Gaps of 2 and 4 elements keep the
+    strides even."""
+    rng = np.random.default_rng(95 + q)
+    m, n = (q, nrhs) if side == 0 else (nrhs, q)
+    rel = run_batch(rng, np.float64, side, uplo, trans, diag, m, n, 3, alpha, pad=0, gap=(2, 4))
+    assert rel <= 1e3 * _u(np.float64), (q, rel)
 
 
 def test_batched_trsm_rejects_bad_leading_dims():
