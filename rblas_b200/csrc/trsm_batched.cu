@@ -384,35 +384,110 @@ __global__ void __launch_bounds__(kTbThreads, 2)
     }
     __syncthreads();
 
+    // Each warp walks a fixed sequence of 16 x 64 fragment tiles -- for every
+    // block b, W_b's rows 16 xm.. (the X step, warps with an (xm, xn) pair)
+    // and then A's rows r0 = o + nb + 16 warp, +128, ... of block b's
+    // columns (the trailing update) -- in halves of four k-steps. A half's
+    // loads are issued while the DMMAs of the half before it run, across the
+    // block's barriers too: A and W do not depend on Y.
+    const bool xw = warp < 4 * NBLK;
+    const int xm = warp % 4, xn = warp / 4;
+    // DMMA fragment rows g and g+8 take the adjacent rows 2g and 2g+1 of
+    // the 16-row block (the output rows follow), so each pair is one
+    // 16-byte load; the fragment layout is in simt_tile.cuh (dmma_16x8x8)
+    auto first_trail = [&](int b) { return b * kInvNB + min(kInvNB, q - b * kInvNB) + 16 * warp; };
+    // the tile after (kind, b, r0): kind 0 W_b, 1 A rows r0 of block b, 2 none
+    auto next_tile = [&](int& kind, int& b, int& r0) {
+        const int r = kind == 0 ? first_trail(b) : r0 + 16 * 8;
+        if (r < q) {
+            kind = 1;
+            r0 = r;
+            return;
+        }
+        for (int bb = b + 1; bb < nblocks; ++bb) {
+            if (xw) {
+                kind = 0;
+                b = bb;
+                return;
+            }
+            if (first_trail(bb) < q) {
+                kind = 1;
+                b = bb;
+                r0 = first_trail(bb);
+                return;
+            }
+        }
+        kind = 2;
+    };
+    // k-steps 4h .. 4h+3 of a tile into f (W is column-major 64 x 64, zero
+    // outside the block; A rows past q read as zero)
+    auto load_half = [&](int kind, int b, int r0, int h, double (&f)[4][4]) {
+        if (kind == 0) {
+            const double* Wb = Wm + static_cast<size_t>(b) * (kInvNB * kInvNB) + 16 * xm + 2 * g;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = 8 * (4 * h + kk) + t;
+                const double2 lo = __ldg(reinterpret_cast<const double2*>(Wb + 64 * k));
+                const double2 hi = __ldg(reinterpret_cast<const double2*>(Wb + 64 * (k + 4)));
+                f[kk][0] = lo.x;
+                f[kk][1] = lo.y;
+                f[kk][2] = hi.x;
+                f[kk][3] = hi.y;
+            }
+        } else if (kind == 1) {
+            const int o = b * kInvNB, ra = r0 + 2 * g, rb = ra + 1;
+            if (p.vec_a && r0 + 16 <= q) {
+                // r0 is even (o + 64 + 16 i), so every pair starts on 16 bytes
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = o + 8 * (4 * h + kk) + t;
+                    const double2 lo = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k)));
+                    const double2 hi = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k + 4)));
+                    f[kk][0] = lo.x;
+                    f[kk][1] = lo.y;
+                    f[kk][2] = hi.x;
+                    f[kk][3] = hi.y;
+                }
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = o + 8 * (4 * h + kk) + t;
+                    f[kk][0] = (ra < q) ? __ldg(a_ptr(A, p, ra, k)) : 0.0;
+                    f[kk][1] = (rb < q) ? __ldg(a_ptr(A, p, rb, k)) : 0.0;
+                    f[kk][2] = (ra < q) ? __ldg(a_ptr(A, p, ra, k + 4)) : 0.0;
+                    f[kk][3] = (rb < q) ? __ldg(a_ptr(A, p, rb, k + 4)) : 0.0;
+                }
+            }
+        }
+    };
+    int kind = 0, tb = 0, tr0 = 0;      // W_0, or for a warp without X work
+    if (!xw) next_tile(kind, tb, tr0);  // its first trailing tile
+    double fa[4][4], fb[4][4];  // the current tile's halves
+    load_half(kind, tb, tr0, 0, fa);
+
     for (int b = 0; b < nblocks; ++b) {
         const int o = b * kInvNB, nb = min(kInvNB, q - o);
         // ---- X_b = W_b * Y_b: 4 m-blocks x NBLK n-blocks, one (m, n) pair per warp
-        const double* Wb = Wm + static_cast<size_t>(b) * (kInvNB * kInvNB);
         double xacc[4] = {0.0, 0.0, 0.0, 0.0};
-        const bool xw = warp < 4 * NBLK;
-        const int xm = warp % 4, xn = warp / 4;
-        // DMMA fragment rows g and g+8 take the adjacent rows 2g and 2g+1 of
-        // the 16-row block (the output rows follow), so each pair is one
-        // 16-byte load; the fragment layout is in simt_tile.cuh (dmma_16x8x8)
-        if (xw) {
-            double a[8][4];
+        if (xw) {  // the current tile is W_b
+            load_half(kind, tb, tr0, 1, fb);
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {  // W is column-major 64 x 64, zero outside the block
-                const int r = 16 * xm + 2 * g, k = 8 * kk + t;
-                const double2 lo = __ldg(reinterpret_cast<const double2*>(Wb + r + 64 * k));
-                const double2 hi = __ldg(reinterpret_cast<const double2*>(Wb + r + 64 * (k + 4)));
-                a[kk][0] = lo.x;
-                a[kk][1] = lo.y;
-                a[kk][2] = hi.x;
-                a[kk][3] = hi.y;
-            }
-#pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
+            for (int kk = 0; kk < 4; ++kk) {
                 const int k = 8 * kk + t;
                 double bf[2];
                 bf[0] = (k < nb) ? Y[(o + k) * YS + 8 * xn + g] : 0.0;
                 bf[1] = (k + 4 < nb) ? Y[(o + k + 4) * YS + 8 * xn + g] : 0.0;
-                dmma_16x8x8(xacc, a[kk], bf);
+                dmma_16x8x8(xacc, fa[kk], bf);
+            }
+            next_tile(kind, tb, tr0);
+            load_half(kind, tb, tr0, 0, fa);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = 8 * (4 + kk) + t;
+                double bf[2];
+                bf[0] = (k < nb) ? Y[(o + k) * YS + 8 * xn + g] : 0.0;
+                bf[1] = (k + 4 < nb) ? Y[(o + k + 4) * YS + 8 * xn + g] : 0.0;
+                dmma_16x8x8(xacc, fb[kk], bf);
             }
         }
         __syncthreads();  // every read of Y_b is done
@@ -429,42 +504,30 @@ __global__ void __launch_bounds__(kTbThreads, 2)
         }
         __syncthreads();
         // ---- trailing rows -= L[trailing, block] * X_b, 16-row m-blocks dealt to the warps
-        const int r_first = o + nb;
-        for (int r0 = r_first + 16 * warp; r0 < q; r0 += 16 * 8) {
-            double a[8][4];
-            const int ra = r0 + 2 * g, rb = ra + 1;  // fragment rows g and g+8 (see the X step)
-            if (p.vec_a && r0 + 16 <= q) {
-                // r0 is even (o + 64 + 16 * i), so every pair starts on 16 bytes
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {  // nb == 64 here: only the last block has no trailing rows
-                    const int k = o + 8 * kk + t;
-                    const double2 lo = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k)));
-                    const double2 hi = __ldg(reinterpret_cast<const double2*>(a_ptr(A, p, ra, k + 4)));
-                    a[kk][0] = lo.x;
-                    a[kk][1] = lo.y;
-                    a[kk][2] = hi.x;
-                    a[kk][3] = hi.y;
-                }
-            } else {
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {
-                    const int k = o + 8 * kk + t;
-                    a[kk][0] = (ra < q) ? __ldg(a_ptr(A, p, ra, k)) : 0.0;
-                    a[kk][1] = (rb < q) ? __ldg(a_ptr(A, p, rb, k)) : 0.0;
-                    a[kk][2] = (ra < q) ? __ldg(a_ptr(A, p, ra, k + 4)) : 0.0;
-                    a[kk][3] = (rb < q) ? __ldg(a_ptr(A, p, rb, k + 4)) : 0.0;
-                }
-            }
+        for (int r0 = first_trail(b); r0 < q; r0 += 16 * 8) {  // the current tile is A rows r0
+            const int ra = r0 + 2 * g, rb = ra + 1;
+            load_half(kind, tb, tr0, 1, fb);
             double acc[NBLK][4];
 #pragma unroll
             for (int n = 0; n < NBLK; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
+            for (int kk = 0; kk < 4; ++kk) {
                 const int k = o + 8 * kk + t;
 #pragma unroll
                 for (int n = 0; n < NBLK; ++n) {
                     double bf[2] = {Y[k * YS + 8 * n + g], Y[(k + 4) * YS + 8 * n + g]};
-                    dmma_16x8x8(acc[n], a[kk], bf);
+                    dmma_16x8x8(acc[n], fa[kk], bf);
+                }
+            }
+            next_tile(kind, tb, tr0);
+            load_half(kind, tb, tr0, 0, fa);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = o + 8 * (4 + kk) + t;
+#pragma unroll
+                for (int n = 0; n < NBLK; ++n) {
+                    double bf[2] = {Y[k * YS + 8 * n + g], Y[(k + 4) * YS + 8 * n + g]};
+                    dmma_16x8x8(acc[n], fb[kk], bf);
                 }
             }
 #pragma unroll
