@@ -126,10 +126,30 @@ struct TimedLaunch {
     std::string name;
     double work;
     cudaEvent_t e0, e1;
+    int dev;
 };
 std::mutex g_timing_mu;
 std::atomic<bool> g_timing_on{false};
 std::vector<TimedLaunch*> g_timed;
+// events of reported launches, reused per device: creating two per launch
+// cost more host time than a short kernel runs, so the timed region starved
+// the GPU
+std::map<int, std::vector<cudaEvent_t>> g_event_pool;
+
+cudaEvent_t pooled_event(int dev) {
+    {
+        std::lock_guard<std::mutex> lk(g_timing_mu);
+        std::vector<cudaEvent_t>& v = g_event_pool[dev];
+        if (!v.empty()) {
+            cudaEvent_t e = v.back();
+            v.pop_back();
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
 }  // namespace
 
 bool kernel_timing_on() { return g_timing_on.load(std::memory_order_relaxed); }
@@ -137,9 +157,9 @@ bool kernel_timing_on() { return g_timing_on.load(std::memory_order_relaxed); }
 void kernel_timing_begin(const char* name, double work, cudaStream_t st, KernelTimer* t) {
     t->slot = nullptr;
     if (!kernel_timing_on()) return;
-    TimedLaunch* L = new TimedLaunch{name, work, nullptr, nullptr};
-    cudaEventCreate(&L->e0);
-    cudaEventCreate(&L->e1);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    TimedLaunch* L = new TimedLaunch{name, work, pooled_event(dev), pooled_event(dev), dev};
     cudaEventRecord(L->e0, st);
     t->slot = L;
 }
@@ -160,7 +180,7 @@ constexpr int kMaxDevices = 64;
 
 // Per-device state for host-slice calls: an internal stream, grow-only
 // staging buffers for A, B, C, and the device error word.
-constexpr int kHostPanels = 4;  // column panels of a large host-slice GEMM
+constexpr int kHostPanels = 8;  // column panels of a large host-slice GEMM
 
 struct DeviceCtx {
     std::mutex mu;
@@ -925,8 +945,11 @@ int rb_kernel_timing_report(char* buf, size_t buf_len) {
         a.first += 1;
         a.second.first += ms;
         a.second.second += L->work;
-        cudaEventDestroy(L->e0);
-        cudaEventDestroy(L->e1);
+        {
+            std::lock_guard<std::mutex> lk(g_timing_mu);
+            g_event_pool[L->dev].push_back(L->e0);
+            g_event_pool[L->dev].push_back(L->e1);
+        }
         delete L;
     }
     std::string out;
