@@ -496,7 +496,11 @@ def run_ours(args):
                                                   B3.data_ptr(), k3, 1.0, C3.data_ptr(), m3, np.float32,
                                                   prec=prec, stream=sh)),
             2.0 * m3 * n3 * k3, (("plain", Precision.Plain), ("bf16x3", Precision.Bf16x3), ("bf16x6", Precision.Bf16x6)), 5)
-        others["c3_sgemm_65536x128x8192"]["min_bytes"] = 4 * (m3 * k3 + k3 * n3 + 2 * m3 * n3)
+        c3 = others["c3_sgemm_65536x128x8192"]
+        c3["min_bytes"] = 4 * (m3 * k3 + k3 * n3 + 2 * m3 * n3)
+        # near the HBM ridge: the minimum bytes (A, B once, C read and written) over each form's time
+        for form in ("plain", "bf16x3", "bf16x6"):
+            c3[form]["min_bytes_gbs"] = c3["min_bytes"] / (c3[form]["ms"] * 1e-3) / 1e9
         del A3, B3, C3
         # C4 complex: ConjTrans/NoTrans 2048^3, alpha = (1, 0.5), beta = 0; 8mnk real flop (4M)
         n4 = 2048
