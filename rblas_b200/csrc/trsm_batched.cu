@@ -266,9 +266,11 @@ constexpr size_t kTbSmemMax = 227 * 1024;
 // busy. The f64 path instead turns every step into a GEMM on DMMA
 // (mma.sync m16n8k8 f64), blocked like the substitution:
 //   1. trsm_inv_diag_kernel inverts every 64 x 64 diagonal block of every
-//      member once, W_b = inv(L_bb) (forward substitution of the unit
-//      vectors, one column per thread held in registers; Unit takes the
-//      diagonal as 1), into a workspace;
+//      member once, W_b = inv(L_bb), into a workspace, by recursive doubling:
+//      the four 16 x 16 diagonal blocks by forward substitution, then
+//      inv([[A, 0], [C, D]]) = [[inv A, 0], [-inv D * C * inv A, inv D]]
+//      twice (16 -> 32 -> 64) with the products on DMMA (Unit takes the
+//      diagonal as 1);
 //   2. trsm_dmma_kernel keeps the member's q x RB slice Y = alpha*B in shared
 //      memory and for each block b computes X_b = W_b * Y_b, then
 //      Y_trailing -= L[trailing, b] * X_b. Both products read A and W as
@@ -279,56 +281,128 @@ constexpr size_t kTbSmemMax = 227 * 1024;
 // stays within the normwise backward-error bound the tests state.
 constexpr int kInvNB = 64;
 
-constexpr int kInvSmem = kInvNB * (kInvNB + 1) * static_cast<int>(sizeof(double));
+// Column-major 64 x 64 f64 tiles in shared memory with columns padded to
+// 68 doubles: the global loads of A's columns, the stores of W and the DMMA
+// fragment reads below (a half-warp on rows g, k-columns t, or k-rows t,
+// columns g, g and t < 4) then touch distinct banks.
+constexpr int kInvLD = 68;
+constexpr int kInvThreads = 128;
+// L block, W (its inverse), and a 32-column temporary
+constexpr int kInvSmem = (2 * kInvNB + 32) * kInvLD * static_cast<int>(sizeof(double));
 
-__global__ void __launch_bounds__(kInvNB) trsm_inv_diag_kernel(const double* __restrict__ A0, TbParams p,
-                                                                double* __restrict__ W, int nblocks) {
+// C(16 x 16) += A(16 x K) * B(K x 16), A and B column-major in shared memory
+// with column stride kInvLD; c[nb] holds columns 8 nb .. 8 nb + 7 in the DMMA
+// accumulator layout (simt_tile.cuh, dmma_16x8x8).
+template <int K>
+__device__ __forceinline__ void inv_mm16(const double* As, const double* Bs, double (&c)[2][4], int g, int t) {
+#pragma unroll
+    for (int kk = 0; kk < K / 8; ++kk) {
+        const int k = 8 * kk + t;
+        const double a[4] = {As[k * kInvLD + g], As[k * kInvLD + g + 8], As[(k + 4) * kInvLD + g],
+                             As[(k + 4) * kInvLD + g + 8]};
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) {
+            const double b[2] = {Bs[(8 * nb + g) * kInvLD + k], Bs[(8 * nb + g) * kInvLD + k + 4]};
+            dmma_16x8x8(c[nb], a, b);
+        }
+    }
+}
+
+// D(16 x 16) = s * c, D column-major in shared memory with column stride kInvLD
+__device__ __forceinline__ void inv_store16(double* Ds, const double (&c)[2][4], double s, int g, int t) {
+#pragma unroll
+    for (int nb = 0; nb < 2; ++nb) {
+        const int col = 8 * nb + 2 * t;
+        Ds[col * kInvLD + g] = s * c[nb][0];
+        Ds[(col + 1) * kInvLD + g] = s * c[nb][1];
+        Ds[col * kInvLD + g + 8] = s * c[nb][2];
+        Ds[(col + 1) * kInvLD + g + 8] = s * c[nb][3];
+    }
+}
+
+__global__ void __launch_bounds__(kInvThreads) trsm_inv_diag_kernel(const double* __restrict__ A0, TbParams p,
+                                                                     double* __restrict__ W, int nblocks) {
     extern __shared__ __align__(16) unsigned char inv_smem[];
-    // L[r][c] of the diagonal block, zero outside it (and zero on the
-    // diagonal for Unit); afterwards the same buffer holds the inverse
-    auto L = reinterpret_cast<double (*)[kInvNB + 1]>(inv_smem);
+    // element (r, c) of a tile at [c * kInvLD + r]
+    double* Ls = reinterpret_cast<double*>(inv_smem);  // L block
+    double* Ws = Ls + kInvNB * kInvLD;                  // its inverse
+    double* Ts = Ws + kInvNB * kInvLD;                  // 32-column temporary
     const int b = blockIdx.x, member = blockIdx.y;
     const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
     const int o = b * kInvNB, nb = min(kInvNB, p.q - o);
-    const int j = threadIdx.x;
-    double w[kInvNB];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+
+    // L (lower part of the block; Unit puts 1 on the diagonal; rows and
+    // columns past nb are the identity), W zero. Thread tid & 63 loads row r
+    // of columns c = tid >> 6, +2, ...: 32 loads in flight.
     {
-        // thread r loads row r of the block; the loop is unrolled so that
-        // all of the row's loads are in flight at once (threads r = 0..63 of
-        // one column c read consecutive addresses when A's rows are fast)
-        const int r = j;
+        const int r = tid & 63, c0 = tid >> 6;
+        double v[kInvNB / 2];
 #pragma unroll
-        for (int c = 0; c < kInvNB; ++c) {
+        for (int i = 0; i < kInvNB / 2; ++i) {
+            const int c = c0 + 2 * i;
             const bool in = r < nb && (c < r || (c == r && !p.unit));
-            w[c] = in ? __ldg(a_ptr(A, p, o + r, o + c)) : 0.0;
+            v[i] = in ? __ldg(a_ptr(A, p, o + r, o + c)) : (c == r ? 1.0 : 0.0);
         }
 #pragma unroll
-        for (int c = 0; c < kInvNB; ++c) L[r][c] = w[c];
+        for (int i = 0; i < kInvNB / 2; ++i) {
+            Ls[(c0 + 2 * i) * kInvLD + r] = v[i];
+            Ws[(c0 + 2 * i) * kInvLD + r] = 0.0;
+        }
     }
     __syncthreads();
-    // Thread j solves column j of the inverse, rows in order:
-    //   w_r = (delta_rj - sum_{s<r} L[r][s] w_s) / L[r][r]  (w_s = 0 above row j).
-    // Both loops are unrolled, so the column stays in registers; every thread
-    // runs the same sequence (no divergence) and L[r][s] is one broadcast
-    // read. Four partial sums (s mod 4) keep the dependent chain short.
+    // the four 16 x 16 diagonal blocks: thread (blk, c) solves column c of
+    // block blk by forward substitution, the column held in registers
+    if (tid < 64) {
+        const int blk = tid >> 4, c = tid & 15, d = 16 * blk;
+        double w[16];
 #pragma unroll
-    for (int r = 0; r < kInvNB; ++r) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int r = 0; r < 16; ++r) {
+            double acc[2] = {0.0, 0.0};
 #pragma unroll
-        for (int s = 0; s < r; ++s) acc[s & 3] = fma(L[r][s], w[s], acc[s & 3]);
-        double v = ((r == j) ? 1.0 : 0.0) - ((acc[0] + acc[1]) + (acc[2] + acc[3]));
-        if (r >= nb || j >= nb || r < j) v = 0.0;
-        else if (!p.unit) v = v / L[r][r];
-        w[r] = v;
+            for (int s = 0; s < r; ++s) acc[s & 1] = fma(Ls[(d + s) * kInvLD + d + r], w[s], acc[s & 1]);
+            const double v = ((r == c) ? 1.0 : 0.0) - (acc[0] + acc[1]);
+            w[r] = (r < c) ? 0.0 : v / Ls[(d + r) * kInvLD + d + r];
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) Ws[(d + c) * kInvLD + d + r] = w[r];
     }
-    __syncthreads();  // every thread is done reading L
-#pragma unroll
-    for (int r = 0; r < kInvNB; ++r) L[r][j] = w[r];
     __syncthreads();
+    // 16 -> 32: warp h (0, 1) forms W[hi][lo] of the 32 x 32 diagonal block h
+    // (lo, hi = its 16-row halves): T = L[hi][lo] * W[lo][lo], then
+    // W[hi][lo] = -W[hi][hi] * T
+    if (warp < 2) {
+        const int lo = 32 * warp, hi = lo + 16;
+        double* Tw = Ts + 16 * warp * kInvLD;  // 16 columns of the temporary
+        double c[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        inv_mm16<16>(Ls + lo * kInvLD + hi, Ws + lo * kInvLD + lo, c, g, t);
+        inv_store16(Tw, c, 1.0, g, t);
+        __syncwarp();
+        double e[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        inv_mm16<16>(Ws + hi * kInvLD + hi, Tw, e, g, t);
+        inv_store16(Ws + lo * kInvLD + hi, e, -1.0, g, t);
+    }
+    __syncthreads();
+    // 32 -> 64: T = L[32:64][0:32] * W[0:32][0:32], then
+    // W[32:64][0:32] = -W[32:64][32:64] * T; warp w takes the 16 x 16 tile
+    // (mi, ni) = (w >> 1, w & 1) of each product
+    {
+        const int mi = warp >> 1, ni = warp & 1;
+        double c[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        inv_mm16<32>(Ls + 32 + 16 * mi, Ws + 16 * ni * kInvLD, c, g, t);
+        inv_store16(Ts + 16 * ni * kInvLD + 16 * mi, c, 1.0, g, t);
+        __syncthreads();
+        double e[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        inv_mm16<32>(Ws + 32 * kInvLD + 32 + 16 * mi, Ts + 16 * ni * kInvLD, e, g, t);
+        inv_store16(Ws + 16 * ni * kInvLD + 32 + 16 * mi, e, -1.0, g, t);
+    }
+    __syncthreads();
+    // W_b column-major, zero outside the block's nb x nb (coalesced stores)
     double* Wb = W + (static_cast<size_t>(member) * nblocks + b) * (kInvNB * kInvNB);
-    for (int idx = threadIdx.x; idx < kInvNB * kInvNB; idx += kInvNB) {
-        const int r = idx % kInvNB, c = idx / kInvNB;  // column-major: coalesced stores
-        Wb[idx] = L[r][c];
+    for (int idx = tid; idx < kInvNB * kInvNB; idx += kInvThreads) {
+        const int r = idx % kInvNB, c = idx / kInvNB;
+        Wb[idx] = (r < nb && c < nb) ? Ws[c * kInvLD + r] : 0.0;
     }
 }
 
@@ -588,7 +662,8 @@ cudaError_t td_launch(const double* A, double* B, double alpha, const TbParams& 
         const size_t nm = std::min(chunk, batch - b0);
         const double* Ac = A + b0 * p.stride_a;
         double* Bc = B + b0 * p.stride_b;
-        trsm_inv_diag_kernel<<<dim3(nblocks, static_cast<unsigned>(nm)), kInvNB, kInvSmem, st>>>(Ac, p, W, nblocks);
+        trsm_inv_diag_kernel<<<dim3(nblocks, static_cast<unsigned>(nm)), kInvThreads, kInvSmem, st>>>(Ac, p, W,
+                                                                                              nblocks);
         trsm_dmma_kernel<RB><<<dim3((p.nrhs + RB - 1) / RB, static_cast<unsigned>(nm)), kTbThreads, smem, st>>>(
             Ac, Bc, alpha, p, W, nblocks);
         count_launch(2);
