@@ -287,8 +287,9 @@ constexpr int kInvNB = 64;
 // columns g, g and t < 4) then touch distinct banks.
 constexpr int kInvLD = 68;
 constexpr int kInvThreads = 128;
-// L block, W (its inverse), and a 32-column temporary
-constexpr int kInvSmem = (2 * kInvNB + 32) * kInvLD * static_cast<int>(sizeof(double));
+// L block and W (its inverse); the temporaries live in L's upper triangle,
+// which is zero and never read (three CTAs per SM)
+constexpr int kInvSmem = 2 * kInvNB * kInvLD * static_cast<int>(sizeof(double));
 
 // C(16 x 16) += A(16 x K) * B(K x 16), A and B column-major in shared memory
 // with column stride kInvLD; c[nb] holds columns 8 nb .. 8 nb + 7 in the DMMA
@@ -324,9 +325,8 @@ __global__ void __launch_bounds__(kInvThreads) trsm_inv_diag_kernel(const double
                                                                      double* __restrict__ W, int nblocks) {
     extern __shared__ __align__(16) unsigned char inv_smem[];
     // element (r, c) of a tile at [c * kInvLD + r]
-    double* Ls = reinterpret_cast<double*>(inv_smem);  // L block
+    double* Ls = reinterpret_cast<double*>(inv_smem);  // L block (lower part read)
     double* Ws = Ls + kInvNB * kInvLD;                  // its inverse
-    double* Ts = Ws + kInvNB * kInvLD;                  // 32-column temporary
     const int b = blockIdx.x, member = blockIdx.y;
     const double* A = A0 + static_cast<size_t>(member) * p.stride_a;
     const int o = b * kInvNB, nb = min(kInvNB, p.q - o);
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kInvThreads) trsm_inv_diag_kernel(const double
     // W[hi][lo] = -W[hi][hi] * T
     if (warp < 2) {
         const int lo = 32 * warp, hi = lo + 16;
-        double* Tw = Ts + 16 * warp * kInvLD;  // 16 columns of the temporary
+        double* Tw = Ls + hi * kInvLD + lo;  // L[lo][hi]: upper, unused
         double c[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
         inv_mm16<16>(Ls + lo * kInvLD + hi, Ws + lo * kInvLD + lo, c, g, t);
         inv_store16(Tw, c, 1.0, g, t);
@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(kInvThreads) trsm_inv_diag_kernel(const double
     {
         const int mi = warp >> 1, ni = warp & 1;
         double c[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        double* Ts = Ls + 32 * kInvLD;  // L[0:32][32:64]: upper, unused
         inv_mm16<32>(Ls + 32 + 16 * mi, Ws + 16 * ni * kInvLD, c, g, t);
         inv_store16(Ts + 16 * ni * kInvLD + 16 * mi, c, 1.0, g, t);
         __syncthreads();
