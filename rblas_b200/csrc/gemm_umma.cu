@@ -1184,12 +1184,54 @@ void launch_ozaki_slices(dim3 grid, cudaStream_t st, const double* x, size_t rs,
 // out[1] = bf16(x - out[0]), out[2] = bf16(x - out[0] - out[1]); every
 // difference is exact in FP32.
 // One 64 x 64 tile of the R x K view per 256-thread block (K tile bx, row tile by).
+// The f32 tile loader with 16-byte loads along the view's contiguous
+// dimension when its lines start on 16 bytes (4 loads per thread instead of
+// 16); the element loader otherwise.
+__device__ __forceinline__ void load_tile_f32(const float* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                                              int r0, int p0, float (*tile)[kTile + 1]) {
+    const bool kcontig = (ps == 1);
+    const size_t ld = kcontig ? rs : ps;         // between the contiguous lines
+    const int L = kcontig ? R : K, E = kcontig ? K : R;
+    const int l0 = kcontig ? r0 : p0, e0 = kcontig ? p0 : r0;
+    if ((!kcontig && rs != 1) || (reinterpret_cast<uintptr_t>(x) & 15) != 0 || (ld & 3) != 0) {
+        load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
+        return;
+    }
+    constexpr int PER = kTile * kTile / 4 / kTileThreads;  // float4 per thread
+    float4 v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
+        const int l = l0 + idx / (kTile / 4), e = e0 + 4 * (idx % (kTile / 4));
+        const float* src = x + static_cast<size_t>(l) * ld + e;
+        if (l < L && e + 3 < E) {
+            v[i] = __ldg(reinterpret_cast<const float4*>(src));
+        } else {
+            v[i].x = (l < L && e < E) ? src[0] : 0.f;
+            v[i].y = (l < L && e + 1 < E) ? src[1] : 0.f;
+            v[i].z = (l < L && e + 2 < E) ? src[2] : 0.f;
+            v[i].w = (l < L && e + 3 < E) ? src[3] : 0.f;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
+        const int ln = idx / (kTile / 4), el = 4 * (idx % (kTile / 4));
+        const float w[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (kcontig) tile[ln][el + j] = w[j];  // row = line, column = k
+            else         tile[el + j][ln] = w[j];  // row = contiguous index, column = line (k)
+        }
+    }
+}
+
 __device__ __forceinline__ void bf16_split_tile(const float* __restrict__ x, size_t rs, size_t ps, int R, int K,
                                                 int planes, __nv_bfloat16* __restrict__ out, size_t kp, size_t plane,
                                                 int bx, int by) {
     __shared__ float tile[kTile][kTile + 1];
     const int r0 = by * kTile, p0 = bx * kTile;
-    load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
+    load_tile_f32(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     for (int job = threadIdx.x; job < kTile * 8; job += blockDim.x) {
         const int r = job >> 3, c = job & 7;  // 64 rows x 8 chunks of 8
@@ -1197,11 +1239,15 @@ __device__ __forceinline__ void bf16_split_tile(const float* __restrict__ x, siz
         __align__(16) __nv_bfloat16 h[3][8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
+            // hi, then the rest rounded again (mid / lo): the third plane only
+            // for the 6-product form
             float v = tile[r][c * 8 + i];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                h[q][i] = __float2bfloat16_rn(v);
-                v = v - __bfloat162float(h[q][i]);
+            h[0][i] = __float2bfloat16_rn(v);
+            v = v - __bfloat162float(h[0][i]);
+            h[1][i] = __float2bfloat16_rn(v);
+            if (planes > 2) {
+                v = v - __bfloat162float(h[1][i]);
+                h[2][i] = __float2bfloat16_rn(v);
             }
         }
         const size_t off = static_cast<size_t>(r0 + r) * kp + p0 + c * 8;
