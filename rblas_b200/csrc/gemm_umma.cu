@@ -1041,15 +1041,45 @@ __device__ __forceinline__ Int floor_scaled(double x, int n) {
 // S slices known at compile time: up to 8 digits the integer fits 64 bits.
 // One 64 x 64 tile of the R x K view per 256-thread block: K tile bx, row
 // tile by.
+// The slice pass's tile: rows of kSliceLD doubles (1 mod 16), and every
+// 16-column group shifted by 4 more, so that the reads below (a half-warp on
+// rows r and groups c, tid = 4r + c) and the loads' stores both touch
+// distinct banks; with 65-double rows the four groups of a row shared theirs.
+constexpr int kSliceLD = 81;
+__device__ __forceinline__ int slice_col(int col) { return col + (col >> 4) * 4; }
+
+__device__ __forceinline__ void load_tile_sliced(const double* __restrict__ x, size_t rs, size_t ps, int R, int K,
+                                                 int r0, int p0, double (*tile)[kSliceLD]) {
+    constexpr int PER = kTile * kTile / kTileThreads;
+    const bool kcontig = (ps == 1);
+    double v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
+        const int a = idx % kTile, b = idx / kTile;
+        const int r = kcontig ? b : a;
+        const int q = kcontig ? a : b;
+        v[i] = (r0 + r < R && p0 + q < K) ? x[static_cast<size_t>(r0 + r) * rs + static_cast<size_t>(p0 + q) * ps]
+                                          : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int idx = threadIdx.x + i * kTileThreads;
+        const int a = idx % kTile, b = idx / kTile;
+        if (kcontig) tile[b][slice_col(a)] = v[i];
+        else         tile[a][slice_col(b)] = v[i];
+    }
+}
+
 template <int S>
 __device__ __forceinline__ void ozaki_slice_tile(const double* __restrict__ x, size_t rs, size_t ps, int R, int K,
                                                  const int* __restrict__ e, int8_t* __restrict__ out, size_t kp,
                                                  size_t plane, int bx, int by) {
     using Int = typename std::conditional<(S <= 8), long long, __int128>::type;
     constexpr int slices = S;
-    __shared__ double tile[kTile][kTile + 1];
+    __shared__ double tile[kTile][kSliceLD];
     const int r0 = by * kTile, p0 = bx * kTile;
-    load_tile<double>(x, rs, ps, R, K, r0, p0, tile);
+    load_tile_sliced(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;  // 64 rows x 4 chunks of 16
     if (r0 + r >= R) return;
@@ -1071,7 +1101,7 @@ __device__ __forceinline__ void ozaki_slice_tile(const double* __restrict__ x, s
             uint32_t lo[4], hi[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const long long Y = (er == kExpSentinel) ? 0LL : floor_scaled<long long>(tile[r][c * 16 + g * 4 + q], n);
+                const long long Y = (er == kExpSentinel) ? 0LL : floor_scaled<long long>(tile[r][slice_col(c * 16 + g * 4 + q)], n);
                 const unsigned long long Z = (static_cast<unsigned long long>(Y) + B) ^ B;
                 lo[q] = static_cast<uint32_t>(Z);
                 hi[q] = static_cast<uint32_t>(Z >> 32);
@@ -1091,7 +1121,7 @@ __device__ __forceinline__ void ozaki_slice_tile(const double* __restrict__ x, s
     for (int t = 0; t < S; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const Int Y = (er == kExpSentinel) ? Int(0) : floor_scaled<Int>(tile[r][c * 16 + i], n);
+        const Int Y = (er == kExpSentinel) ? Int(0) : floor_scaled<Int>(tile[r][slice_col(c * 16 + i)], n);
         int d[S];
 #pragma unroll
         for (int t = 0; t < S; ++t) {
