@@ -1256,12 +1256,17 @@ __device__ __forceinline__ void load_tile_f32(const float* __restrict__ x, size_
     }
 }
 
+// VEC: the 16-byte loader (the single-problem pass over large operands);
+// the grouped pass keeps the element loader, whose kernel stays at five CTAs
+// per SM
+template <bool VEC>
 __device__ __forceinline__ void bf16_split_tile(const float* __restrict__ x, size_t rs, size_t ps, int R, int K,
                                                 int planes, __nv_bfloat16* __restrict__ out, size_t kp, size_t plane,
                                                 int bx, int by) {
     __shared__ float tile[kTile][kTile + 1];
     const int r0 = by * kTile, p0 = bx * kTile;
-    load_tile_f32(x, rs, ps, R, K, r0, p0, tile);
+    if constexpr (VEC) load_tile_f32(x, rs, ps, R, K, r0, p0, tile);
+    else               load_tile<float>(x, rs, ps, R, K, r0, p0, tile);
     __syncthreads();
     for (int job = threadIdx.x; job < kTile * 8; job += blockDim.x) {
         const int r = job >> 3, c = job & 7;  // 64 rows x 8 chunks of 8
@@ -1269,13 +1274,14 @@ __device__ __forceinline__ void bf16_split_tile(const float* __restrict__ x, siz
         __align__(16) __nv_bfloat16 h[3][8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            // hi, then the rest rounded again (mid / lo): the third plane only
-            // for the 6-product form
+            // hi, then the rest rounded again (mid / lo); the single-problem
+            // pass skips the third plane when the 3xBF16 form does not write
+            // it (the grouped pass, branch-free, measured faster without the test)
             float v = tile[r][c * 8 + i];
             h[0][i] = __float2bfloat16_rn(v);
             v = v - __bfloat162float(h[0][i]);
             h[1][i] = __float2bfloat16_rn(v);
-            if (planes > 2) {
+            if (!VEC || planes > 2) {
                 v = v - __bfloat162float(h[1][i]);
                 h[2][i] = __float2bfloat16_rn(v);
             }
@@ -1290,7 +1296,7 @@ __global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict
                                                          int R, int K, int planes,
                                                          __nv_bfloat16* __restrict__ out, size_t kp,
                                                          size_t plane) {
-    bf16_split_tile(x, rs, ps, R, K, planes, out, kp, plane, blockIdx.x, blockIdx.y);
+    bf16_split_tile<true>(x, rs, ps, R, K, planes, out, kp, plane, blockIdx.x, blockIdx.y);
 }
 
 // One operand of a grouped BF16-split launch, viewed as R x K, and its
@@ -1314,7 +1320,7 @@ __global__ void __launch_bounds__(256) bf16_split_grouped_kernel(const BsOperand
     }
     const BsOperand& o = ops[lo];
     const int b = blockIdx.x - o.start;
-    bf16_split_tile(o.x, o.rs, o.ps, o.R, o.K, o.planes, o.out, o.kp, o.plane, b % o.gx, b / o.gx);
+    bf16_split_tile<false>(o.x, o.rs, o.ps, o.R, o.K, o.planes, o.out, o.kp, o.plane, b % o.gx, b / o.gx);
 }
 
 CUresult make_tmap_planes(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem,
