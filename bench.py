@@ -1095,19 +1095,21 @@ def run_level3_only(args):
 
 
 def run_trsm_batched_only(args):
-    """The batched f64 trsm of the C4 configuration (512 x 512 lower, 64
-    right-hand sides) on `--trsm-batched BATCH` members, launched warmup +
-    steps times (for ncu captures on a bounded batch)."""
+    """The batched trsm of the C4 configuration (512 x 512 lower, 64
+    right-hand sides; f64, or f32 with `--dtype f32`) on `--trsm-batched BATCH`
+    members, launched warmup + steps times (for ncu captures on a bounded
+    batch)."""
     import torch
 
     from rblas_b200 import level3
 
     q, nrhs, batch = 512, 64, args.trsm_batched
+    tdt, ndt = (torch.float32, np.float32) if args.dtype == "f32" else (torch.float64, np.float64)
     g = torch.Generator(device="cuda")
     g.manual_seed(8)
-    A = torch.randn(q * q * batch, dtype=torch.float64, device="cuda", generator=g) * (0.1 / q ** 0.5)
+    A = torch.randn(q * q * batch, dtype=tdt, device="cuda", generator=g) * (0.1 / q ** 0.5)
     A.view(batch, q, q).diagonal(dim1=1, dim2=2).uniform_(1.0, 2.0)
-    B = torch.rand(q * nrhs * batch, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    B = torch.rand(q * nrhs * batch, dtype=tdt, device="cuda", generator=g) * 2 - 1
     sh = torch.cuda.current_stream().cuda_stream
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -1115,11 +1117,11 @@ def run_trsm_batched_only(args):
         if i == args.warmup:
             e0.record()
         level3.trsm_batched_dev(0, 1, 0, 0, q, nrhs, 1.0, A.data_ptr(), q, q * q, B.data_ptr(), q, q * nrhs,
-                                batch, np.float64, stream=sh)
+                                batch, ndt, stream=sh)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    print(json.dumps({"trsm_batched": [q, nrhs, batch], "ms": ms,
+    print(json.dumps({"trsm_batched": [q, nrhs, batch], "dtype": args.dtype, "ms": ms,
                       "tflops": q * q * nrhs * batch / (ms * 1e-3) / 1e12}))
 
 
