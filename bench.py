@@ -1039,6 +1039,7 @@ def run_level3_only(args):
     g.manual_seed(9)
     prec = {"plain": Precision.Plain, "ozaki": Precision.Ozaki, "bf16x3": Precision.Bf16x3,
             "bf16x6": Precision.Bf16x6}[args.form if args.form != "auto" else "plain"]
+    dev_one = None  # the same routine on the device copies (trsm, trmm)
     if args.cplx:
         dt = torch.float64 if args.dtype == "f64" else torch.float32
         A, B, C = (torch.randn(2 * x, dtype=dt, device="cuda", generator=g) for x in (k * m, k * n, m * n))
@@ -1056,7 +1057,12 @@ def run_level3_only(args):
         B = torch.randn(max(m, k) * max(n, k), dtype=torch.float64, device="cuda", generator=g)
         C = torch.randn(m * max(n, m), dtype=torch.float64, device="cuda", generator=g)
         name = args.level3
-        hA, hB, hC = (np.ascontiguousarray(t.cpu().numpy()) for t in (A, B, C))
+
+        def pinned(t):
+            h = torch.empty(t.numel(), dtype=t.dtype, pin_memory=True)
+            h.copy_(t)
+            return h.numpy()
+        hA, hB, hC = (pinned(t) for t in (A, B, C))
         vp = lambda x: Cc.c_void_p(x.ctypes.data)  # noqa: E731
         err = _lib.RbError()
         if name == "syrk":
@@ -1071,27 +1077,42 @@ def run_level3_only(args):
         elif name == "trmm":
             def one():
                 lib.rb_dtrmm(0, 1, 0, 0, m, n, 1.0, vp(hA), m, hA.size, vp(hB), m, hB.size, Cc.byref(err))
+
+            def dev_one():
+                lib.rb_dtrmm_dev(0, 1, 0, 0, m, n, 1.0, Cc.c_void_p(A.data_ptr()), m, Cc.c_void_p(B.data_ptr()),
+                                 m, Cc.c_void_p(sh), Cc.byref(err))
             work = 1.0 * m * m * n
         else:
             def one():
                 lib.rb_dtrsm(0, 1, 0, 0, m, n, 1.0, vp(hA), m, hA.size, vp(hB), m, hB.size, Cc.byref(err))
+
+            def dev_one():
+                lib.rb_dtrsm_dev(0, 1, 0, 0, m, n, 1.0, Cc.c_void_p(A.data_ptr()), m, Cc.c_void_p(B.data_ptr()),
+                                 m, Cc.c_void_p(sh), Cc.byref(err))
             work = 1.0 * m * m * n
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     import time as _t
-    t0 = 0.0
-    for i in range(args.warmup + args.steps):
-        if i == args.warmup:
-            torch.cuda.synchronize()
-            e0.record()
-            t0 = _t.perf_counter()
-        one()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    print(json.dumps({"level3_only": args.level3 or "complex", "shape": [m, n, k], "ms": ms,
-                      "wall_ms": (_t.perf_counter() - t0) * 1e3 / max(args.steps, 1),
-                      "tflops": work / (ms * 1e-3) / 1e12}))
+
+    def timed(fn):
+        t0 = 0.0
+        for i in range(args.warmup + args.steps):
+            if i == args.warmup:
+                torch.cuda.synchronize()
+                e0.record()
+                t0 = _t.perf_counter()
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / max(args.steps, 1), (_t.perf_counter() - t0) * 1e3 / max(args.steps, 1)
+    ms, wall = timed(one)
+    out = {"level3_only": args.level3 or "complex", "shape": [m, n, k], "ms": ms, "wall_ms": wall,
+           "tflops": work / (ms * 1e-3) / 1e12}
+    if dev_one is not None:
+        dms, _ = timed(dev_one)
+        out["device_ms"] = dms
+        out["device_tflops"] = work / (dms * 1e-3) / 1e12
+    print(json.dumps(out))
 
 
 def run_trsm_batched_only(args):

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 
 #include "../../include/rblas_b200.h"
 #include "rb_device.cuh"
@@ -216,10 +217,10 @@ __global__ void tri_expand_kernel(const T* __restrict__ a, size_t lda, int q, in
     }
 }
 
-constexpr int kNbReal = 64, kNbCplx = 32;
+constexpr int kNbCplx = 32;
 
-// Solve one diagonal block by substitution for `nvec` independent vectors,
-// one thread per vector. The block of op(A) (nb x nb, origin (o, o) in op(A)
+// Solve one diagonal block of a complex trsm by substitution for `nvec`
+// independent vectors, one thread per vector. The block of op(A) (nb x nb, origin (o, o) in op(A)
 // coordinates) is staged in shared memory.
 //   side Left : op(A)_blk x = v, v = B[o+t, j] (column j), t < nb.
 //   side Right: x op(A)_blk = v, v = B[i, o+t] (row i).
@@ -228,7 +229,7 @@ template <typename T, bool CX>
 __global__ void trsm_diag_kernel(int side, int eff_upper, int trans, int diag, int nb, int o,
                                  const T* __restrict__ a, size_t lda, T* __restrict__ b, size_t ldb,
                                  int nvec) {
-    constexpr int NB = CX ? kNbCplx : kNbReal;
+    constexpr int NB = kNbCplx;
     constexpr int W = CX ? 2 : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* blk = reinterpret_cast<T*>(smem_raw);  // [r][c] of op(A)_blk, row-major, W components
@@ -447,13 +448,24 @@ static int update_gemm(bool a_first, size_t m, size_t n, size_t k, const T* X, s
     }
 }
 
+// Blocked substitution over diagonal blocks of op(A) (src/level3.rs:390-520
+// solves row by row; the blocking only regroups the same updates), the
+// order halved recursively at whole blocks so that the off-diagonal updates
+// are a few large GEMMs. The diagonal blocks:
+//   real types    kTrsmDiagReal rows, each solved by the batched trsm with
+//                 one member, whose grid spans the right-hand sides in 8-32
+//                 wide slices (f64 on the FP64 tensor cores against inverted
+//                 64 x 64 blocks);
+//   complex types kNbCplx rows by trsm_diag_kernel, one thread per
+//                 right-hand side.
+constexpr size_t kTrsmDiagReal = 512;
+
 template <typename T, bool CX>
 int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A,
              size_t lda, T* B, size_t ldb, cudaStream_t st, int32_t* ce) {
     constexpr int W = CX ? 2 : 1;
-    constexpr int NB = CX ? kNbCplx : kNbReal;
+    constexpr size_t NB = CX ? static_cast<size_t>(kNbCplx) : kTrsmDiagReal;
     if (m == 0 || n == 0) return RB_OK;
-    cudaError_t e;
     const bool alpha_one = (ar == T(1)) && (!CX || ai == T(0));
     if (!alpha_one) {  // src/level3.rs:403-409
         scale_b_kernel<T, CX><<<grid_for(m * n), 256, 0, st>>>(B, ldb, (int)m, (int)n, ar, ai);
@@ -463,49 +475,61 @@ int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, 
     const bool eff_upper = (uplo == RB_UPPER) != tr;  // src/level3.rs:423-426
     const size_t q = (side == RB_LEFT) ? m : n;       // order of op(A)
     const size_t nvec = (side == RB_LEFT) ? n : m;
-    const int smem = NB * NB * W * static_cast<int>(sizeof(T));
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(trsm_diag_kernel<T, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
+    if constexpr (CX) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(trsm_diag_kernel<T, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(NB * NB * W * sizeof(T)));
+            attr = true;
+        }
     }
     // op(A)[r0:, c0:] as a stored sub-matrix and its transpose flag
     auto sub = [&](size_t r0, size_t c0) -> const T* {
         const size_t off = tr ? (c0 + r0 * lda) : (r0 + c0 * lda);
         return A + W * off;
     };
-    const int nblocks = static_cast<int>((q + NB - 1) / NB);
     const bool forward = (side == RB_LEFT) ? !eff_upper : eff_upper;
-    for (int bi = 0; bi < nblocks; ++bi) {
-        const int blk = forward ? bi : nblocks - 1 - bi;
-        const size_t o = static_cast<size_t>(blk) * NB;
-        const size_t nb = std::min<size_t>(NB, q - o);
-        trsm_diag_kernel<T, CX><<<(int)((nvec + 127) / 128), 128, smem, st>>>(
-            side, eff_upper, trans, diag, (int)nb, (int)o, A, lda, B, ldb, (int)nvec);
-        count_launch();
-        if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, ce);
-        int rc = RB_OK;
-        if (side == RB_LEFT) {
-            // rows still to solve: after the block (forward) or before it (backward)
-            const T* X = B + W * o;
-            if (forward && o + nb < q) {
-                rc = update_gemm<T, CX>(true, q - o - nb, n, nb, X, ldb, sub(o + nb, o), lda, trans,
-                                        B + W * (o + nb), ldb, st, ce);
-            } else if (!forward && o > 0) {
-                rc = update_gemm<T, CX>(true, o, n, nb, X, ldb, sub(0, o), lda, trans, B, ldb, st, ce);
-            }
+    // one diagonal block [o, o + nb) of op(A)'s order
+    auto leaf = [&](size_t o, size_t nb) -> int {
+        if constexpr (CX) {
+            trsm_diag_kernel<T, CX><<<(int)((nvec + 127) / 128), 128, NB * NB * W * sizeof(T), st>>>(
+                side, eff_upper, trans, diag, (int)nb, (int)o, A, lda, B, ldb, (int)nvec);
+            count_launch();
+            const cudaError_t le = cudaGetLastError();
+            return le == cudaSuccess ? RB_OK : fail(le, ce);
         } else {
-            const T* X = B + W * o * ldb;
-            if (forward && o + nb < q) {
-                rc = update_gemm<T, CX>(false, m, q - o - nb, nb, X, ldb, sub(o, o + nb), lda, trans,
-                                        B + W * (o + nb) * ldb, ldb, st, ce);
-            } else if (!forward && o > 0) {
-                rc = update_gemm<T, CX>(false, m, o, nb, X, ldb, sub(o, 0), lda, trans, B, ldb, st, ce);
-            }
+            // the diagonal block of op(A) is op() of A's diagonal block
+            return trsm_batched_dev<T>(side, uplo, trans, diag, side == RB_LEFT ? nb : m, side == RB_LEFT ? n : nb,
+                                       T(1), A + o + o * lda, lda, 0, side == RB_LEFT ? B + o : B + o * ldb, ldb, 0,
+                                       1, st, ce, nullptr);
+        }
+    };
+    // [o, o + len) split at o + h into P1 = [o, o + h) and P2 = [o + h, o + len):
+    // forward solves P1, then B(P2) -= op(A)(P2, P1) X(P1) (Left) or
+    // X(:, P1) op(A)(P1, P2) (Right), then P2; backward the mirror image.
+    // Halving at whole blocks gives the same updates as a block-by-block
+    // loop, grouped into a few GEMMs with K up to q / 2.
+    std::function<int(size_t, size_t)> solve = [&](size_t o, size_t len) -> int {
+        const size_t nblk = (len + NB - 1) / NB;
+        if (nblk <= 1) return leaf(o, len);
+        const size_t h = (nblk / 2) * NB, o2 = o + h, l2 = len - h;
+        int rc = forward ? solve(o, h) : solve(o2, l2);
+        if (rc != RB_OK) return rc;
+        if (side == RB_LEFT) {
+            rc = forward ? update_gemm<T, CX>(true, l2, n, h, B + W * o, ldb, sub(o2, o), lda, trans, B + W * o2,
+                                              ldb, st, ce)
+                         : update_gemm<T, CX>(true, h, n, l2, B + W * o2, ldb, sub(o, o2), lda, trans, B + W * o,
+                                              ldb, st, ce);
+        } else {
+            rc = forward ? update_gemm<T, CX>(false, m, l2, h, B + W * o * ldb, ldb, sub(o, o2), lda, trans,
+                                              B + W * o2 * ldb, ldb, st, ce)
+                         : update_gemm<T, CX>(false, m, h, l2, B + W * o2 * ldb, ldb, sub(o2, o), lda, trans,
+                                              B + W * o * ldb, ldb, st, ce);
         }
         if (rc != RB_OK) return rc;
-    }
-    return RB_OK;
+        return forward ? solve(o2, l2) : solve(o, h);
+    };
+    return solve(0, q);
 }
 
 // B := alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular: op(A)

@@ -237,14 +237,50 @@ def test_trsm_parity(dtype, side, uplo, trans):
     assert rb.device_error()[0] == 0
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("uplo", [0, 1])
+@pytest.mark.parametrize("trans", [0, 1])
+def test_trsm_blocked_parity(dtype, side, uplo, trans):
+    """Orders above one 512-row diagonal block (1100: two full blocks and a
+    ragged 76-row one), so the real types' blocked path runs its GEMM
+    updates between the diagonal solves. Forward error as in
+    test_trsm_parity, and the normwise backward error
+    ||op(A) X - alpha B||_F / (||A_tri||_F ||X||_F + |alpha| ||B||_F) within
+    4 * q * u."""
+    rng = np.random.default_rng(70 + 4 * side + 2 * uplo + trans)
+    q, nr = 1100, 70
+    m, n = (q, nr) if side == 0 else (nr, q)
+    for diag in (0, 1):
+        a = tri_matrix(rng, q, uplo, dtype)
+        b0 = rng.uniform(-1, 1, m * n).astype(dtype)
+        b = b0.copy()
+        ref = b0.copy()
+        level3.trsm(side, uplo, trans, diag, m, n, 0.75, a, q, b, m)
+        oracle.trsm(side, uplo, trans, diag, m, n, 0.75, a, q, ref, m)
+        rel = np.max(np.abs(b.astype(np.float64) - ref)) / np.max(np.abs(ref))
+        assert rel <= 1e3 * _u(dtype), (diag, rel)
+        A = a.reshape(q, q, order="F").astype(np.float64)
+        T = np.tril(A) if uplo == 1 else np.triu(A)
+        if diag == 1:
+            np.fill_diagonal(T, 1.0)
+        opA = T.T if trans else T
+        X = b.reshape(m, n, order="F").astype(np.float64)
+        B0 = b0.reshape(m, n, order="F").astype(np.float64)
+        R = (opA @ X if side == 0 else X @ opA) - 0.75 * B0
+        back = np.linalg.norm(R) / (np.linalg.norm(T) * np.linalg.norm(X) + 0.75 * np.linalg.norm(B0))
+        assert back <= 4 * q * _u(dtype), (diag, back)
+    assert rb.device_error()[0] == 0
+
+
 def test_trsm_alpha_zero_and_unit_diag_ignore_diagonal():
     rng = np.random.default_rng(50)
-    m, n = 40, 9
-    a = tri_matrix(rng, m, 1, np.float64)
-    A = a.reshape(m, m, order="F")
-    A[np.diag_indices(m)] = np.nan  # Unit: the diagonal is never read
-    b = rng.uniform(-1, 1, m * n)
-    ref = b.copy()
-    level3.trsm(0, 1, 0, 1, m, n, 1.0, a, m, b, m)
-    oracle.trsm(0, 1, 0, 1, m, n, 1.0, a, m, ref, m)
-    assert np.max(np.abs(b - ref)) < 1e-12
+    for m, n in [(40, 9), (600, 9)]:  # one diagonal block; two (the blocked path)
+        a = tri_matrix(rng, m, 1, np.float64)
+        A = a.reshape(m, m, order="F")
+        A[np.diag_indices(m)] = np.nan  # Unit: the diagonal is never read
+        b = rng.uniform(-1, 1, m * n)
+        ref = b.copy()
+        level3.trsm(0, 1, 0, 1, m, n, 1.0, a, m, b, m)
+        oracle.trsm(0, 1, 0, 1, m, n, 1.0, a, m, ref, m)
+        assert np.max(np.abs(b - ref)) < 1e-12, m
