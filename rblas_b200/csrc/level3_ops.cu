@@ -147,28 +147,64 @@ __global__ void cplx_epilogue_kernel(const T* __restrict__ P, size_t ldp, int m,
 
 // full (q x q, ld = ldf) from the uplo triangle of A (src/level3.rs:359-381,
 // src/complex3.rs:190-214). CX: complex interleaved; herm: conjugate mirror
-// and real diagonal.
+// and real diagonal. One 32 x 32 tile of `full` per CTA (32 x 8 threads):
+// the tile is staged from its stored counterpart in A (itself, or the
+// transposed tile across the diagonal) with column reads, so both the global
+// reads and the writes run down columns; the diagonal tile holds both halves.
+constexpr int kSymTile = 32;
+
 template <typename T, bool CX>
-__global__ void sym_expand_kernel(const T* __restrict__ a, size_t lda, int q, int uplo, int herm,
-                                  T* __restrict__ full, size_t ldf) {
-    const size_t total = static_cast<size_t>(q) * q;
-    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const size_t j = idx / q, i = idx - j * q;
-        const bool stored = (uplo == RB_UPPER) ? (i <= j) : (i >= j);
-        const size_t src = stored ? (i + j * lda) : (j + i * lda);
-        if constexpr (CX) {
-            T re = a[2 * src], im = a[2 * src + 1];
-            if (herm) {
-                if (i == j) im = T(0);
-                else if (!stored) im = T(0) - im;
-            }
-            full[2 * (i + j * ldf)] = re;
-            full[2 * (i + j * ldf) + 1] = im;
-        } else {
-            full[i + j * ldf] = a[src];
+struct SymElem {
+    T v;
+};
+template <typename T>
+struct SymElem<T, true> {
+    T re, im;
+};
+
+template <typename T, bool CX>
+__global__ void __launch_bounds__(256) sym_expand_kernel(const T* __restrict__ a, size_t lda, int q, int uplo,
+                                                         int herm, T* __restrict__ full, size_t ldf) {
+    using E = SymElem<T, CX>;
+    __shared__ E S[kSymTile][kSymTile + 1];  // S[c][r] = A(r0 + r, c0 + c)
+    const int I = blockIdx.x, J = blockIdx.y, tx = threadIdx.x, ty = threadIdx.y;
+    // the tile's own position is stored (or on the diagonal): stage it; else
+    // stage the tile across the diagonal
+    const bool same = (uplo == RB_UPPER) ? (I <= J) : (I >= J);
+    const int r0 = (same ? I : J) * kSymTile, c0 = (same ? J : I) * kSymTile;
+    for (int k = ty; k < kSymTile; k += 8) {
+        const int r = r0 + tx, c = c0 + k;
+        if (r < q && c < q) {
+            const T* src = a + (CX ? 2 : 1) * (static_cast<size_t>(r) + static_cast<size_t>(c) * lda);
+            if constexpr (CX) S[k][tx] = E{src[0], src[1]};
+            else S[k][tx] = E{src[0]};
         }
     }
+    __syncthreads();
+    for (int k = ty; k < kSymTile; k += 8) {
+        const int gi = I * kSymTile + tx, gj = J * kSymTile + k;
+        if (gi >= q || gj >= q) continue;
+        const bool stored = (uplo == RB_UPPER) ? (gi <= gj) : (gi >= gj);
+        // A(gi, gj) when stored (own tile: S[k][tx]); else A(gj, gi) (S[tx][k]
+        // in the own diagonal tile and in the tile across the diagonal alike)
+        E v = (same && stored) ? S[k][tx] : S[tx][k];
+        T* dst = full + (CX ? 2 : 1) * (static_cast<size_t>(gi) + static_cast<size_t>(gj) * ldf);
+        if constexpr (CX) {
+            if (herm) {
+                if (gi == gj) v.im = T(0);
+                else if (!stored) v.im = T(0) - v.im;
+            }
+            dst[0] = v.re;
+            dst[1] = v.im;
+        } else {
+            dst[0] = v.v;
+        }
+    }
+}
+
+inline dim3 sym_grid(size_t q) {
+    const unsigned t = static_cast<unsigned>((q + kSymTile - 1) / kSymTile);
+    return dim3(t, t);
 }
 
 // ---- trsm pieces ------------------------------------------------------------
@@ -388,7 +424,8 @@ int symm_dev(int side, int uplo, size_t m, size_t n, T alpha, const T* A, size_t
     void* full = nullptr;
     cudaError_t e = scratch_alloc(&full, ldf * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
-    sym_expand_kernel<T, false><<<grid_for(q * q), 256, 0, st>>>(A, lda, (int)q, uplo, 0, static_cast<T*>(full), ldf);
+    sym_expand_kernel<T, false><<<sym_grid(q), dim3(kSymTile, 8), 0, st>>>(A, lda, (int)q, uplo, 0,
+                                                                           static_cast<T*>(full), ldf);
     count_launch();
     int rc;
     if (side == RB_LEFT)
@@ -410,7 +447,8 @@ int hesy_dev(int herm, int side, int uplo, size_t m, size_t n, T ar, T ai, const
     void* full = nullptr;
     cudaError_t e = scratch_alloc(&full, 2 * q * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
-    sym_expand_kernel<T, true><<<grid_for(q * q), 256, 0, st>>>(A, lda, (int)q, uplo, herm, static_cast<T*>(full), q);
+    sym_expand_kernel<T, true><<<sym_grid(q), dim3(kSymTile, 8), 0, st>>>(A, lda, (int)q, uplo, herm,
+                                                                          static_cast<T*>(full), q);
     count_launch();
     int rc;
     if (side == RB_LEFT)
