@@ -570,46 +570,98 @@ int trsm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, 
     return solve(0, q);
 }
 
-// B := alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular: op(A)
-// expanded to a full matrix, one GEMM into scratch, copied back into B.
+// B := alpha*op(A)*B (Left) or alpha*B*op(A) (Right), A triangular, in place.
+// The order of op(A) is halved recursively at whole kTrmmLeaf blocks:
+// with op(A) = [[T11, T12], [T21, T22]] (one of T12 / T21 zero) and B split
+// to match, each half of B is multiplied by its diagonal block (recursion)
+// before or after the off-diagonal product is added to it (a GEMM with
+// beta = 1), in the order that reads the other half of B before it changes:
+//   Left  lower: B2 := T22 B2; B2 += T21 B1; B1 := T11 B1
+//   Left  upper: B1 := T11 B1; B1 += T12 B2; B2 := T22 B2
+//   Right lower: B1 := B1 T11; B1 += B2 T21; B2 := B2 T22
+//   Right upper: B2 := B2 T22; B2 += B1 T12; B1 := B1 T11
+// A leaf block is expanded by tri_expand_kernel (the referenced triangle,
+// zeros elsewhere, ones on a Unit diagonal) and multiplied by one GEMM into
+// scratch, which is copied back into B. The unreferenced triangle and a Unit
+// diagonal are never read. Only the T21 / T12 blocks and the leaves' squares
+// are multiplied: about half the flops of one GEMM by the full op(A).
+constexpr size_t kTrmmLeaf = 512;
+
 template <typename T, bool CX>
 int trmm_dev(int side, int uplo, int trans, int diag, size_t m, size_t n, T ar, T ai, const T* A, size_t lda, T* B,
              size_t ldb, cudaStream_t st, int32_t* ce) {
     if (m == 0 || n == 0) return RB_OK;
     constexpr int W = CX ? 2 : 1;
-    const size_t q = (side == RB_LEFT) ? m : n;
+    const bool left = side == RB_LEFT;
+    const size_t q = left ? m : n;
+    const size_t L = std::min(q, kTrmmLeaf);
     const size_t vec = 16 / (W * sizeof(T)) > 0 ? 16 / (W * sizeof(T)) : 1;
-    const size_t ldf = rup(q, vec), ldo = rup(m, vec);
-    const size_t full_bytes = rup(W * ldf * q * sizeof(T), 256);
+    const size_t ldf = rup(L, vec), ldo = rup(left ? L : m, vec), out_cols = left ? n : L;
+    const size_t full_bytes = rup(W * ldf * L * sizeof(T), 256);
     void* buf = nullptr;
-    cudaError_t e = scratch_alloc(&buf, full_bytes + W * ldo * n * sizeof(T), st);
+    cudaError_t e = scratch_alloc(&buf, full_bytes + W * ldo * out_cols * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
     T* full = static_cast<T*>(buf);
     T* out = reinterpret_cast<T*>(static_cast<uint8_t*>(buf) + full_bytes);
-    tri_expand_kernel<T, CX><<<grid_for(q * q), 256, 0, st>>>(A, lda, static_cast<int>(q), uplo, trans, diag, full,
-                                                               ldf);
-    count_launch();
-    int rc;
-    if constexpr (CX) {
-        if (side == RB_LEFT)
-            rc = complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, n, m, ar, ai, full, ldf, B, ldb, T(0), T(0), out, ldo,
-                                     RB_PREC_PLAIN, st, ce);
+    const bool tr = trans != RB_NO_TRANS;
+    const bool eff_upper = (uplo == RB_UPPER) != tr;
+    // op(A)[r0:, c0:] as a stored sub-matrix (read through the GEMM's transpose)
+    auto sub = [&](size_t r0, size_t c0) -> const T* { return A + W * (tr ? (c0 + r0 * lda) : (r0 + c0 * lda)); };
+    auto bl = [&](size_t o) -> T* { return B + W * (left ? o : o * ldb); };  // B's rows / columns from o
+    // target += alpha * op(A)(r0.., c0..) X (Left) or alpha * X op(A)(r0.., c0..) (Right)
+    auto add = [&](size_t rows, size_t cols, size_t r0, size_t c0, const T* X, T* target) -> int {
+        if constexpr (CX) {
+            if (left)
+                return complex_gemm_dev<T>(trans, RB_NO_TRANS, rows, n, cols, ar, ai, sub(r0, c0), lda, X, ldb, T(1),
+                                           T(0), target, ldb, RB_PREC_PLAIN, st, ce);
+            return complex_gemm_dev<T>(RB_NO_TRANS, trans, m, cols, rows, ar, ai, X, ldb, sub(r0, c0), lda, T(1),
+                                       T(0), target, ldb, RB_PREC_PLAIN, st, ce);
+        } else {
+            if (left)
+                return gemm_colmajor_dev<T>(tr, false, rows, n, cols, ar, sub(r0, c0), lda, X, ldb, T(1), target, ldb,
+                                            RB_PREC_PLAIN, st, 0, ce);
+            return gemm_colmajor_dev<T>(false, tr, m, cols, rows, ar, X, ldb, sub(r0, c0), lda, T(1), target, ldb,
+                                        RB_PREC_PLAIN, st, 0, ce);
+        }
+    };
+    auto leaf = [&](size_t o, size_t nb) -> int {
+        tri_expand_kernel<T, CX><<<grid_for(nb * nb), 256, 0, st>>>(A + W * (o + o * lda), lda, static_cast<int>(nb),
+                                                                     uplo, trans, diag, full, ldf);
+        count_launch();
+        const size_t rows = left ? nb : m, cols = left ? n : nb;
+        int rc;
+        if constexpr (CX) {
+            rc = left ? complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, nb, n, nb, ar, ai, full, ldf, bl(o), ldb, T(0),
+                                            T(0), out, ldo, RB_PREC_PLAIN, st, ce)
+                      : complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, nb, nb, ar, ai, bl(o), ldb, full, ldf, T(0),
+                                            T(0), out, ldo, RB_PREC_PLAIN, st, ce);
+        } else {
+            rc = left ? gemm_colmajor_dev<T>(false, false, nb, n, nb, ar, full, ldf, bl(o), ldb, T(0), out, ldo,
+                                             RB_PREC_PLAIN, st, 0, ce)
+                      : gemm_colmajor_dev<T>(false, false, m, nb, nb, ar, bl(o), ldb, full, ldf, T(0), out, ldo,
+                                             RB_PREC_PLAIN, st, 0, ce);
+        }
+        if (rc != RB_OK) return rc;
+        const cudaError_t ce2 = cudaMemcpy2DAsync(bl(o), W * ldb * sizeof(T), out, W * ldo * sizeof(T),
+                                                  W * rows * sizeof(T), cols, cudaMemcpyDeviceToDevice, st);
+        return ce2 == cudaSuccess ? RB_OK : fail(ce2, ce);
+    };
+    std::function<int(size_t, size_t)> mul = [&](size_t o, size_t len) -> int {
+        const size_t nblk = (len + L - 1) / L;
+        if (nblk <= 1) return leaf(o, len);
+        const size_t h = (nblk / 2) * L, o2 = o + h, l2 = len - h;
+        // the half whose product reads the other half's old values goes first
+        const bool second_first = left ? !eff_upper : eff_upper;
+        int rc = second_first ? mul(o2, l2) : mul(o, h);
+        if (rc != RB_OK) return rc;
+        if (left)
+            rc = eff_upper ? add(h, l2, o, o2, bl(o2), bl(o)) : add(l2, h, o2, o, bl(o), bl(o2));
         else
-            rc = complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, n, n, ar, ai, B, ldb, full, ldf, T(0), T(0), out, ldo,
-                                     RB_PREC_PLAIN, st, ce);
-    } else {
-        if (side == RB_LEFT)
-            rc = gemm_colmajor_dev<T>(false, false, m, n, m, ar, full, ldf, B, ldb, T(0), out, ldo, RB_PREC_PLAIN, st,
-                                      0, ce);
-        else
-            rc = gemm_colmajor_dev<T>(false, false, m, n, n, ar, B, ldb, full, ldf, T(0), out, ldo, RB_PREC_PLAIN, st,
-                                      0, ce);
-    }
-    if (rc == RB_OK) {
-        e = cudaMemcpy2DAsync(B, W * ldb * sizeof(T), out, W * ldo * sizeof(T), W * m * sizeof(T), n,
-                              cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) rc = fail(e, ce);
-    }
+            rc = eff_upper ? add(h, l2, o, o2, bl(o), bl(o2)) : add(l2, h, o2, o, bl(o2), bl(o));
+        if (rc != RB_OK) return rc;
+        return second_first ? mul(o, h) : mul(o2, l2);
+    };
+    const int rc = mul(0, q);
     cudaFreeAsync(buf, st);
     return rc;
 }

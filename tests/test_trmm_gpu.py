@@ -72,6 +72,36 @@ def test_trmm_parity(dt, side, uplo, trans):
             assert np.array_equal(pad, b0.reshape(n, ldb).T[m:, :])  # rows beyond m untouched
 
 
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.complex128])
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("uplo", [0, 1])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+def test_trmm_recursive_parity(dt, side, uplo, trans):
+    """Order 1100 (two 512-row leaves and a ragged 76-row one): the halves
+    are multiplied by their diagonal blocks and the off-diagonal products
+    added in the order that reads each half before it changes."""
+    cx = np.issubdtype(np.dtype(dt), np.complexfloating)
+    if trans == 2 and not cx:
+        pytest.skip("ConjTrans == Trans for real types")
+    rng = np.random.default_rng(200 + side + 2 * uplo + 4 * trans)
+    q, nr = 1100, 40
+    m, n = (q, nr) if side == 0 else (nr, q)
+    for diag in (0, 1):
+        lda, ldb = q + 2, m + 3
+        a, mask = _tri(rng, q, lda, uplo, diag, dt)
+        b0 = (rng.standard_normal(ldb * n) + (1j * rng.standard_normal(ldb * n) if cx else 0)).astype(dt)
+        alpha = (0.75 - 0.5j) if cx else 0.75
+        b = b0.copy()
+        (complex3 if cx else level3).trmm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb)
+        B0 = b0.reshape(n, ldb).T[:m, :].astype(np.complex128 if cx else np.float64)
+        opA = _dense_op(a.astype(np.complex128 if cx else np.float64), lda, q, mask, diag, trans)
+        ref = alpha * (opA @ B0 if side == 0 else B0 @ opA)
+        got = b.reshape(n, ldb).T[:m, :]
+        den = abs(alpha) * np.linalg.norm(opA) * np.linalg.norm(B0)
+        assert np.linalg.norm(got.astype(np.complex128) - ref) <= 4 * q * _u(dt) * den, (diag,)
+        assert np.array_equal(b.reshape(n, ldb).T[m:, :], b0.reshape(n, ldb).T[m:, :])
+
+
 def test_trmm_known_answer_and_alpha_zero():
     a = np.array([1.0, 0.0, 2.0, 3.0])  # [[1, 2], [0, 3]] column-major, upper
     b = np.array([1.0, 0.0, 0.0, 1.0])
