@@ -415,6 +415,16 @@ int syrk_dev(int uplo, int trans, size_t n, size_t k, T alpha, const T* A, size_
 // ---------------------------------------------------------------------------
 // symm (real) and symm / hemm (complex)
 // ---------------------------------------------------------------------------
+template <typename T, bool CX>
+int sym_full_dev(int herm, int uplo, size_t q, const T* A, size_t lda, T* full, size_t ldf, cudaStream_t st,
+                 int32_t* ce) {
+    if (q == 0) return RB_OK;
+    sym_expand_kernel<T, CX><<<sym_grid(q), dim3(kSymTile, 8), 0, st>>>(A, lda, (int)q, uplo, herm, full, ldf);
+    count_launch();
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? RB_OK : fail(e, ce);
+}
+
 template <typename T>
 int symm_dev(int side, int uplo, size_t m, size_t n, T alpha, const T* A, size_t lda, const T* B,
              size_t ldb, T beta, T* C, size_t ldc, int prec, cudaStream_t st, int32_t* ce) {
@@ -424,10 +434,11 @@ int symm_dev(int side, int uplo, size_t m, size_t n, T alpha, const T* A, size_t
     void* full = nullptr;
     cudaError_t e = scratch_alloc(&full, ldf * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
-    sym_expand_kernel<T, false><<<sym_grid(q), dim3(kSymTile, 8), 0, st>>>(A, lda, (int)q, uplo, 0,
-                                                                           static_cast<T*>(full), ldf);
-    count_launch();
-    int rc;
+    int rc = sym_full_dev<T, false>(0, uplo, q, A, lda, static_cast<T*>(full), ldf, st, ce);
+    if (rc != RB_OK) {
+        cudaFreeAsync(full, st);
+        return rc;
+    }
     if (side == RB_LEFT)
         rc = gemm_colmajor_dev<T>(false, false, m, n, m, alpha, static_cast<T*>(full), ldf, B, ldb, beta, C,
                                   ldc, prec, st, 0, ce);
@@ -447,10 +458,11 @@ int hesy_dev(int herm, int side, int uplo, size_t m, size_t n, T ar, T ai, const
     void* full = nullptr;
     cudaError_t e = scratch_alloc(&full, 2 * q * q * sizeof(T), st);
     if (e != cudaSuccess) return fail(e, ce);
-    sym_expand_kernel<T, true><<<sym_grid(q), dim3(kSymTile, 8), 0, st>>>(A, lda, (int)q, uplo, herm,
-                                                                          static_cast<T*>(full), q);
-    count_launch();
-    int rc;
+    int rc = sym_full_dev<T, true>(herm, uplo, q, A, lda, static_cast<T*>(full), q, st, ce);
+    if (rc != RB_OK) {
+        cudaFreeAsync(full, st);
+        return rc;
+    }
     if (side == RB_LEFT)
         rc = complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, m, n, m, ar, ai, static_cast<T*>(full), q, B, ldb,
                                  br, bi, C, ldc, prec, st, ce);
@@ -685,6 +697,14 @@ template int syrk_dev<float>(int, int, size_t, size_t, float, const float*, size
                              cudaStream_t, int32_t*);
 template int syrk_dev<double>(int, int, size_t, size_t, double, const double*, size_t, double, double*,
                               size_t, cudaStream_t, int32_t*);
+template int sym_full_dev<float, false>(int, int, size_t, const float*, size_t, float*, size_t, cudaStream_t,
+                                        int32_t*);
+template int sym_full_dev<double, false>(int, int, size_t, const double*, size_t, double*, size_t, cudaStream_t,
+                                         int32_t*);
+template int sym_full_dev<float, true>(int, int, size_t, const float*, size_t, float*, size_t, cudaStream_t,
+                                       int32_t*);
+template int sym_full_dev<double, true>(int, int, size_t, const double*, size_t, double*, size_t, cudaStream_t,
+                                        int32_t*);
 template int symm_dev<float>(int, int, size_t, size_t, float, const float*, size_t, const float*, size_t,
                              float, float*, size_t, int, cudaStream_t, int32_t*);
 template int symm_dev<double>(int, int, size_t, size_t, double, const double*, size_t, const double*,

@@ -682,6 +682,111 @@ rb_status host_run(HostMat* mats, int nm, rb_error* err, F&& body) {
     return check_device_word(ctx, err);
 }
 
+// A Level-3 host call whose first matrix (the triangular or symmetric A) is
+// needed whole and whose other matrices (B, and C) split into independent
+// panels along `extent`: columns (by_cols) or rows. A is uploaded once and
+// `prologue(dA, ldA, stream, &cuda_err)` runs on it on the internal stream;
+// then each panel's slices of the other matrices are uploaded, computed by
+// `panel(dA, ldA, dev_ptrs, dev_lds, offset, length, stream, &cuda_err)`
+// (dev_ptrs at the panel's first row / column) and downloaded on a panel
+// stream of its own, so the copies of different panels overlap each other
+// and the kernels (uploads and downloads use separate copy engines);
+// `finish(stream)` runs on the internal stream after every panel. Calls
+// under 64 MB, or too narrow for two 256-wide panels, run whole through
+// host_run.
+template <typename Pro, typename Pan, typename Fin>
+rb_status host_run_split(HostMat* mats, int nm, bool by_cols, size_t extent, rb_error* err, Pro&& prologue,
+                         Pan&& panel, Fin&& finish) {
+    size_t total = 0;
+    for (int i = 0; i < nm; ++i)
+        total += mats[i].rows * mats[i].cols * mats[i].elem * ((mats[i].in ? 1 : 0) + (mats[i].out ? 1 : 0));
+    if (total < (size_t(64) << 20) || extent < 2 * 256) {
+        return host_run(mats, nm, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
+            int rc = prologue(d[0], ld[0], st, ce);
+            if (rc == RB_OK) rc = panel(d[0], ld[0], d + 1, ld + 1, size_t(0), extent, st, ce);
+            finish(st);
+            return rc;
+        });
+    }
+    cudaError_t e;
+    DeviceCtx* ctx = ctx_for_current(&e);
+    if (!ctx) return cuda_fail(err, e);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    void* dptr[3] = {nullptr, nullptr, nullptr};
+    size_t dld[3] = {0, 0, 0};
+    for (int i = 0; i < nm; ++i) {
+        const HostMat& h = mats[i];
+        const size_t per16 = (h.elem >= 16) ? 1 : 16 / h.elem;
+        dld[i] = std::max<size_t>((h.rows + per16 - 1) / per16 * per16, per16);
+        if ((e = ensure_buf(ctx, i, dld[i] * std::max<size_t>(h.cols, 1) * h.elem)) != cudaSuccess)
+            return cuda_fail(err, e);
+        dptr[i] = ctx->buf[i];
+    }
+    cudaStream_t st = ctx->stream;
+    const HostMat& a = mats[0];
+    e = cudaMemcpy2DAsync(dptr[0], dld[0] * a.elem, a.src, a.ld * a.elem, a.rows * a.elem, a.cols,
+                          cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(err, e);
+    int32_t ce = 0;
+    int rc = prologue(dptr[0], dld[0], st, &ce);
+    if (rc != RB_OK) {
+        finish(st);
+        cudaStreamSynchronize(st);
+        set_err(err, rc, 0, 0, 0, ce);
+        return static_cast<rb_status>(rc);
+    }
+    if ((e = cudaEventRecord(ctx->a_ready, st)) != cudaSuccess) return cuda_fail(err, e);
+    // the slice [off, off + len) of matrix i along the split, on the host and on the device
+    auto copy = [&](int i, size_t off, size_t len, bool up, cudaStream_t sp) -> cudaError_t {
+        const HostMat& h = mats[i];
+        const size_t el = h.elem;
+        uint8_t* dev = static_cast<uint8_t*>(dptr[i]) + (by_cols ? off * dld[i] : off) * el;
+        const size_t hoff = (by_cols ? off * h.ld : off) * el;
+        const size_t width = (by_cols ? h.rows : len) * el, height = by_cols ? len : h.cols;
+        if (up)
+            return cudaMemcpy2DAsync(dev, dld[i] * el, static_cast<const uint8_t*>(h.src) + hoff, h.ld * el, width,
+                                     height, cudaMemcpyHostToDevice, sp);
+        return cudaMemcpy2DAsync(static_cast<uint8_t*>(h.dst) + hoff, h.ld * el, dev, dld[i] * el, width, height,
+                                 cudaMemcpyDeviceToHost, sp);
+    };
+    const size_t width = std::max<size_t>(256, (extent + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
+    rb_status ps = RB_OK;
+    int used = 0;
+    for (size_t off = 0; off < extent && ps == RB_OK; off += width, ++used) {
+        const size_t len = std::min(width, extent - off);
+        cudaStream_t sp = ctx->pstream[used];
+        e = cudaStreamWaitEvent(sp, ctx->a_ready, 0);
+        for (int i = 1; i < nm && e == cudaSuccess; ++i)
+            if (mats[i].in) e = copy(i, off, len, true, sp);
+        if (e != cudaSuccess) {
+            ps = cuda_fail(err, e);
+            break;
+        }
+        void* pp[2] = {nullptr, nullptr};
+        for (int i = 1; i < nm; ++i)
+            pp[i - 1] = static_cast<uint8_t*>(dptr[i]) + (by_cols ? off * dld[i] : off) * mats[i].elem;
+        rc = panel(dptr[0], dld[0], pp, dld + 1, off, len, sp, &ce);
+        if (rc != RB_OK) {
+            set_err(err, rc, 0, 0, 0, ce);
+            ps = static_cast<rb_status>(rc);
+            break;
+        }
+        for (int i = 1; i < nm && e == cudaSuccess; ++i)
+            if (mats[i].out) e = copy(i, off, len, false, sp);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->pdone[used], sp);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->pdone[used], 0);
+        if (e != cudaSuccess) ps = cuda_fail(err, e);
+    }
+    if (ps != RB_OK) {
+        for (int i = 0; i < used + 1 && i < kHostPanels; ++i) cudaStreamSynchronize(ctx->pstream[i]);
+        finish(st);
+        cudaStreamSynchronize(st);
+        return ps;
+    }
+    finish(st);
+    return check_device_word(ctx, err);
+}
+
 bool valid_uplo(int v) { return v == RB_UPPER || v == RB_LOWER; }
 bool valid_side(int v) { return v == RB_LEFT || v == RB_RIGHT; }
 bool valid_diag(int v) { return v == RB_NON_UNIT || v == RB_UNIT; }
@@ -1048,18 +1153,45 @@ rb_status symm_host(int herm, rb_side side, rb_uplo uplo, size_t m, size_t n, T 
     if (m == 0 || n == 0) return RB_OK;
     const size_t el = (CX ? 2 : 1) * sizeof(T);
     const bool beta0 = (br == T(0) && (!CX || bi == T(0)));
+    const bool left = side == RB_LEFT;
     HostMat mats[3] = {{a, nullptr, q, q, lda, el, true, false},
                        {b, nullptr, m, n, ldb, el, true, false},
                        {c, c, m, n, ldc, el, !beta0, true}};
-    return host_run(mats, 3, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
-        if constexpr (CX)
-            return hesy_dev<T>(herm, side, uplo, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
-                               static_cast<const T*>(d[1]), ld[1], br, bi, static_cast<T*>(d[2]), ld[2], prec, st,
-                               ce);
-        else
-            return symm_dev<T>(side, uplo, m, n, ar, static_cast<const T*>(d[0]), ld[0],
-                               static_cast<const T*>(d[1]), ld[1], br, static_cast<T*>(d[2]), ld[2], prec, st, ce);
-    });
+    // the full operand is mirrored once; panels of B and C (columns for
+    // Left, rows for Right) are independent GEMMs against it
+    const size_t ldf = CX ? q : (q + 16 / sizeof(T) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
+    T* full = nullptr;
+    return host_run_split(
+        mats, 3, left, left ? n : m, err,
+        [&](void* dA, size_t ldA, cudaStream_t st, int32_t* ce) {
+            void* f = nullptr;
+            const cudaError_t e = scratch_alloc(&f, ldf * q * el, st);
+            if (e != cudaSuccess) {
+                if (ce) *ce = static_cast<int32_t>(e);
+                return static_cast<int>(e == cudaErrorMemoryAllocation ? RB_ERR_ALLOC : RB_ERR_CUDA);
+            }
+            full = static_cast<T*>(f);
+            return sym_full_dev<T, CX>(herm, uplo, q, static_cast<const T*>(dA), ldA, full, ldf, st, ce);
+        },
+        [&](void*, size_t, void** d, size_t* ld, size_t, size_t len, cudaStream_t sp, int32_t* ce) {
+            const T* B = static_cast<const T*>(d[0]);
+            T* C = static_cast<T*>(d[1]);
+            const size_t pm = left ? m : len, pn = left ? len : n;
+            if constexpr (CX) {
+                return left ? complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, pm, pn, q, ar, ai, full, ldf, B, ld[0], br,
+                                                  bi, C, ld[1], prec, sp, ce)
+                            : complex_gemm_dev<T>(RB_NO_TRANS, RB_NO_TRANS, pm, pn, q, ar, ai, B, ld[0], full, ldf, br,
+                                                  bi, C, ld[1], prec, sp, ce);
+            } else {
+                return left ? gemm_colmajor_dev<T>(false, false, pm, pn, q, ar, full, ldf, B, ld[0], br, C, ld[1],
+                                                   prec, sp, 0, ce)
+                            : gemm_colmajor_dev<T>(false, false, pm, pn, q, ar, B, ld[0], full, ldf, br, C, ld[1],
+                                                   prec, sp, 0, ce);
+            }
+        },
+        [&](cudaStream_t st) {
+            if (full) cudaFreeAsync(full, st);
+        });
 }
 
 template <typename T, bool CX>
@@ -1073,11 +1205,16 @@ rb_status trsm_host(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag
     if ((s = check_matrix(RB_COL_MAJOR, 'b', m, n, ldb, b_len, true, err))) return s;
     if (m == 0 || n == 0) return RB_OK;
     const size_t el = (CX ? 2 : 1) * sizeof(T);
+    const bool left = side == RB_LEFT;
     HostMat mats[2] = {{a, nullptr, q, q, lda, el, true, false}, {b, b, m, n, ldb, el, true, true}};
-    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
-        return trsm_dev<T, CX>(side, uplo, trans, diag, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
-                               static_cast<T*>(d[1]), ld[1], st, ce);
-    });
+    // columns of B (Left) or rows (Right) are independent solves
+    return host_run_split(
+        mats, 2, left, left ? n : m, err, [](void*, size_t, cudaStream_t, int32_t*) { return static_cast<int>(RB_OK); },
+        [&](void* dA, size_t ldA, void** d, size_t* ld, size_t, size_t len, cudaStream_t sp, int32_t* ce) {
+            return trsm_dev<T, CX>(side, uplo, trans, diag, left ? m : len, left ? len : n, ar, ai,
+                                   static_cast<const T*>(dA), ldA, static_cast<T*>(d[0]), ld[0], sp, ce);
+        },
+        [](cudaStream_t) {});
 }
 
 // trmm: no rblas counterpart (its README lists trmm as remaining Level 3);
@@ -1093,11 +1230,16 @@ rb_status trmm_host(rb_side side, rb_uplo uplo, rb_transpose trans, rb_diag diag
     if ((s = check_matrix(RB_COL_MAJOR, 'b', m, n, ldb, b_len, true, err))) return s;
     if (m == 0 || n == 0) return RB_OK;
     const size_t el = (CX ? 2 : 1) * sizeof(T);
+    const bool left = side == RB_LEFT;
     HostMat mats[2] = {{a, nullptr, q, q, lda, el, true, false}, {b, b, m, n, ldb, el, true, true}};
-    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
-        return trmm_dev<T, CX>(side, uplo, trans, diag, m, n, ar, ai, static_cast<const T*>(d[0]), ld[0],
-                               static_cast<T*>(d[1]), ld[1], st, ce);
-    });
+    // columns of B (Left) or rows (Right) are independent products
+    return host_run_split(
+        mats, 2, left, left ? n : m, err, [](void*, size_t, cudaStream_t, int32_t*) { return static_cast<int>(RB_OK); },
+        [&](void* dA, size_t ldA, void** d, size_t* ld, size_t, size_t len, cudaStream_t sp, int32_t* ce) {
+            return trmm_dev<T, CX>(side, uplo, trans, diag, left ? m : len, left ? len : n, ar, ai,
+                                   static_cast<const T*>(dA), ldA, static_cast<T*>(d[0]), ld[0], sp, ce);
+        },
+        [](cudaStream_t) {});
 }
 
 rb_status dev_status(int rc, int32_t ce, rb_error* err) {

@@ -138,6 +138,18 @@ def trsm(side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
     _lib.check(st, err)
 
 
+def trsm_dev(side, uplo, trans, diag, m, n, alpha, a_ptr, lda, b_ptr, ldb, stream=0):
+    """f64 trsm on device pointers (rb_dtrsm_dev), in place of B; enqueued
+    on `stream`, no synchronisation."""
+    from .types import Diag, Side, Uplo
+    lib = _lib.load()
+    err = _lib.RbError()
+    st = lib.rb_dtrsm_dev(int(Side(side)), int(Uplo(uplo)), int(Transpose(trans)), int(Diag(diag)), m, n, alpha,
+                          C.c_void_p(a_ptr), lda, C.c_void_p(b_ptr), ldb, C.c_void_p(stream) if stream else None,
+                          C.byref(err))
+    _lib.check(st, err)
+
+
 def trsm_batched_dev(side, uplo, trans, diag, m, n, alpha, a_ptr, lda, stride_a, b_ptr, ldb, stride_b,
                      batch, dtype, stream=0):
     """Batched trsm on device pointers (rb_?trsm_batched_dev): problem i is
