@@ -399,20 +399,6 @@ int complex_gemm_dev(int transa, int transb, size_t m, size_t n, size_t k, T ar,
 }
 
 // ---------------------------------------------------------------------------
-// syrk
-// ---------------------------------------------------------------------------
-template <typename T>
-int syrk_dev(int uplo, int trans, size_t n, size_t k, T alpha, const T* A, size_t lda, T beta, T* C,
-             size_t ldc, cudaStream_t st, int32_t* ce) {
-    if (n == 0) return RB_OK;
-    const int tri = (uplo == RB_UPPER) ? 1 : 2;
-    const bool t = trans != RB_NO_TRANS;
-    // C = alpha * op(A) op(A)^T: (None, Trans) for A stored n x k, (Trans, None) for k x n
-    return gemm_colmajor_dev<T>(t, !t, n, n, k, alpha, A, lda, A, lda, beta, C, ldc, RB_PREC_PLAIN, st,
-                                tri, ce);
-}
-
-// ---------------------------------------------------------------------------
 // symm (real) and symm / hemm (complex)
 // ---------------------------------------------------------------------------
 template <typename T, bool CX>
@@ -693,10 +679,6 @@ template int complex_gemm_dev<float>(int, int, size_t, size_t, size_t, float, fl
 template int complex_gemm_dev<double>(int, int, size_t, size_t, size_t, double, double, const double*, size_t,
                                       const double*, size_t, double, double, double*, size_t, int,
                                       cudaStream_t, int32_t*);
-template int syrk_dev<float>(int, int, size_t, size_t, float, const float*, size_t, float, float*, size_t,
-                             cudaStream_t, int32_t*);
-template int syrk_dev<double>(int, int, size_t, size_t, double, const double*, size_t, double, double*,
-                              size_t, cudaStream_t, int32_t*);
 template int sym_full_dev<float, false>(int, int, size_t, const float*, size_t, float*, size_t, cudaStream_t,
                                         int32_t*);
 template int sym_full_dev<double, false>(int, int, size_t, const double*, size_t, double*, size_t, cudaStream_t,

@@ -1130,13 +1130,31 @@ rb_status syrk_host(rb_uplo uplo, rb_transpose trans, size_t n, size_t k, T alph
     if ((s = check_matrix(RB_COL_MAJOR, 'a', t ? k : n, t ? n : k, lda, a_len, true, err))) return s;
     if ((s = check_matrix(RB_COL_MAJOR, 'c', n, n, ldc, c_len, true, err))) return s;
     if (n == 0) return RB_OK;
-    // the other triangle of C is preserved, so C is always staged in
+    // the other triangle of C is preserved, so C is always staged in. Column
+    // panels of C are independent: panel [j0, j0 + len) of the lower triangle
+    // is rows j0.. (one triangle-masked product whose origin is on the
+    // diagonal); of the upper, rows ..j0 (a plain product) above the masked
+    // diagonal block.
     HostMat mats[2] = {{a, nullptr, t ? k : n, t ? n : k, lda, sizeof(T), k > 0, false},
                        {c, c, n, n, ldc, sizeof(T), true, true}};
-    return host_run(mats, 2, err, [&](void** d, size_t* ld, cudaStream_t st, int32_t* ce) {
-        return syrk_dev<T>(uplo, trans, n, k, alpha, static_cast<const T*>(d[0]), ld[0], beta,
-                           static_cast<T*>(d[1]), ld[1], st, ce);
-    });
+    return host_run_split(
+        mats, 2, true, n, err, [](void*, size_t, cudaStream_t, int32_t*) { return static_cast<int>(RB_OK); },
+        [&](void* dA, size_t ldA, void** d, size_t* ld, size_t j0, size_t len, cudaStream_t sp, int32_t* ce) {
+            const T* A = static_cast<const T*>(dA);
+            auto rows = [&](size_t r) { return t ? A + r * ldA : A + r; };  // op(A) from row r
+            T* Cp = static_cast<T*>(d[0]);                                  // C(0, j0)
+            if (uplo == RB_LOWER)
+                return gemm_colmajor_dev<T>(t, !t, n - j0, len, k, alpha, rows(j0), ldA, rows(j0), ldA, beta, Cp + j0,
+                                            ld[0], RB_PREC_PLAIN, sp, 2, ce);
+            if (j0 > 0) {
+                const int rc = gemm_colmajor_dev<T>(t, !t, j0, len, k, alpha, rows(0), ldA, rows(j0), ldA, beta, Cp,
+                                                    ld[0], RB_PREC_PLAIN, sp, 0, ce);
+                if (rc != RB_OK) return rc;
+            }
+            return gemm_colmajor_dev<T>(t, !t, len, len, k, alpha, rows(j0), ldA, rows(j0), ldA, beta, Cp + j0, ld[0],
+                                        RB_PREC_PLAIN, sp, 1, ce);
+        },
+        [](cudaStream_t) {});
 }
 
 template <typename T, bool CX>

@@ -162,9 +162,6 @@ template <typename T>
 int complex_gemm_dev(int transa, int transb, size_t m, size_t n, size_t k, T ar, T ai, const T* A,
                      size_t lda, const T* B, size_t ldb, T br, T bi, T* C, size_t ldc, int prec,
                      cudaStream_t st, int32_t* ce);
-template <typename T>
-int syrk_dev(int uplo, int trans, size_t n, size_t k, T alpha, const T* A, size_t lda, T beta, T* C,
-             size_t ldc, cudaStream_t st, int32_t* ce);
 // The full q x q operand of symm / hemm (ld = ldf) from the uplo triangle of A
 // (complex: interleaved; herm: conjugate mirror and real diagonal).
 template <typename T, bool CX>

@@ -1,8 +1,9 @@
-"""GPU tests of the pipelined host path of symm / hemm, trsm and trmm: calls
+"""GPU tests of the pipelined host path of symm / hemm, syrk, trsm and trmm: calls
 of at least 64 MB upload A once and run independent panels of B (and C) --
 columns for side Left, rows for Right -- on their own streams. Checked
 against dense float64 / complex128 numpy evaluations: symm and trmm within
-the normwise bound 4*q*u of |alpha| ||op(A)|| ||B|| (+ |beta| ||C||), trsm by
+the normwise bound 4*q*u of |alpha| ||op(A)|| ||B|| (+ |beta| ||C||), syrk
+within 4*k*u of |alpha| ||A||^2 + |beta| ||C_tri||, trsm by
 the normwise backward error ||op(A) X - alpha B|| / (||A_tri|| ||X|| +
 |alpha| ||B||) within 4*q*u, and for the real trsm / trmm also against the
 device-pointer call on the same operands (which runs unsplit). Padded
@@ -116,4 +117,30 @@ def test_symm_host_panels(dt, side, m, n, beta):
     den = abs(alpha) * np.linalg.norm(opS) * np.linalg.norm(Bm) + abs(beta) * np.linalg.norm(C0[:m, :])
     assert np.linalg.norm(c[:m, :] - ref) <= 4 * q * _u(dt) * den
     assert np.array_equal(c[m:, :], C0[m:, :])
+    assert rb.device_error()[0] == 0
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("uplo", [0, 1])
+@pytest.mark.parametrize("trans", [0, 1])
+def test_syrk_host_panels(dt, uplo, trans):
+    """Column panels of C: the lower triangle's panel is one masked product
+    from the diagonal down, the upper's a plain product above a masked
+    diagonal block; the other triangle comes back unchanged."""
+    rng = np.random.default_rng(600 + 2 * uplo + trans)
+    n, k = 3000, 1000
+    ar, ac = (k, n) if trans else (n, k)
+    lda, ldc = ar + 1, n + 2
+    A = np.asfortranarray(rng.uniform(-1, 1, (lda, ac)).astype(dt))
+    C0 = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)).astype(dt))
+    c = C0.copy(order="F")
+    level3.syrk(uplo, trans, n, k, 1.5, A.reshape(-1, order="F"), lda, -0.5, c.reshape(-1, order="F"), ldc)
+    opA = (A[:ar, :].T if trans else A[:ar, :]).astype(np.float64)
+    ref = 1.5 * opA @ opA.T - 0.5 * C0[:n, :].astype(np.float64)
+    mask = np.triu(np.ones((n, n), bool)) if uplo == 0 else np.tril(np.ones((n, n), bool))
+    got = c[:n, :]
+    assert np.array_equal(got[~mask], C0[:n, :][~mask]), "other triangle modified"
+    assert np.array_equal(c[n:, :], C0[n:, :])
+    den = 1.5 * np.linalg.norm(opA) ** 2 + 0.5 * np.linalg.norm(C0[:n, :][mask])
+    assert np.linalg.norm(got[mask].astype(np.float64) - ref[mask]) <= 4 * k * _u(dt) * den
     assert rb.device_error()[0] == 0
