@@ -180,7 +180,8 @@ constexpr int kMaxDevices = 64;
 
 // Per-device state for host-slice calls: an internal stream, grow-only
 // staging buffers for A, B, C, and the device error word.
-constexpr int kHostPanels = 8;  // column panels of a large host-slice GEMM
+constexpr int kHostSplit = 8;                   // panels of a large host-slice call, by width
+constexpr int kHostPanels = kHostSplit + 1;     // the last one split in two
 
 struct DeviceCtx {
     std::mutex mu;
@@ -227,6 +228,24 @@ DeviceCtx* ctx_for_current(cudaError_t* e) {
     }
     *e = cudaSuccess;
     return &c;
+}
+
+// Panels of a pipelined host call along `extent`: widths of a multiple of
+// 256 (every kernel's tile width divides 256, and offsets stay 16-byte
+// aligned) giving at most kHostSplit panels; the last one, when at least 512
+// wide, is split in two, so the GEMM and download that wait behind the last
+// upload are half as long. Returns the number of panels.
+int panel_plan(size_t extent, size_t* lens) {
+    const size_t width = std::max<size_t>(256, (extent + kHostSplit * 256 - 1) / (kHostSplit * 256) * 256);
+    int np = 0;
+    for (size_t off = 0; off < extent; off += lens[np++]) lens[np] = std::min(width, extent - off);
+    if (np > 0 && np < kHostPanels && lens[np - 1] >= 512) {
+        const size_t first = (lens[np - 1] / 2 + 255) / 256 * 256;
+        lens[np] = lens[np - 1] - first;
+        lens[np - 1] = first;
+        ++np;
+    }
+    return np;
 }
 
 cudaError_t ensure_buf(DeviceCtx* c, int slot, size_t bytes) {
@@ -518,8 +537,8 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
     // download overlap the others' (host-to-device and device-to-host copies
     // use separate engines). Every element of C is computed from the same
     // operands in the same order as in one whole call, so results are the
-    // same bit for bit. Panels are multiples of 256 columns (every kernel's
-    // tile width divides 256, and the offsets stay 16-byte aligned).
+    // same bit for bit. Panels start at multiples of 256 columns
+    // (panel_plan).
     const size_t el = sizeof(T);
     const size_t total_bytes = (need_ab ? (a_rows * a_cols + b_rows * b_cols) * el : 0) +
                                p.m * p.n * el * (read_c ? 2 : 1);
@@ -530,7 +549,8 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
     const bool whole_call = prec == RB_PREC_PLAIN &&
                             (plain_split(p, &whole) || (sizeof(T) == 4 && simt_narrow_f32(p.m, p.n)));
     if (total_bytes >= (size_t(64) << 20) && p.n >= 2 * 256 && !whole_call) {
-        const size_t width = std::max<size_t>(256, (p.n + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
+        size_t lens[kHostPanels];
+        const int np = panel_plan(p.n, lens);
         if (need_ab) {
             e = cudaMemcpy2DAsync(dA, lda_d * el, p.a, p.lda * el, a_rows * el, a_cols, cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) return cuda_fail(err, e);
@@ -538,8 +558,8 @@ rb_status host_gemm(rb_layout layout, rb_transpose transa, rb_transpose transb, 
         if ((e = cudaEventRecord(ctx->a_ready, st)) != cudaSuccess) return cuda_fail(err, e);
         rb_status ps = RB_OK;
         int used = 0;
-        for (size_t j0 = 0; j0 < p.n && ps == RB_OK; j0 += width, ++used) {
-            const size_t jn = std::min(width, p.n - j0);
+        for (size_t j0 = 0; used < np && ps == RB_OK; j0 += lens[used], ++used) {
+            const size_t jn = lens[used];
             cudaStream_t sp = ctx->pstream[used];
             e = cudaStreamWaitEvent(sp, ctx->a_ready, 0);
             if (e == cudaSuccess && need_ab) {
@@ -749,11 +769,12 @@ rb_status host_run_split(HostMat* mats, int nm, bool by_cols, size_t extent, rb_
         return cudaMemcpy2DAsync(static_cast<uint8_t*>(h.dst) + hoff, h.ld * el, dev, dld[i] * el, width, height,
                                  cudaMemcpyDeviceToHost, sp);
     };
-    const size_t width = std::max<size_t>(256, (extent + kHostPanels * 256 - 1) / (kHostPanels * 256) * 256);
+    size_t lens[kHostPanels];
+    const int np = panel_plan(extent, lens);
     rb_status ps = RB_OK;
     int used = 0;
-    for (size_t off = 0; off < extent && ps == RB_OK; off += width, ++used) {
-        const size_t len = std::min(width, extent - off);
+    for (size_t off = 0; used < np && ps == RB_OK; off += lens[used], ++used) {
+        const size_t len = lens[used];
         cudaStream_t sp = ctx->pstream[used];
         e = cudaStreamWaitEvent(sp, ctx->a_ready, 0);
         for (int i = 1; i < nm && e == cudaSuccess; ++i)
