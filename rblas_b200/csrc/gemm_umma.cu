@@ -369,6 +369,282 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------
+// 3xBF16 with A split inside the GEMM (A rows contiguous: NoTrans).
+//
+// Two passes read A, write its hi / lo planes and read the planes again:
+// about three times A's bytes, which is most of the time of a tall-skinny
+// product (65536 x 128 x 8192: A is 2.1 GB, the GEMM itself ~0.3 ms of
+// tensor work). Here TMA brings 128 x 64 f32 tiles of A (128 contiguous rows
+// per K column) into shared memory, and the four epilogue warps split them,
+// between their accumulator promotions, into the hi / lo planes in the
+// 128-byte-swizzled K-major layout the UMMA descriptors read: row r's 16-byte
+// chunk c at r * 128 + ((c ^ (r & 7)) * 16), the layout a TMA load of the
+// planes produces. The split is the split pass's (hi = rn(x), lo = rn(x -
+// hi)) and the products, their order and the promotions are
+// umma_gemm_kernel<kModeBf16x3>'s, so the results are the two-pass form's bit
+// for bit. B's planes come from the split pass (B is small). Rings: A's f32
+// tiles (released once split), A's planes (released by the MMAs), B's planes.
+// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..5 splitter and
+// epilogue (tile row quarter * 32 + lane in both roles).
+// ------------------------------------------------------------------------------
+constexpr int kFzF32Stages = 3, kFzPlaneStages = 2, kFzBStages = 2;
+constexpr int kFzF32Tile = kUM * 64 * 4;         // 64 K columns of 128 f32 rows: 32 KiB
+constexpr int kFzPlanes = 2 * kATile;            // hi and lo planes of one 128 x 64 tile: 32 KiB
+constexpr int kFzSmem = kFzF32Stages * kFzF32Tile + (kFzPlaneStages + kFzBStages) * kFzPlanes + 256 + 1024;
+static_assert(kFzSmem <= 232448, "the fused kernel's rings must fit one CTA's shared memory");
+
+struct FzBar {
+    uint64_t f_full[kFzF32Stages], f_empty[kFzF32Stages];
+    uint64_t a_full[kFzPlaneStages], a_empty[kFzPlaneStages];
+    uint64_t b_full[kFzBStages], b_empty[kFzBStages];
+    uint64_t acc_full[2], acc_empty[2], drain;
+    uint32_t tmem_base;
+};
+static_assert(sizeof(FzBar) <= 256, "the fused kernel reserves 256 bytes of shared memory for its barriers");
+
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo_elem, __nv_bfloat16 hi_elem) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(lo_elem)) |
+           (static_cast<uint32_t>(__bfloat16_as_ushort(hi_elem)) << 16);
+}
+
+__global__ void __launch_bounds__(192, 1)
+    umma_bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
+                             const __grid_constant__ UParams p) {
+    using Cfg = UCfg<kModeBf16x3>;
+    constexpr int UN = Cfg::UN;
+    constexpr int FS = kFzF32Stages, PS = kFzPlaneStages, BS = kFzBStages;
+    constexpr int KSTEPS = 4;
+    constexpr uint32_t IDESC = umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
+    constexpr uint32_t TMEM_COLS = 2 * UN;
+    static_assert(UN * kRowBytes == kATile, "B plane tiles are as large as A's");
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint8_t* f32s = smem;                        // FS x 32 KiB, [k][row] f32
+    uint8_t* aps = f32s + FS * kFzF32Tile;       // PS x (hi, lo), swizzled K-major
+    uint8_t* bps = aps + PS * kFzPlanes;         // BS x (hi, lo), by TMA
+    FzBar* bar = reinterpret_cast<FzBar*>(bps + BS * kFzPlanes);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < FS; ++s) {
+            mbar_init(&bar->f_full[s], 1);
+            mbar_init(&bar->f_empty[s], 4);
+        }
+        for (int s = 0; s < PS; ++s) {
+            mbar_init(&bar->a_full[s], 4);
+            mbar_init(&bar->a_empty[s], 1);
+        }
+        for (int s = 0; s < BS; ++s) {
+            mbar_init(&bar->b_full[s], 1);
+            mbar_init(&bar->b_empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&bar->acc_full[b], 1);
+            mbar_init(&bar->acc_empty[b], 4);
+        }
+        mbar_init(&bar->drain, 1);
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&bar->tmem_base, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bar->tmem_base;
+    const int items = p.num_tiles;
+    uint32_t* const err = p.err;
+    bool ok = true;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------ TMA producer ------------------------------
+        prefetch_tmap(&tmA32);
+        prefetch_tmap(&tmB);
+        uint32_t nf = 0, nb = 0;  // f32 tiles and B plane tiles issued
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            int tm, tn;
+            raster_tile(item, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * UN;
+            for (int kt = 0; kt < p.num_kt; ++kt) {
+                const int fs = nf % FS;
+                if (nf >= FS && !mbar_wait(&bar->f_empty[fs], ((nf / FS) - 1) & 1, err, 0x211)) {
+                    ok = false;
+                    break;
+                }
+                mbar_arrive_expect_tx(&bar->f_full[fs], kFzF32Tile);
+                tma_load_2d(f32s + fs * kFzF32Tile, &tmA32, &bar->f_full[fs], m0, kt * 64);
+                ++nf;
+                const int bs = nb % BS;
+                if (nb >= BS && !mbar_wait(&bar->b_empty[bs], ((nb / BS) - 1) & 1, err, 0x212)) {
+                    ok = false;
+                    break;
+                }
+                mbar_arrive_expect_tx(&bar->b_full[bs], kFzPlanes);
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    tma_load_3d(bps + bs * kFzPlanes + q * kATile, &tmB, &bar->b_full[bs], kt * 64, n0, q);
+                ++nb;
+            }
+        }
+        if (!ok) {  // this CTA's copies land before it exits
+            for (uint32_t j = nf > (uint32_t)FS ? nf - FS : 0; j < nf; ++j)
+                mbar_wait_drain(&bar->f_full[j % FS], (j / FS) & 1);
+            for (uint32_t j = nb > (uint32_t)BS ? nb - BS : 0; j < nb; ++j)
+                mbar_wait_drain(&bar->b_full[j % BS], (j / BS) & 1);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------ MMA issuer ------------------------------
+        uint32_t it = 0, uc = 0;
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            for (int u = 0; ok && u < p.kchunks; ++u, ++uc) {
+                const int kt0 = u * p.kt_per_chunk, kt1 = min(p.num_kt, kt0 + p.kt_per_chunk);
+                const uint32_t b = uc & 1;
+                if (uc >= 2 && !mbar_wait(&bar->acc_empty[b], ((uc >> 1) - 1) & 1, err, 0x213)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + b * UN;
+                uint32_t accumulate = 0;
+                for (int kt = kt0; kt < kt1; ++kt, ++it) {
+                    const int ps = it % PS, bs = it % BS;
+                    if (!mbar_wait(&bar->a_full[ps], (it / PS) & 1, err, 0x214) ||
+                        !mbar_wait(&bar->b_full[bs], (it / BS) & 1, err, 0x215)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(aps + ps * kFzPlanes);
+                    const uint32_t sb = smem_u32(bps + bs * kFzPlanes);
+#pragma unroll
+                    for (int kk = 0; kk < KSTEPS; ++kk) {
+#pragma unroll
+                        for (int q = 0; q < Cfg::NPROD; ++q)
+                            umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
+                                     sw128_kmajor_desc(sb + Cfg::pb(q) * kATile) + 2 * kk, IDESC,
+                                     q == 0 ? accumulate : 1u);
+                        accumulate = 1;
+                    }
+                    tc_commit(&bar->a_empty[ps]);  // plane stages free once these MMAs complete
+                    tc_commit(&bar->b_empty[bs]);
+                }
+                if (ok) tc_commit(&bar->acc_full[b]);
+            }
+        }
+        tc_commit(&bar->drain);
+        mbar_wait_drain(&bar->drain, 0);
+    } else if (warp >= 2) {
+        // ------------------------- splitter and epilogue -------------------------
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;  // tile row: TMEM lane and split row
+        uint32_t it = 0, uc = 0;
+        for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
+            int tm, tn;
+            raster_tile(item, p.tiles_m, p.tiles_n, tm, tn);
+            const int m0 = tm * kUM, n0 = tn * UN;
+            const int r = m0 + row;
+            const bool row_ok = r < p.m;
+            float sum[UN];
+#pragma unroll
+            for (int j = 0; j < UN; ++j) sum[j] = 0.f;
+            int promoted = 0;
+            // add unit `promoted`'s FP32 partial (TMEM) into sum, as umma_body does
+            auto promote = [&]() -> bool {
+                const uint32_t b = uc & 1;
+                if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, err, 0x216)) return false;
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+#pragma unroll
+                for (int ch = 0; ch < UN / 32; ++ch) {
+                    uint32_t v[32];
+                    tmem_ld32(taddr + ch * 32, v);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->acc_empty[b]);
+                ++uc;
+                ++promoted;
+                return true;
+            };
+            for (int kt = 0; kt < p.num_kt; ++kt, ++it) {
+                const int fs = it % FS, ps = it % PS;
+                if ((it >= PS && !mbar_wait(&bar->a_empty[ps], ((it / PS) - 1) & 1, err, 0x217)) ||
+                    !mbar_wait(&bar->f_full[fs], (it / FS) & 1, err, 0x218)) {
+                    ok = false;
+                    break;
+                }
+                const float* F = reinterpret_cast<const float*>(f32s + fs * kFzF32Tile);  // F[k * 128 + row]
+                uint8_t* hi = aps + ps * kFzPlanes;
+                uint8_t* lo = hi + kATile;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    uint32_t h[4], l[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float v0 = F[(c * 8 + 2 * j) * kUM + row], v1 = F[(c * 8 + 2 * j + 1) * kUM + row];
+                        const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+                        h[j] = pack_bf16x2(h0, h1);
+                        l[j] = pack_bf16x2(__float2bfloat16_rn(v0 - __bfloat162float(h0)),
+                                           __float2bfloat16_rn(v1 - __bfloat162float(h1)));
+                    }
+                    const uint32_t off = static_cast<uint32_t>(row) * kRowBytes + ((c ^ (row & 7)) << 4);
+                    *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+                }
+                fence_proxy_async_smem();  // the planes' generic stores, visible to the tensor cores
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&bar->a_full[ps]);
+                    mbar_arrive(&bar->f_empty[fs]);
+                }
+                // once unit u's last tile is split, unit u - 1 is promoted: the
+                // MMAs of unit u + 1 wait for that buffer, and the split of
+                // unit u + 1's tiles waits for unit u's MMAs
+                if ((kt + 1) % p.kt_per_chunk == 0 || kt + 1 == p.num_kt) {
+                    if (kt / p.kt_per_chunk >= 1 && !promote()) {
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+            while (ok && promoted < p.kchunks)
+                if (!promote()) ok = false;
+            if (ok && row_ok) {
+#pragma unroll
+                for (int g = 0; g < UN / 16; ++g) {
+                    float cv[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int col = n0 + g * 16 + jj;
+                        cv[jj] = (p.beta_mode != 0 && col < p.n) ? p.cin[r + static_cast<size_t>(col) * p.ldc] : 0.f;
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int col = n0 + g * 16 + jj;
+                        if (col < p.n) {
+                            const float tb = (p.beta_mode == 2) ? p.beta_f * cv[jj] : cv[jj];
+                            p.c[r + static_cast<size_t>(col) * p.ldc] = fmaf(p.alpha_f, sum[g * 16 + jj], tb);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------------------
 // Ozaki GEMM kernel.
 //
 // Slice products of equal weight (t + u = d: digit t has weight 2^-(7+8t))
@@ -1436,12 +1712,44 @@ static void operand_views(bool ta, bool tb, size_t lda, size_t ldb, size_t& ars,
     if (!tb) { brs = ldb; bps = 1; } else { brs = 1; bps = ldb; }
 }
 
+// 3xBF16 splits A inside the GEMM (umma_bf16x3_fused_kernel) when A's rows
+// are contiguous (NoTrans, 16-byte aligned base and column stride) and C has
+// at most two 128-wide column tiles, so the f32 tiles TMA brings are read
+// about once: there the split pass's read and write of A cost more than the
+// GEMM. Wider products keep the two passes (their GEMM is compute-bound and
+// the deeper plane ring of the two-pass kernel feeds it better).
+bool bf16x3_fused_a(bool ta, int n, const float* A, size_t lda) {
+    return !ta && n <= 256 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda & 3) == 0;
+}
+
+cudaError_t launch_bf16x3_fused(const CUtensorMap& ta32, const CUtensorMap& tb, const UParams& p, cudaStream_t st) {
+    auto kern = umma_bf16x3_fused_kernel;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kFzSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = p.num_tiles < sms ? p.num_tiles : sms;
+    KernelTimer tm;
+    kernel_timing_begin("umma_bf16x3", 2.0 * p.m * p.n * static_cast<double>(p.k) * UCfg<kModeBf16x3>::NPROD, st,
+                        &tm);
+    kern<<<grid, 192, kFzSmem, st>>>(ta32, tb, p);
+    kernel_timing_end(&tm, st);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, int k, float alpha,
                                    const float* A, size_t lda, const float* B, size_t ldb, float beta,
                                    float* C, size_t ldc, cudaStream_t st, CUresult* cu_err) {
     constexpr int UN = 128;
+    const bool fused = planes == 2 && bf16x3_fused_a(ta, n, A, lda);
     const size_t kp = round_up(static_cast<size_t>(k), 8);  // 16-byte rows of bf16
-    const size_t pa = static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
+    const size_t pa = fused ? 0 : static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
     void* buf = nullptr;
     const size_t a_bytes = round_up(planes * pa * sizeof(__nv_bfloat16), 256);
     cudaError_t e = scratch_alloc(&buf, a_bytes + planes * pb * sizeof(__nv_bfloat16), st);
@@ -1452,11 +1760,17 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     operand_views(ta, tb, lda, ldb, ars, aps, brs, bps);
     const dim3 ga((k + kTile - 1) / kTile, (m + kTile - 1) / kTile);
     const dim3 gb((k + kTile - 1) / kTile, (n + kTile - 1) / kTile);
-    bf16_split_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, planes, sa, kp, pa);
+    if (!fused) {
+        bf16_split_kernel<<<ga, 256, 0, st>>>(A, ars, aps, m, k, planes, sa, kp, pa);
+        count_launch();
+    }
     bf16_split_kernel<<<gb, 256, 0, st>>>(B, brs, bps, n, k, planes, sb, kp, pb);
-    count_launch(2);
+    count_launch();
     CUtensorMap tma, tmb;
-    CUresult r = make_tmap_planes(&tma, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, m, planes, kp, kUM);
+    // fused: A itself as an m x k f32 tensor, 128-row x 64-column boxes
+    CUresult r = fused ? make_tmap_2d(&tma, A, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), m, k, lda, kUM, 64,
+                                      false)
+                       : make_tmap_planes(&tma, sa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, m, planes, kp, kUM);
     if (r == CUDA_SUCCESS) r = make_tmap_planes(&tmb, sb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, k, n, planes, kp, UN);
     if (r != CUDA_SUCCESS) {
         if (cu_err) *cu_err = r;
@@ -1476,7 +1790,8 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     p.c = C; p.ldc = ldc;
     p.cin = C;
     p.err = device_error_word();
-    e = (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
+    e = fused ? launch_bf16x3_fused(tma, tmb, p, st)
+              : (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
     cudaFreeAsync(buf, st);
     return e;
 }
