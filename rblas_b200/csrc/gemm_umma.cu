@@ -384,10 +384,17 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // umma_gemm_kernel<kModeBf16x3>'s, so the results are the two-pass form's bit
 // for bit. B's planes come from the split pass (B is small). Rings: A's f32
 // tiles (released once split), A's planes (released by the MMAs), B's planes.
-// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..5 splitter and
-// epilogue (tile row quarter * 32 + lane in both roles).
+// Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 splitter and
+// epilogue: tile row quarter * 32 + lane (quarter = warp % 4, the TMEM lane
+// quarter the warp may read) in both roles, and one half of the tile -- K
+// chunks 4h..4h+3 of each 64-column K tile to split, columns 64h..64h+63 to
+// promote and write -- for h = (warp - 2) / 4. Two such warps per scheduler
+// hide each other's latencies, and 64 running sums per thread leave
+// registers for the split.
 // ------------------------------------------------------------------------------
 constexpr int kFzF32Stages = 3, kFzPlaneStages = 2, kFzBStages = 2;
+constexpr int kFzThreads = 320;
+constexpr int kFzEpiWarps = 8;
 constexpr int kFzF32Tile = kUM * 64 * 4;         // 64 K columns of 128 f32 rows: 32 KiB
 constexpr int kFzPlanes = 2 * kATile;            // hi and lo planes of one 128 x 64 tile: 32 KiB
 constexpr int kFzSmem = kFzF32Stages * kFzF32Tile + (kFzPlaneStages + kFzBStages) * kFzPlanes + 256 + 1024;
@@ -402,12 +409,7 @@ struct FzBar {
 };
 static_assert(sizeof(FzBar) <= 256, "the fused kernel reserves 256 bytes of shared memory for its barriers");
 
-__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo_elem, __nv_bfloat16 hi_elem) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo_elem)) |
-           (static_cast<uint32_t>(__bfloat16_as_ushort(hi_elem)) << 16);
-}
-
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kFzThreads, 1)
     umma_bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
                              const __grid_constant__ UParams p) {
     using Cfg = UCfg<kModeBf16x3>;
@@ -429,10 +431,10 @@ __global__ void __launch_bounds__(192, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < FS; ++s) {
             mbar_init(&bar->f_full[s], 1);
-            mbar_init(&bar->f_empty[s], 4);
+            mbar_init(&bar->f_empty[s], kFzEpiWarps);
         }
         for (int s = 0; s < PS; ++s) {
-            mbar_init(&bar->a_full[s], 4);
+            mbar_init(&bar->a_full[s], kFzEpiWarps);
             mbar_init(&bar->a_empty[s], 1);
         }
         for (int s = 0; s < BS; ++s) {
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(192, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&bar->acc_full[b], 1);
-            mbar_init(&bar->acc_empty[b], 4);
+            mbar_init(&bar->acc_empty[b], kFzEpiWarps);
         }
         mbar_init(&bar->drain, 1);
         fence_barrier_init();
@@ -537,27 +539,29 @@ __global__ void __launch_bounds__(192, 1)
         mbar_wait_drain(&bar->drain, 0);
     } else if (warp >= 2) {
         // ------------------------- splitter and epilogue -------------------------
-        const int quarter = warp & 3;
+        constexpr int HC = UN / 2;  // columns per warp
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;  // tile row: TMEM lane and split row
         uint32_t it = 0, uc = 0;
         for (int item = blockIdx.x; ok && item < items; item += gridDim.x) {
             int tm, tn;
             raster_tile(item, p.tiles_m, p.tiles_n, tm, tn);
-            const int m0 = tm * kUM, n0 = tn * UN;
+            const int m0 = tm * kUM, n0 = tn * UN + half * HC;
             const int r = m0 + row;
             const bool row_ok = r < p.m;
-            float sum[UN];
+            float sum[HC];
 #pragma unroll
-            for (int j = 0; j < UN; ++j) sum[j] = 0.f;
+            for (int j = 0; j < HC; ++j) sum[j] = 0.f;
             int promoted = 0;
             // add unit `promoted`'s FP32 partial (TMEM) into sum, as umma_body does
             auto promote = [&]() -> bool {
                 const uint32_t b = uc & 1;
                 if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, err, 0x216)) return false;
                 tc_fence_after();
-                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN;
+                const uint32_t taddr =
+                    tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN + half * HC;
 #pragma unroll
-                for (int ch = 0; ch < UN / 32; ++ch) {
+                for (int ch = 0; ch < HC / 32; ++ch) {
                     uint32_t v[32];
                     tmem_ld32(taddr + ch * 32, v);
                     tmem_ld_wait();
@@ -581,16 +585,20 @@ __global__ void __launch_bounds__(192, 1)
                 const float* F = reinterpret_cast<const float*>(f32s + fs * kFzF32Tile);  // F[k * 128 + row]
                 uint8_t* hi = aps + ps * kFzPlanes;
                 uint8_t* lo = hi + kATile;
+                float v[32];  // this warp's half of the row's 64 K values
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
+                for (int e = 0; e < 32; ++e) v[e] = F[(half * 32 + e) * kUM + row];
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    const int c = half * 4 + c4;
                     uint32_t h[4], l[4];
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        const float v0 = F[(c * 8 + 2 * j) * kUM + row], v1 = F[(c * 8 + 2 * j + 1) * kUM + row];
-                        const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
-                        h[j] = pack_bf16x2(h0, h1);
-                        l[j] = pack_bf16x2(__float2bfloat16_rn(v0 - __bfloat162float(h0)),
-                                           __float2bfloat16_rn(v1 - __bfloat162float(h1)));
+                        const float v0 = v[c4 * 8 + 2 * j], v1 = v[c4 * 8 + 2 * j + 1];
+                        const __nv_bfloat162 hb = __floats2bfloat162_rn(v0, v1);  // rn(v0) low, rn(v1) high
+                        const __nv_bfloat162 lb = __floats2bfloat162_rn(v0 - __low2float(hb), v1 - __high2float(hb));
+                        h[j] = *reinterpret_cast<const uint32_t*>(&hb);
+                        l[j] = *reinterpret_cast<const uint32_t*>(&lb);
                     }
                     const uint32_t off = static_cast<uint32_t>(row) * kRowBytes + ((c ^ (row & 7)) << 4);
                     *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
@@ -616,7 +624,7 @@ __global__ void __launch_bounds__(192, 1)
                 if (!promote()) ok = false;
             if (ok && row_ok) {
 #pragma unroll
-                for (int g = 0; g < UN / 16; ++g) {
+                for (int g = 0; g < HC / 16; ++g) {
                     float cv[16];
 #pragma unroll
                     for (int jj = 0; jj < 16; ++jj) {
@@ -1737,7 +1745,7 @@ cudaError_t launch_bf16x3_fused(const CUtensorMap& ta32, const CUtensorMap& tb, 
     KernelTimer tm;
     kernel_timing_begin("umma_bf16x3", 2.0 * p.m * p.n * static_cast<double>(p.k) * UCfg<kModeBf16x3>::NPROD, st,
                         &tm);
-    kern<<<grid, 192, kFzSmem, st>>>(ta32, tb, p);
+    kern<<<grid, kFzThreads, kFzSmem, st>>>(ta32, tb, p);
     kernel_timing_end(&tm, st);
     count_launch();
     return cudaGetLastError();
