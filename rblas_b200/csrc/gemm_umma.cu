@@ -369,21 +369,26 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------
-// 3xBF16 with A split inside the GEMM (A rows contiguous: NoTrans).
+// The BF16-split forms with A split inside the GEMM (A rows contiguous:
+// NoTrans).
 //
-// Two passes read A, write its hi / lo planes and read the planes again:
-// about three times A's bytes, which is most of the time of a tall-skinny
-// product (65536 x 128 x 8192: A is 2.1 GB, the GEMM itself ~0.3 ms of
-// tensor work). Here TMA brings 128 x 64 f32 tiles of A (128 contiguous rows
-// per K column) into shared memory, and the four epilogue warps split them,
-// between their accumulator promotions, into the hi / lo planes in the
-// 128-byte-swizzled K-major layout the UMMA descriptors read: row r's 16-byte
-// chunk c at r * 128 + ((c ^ (r & 7)) * 16), the layout a TMA load of the
-// planes produces. The split is the split pass's (hi = rn(x), lo = rn(x -
-// hi)) and the products, their order and the promotions are
-// umma_gemm_kernel<kModeBf16x3>'s, so the results are the two-pass form's bit
-// for bit. B's planes come from the split pass (B is small). Rings: A's f32
-// tiles (released once split), A's planes (released by the MMAs), B's planes.
+// Two passes read A, write its planes and read the planes again: about three
+// times A's bytes, which is most of the time of a tall-skinny product
+// (65536 x 128 x 8192: A is 2.1 GB, the GEMM itself ~0.3 ms of tensor work in
+// 3xBF16). Here TMA brings 128 x 64 f32 tiles of A (128 contiguous rows per K
+// column) into shared memory, and the epilogue warps split them, between
+// their accumulator promotions, into the planes (hi, lo for 3xBF16; hi, mid,
+// lo for BF16X6) in the 128-byte-swizzled K-major layout the UMMA
+// descriptors read: row r's 16-byte chunk c at r * 128 + ((c ^ (r & 7)) *
+// 16), the layout a TMA load of the planes produces. The split is the split
+// pass's (hi = rn(x), then each next plane rn of what is left) and the
+// products, their order, the accumulators and the promotions are
+// umma_gemm_kernel<MODE>'s, so the results are the two-pass form's bit for
+// bit. B's planes come from the split pass (B is small). Rings: A's f32
+// tiles (released as soon as the splitters hold them in registers), A's
+// planes (released by the MMAs), B's planes. BF16X6's three-plane stages
+// leave room for one f32 stage only; its refill overlaps the conversion and
+// the wait for a free plane stage.
 // Warps: 0 TMA producer, 1 TMEM owner / MMA issuer, 2..9 splitter and
 // epilogue: tile row quarter * 32 + lane (quarter = warp % 4, the TMEM lane
 // quarter the warp may read) in both roles, and one half of the tile -- K
@@ -392,40 +397,56 @@ __global__ void __launch_bounds__(UCfg<MODE>::THREADS, 1)
 // hide each other's latencies, and 64 running sums per thread leave
 // registers for the split.
 // ------------------------------------------------------------------------------
-constexpr int kFzF32Stages = 3, kFzPlaneStages = 2, kFzBStages = 2;
+template <int MODE> struct FzCfg;
+template <> struct FzCfg<kModeBf16x3> { static constexpr int FS = 3, PS = 2, BS = 2; };
+template <> struct FzCfg<kModeBf16x6> { static constexpr int FS = 1, PS = 2, BS = 2; };
+constexpr int kFzMaxStages = 3;
 constexpr int kFzThreads = 320;
 constexpr int kFzEpiWarps = 8;
-constexpr int kFzF32Tile = kUM * 64 * 4;         // 64 K columns of 128 f32 rows: 32 KiB
-constexpr int kFzPlanes = 2 * kATile;            // hi and lo planes of one 128 x 64 tile: 32 KiB
-constexpr int kFzSmem = kFzF32Stages * kFzF32Tile + (kFzPlaneStages + kFzBStages) * kFzPlanes + 256 + 1024;
-static_assert(kFzSmem <= 232448, "the fused kernel's rings must fit one CTA's shared memory");
+constexpr int kFzF32Tile = kUM * 64 * 4;  // 64 K columns of 128 f32 rows: 32 KiB
+template <int MODE>
+constexpr int fz_smem_bytes() {
+    using F = FzCfg<MODE>;
+    // f32 stages, then A's and B's plane stages (NA planes of one 128 x 64 tile each)
+    return F::FS * kFzF32Tile + (F::PS + F::BS) * UCfg<MODE>::NA * kATile + 256 + 1024;
+}
+static_assert(fz_smem_bytes<kModeBf16x3>() <= 232448 && fz_smem_bytes<kModeBf16x6>() <= 232448,
+              "the fused kernels' rings must fit one CTA's shared memory");
 
 struct FzBar {
-    uint64_t f_full[kFzF32Stages], f_empty[kFzF32Stages];
-    uint64_t a_full[kFzPlaneStages], a_empty[kFzPlaneStages];
-    uint64_t b_full[kFzBStages], b_empty[kFzBStages];
+    uint64_t f_full[kFzMaxStages], f_empty[kFzMaxStages];
+    uint64_t a_full[kFzMaxStages], a_empty[kFzMaxStages];
+    uint64_t b_full[kFzMaxStages], b_empty[kFzMaxStages];
     uint64_t acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
 };
-static_assert(sizeof(FzBar) <= 256, "the fused kernel reserves 256 bytes of shared memory for its barriers");
+static_assert(sizeof(FzBar) <= 256, "the fused kernels reserve 256 bytes of shared memory for their barriers");
 
+template <int MODE>
 __global__ void __launch_bounds__(kFzThreads, 1)
-    umma_bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
-                             const __grid_constant__ UParams p) {
-    using Cfg = UCfg<kModeBf16x3>;
-    constexpr int UN = Cfg::UN;
-    constexpr int FS = kFzF32Stages, PS = kFzPlaneStages, BS = kFzBStages;
+    umma_split_fused_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
+                            const __grid_constant__ UParams p) {
+    using Cfg = UCfg<MODE>;
+    constexpr int UN = Cfg::UN, NP = Cfg::NA;
+    constexpr int FS = FzCfg<MODE>::FS, PS = FzCfg<MODE>::PS, BS = FzCfg<MODE>::BS;
+    static_assert(FS <= kFzMaxStages && PS <= kFzMaxStages && BS <= kFzMaxStages, "FzBar holds the rings");
+    static_assert(Cfg::NB == NP, "A and B have the same planes");
+    constexpr int PLANES = NP * kATile;  // one plane stage: NP planes of a 128 x 64 tile
     constexpr int KSTEPS = 4;
     constexpr uint32_t IDESC = umma_idesc(1, 1, kUM, UN);  // f32 <- bf16
-    constexpr uint32_t TMEM_COLS = 2 * UN;
+    // BF16X6 keeps hi*hi in an accumulator of its own, as umma_body does
+    constexpr bool SPLIT_ACC = (MODE == kModeBf16x6);
+    constexpr uint32_t ACC_COLS = SPLIT_ACC ? 2 * UN : UN;  // per accumulator buffer
+    constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;
+    static_assert(TMEM_COLS <= 512, "two buffers must fit the SM's TMEM");
     static_assert(UN * kRowBytes == kATile, "B plane tiles are as large as A's");
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint8_t* f32s = smem;                        // FS x 32 KiB, [k][row] f32
-    uint8_t* aps = f32s + FS * kFzF32Tile;       // PS x (hi, lo), swizzled K-major
-    uint8_t* bps = aps + PS * kFzPlanes;         // BS x (hi, lo), by TMA
-    FzBar* bar = reinterpret_cast<FzBar*>(bps + BS * kFzPlanes);
+    uint8_t* aps = f32s + FS * kFzF32Tile;       // PS x NP planes, swizzled K-major
+    uint8_t* bps = aps + PS * PLANES;            // BS x NP planes, by TMA
+    FzBar* bar = reinterpret_cast<FzBar*>(bps + BS * PLANES);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -483,10 +504,10 @@ __global__ void __launch_bounds__(kFzThreads, 1)
                     ok = false;
                     break;
                 }
-                mbar_arrive_expect_tx(&bar->b_full[bs], kFzPlanes);
+                mbar_arrive_expect_tx(&bar->b_full[bs], PLANES);
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
-                    tma_load_3d(bps + bs * kFzPlanes + q * kATile, &tmB, &bar->b_full[bs], kt * 64, n0, q);
+                for (int q = 0; q < NP; ++q)
+                    tma_load_3d(bps + bs * PLANES + q * kATile, &tmB, &bar->b_full[bs], kt * 64, n0, q);
                 ++nb;
             }
         }
@@ -508,7 +529,8 @@ __global__ void __launch_bounds__(kFzThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d_tmem = tmem_base + b * UN;
+                const uint32_t d_tmem = tmem_base + b * ACC_COLS;        // the products (all, or all but hi*hi)
+                const uint32_t d_big = SPLIT_ACC ? d_tmem + UN : d_tmem;  // hi*hi
                 uint32_t accumulate = 0;
                 for (int kt = kt0; kt < kt1; ++kt, ++it) {
                     const int ps = it % PS, bs = it % BS;
@@ -518,15 +540,17 @@ __global__ void __launch_bounds__(kFzThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t sa = smem_u32(aps + ps * kFzPlanes);
-                    const uint32_t sb = smem_u32(bps + bs * kFzPlanes);
+                    const uint32_t sa = smem_u32(aps + ps * PLANES);
+                    const uint32_t sb = smem_u32(bps + bs * PLANES);
 #pragma unroll
                     for (int kk = 0; kk < KSTEPS; ++kk) {
 #pragma unroll
-                        for (int q = 0; q < Cfg::NPROD; ++q)
-                            umma_f16(d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
+                        for (int q = 0; q < Cfg::NPROD; ++q) {
+                            const bool big = SPLIT_ACC && q == Cfg::NPROD - 1;
+                            umma_f16(big ? d_big : d_tmem, sw128_kmajor_desc(sa + Cfg::pa(q) * kATile) + 2 * kk,
                                      sw128_kmajor_desc(sb + Cfg::pb(q) * kATile) + 2 * kk, IDESC,
-                                     q == 0 ? accumulate : 1u);
+                                     (q == 0 || big) ? accumulate : 1u);
+                        }
                         accumulate = 1;
                     }
                     tc_commit(&bar->a_empty[ps]);  // plane stages free once these MMAs complete
@@ -559,14 +583,18 @@ __global__ void __launch_bounds__(kFzThreads, 1)
                 if (!mbar_wait(&bar->acc_full[b], (uc >> 1) & 1, err, 0x216)) return false;
                 tc_fence_after();
                 const uint32_t taddr =
-                    tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * UN + half * HC;
+                    tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + b * ACC_COLS + half * HC;
+                // the smaller products first, then hi*hi (SPLIT_ACC)
 #pragma unroll
-                for (int ch = 0; ch < HC / 32; ++ch) {
-                    uint32_t v[32];
-                    tmem_ld32(taddr + ch * 32, v);
-                    tmem_ld_wait();
+                for (int part = 0; part < (SPLIT_ACC ? 2 : 1); ++part) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                    for (int ch = 0; ch < HC / 32; ++ch) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + part * UN + ch * 32, v);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) sum[ch * 32 + j] += __uint_as_float(v[j]);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -577,39 +605,56 @@ __global__ void __launch_bounds__(kFzThreads, 1)
             };
             for (int kt = 0; kt < p.num_kt; ++kt, ++it) {
                 const int fs = it % FS, ps = it % PS;
-                if ((it >= PS && !mbar_wait(&bar->a_empty[ps], ((it / PS) - 1) & 1, err, 0x217)) ||
-                    !mbar_wait(&bar->f_full[fs], (it / FS) & 1, err, 0x218)) {
+                if (!mbar_wait(&bar->f_full[fs], (it / FS) & 1, err, 0x218)) {
                     ok = false;
                     break;
                 }
-                const float* F = reinterpret_cast<const float*>(f32s + fs * kFzF32Tile);  // F[k * 128 + row]
-                uint8_t* hi = aps + ps * kFzPlanes;
-                uint8_t* lo = hi + kATile;
-                float v[32];  // this warp's half of the row's 64 K values
+                // this warp's half of the row's 64 K values, split into NP
+                // planes of packed bf16 pairs: pl[q][c4][j] holds plane q of K
+                // values 8 c4 + 2 j (low half) and 8 c4 + 2 j + 1 (high half)
+                uint32_t pl[NP][4][4];
+                {
+                    const float* F = reinterpret_cast<const float*>(f32s + fs * kFzF32Tile);  // F[k * 128 + row]
+                    float v[32];
 #pragma unroll
-                for (int e = 0; e < 32; ++e) v[e] = F[(half * 32 + e) * kUM + row];
+                    for (int e = 0; e < 32; ++e) v[e] = F[(half * 32 + e) * kUM + row];
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            float v0 = v[c4 * 8 + 2 * j], v1 = v[c4 * 8 + 2 * j + 1];
+#pragma unroll
+                            for (int q = 0; q < NP; ++q) {
+                                const __nv_bfloat162 hb = __floats2bfloat162_rn(v0, v1);  // rn(v0) low, rn(v1) high
+                                pl[q][c4][j] = *reinterpret_cast<const uint32_t*>(&hb);
+                                if (q + 1 < NP) {
+                                    v0 -= __low2float(hb);
+                                    v1 -= __high2float(hb);
+                                }
+                            }
+                        }
+                }
+                // the f32 stage is free once every lane's reads have been used
+                __threadfence_block();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->f_empty[fs]);
+                if (it >= PS && !mbar_wait(&bar->a_empty[ps], ((it / PS) - 1) & 1, err, 0x217)) {
+                    ok = false;
+                    break;
+                }
+                uint8_t* dst = aps + ps * PLANES;
 #pragma unroll
                 for (int c4 = 0; c4 < 4; ++c4) {
                     const int c = half * 4 + c4;
-                    uint32_t h[4], l[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float v0 = v[c4 * 8 + 2 * j], v1 = v[c4 * 8 + 2 * j + 1];
-                        const __nv_bfloat162 hb = __floats2bfloat162_rn(v0, v1);  // rn(v0) low, rn(v1) high
-                        const __nv_bfloat162 lb = __floats2bfloat162_rn(v0 - __low2float(hb), v1 - __high2float(hb));
-                        h[j] = *reinterpret_cast<const uint32_t*>(&hb);
-                        l[j] = *reinterpret_cast<const uint32_t*>(&lb);
-                    }
                     const uint32_t off = static_cast<uint32_t>(row) * kRowBytes + ((c ^ (row & 7)) << 4);
-                    *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-                    *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+#pragma unroll
+                    for (int q = 0; q < NP; ++q)
+                        *reinterpret_cast<uint4*>(dst + q * kATile + off) =
+                            make_uint4(pl[q][c4][0], pl[q][c4][1], pl[q][c4][2], pl[q][c4][3]);
                 }
                 fence_proxy_async_smem();  // the planes' generic stores, visible to the tensor cores
                 __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&bar->a_full[ps]);
-                    mbar_arrive(&bar->f_empty[fs]);
-                }
+                if (lane == 0) mbar_arrive(&bar->a_full[ps]);
                 // once unit u's last tile is split, unit u - 1 is promoted: the
                 // MMAs of unit u + 1 wait for that buffer, and the split of
                 // unit u + 1's tiles waits for unit u's MMAs
@@ -1720,21 +1765,24 @@ static void operand_views(bool ta, bool tb, size_t lda, size_t ldb, size_t& ars,
     if (!tb) { brs = ldb; bps = 1; } else { brs = 1; bps = ldb; }
 }
 
-// 3xBF16 splits A inside the GEMM (umma_bf16x3_fused_kernel) when A's rows
-// are contiguous (NoTrans, 16-byte aligned base and column stride) and C has
-// at most two 128-wide column tiles, so the f32 tiles TMA brings are read
-// about once: there the split pass's read and write of A cost more than the
-// GEMM. Wider products keep the two passes (their GEMM is compute-bound and
-// the deeper plane ring of the two-pass kernel feeds it better).
-bool bf16x3_fused_a(bool ta, int n, const float* A, size_t lda) {
+// The BF16-split forms split A inside the GEMM (umma_split_fused_kernel) when
+// A's rows are contiguous (NoTrans, 16-byte aligned base and column stride)
+// and C has at most two 128-wide column tiles, so the f32 tiles TMA brings
+// are read about once: there the split pass's read and write of A cost more
+// than the GEMM. Wider products keep the two passes (their GEMM is
+// compute-bound and the deeper plane ring of the two-pass kernel feeds it
+// better).
+bool bf16_fused_a(bool ta, int n, const float* A, size_t lda) {
     return !ta && n <= 256 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda & 3) == 0;
 }
 
-cudaError_t launch_bf16x3_fused(const CUtensorMap& ta32, const CUtensorMap& tb, const UParams& p, cudaStream_t st) {
-    auto kern = umma_bf16x3_fused_kernel;
+template <int MODE>
+cudaError_t launch_bf16_fused(const CUtensorMap& ta32, const CUtensorMap& tb, const UParams& p, cudaStream_t st) {
+    auto kern = umma_split_fused_kernel<MODE>;
+    constexpr int smem = fz_smem_bytes<MODE>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kFzSmem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
@@ -1742,10 +1790,10 @@ cudaError_t launch_bf16x3_fused(const CUtensorMap& ta32, const CUtensorMap& tb, 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = p.num_tiles < sms ? p.num_tiles : sms;
+    const char* name = (MODE == kModeBf16x3) ? "umma_bf16x3" : "umma_bf16x6";
     KernelTimer tm;
-    kernel_timing_begin("umma_bf16x3", 2.0 * p.m * p.n * static_cast<double>(p.k) * UCfg<kModeBf16x3>::NPROD, st,
-                        &tm);
-    kern<<<grid, kFzThreads, kFzSmem, st>>>(ta32, tb, p);
+    kernel_timing_begin(name, 2.0 * p.m * p.n * static_cast<double>(p.k) * UCfg<MODE>::NPROD, st, &tm);
+    kern<<<grid, kFzThreads, smem, st>>>(ta32, tb, p);
     kernel_timing_end(&tm, st);
     count_launch();
     return cudaGetLastError();
@@ -1755,7 +1803,7 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
                                    const float* A, size_t lda, const float* B, size_t ldb, float beta,
                                    float* C, size_t ldc, cudaStream_t st, CUresult* cu_err) {
     constexpr int UN = 128;
-    const bool fused = planes == 2 && bf16x3_fused_a(ta, n, A, lda);
+    const bool fused = bf16_fused_a(ta, n, A, lda);
     const size_t kp = round_up(static_cast<size_t>(k), 8);  // 16-byte rows of bf16
     const size_t pa = fused ? 0 : static_cast<size_t>(m) * kp, pb = static_cast<size_t>(n) * kp;
     void* buf = nullptr;
@@ -1798,8 +1846,11 @@ cudaError_t launch_bf16_split_gemm(int planes, bool ta, bool tb, int m, int n, i
     p.c = C; p.ldc = ldc;
     p.cin = C;
     p.err = device_error_word();
-    e = fused ? launch_bf16x3_fused(tma, tmb, p, st)
-              : (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
+    if (fused)
+        e = (planes == 2) ? launch_bf16_fused<kModeBf16x3>(tma, tmb, p, st)
+                          : launch_bf16_fused<kModeBf16x6>(tma, tmb, p, st);
+    else
+        e = (planes == 2) ? launch_umma<kModeBf16x3>(tma, tmb, p, st) : launch_umma<kModeBf16x6>(tma, tmb, p, st);
     cudaFreeAsync(buf, st);
     return e;
 }

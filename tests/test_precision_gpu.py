@@ -241,16 +241,17 @@ def test_ozaki_unit_parallel_matches_fused_epilogue_exactly(layout, ta, tb, m, n
         assert torch.equal(got, ref) or torch.allclose(got, ref, rtol=0, atol=0, equal_nan=True)
 
 
+@pytest.mark.parametrize("prec", [Precision.Bf16x3, Precision.Bf16x6])
 @pytest.mark.parametrize("m,n,k,beta", [(1000, 200, 777, -0.5), (300, 128, 64, 0.0), (129, 1, 4096, 1.0),
                                         (65536, 128, 8192, 1.0)])
-def test_bf16x3_split_in_gemm_matches_two_pass_exactly(m, n, k, beta):
+def test_bf16_split_in_gemm_matches_two_pass_exactly(m, n, k, beta, prec):
     """An A with contiguous rows (ColMajor NoTrans) and at most two 128-wide
-    column tiles runs 3xBF16 with A split inside the GEMM; the same product
-    with A stored transposed (Trans) takes the split pass and the two-pass
-    kernel. Same planes, same products in the same order, same promotions:
-    equal bit for bit. Ragged rows, columns and K, a partial last
-    accumulation unit, beta = 0 with NaN C0, and the tall-skinny
-    65536 x 128 x 8192 configuration."""
+    column tiles runs the BF16-split form with A split inside the GEMM; the
+    same product with A stored transposed (Trans) takes the split pass and
+    the two-pass kernel. Same planes, same products in the same order, same
+    accumulators and promotions: equal bit for bit. Ragged rows, columns and
+    K, a partial last accumulation unit, beta = 0 with NaN C0, and the
+    tall-skinny 65536 x 128 x 8192 configuration."""
     torch = pytest.importorskip("torch")
     g = torch.Generator(device="cuda")
     g.manual_seed(m + n + k)
@@ -262,9 +263,9 @@ def test_bf16x3_split_in_gemm_matches_two_pass_exactly(m, n, k, beta):
         C0.fill_(float("nan"))
     fused, two_pass = C0.clone(), C0.clone()
     level3.gemm_dev(Layout.ColMajor, 0, 0, m, n, k, 1.25, A.data_ptr(), m, B.data_ptr(), k, beta, fused.data_ptr(),
-                    m, np.float32, prec=Precision.Bf16x3)
+                    m, np.float32, prec=prec)
     level3.gemm_dev(Layout.ColMajor, 1, 0, m, n, k, 1.25, At.data_ptr(), k, B.data_ptr(), k, beta,
-                    two_pass.data_ptr(), m, np.float32, prec=Precision.Bf16x3)
+                    two_pass.data_ptr(), m, np.float32, prec=prec)
     torch.cuda.synchronize()
     assert not torch.isnan(fused).any()
     assert torch.equal(fused, two_pass)
