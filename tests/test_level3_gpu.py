@@ -6,7 +6,8 @@ routines on the same seeded inputs.
 Tolerances: GEMM-shaped results use the normwise bound 4*k*u (k the inner
 dimension; for complex 4M/1M, u of the real type); trsm results (well
 conditioned, diagonal in [1, 2], off-diagonal entries U[-0.1, 0.1]/order)
-use a componentwise relative bound of 1e3*u on the solution.
+use a componentwise relative bound of 1e3*u on the solution and the
+normwise backward error bound 4*q*u (q the triangle's order).
 """
 from __future__ import annotations
 
@@ -234,7 +235,26 @@ def test_trsm_parity(dtype, side, uplo, trans):
             oracle.trsm(side, uplo, trans, diag, m, n, alpha, a, q, ref, m)
             rel = np.max(np.abs(b.astype(np.complex128) - ref)) / max(np.max(np.abs(ref)), 1e-30)
             assert rel <= 1e3 * _u(dtype), ((m, n), diag, rel)
+            # normwise backward error of the GPU solution, which a wrong-order
+            # update would push far past the bound even where the forward
+            # error stays small
+            back = _trsm_backward_error(a, b, b0, alpha, side, uplo, trans, diag, m, n, q)
+            assert back <= 4 * q * _u(dtype), ((m, n), diag, back)
     assert rb.device_error()[0] == 0
+
+
+def _trsm_backward_error(a, x, b0, alpha, side, uplo, trans, diag, m, n, q):
+    """||op(A) X - alpha B||_F / (||A_tri||_F ||X||_F + |alpha| ||B||_F) in
+    complex128, for trans 0 (NoTrans), 1 (Trans) or 2 (ConjTrans)."""
+    A = a.reshape(q, q, order="F").astype(np.complex128)
+    T = np.tril(A) if uplo == 1 else np.triu(A)
+    if diag == 1:
+        np.fill_diagonal(T, 1.0)
+    opA = T if trans == 0 else (T.T if trans == 1 else T.conj().T)
+    X = x.reshape(m, n, order="F").astype(np.complex128)
+    B0 = b0.reshape(m, n, order="F").astype(np.complex128)
+    R = (opA @ X if side == 0 else X @ opA) - alpha * B0
+    return np.linalg.norm(R) / (np.linalg.norm(T) * np.linalg.norm(X) + abs(alpha) * np.linalg.norm(B0))
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
