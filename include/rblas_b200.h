@@ -118,7 +118,11 @@ rb_status rb_dgemm_prec(rb_layout layout, rb_transpose transa, rb_transpose tran
 /* Device-pointer GEMM (same math as level3::gemm, src/level3.rs:32-62),
  * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
  * Leading dimensions are validated (InvalidLeadingDim); buffer lengths are
- * the caller's responsibility. Returns when the work is enqueued. */
+ * the caller's responsibility. Returns when the work is enqueued.
+ * The BF16 forms take stream-ordered scratch for the operands' bf16 planes;
+ * for a column-major product (after RowMajor's swap) with A NoTrans,
+ * 16-byte aligned, lda a multiple of 4 and n <= 256, A is split inside the
+ * GEMM and only B's planes take scratch (same results bit for bit). */
 rb_status rb_sgemm_dev(rb_layout layout, rb_transpose transa, rb_transpose transb, size_t m,
                        size_t n, size_t k, float alpha, const float* a, size_t lda,
                        const float* b, size_t ldb, float beta, float* c, size_t ldc,
