@@ -16,6 +16,10 @@
 //! Beside the drop-in (the plain form: true FP32 / FP64 products) the
 //! precision forms are reachable through [`level3::try_gemm_prec`]: 3xBF16 /
 //! BF16X6 for f32 and Ozaki INT8-slice emulation for f64.
+//!
+//! [`level1`], [`level2`], [`complex1`] and [`complex2`] are the same for
+//! rblas's vector and matrix-vector routines; like rblas's, they panic on
+//! arguments they cannot use.
 
 use core::fmt;
 use std::os::raw::c_void;
@@ -136,6 +140,65 @@ pub mod ffi {
                             ldc: usize, prec: i32, stream: *mut c_void, err: *mut RbError) -> i32;
         pub fn rb_device_error(clear: i32, detail: *mut u32) -> i32;
     }
+
+    // Level 1 and Level 2, host slices + lengths (src/level1.rs:17-163,
+    // src/complex1.rs:8-112, src/level2.rs:11-89, src/complex2.rs:11-145)
+    macro_rules! real_vec_ffi {
+        ($t:ty, $axpy:ident, $scal:ident, $copy:ident, $swap:ident, $dot:ident, $asum:ident, $nrm2:ident,
+         $gemv:ident, $ger:ident) => {
+            extern "C" {
+                pub fn $axpy(n: usize, alpha: $t, x: *const $t, incx: usize, x_len: usize, y: *mut $t, incy: usize,
+                             y_len: usize, err: *mut RbError) -> i32;
+                pub fn $scal(n: usize, alpha: $t, x: *mut $t, incx: usize, x_len: usize, err: *mut RbError) -> i32;
+                pub fn $copy(n: usize, x: *const $t, incx: usize, x_len: usize, y: *mut $t, incy: usize,
+                             y_len: usize, err: *mut RbError) -> i32;
+                pub fn $swap(n: usize, x: *mut $t, incx: usize, x_len: usize, y: *mut $t, incy: usize, y_len: usize,
+                             err: *mut RbError) -> i32;
+                pub fn $dot(n: usize, x: *const $t, incx: usize, x_len: usize, y: *const $t, incy: usize,
+                            y_len: usize, result: *mut $t, err: *mut RbError) -> i32;
+                pub fn $asum(n: usize, x: *const $t, incx: usize, x_len: usize, result: *mut $t,
+                             err: *mut RbError) -> i32;
+                pub fn $nrm2(n: usize, x: *const $t, incx: usize, x_len: usize, result: *mut $t,
+                             err: *mut RbError) -> i32;
+                pub fn $gemv(layout: i32, trans: i32, m: usize, n: usize, alpha: $t, a: *const $t, lda: usize,
+                             a_len: usize, x: *const $t, incx: usize, x_len: usize, beta: $t, y: *mut $t,
+                             incy: usize, y_len: usize, err: *mut RbError) -> i32;
+                pub fn $ger(layout: i32, m: usize, n: usize, alpha: $t, x: *const $t, incx: usize, x_len: usize,
+                            y: *const $t, incy: usize, y_len: usize, a: *mut $t, lda: usize, a_len: usize,
+                            err: *mut RbError) -> i32;
+            }
+        };
+    }
+    real_vec_ffi!(f32, rb_saxpy, rb_sscal, rb_scopy, rb_sswap, rb_sdot, rb_sasum, rb_snrm2, rb_sgemv, rb_sger);
+    real_vec_ffi!(f64, rb_daxpy, rb_dscal, rb_dcopy, rb_dswap, rb_ddot, rb_dasum, rb_dnrm2, rb_dgemv, rb_dger);
+
+    macro_rules! complex_vec_ffi {
+        ($t:ty, $r:ty, $axpy:ident, $scal:ident, $dotu:ident, $dotc:ident, $nrm2:ident, $gemv:ident,
+         $geru:ident, $gerc:ident) => {
+            extern "C" {
+                pub fn $axpy(n: usize, alpha: $t, x: *const $t, incx: usize, x_len: usize, y: *mut $t, incy: usize,
+                             y_len: usize, err: *mut RbError) -> i32;
+                pub fn $scal(n: usize, alpha: $t, x: *mut $t, incx: usize, x_len: usize, err: *mut RbError) -> i32;
+                pub fn $dotu(n: usize, x: *const $t, incx: usize, x_len: usize, y: *const $t, incy: usize,
+                             y_len: usize, result: *mut $t, err: *mut RbError) -> i32;
+                pub fn $dotc(n: usize, x: *const $t, incx: usize, x_len: usize, y: *const $t, incy: usize,
+                             y_len: usize, result: *mut $t, err: *mut RbError) -> i32;
+                pub fn $nrm2(n: usize, x: *const $t, incx: usize, x_len: usize, result: *mut $r,
+                             err: *mut RbError) -> i32;
+                pub fn $gemv(layout: i32, trans: i32, m: usize, n: usize, alpha: $t, a: *const $t, lda: usize,
+                             a_len: usize, x: *const $t, incx: usize, x_len: usize, beta: $t, y: *mut $t,
+                             incy: usize, y_len: usize, err: *mut RbError) -> i32;
+                pub fn $geru(layout: i32, m: usize, n: usize, alpha: $t, x: *const $t, incx: usize, x_len: usize,
+                             y: *const $t, incy: usize, y_len: usize, a: *mut $t, lda: usize, a_len: usize,
+                             err: *mut RbError) -> i32;
+                pub fn $gerc(layout: i32, m: usize, n: usize, alpha: $t, x: *const $t, incx: usize, x_len: usize,
+                             y: *const $t, incy: usize, y_len: usize, a: *mut $t, lda: usize, a_len: usize,
+                             err: *mut RbError) -> i32;
+            }
+        };
+    }
+    complex_vec_ffi!(C32, f32, rb_caxpy, rb_cscal, rb_cdotu, rb_cdotc, rb_scnrm2, rb_cgemv, rb_cgeru, rb_cgerc);
+    complex_vec_ffi!(C64, f64, rb_zaxpy, rb_zscal, rb_zdotu, rb_zdotc, rb_dznrm2, rb_zgemv, rb_zgeru, rb_zgerc);
 }
 
 use ffi::RbError;
@@ -434,6 +497,294 @@ pub mod complex3 {
         let mut e = RbError::default();
         let st = unsafe { T::trsm_raw(side(s), uplo(u), trans(t), diag(d), m, n, alpha, a, lda, b, ldb, &mut e) };
         blas(check(st, &e)).unwrap()
+    }
+}
+
+/// rblas's Level-1 and Level-2 routines panic on arguments they cannot use
+/// (a stride of zero, a slice shorter than the strided range); so do these,
+/// with the library's message. Device failures panic too.
+fn must(status: i32, e: &RbError) {
+    if let Err(err) = check(status, e) {
+        panic!("{err}");
+    }
+}
+
+/// Element types of the real Level-1 / Level-2 routines (f32 / f64).
+pub trait GpuVecFloat: GpuFloat + Default {
+    #[doc(hidden)]
+    unsafe fn axpy_raw(n: usize, alpha: Self, x: &[Self], incx: usize, y: &mut [Self], incy: usize,
+                       e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn scal_raw(n: usize, alpha: Self, x: &mut [Self], incx: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn copy_raw(n: usize, x: &[Self], incx: usize, y: &mut [Self], incy: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn swap_raw(n: usize, x: &mut [Self], incx: usize, y: &mut [Self], incy: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn dot_raw(n: usize, x: &[Self], incx: usize, y: &[Self], incy: usize, r: &mut Self,
+                      e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn asum_raw(n: usize, x: &[Self], incx: usize, r: &mut Self, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn nrm2_raw(n: usize, x: &[Self], incx: usize, r: &mut Self, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    #[allow(clippy::too_many_arguments)]
+    unsafe fn gemv_raw(l: i32, t: i32, m: usize, n: usize, alpha: Self, a: &[Self], lda: usize, x: &[Self],
+                       incx: usize, beta: Self, y: &mut [Self], incy: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    #[allow(clippy::too_many_arguments)]
+    unsafe fn ger_raw(l: i32, m: usize, n: usize, alpha: Self, x: &[Self], incx: usize, y: &[Self], incy: usize,
+                      a: &mut [Self], lda: usize, e: &mut RbError) -> i32;
+}
+
+macro_rules! real_vec_impl {
+    ($t:ty, $axpy:ident, $scal:ident, $copy:ident, $swap:ident, $dot:ident, $asum:ident, $nrm2:ident,
+     $gemv:ident, $ger:ident) => {
+        impl GpuVecFloat for $t {
+            unsafe fn axpy_raw(n: usize, alpha: Self, x: &[Self], incx: usize, y: &mut [Self], incy: usize,
+                               e: &mut RbError) -> i32 {
+                ffi::$axpy(n, alpha, x.as_ptr(), incx, x.len(), y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn scal_raw(n: usize, alpha: Self, x: &mut [Self], incx: usize, e: &mut RbError) -> i32 {
+                ffi::$scal(n, alpha, x.as_mut_ptr(), incx, x.len(), e)
+            }
+            unsafe fn copy_raw(n: usize, x: &[Self], incx: usize, y: &mut [Self], incy: usize,
+                               e: &mut RbError) -> i32 {
+                ffi::$copy(n, x.as_ptr(), incx, x.len(), y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn swap_raw(n: usize, x: &mut [Self], incx: usize, y: &mut [Self], incy: usize,
+                               e: &mut RbError) -> i32 {
+                ffi::$swap(n, x.as_mut_ptr(), incx, x.len(), y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn dot_raw(n: usize, x: &[Self], incx: usize, y: &[Self], incy: usize, r: &mut Self,
+                              e: &mut RbError) -> i32 {
+                ffi::$dot(n, x.as_ptr(), incx, x.len(), y.as_ptr(), incy, y.len(), r, e)
+            }
+            unsafe fn asum_raw(n: usize, x: &[Self], incx: usize, r: &mut Self, e: &mut RbError) -> i32 {
+                ffi::$asum(n, x.as_ptr(), incx, x.len(), r, e)
+            }
+            unsafe fn nrm2_raw(n: usize, x: &[Self], incx: usize, r: &mut Self, e: &mut RbError) -> i32 {
+                ffi::$nrm2(n, x.as_ptr(), incx, x.len(), r, e)
+            }
+            unsafe fn gemv_raw(l: i32, t: i32, m: usize, n: usize, alpha: Self, a: &[Self], lda: usize, x: &[Self],
+                               incx: usize, beta: Self, y: &mut [Self], incy: usize, e: &mut RbError) -> i32 {
+                ffi::$gemv(l, t, m, n, alpha, a.as_ptr(), lda, a.len(), x.as_ptr(), incx, x.len(), beta,
+                           y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn ger_raw(l: i32, m: usize, n: usize, alpha: Self, x: &[Self], incx: usize, y: &[Self],
+                              incy: usize, a: &mut [Self], lda: usize, e: &mut RbError) -> i32 {
+                ffi::$ger(l, m, n, alpha, x.as_ptr(), incx, x.len(), y.as_ptr(), incy, y.len(), a.as_mut_ptr(), lda,
+                          a.len(), e)
+            }
+        }
+    };
+}
+real_vec_impl!(f32, rb_saxpy, rb_sscal, rb_scopy, rb_sswap, rb_sdot, rb_sasum, rb_snrm2, rb_sgemv, rb_sger);
+real_vec_impl!(f64, rb_daxpy, rb_dscal, rb_dcopy, rb_dswap, rb_ddot, rb_dasum, rb_dnrm2, rb_dgemv, rb_dger);
+
+/// `rblas::level1` on the GPU (strided vectors; each call copies them to the
+/// device and back).
+pub mod level1 {
+    use super::*;
+
+    /// Drop-in for `rblas::level1::axpy` (`src/level1.rs:17-41`): y := alpha*x + y.
+    pub fn axpy<T: GpuVecFloat>(n: usize, alpha: T, x: &[T], incx: usize, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::axpy_raw(n, alpha, x, incx, y, incy, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::level1::dot` (`src/level1.rs:45-66`).
+    pub fn dot<T: GpuVecFloat>(n: usize, x: &[T], incx: usize, y: &[T], incy: usize) -> T {
+        let (mut e, mut r) = (RbError::default(), T::default());
+        must(unsafe { T::dot_raw(n, x, incx, y, incy, &mut r, &mut e) }, &e);
+        r
+    }
+
+    /// Drop-in for `rblas::level1::scal` (`src/level1.rs:70-86`): x := alpha*x.
+    pub fn scal<T: GpuVecFloat>(n: usize, alpha: T, x: &mut [T], incx: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::scal_raw(n, alpha, x, incx, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::level1::nrm2` (`src/level1.rs:96-123`).
+    pub fn nrm2<T: GpuVecFloat>(n: usize, x: &[T], incx: usize) -> T {
+        let (mut e, mut r) = (RbError::default(), T::default());
+        must(unsafe { T::nrm2_raw(n, x, incx, &mut r, &mut e) }, &e);
+        r
+    }
+
+    /// Drop-in for `rblas::level1::asum` (`src/level1.rs:127-135`).
+    pub fn asum<T: GpuVecFloat>(n: usize, x: &[T], incx: usize) -> T {
+        let (mut e, mut r) = (RbError::default(), T::default());
+        must(unsafe { T::asum_raw(n, x, incx, &mut r, &mut e) }, &e);
+        r
+    }
+
+    /// Drop-in for `rblas::level1::copy` (`src/level1.rs:139-151`): y := x.
+    pub fn copy<T: GpuVecFloat>(n: usize, x: &[T], incx: usize, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::copy_raw(n, x, incx, y, incy, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::level1::swap` (`src/level1.rs:155-163`).
+    pub fn swap<T: GpuVecFloat>(n: usize, x: &mut [T], incx: usize, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::swap_raw(n, x, incx, y, incy, &mut e) }, &e)
+    }
+}
+
+/// `rblas::level2` on the GPU.
+pub mod level2 {
+    use super::*;
+
+    /// Drop-in for `rblas::level2::gemv` (`src/level2.rs:11-61`): y := alpha*op(A)*x + beta*y.
+    #[allow(clippy::too_many_arguments)]
+    pub fn gemv<T: GpuVecFloat>(l: Layout, t: Transpose, m: usize, n: usize, alpha: T, a: &[T], lda: usize,
+                                x: &[T], incx: usize, beta: T, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::gemv_raw(layout(l), trans(t), m, n, alpha, a, lda, x, incx, beta, y, incy, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::level2::ger` (`src/level2.rs:65-88`): A := alpha*x*y^T + A.
+    #[allow(clippy::too_many_arguments)]
+    pub fn ger<T: GpuVecFloat>(l: Layout, m: usize, n: usize, alpha: T, x: &[T], incx: usize, y: &[T], incy: usize,
+                               a: &mut [T], lda: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::ger_raw(layout(l), m, n, alpha, x, incx, y, incy, a, lda, &mut e) }, &e)
+    }
+}
+
+/// Element types of the complex Level-1 / Level-2 routines (C32 / C64).
+pub trait GpuVecComplex: GpuComplex {
+    /// The real type of `nrm2`'s result.
+    type Real: Copy + Default;
+    #[doc(hidden)]
+    fn zero() -> Self;
+    #[doc(hidden)]
+    unsafe fn axpy_raw(n: usize, alpha: Self, x: &[Self], incx: usize, y: &mut [Self], incy: usize,
+                       e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn scal_raw(n: usize, alpha: Self, x: &mut [Self], incx: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    #[allow(clippy::too_many_arguments)]
+    unsafe fn dot_raw(conj: bool, n: usize, x: &[Self], incx: usize, y: &[Self], incy: usize, r: &mut Self,
+                      e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    unsafe fn nrm2_raw(n: usize, x: &[Self], incx: usize, r: &mut Self::Real, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    #[allow(clippy::too_many_arguments)]
+    unsafe fn gemv_raw(l: i32, t: i32, m: usize, n: usize, alpha: Self, a: &[Self], lda: usize, x: &[Self],
+                       incx: usize, beta: Self, y: &mut [Self], incy: usize, e: &mut RbError) -> i32;
+    #[doc(hidden)]
+    #[allow(clippy::too_many_arguments)]
+    unsafe fn ger_raw(conj: bool, l: i32, m: usize, n: usize, alpha: Self, x: &[Self], incx: usize, y: &[Self],
+                      incy: usize, a: &mut [Self], lda: usize, e: &mut RbError) -> i32;
+}
+
+macro_rules! complex_vec_impl {
+    ($t:ty, $r:ty, $axpy:ident, $scal:ident, $dotu:ident, $dotc:ident, $nrm2:ident, $gemv:ident, $geru:ident,
+     $gerc:ident) => {
+        impl GpuVecComplex for $t {
+            type Real = $r;
+            fn zero() -> Self {
+                Complex::new(0.0, 0.0)
+            }
+            unsafe fn axpy_raw(n: usize, alpha: Self, x: &[Self], incx: usize, y: &mut [Self], incy: usize,
+                               e: &mut RbError) -> i32 {
+                ffi::$axpy(n, alpha, x.as_ptr(), incx, x.len(), y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn scal_raw(n: usize, alpha: Self, x: &mut [Self], incx: usize, e: &mut RbError) -> i32 {
+                ffi::$scal(n, alpha, x.as_mut_ptr(), incx, x.len(), e)
+            }
+            unsafe fn dot_raw(conj: bool, n: usize, x: &[Self], incx: usize, y: &[Self], incy: usize, r: &mut Self,
+                              e: &mut RbError) -> i32 {
+                let f = if conj { ffi::$dotc } else { ffi::$dotu };
+                f(n, x.as_ptr(), incx, x.len(), y.as_ptr(), incy, y.len(), r, e)
+            }
+            unsafe fn nrm2_raw(n: usize, x: &[Self], incx: usize, r: &mut $r, e: &mut RbError) -> i32 {
+                ffi::$nrm2(n, x.as_ptr(), incx, x.len(), r, e)
+            }
+            unsafe fn gemv_raw(l: i32, t: i32, m: usize, n: usize, alpha: Self, a: &[Self], lda: usize, x: &[Self],
+                               incx: usize, beta: Self, y: &mut [Self], incy: usize, e: &mut RbError) -> i32 {
+                ffi::$gemv(l, t, m, n, alpha, a.as_ptr(), lda, a.len(), x.as_ptr(), incx, x.len(), beta,
+                           y.as_mut_ptr(), incy, y.len(), e)
+            }
+            unsafe fn ger_raw(conj: bool, l: i32, m: usize, n: usize, alpha: Self, x: &[Self], incx: usize,
+                              y: &[Self], incy: usize, a: &mut [Self], lda: usize, e: &mut RbError) -> i32 {
+                let f = if conj { ffi::$gerc } else { ffi::$geru };
+                f(l, m, n, alpha, x.as_ptr(), incx, x.len(), y.as_ptr(), incy, y.len(), a.as_mut_ptr(), lda, a.len(),
+                  e)
+            }
+        }
+    };
+}
+complex_vec_impl!(C32, f32, rb_caxpy, rb_cscal, rb_cdotu, rb_cdotc, rb_scnrm2, rb_cgemv, rb_cgeru, rb_cgerc);
+complex_vec_impl!(C64, f64, rb_zaxpy, rb_zscal, rb_zdotu, rb_zdotc, rb_dznrm2, rb_zgemv, rb_zgeru, rb_zgerc);
+
+/// `rblas::complex1` on the GPU.
+pub mod complex1 {
+    use super::*;
+
+    /// Drop-in for `rblas::complex1::axpy` (`src/complex1.rs:8-27`).
+    pub fn axpy<T: GpuVecComplex>(n: usize, alpha: T, x: &[T], incx: usize, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::axpy_raw(n, alpha, x, incx, y, incy, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::complex1::dotu` (`src/complex1.rs:31-47`): x^T y.
+    pub fn dotu<T: GpuVecComplex>(n: usize, x: &[T], incx: usize, y: &[T], incy: usize) -> T {
+        let (mut e, mut r) = (RbError::default(), T::zero());
+        must(unsafe { T::dot_raw(false, n, x, incx, y, incy, &mut r, &mut e) }, &e);
+        r
+    }
+
+    /// Drop-in for `rblas::complex1::dotc` (`src/complex1.rs:51-67`): x^H y.
+    pub fn dotc<T: GpuVecComplex>(n: usize, x: &[T], incx: usize, y: &[T], incy: usize) -> T {
+        let (mut e, mut r) = (RbError::default(), T::zero());
+        must(unsafe { T::dot_raw(true, n, x, incx, y, incy, &mut r, &mut e) }, &e);
+        r
+    }
+
+    /// Drop-in for `rblas::complex1::scal` (`src/complex1.rs:71-81`).
+    pub fn scal<T: GpuVecComplex>(n: usize, alpha: T, x: &mut [T], incx: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::scal_raw(n, alpha, x, incx, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::complex1::nrm2` (`src/complex1.rs:86-112`).
+    pub fn nrm2<T: GpuVecComplex>(n: usize, x: &[T], incx: usize) -> T::Real {
+        let (mut e, mut r) = (RbError::default(), T::Real::default());
+        must(unsafe { T::nrm2_raw(n, x, incx, &mut r, &mut e) }, &e);
+        r
+    }
+}
+
+/// `rblas::complex2` on the GPU.
+pub mod complex2 {
+    use super::*;
+
+    /// Drop-in for `rblas::complex2::gemv` (`src/complex2.rs:11-76`); ConjTrans conjugates A.
+    #[allow(clippy::too_many_arguments)]
+    pub fn gemv<T: GpuVecComplex>(l: Layout, t: Transpose, m: usize, n: usize, alpha: T, a: &[T], lda: usize,
+                                  x: &[T], incx: usize, beta: T, y: &mut [T], incy: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::gemv_raw(layout(l), trans(t), m, n, alpha, a, lda, x, incx, beta, y, incy, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::complex2::geru` (`src/complex2.rs:80-93`): A := alpha*x*y^T + A.
+    #[allow(clippy::too_many_arguments)]
+    pub fn geru<T: GpuVecComplex>(l: Layout, m: usize, n: usize, alpha: T, x: &[T], incx: usize, y: &[T],
+                                  incy: usize, a: &mut [T], lda: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::ger_raw(false, layout(l), m, n, alpha, x, incx, y, incy, a, lda, &mut e) }, &e)
+    }
+
+    /// Drop-in for `rblas::complex2::gerc` (`src/complex2.rs:97-110`): A := alpha*x*y^H + A.
+    #[allow(clippy::too_many_arguments)]
+    pub fn gerc<T: GpuVecComplex>(l: Layout, m: usize, n: usize, alpha: T, x: &[T], incx: usize, y: &[T],
+                                  incy: usize, a: &mut [T], lda: usize) {
+        let mut e = RbError::default();
+        must(unsafe { T::ger_raw(true, layout(l), m, n, alpha, x, incx, y, incy, a, lda, &mut e) }, &e)
     }
 }
 
