@@ -3,8 +3,10 @@
 This image has no Rust toolchain, so the crate's `extern "C"` declarations
 are checked here instead: every function the crate declares (directly, or
 through its declaration macros) must exist in include/rblas_b200.h with the
-same number of parameters, and each pointer parameter must agree in
-mutability (`const T*` <-> `*const`, `T*` <-> `*mut`)."""
+same number of parameters, each parameter must have the matching type
+(size_t <-> usize, double <-> f64, the enums <-> i32, ...), and each pointer
+parameter must agree in mutability (`const T*` <-> `*const`, `T*` <->
+`*mut`)."""
 from __future__ import annotations
 
 import os
@@ -43,6 +45,30 @@ def _rust_kind(p: str) -> str:
     if ty.startswith("*mut"):
         return "mut"
     return "value"
+
+
+# C parameter types and the Rust types that carry them across the ABI
+_C_TO_RUST = {
+    "size_t": "usize", "float": "f32", "double": "f64", "int": "i32", "int32_t": "i32", "uint32_t": "u32",
+    "uint64_t": "u64", "int64_t": "i64", "rb_layout": "i32", "rb_transpose": "i32", "rb_uplo": "i32",
+    "rb_side": "i32", "rb_diag": "i32", "rb_precision": "i32", "rb_complex32": "C32", "rb_complex64": "C64",
+    "rb_error": "RbError", "void": "c_void",
+}
+
+
+def _c_base(p: str) -> str:
+    """The element type of a C parameter (`const double* x` -> f64)."""
+    words = p.replace("*", " ").split()
+    words = [w for w in words if w != "const"]
+    return _C_TO_RUST.get(words[0], words[0])
+
+
+def _rust_base(p: str) -> str:
+    ty = p.split(":", 1)[1].strip()
+    for q in ("*const", "*mut"):
+        if ty.startswith(q):
+            ty = ty[len(q):].strip()
+    return ty
 
 
 def crate_functions():
@@ -84,3 +110,4 @@ def test_crate_ffi_matches_header():
         assert len(params) == len(cp), f"{name}: {len(params)} parameters in the crate, {len(cp)} in the header"
         for rp, c in zip(params, cp):
             assert _rust_kind(rp) == _c_kind(c), f"{name}: `{rp}` against `{c}`"
+            assert _rust_base(rp) == _c_base(c), f"{name}: `{rp}` against `{c}`"
