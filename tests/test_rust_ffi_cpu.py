@@ -52,8 +52,10 @@ _C_TO_RUST = {
     "size_t": "usize", "float": "f32", "double": "f64", "int": "i32", "int32_t": "i32", "uint32_t": "u32",
     "uint64_t": "u64", "int64_t": "i64", "rb_layout": "i32", "rb_transpose": "i32", "rb_uplo": "i32",
     "rb_side": "i32", "rb_diag": "i32", "rb_precision": "i32", "rb_complex32": "C32", "rb_complex64": "C64",
-    "rb_error": "RbError", "void": "c_void",
+    "rb_error": "RbError", "void": "c_void", "char": "c_char", "rb_gemm_problem": "RbGemmProblem",
+    "rb_request_times": "RbRequestTimes",
 }
+_RUST_ALIASES = {"Complex<f32>": "C32", "Complex<f64>": "C64"}
 
 
 def _c_base(p: str) -> str:
@@ -65,10 +67,28 @@ def _c_base(p: str) -> str:
 
 def _rust_base(p: str) -> str:
     ty = p.split(":", 1)[1].strip()
-    for q in ("*const", "*mut"):
-        if ty.startswith(q):
-            ty = ty[len(q):].strip()
-    return ty
+    while ty.startswith(("*const", "*mut")) and " " in ty:
+        ty = ty.split(None, 1)[1].strip()
+    return _RUST_ALIASES.get(ty, ty)
+
+
+def _c_depth(p: str) -> int:
+    return p.count("*")
+
+
+def _rust_depth(p: str) -> int:
+    return p.split(":", 1)[1].count("*")
+
+
+def _check_decls(where: str, decls: dict, hdr: dict):
+    for name, params in decls.items():
+        assert name in hdr, f"{where}: {name} is not declared in the header"
+        cp = hdr[name]
+        assert len(params) == len(cp), f"{where}: {name}: {len(params)} parameters, {len(cp)} in the header"
+        for rp, c in zip(params, cp):
+            assert _rust_kind(rp) == _c_kind(c), f"{where}: {name}: `{rp}` against `{c}`"
+            assert _rust_depth(rp) == _c_depth(c), f"{where}: {name}: `{rp}` against `{c}`"
+            assert _rust_base(rp) == _c_base(c), f"{where}: {name}: `{rp}` against `{c}`"
 
 
 def crate_functions():
@@ -103,11 +123,17 @@ def test_crate_declares_functions():
 
 
 def test_crate_ffi_matches_header():
-    hdr = header_functions()
-    for name, params in crate_functions().items():
-        assert name in hdr, f"{name} is not declared in the header"
-        cp = hdr[name]
-        assert len(params) == len(cp), f"{name}: {len(params)} parameters in the crate, {len(cp)} in the header"
-        for rp, c in zip(params, cp):
-            assert _rust_kind(rp) == _c_kind(c), f"{name}: `{rp}` against `{c}`"
-            assert _rust_base(rp) == _c_base(c), f"{name}: `{rp}` against `{c}`"
+    _check_decls("crate", crate_functions(), header_functions())
+
+
+def test_integration_guide_ffi_matches_header():
+    """The `extern "C"` snippets of the integration guide, the block a
+    maintainer copies into rblas, hold the header's signatures too."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    decls = {}
+    for block in re.findall(r"```rust\n(.*?)```", text, re.S):
+        block = re.sub(r"//[^\n]*", "", block)
+        for m in re.finditer(r"fn (rb_\w+)\s*\(([^)]*)\)", block):
+            decls[m.group(1)] = _split_params(" ".join(m.group(2).split()))
+    assert len(decls) >= 20
+    _check_decls("INTEGRATION.md", decls, header_functions())
