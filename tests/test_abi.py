@@ -204,3 +204,31 @@ def test_grouped_bf16_rejects_bad_tables_before_any_device_work():
     arr[1].dtype = 1
     err = _lib.RbError()
     assert lib.rb_gemm_grouped_bf16_dev(arr, 2, 3, None, C.byref(err)) == 5 and err.got == 1
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every ctypes binding takes as many arguments as its C declaration, and
+    each argument is passed in the declared width: pointers as pointers,
+    size_t as c_size_t, float / double as c_float / c_double, the enums and
+    ints as 32-bit ints, complex scalars as their two-field structures."""
+    import ctypes as C
+
+    from tests.test_rust_ffi_cpu import header_functions as header_params
+
+    scalars = {
+        "size_t": (C.c_size_t,), "float": (C.c_float,), "double": (C.c_double,),
+        "int": (C.c_int, C.c_int32), "int32_t": (C.c_int, C.c_int32), "uint32_t": (C.c_uint32,),
+        "uint64_t": (C.c_uint64,), "int64_t": (C.c_int64,),
+        "rb_complex32": (_lib.RbComplex32,), "rb_complex64": (_lib.RbComplex64,),
+    }
+    for e in ("rb_layout", "rb_transpose", "rb_uplo", "rb_side", "rb_diag", "rb_precision"):
+        scalars[e] = (C.c_int, C.c_int32)
+    for name, cparams in header_params().items():
+        _, args = _lib.SIGNATURES[name]
+        assert len(args) == len(cparams), f"{name}: {len(args)} ctypes arguments, {len(cparams)} in the header"
+        for a, c in zip(args, cparams):
+            if "*" in c:
+                assert a in (C.c_void_p, C.c_char_p) or issubclass(a, C._Pointer), f"{name}: `{c}` as {a}"
+            else:
+                base = c.replace("const ", "").split()[0]
+                assert a in scalars[base], f"{name}: `{c}` as {a}"
