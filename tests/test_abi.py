@@ -211,8 +211,6 @@ def test_ctypes_signatures_match_the_header():
     each argument is passed in the declared width: pointers as pointers,
     size_t as c_size_t, float / double as c_float / c_double, the enums and
     ints as 32-bit ints, complex scalars as their two-field structures."""
-    import ctypes as C
-
     from tests.test_rust_ffi_cpu import header_functions as header_params
 
     scalars = {
@@ -232,3 +230,22 @@ def test_ctypes_signatures_match_the_header():
             else:
                 base = c.replace("const ", "").split()[0]
                 assert a in scalars[base], f"{name}: `{c}` as {a}"
+
+
+def test_ctypes_return_types_match_the_header():
+    """Each binding's restype is the C declaration's return type."""
+    from tests.test_rust_ffi_cpu import header_functions as header_params
+
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "rblas_b200.h")).read(), flags=re.S)
+    expect = {"rb_status": (C.c_int, C.c_int32), "int": (C.c_int, C.c_int32), "int32_t": (C.c_int, C.c_int32),
+              "size_t": (C.c_size_t,), "uint64_t": (C.c_uint64,), "uint32_t": (C.c_uint32,),
+              "double": (C.c_double,), "void": (None,), "const char*": (C.c_char_p,)}
+    seen = 0
+    for m in re.finditer(r"^\s*((?:const\s+)?\w+\s*\**)\s*(rb_\w+)\s*\(", text, re.M):
+        ret, name = " ".join(m.group(1).replace("*", " * ").split()).replace(" *", "*"), m.group(2)
+        if ret.startswith("typedef"):
+            continue
+        res, _ = _lib.SIGNATURES[name]
+        assert res in expect[ret], f"{name}: returns `{ret}`, bound as {res}"
+        seen += 1
+    assert seen == len(header_params())
