@@ -78,3 +78,26 @@ def test_reference_arm_prints_on_rank_zero_only():
                           "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env, timeout=120)
     assert out.returncode == 0
     assert out.stdout.strip() == ""
+
+
+def test_reference_arm_json_line():
+    """`--impl reference` on one process prints one JSON line with the base
+    contract's keys, the arm's CPU baseline and an e2e that moves no bytes
+    (the restated CPU gemm runs on the host cores, no device involved)."""
+    import json
+
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, env=env, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config"):
+        assert key in d, key
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["unit"] == "TFLOP/s"
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
