@@ -249,3 +249,19 @@ def test_ctypes_return_types_match_the_header():
         assert res in expect[ret], f"{name}: returns `{ret}`, bound as {res}"
         seen += 1
     assert seen == len(header_params())
+
+
+def test_no_cpu_fallback_without_a_device():
+    """On a host without a GPU a GEMM call raises instead of computing
+    anywhere else, and leaves C as it was: the library has no CPU path."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from rblas_b200 import level3
+    from rblas_b200.error import DeviceError
+    from rblas_b200.types import Layout, Transpose
+
+    a, b, c = np.ones(4), np.ones(4), np.full(4, 7.0)
+    with pytest.raises(DeviceError):
+        level3.gemm(Layout.ColMajor, Transpose.NoTrans, Transpose.NoTrans, 2, 2, 2, 1.0, a, 2, b, 2, 0.0, c, 2)
+    assert (c == 7.0).all()
