@@ -40,3 +40,14 @@ def test_library_links_no_oracle_code():
     assert not [n for n in needed if "oracle" in n], needed
     allowed = ("libstdc++", "libm.", "libgcc_s", "libc.", "ld-linux", "libdl", "libpthread", "librt")
     assert all(n.startswith(allowed) for n in needed), needed
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without librblas_b200.so the binding raises at load time; nothing
+    falls back to another implementation."""
+    from rblas_b200 import _lib
+
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "librblas_b200.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(ImportError, match="no CPU fallback"):
+        _lib.load()
